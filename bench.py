@@ -1,0 +1,431 @@
+"""Benchmark of the smoke step: ms/step and PCG iterations of the 128^3 plume to relative residual 1e-5.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--n 128]
+
+One JSON line on rank 0. "value" is the device time of one step of the mixed-precision form (FP32 stencils,
+Jacobi-PCG with FP64 dot products and an FP64 true-residual refinement, to 1e-5) with every input resident in
+HBM and L2 flushed between timed steps; "e2e" is the same step driven through the C ABI with the step's host input
+copied in from pinned memory and its result (total density) read back, per step. The plain-FP32 form (FP32
+reductions, no refinement) runs on the same states and is reported beside it. `--impl reference` runs the
+reference's own CUDA library (compiled from its sources into oracle/_ref) on the same scene through the same ABI,
+with the fixed CG iteration count that reaches 1e-5 on this scene. Several GPUs run independent replicas (the step
+does not shard); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "visual-simulation-of-smoke_b200")
+sys.path.insert(0, PKG)
+
+import numpy as np  # noqa: E402
+
+import smoke_abi as abi  # noqa: E402
+
+METRIC = "ms/step and PCG iters at 128³ to rel-res 1e-5: learned+mixed vs plain FP32"
+REF_LIBRARY = os.path.join(ROOT, "oracle", "_ref", "libvisual-simulation-of-smoke.so")
+# Smallest fixed CG iteration count with which the reference reaches relative residual <= 1e-5 on every step of
+# the 128^3 plume (after the spin-up); measured on a B200 with `bench.py --calibrate-reference`.
+REFERENCE_CG_ITERATIONS = 600
+SPINUP_STEPS = 30
+KERNELS_PER_STEP = 10  # vorticity, cell force, face force, advect velocity, rhs, solver, project, scalar prep, advect scalars, density fill
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+class L2Flush:
+    def __init__(self):
+        import torch
+
+        self.buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def __call__(self):
+        self.buf.fill_(1)
+
+
+def run_steps(sim, driver, first_step, count, flush, timed=True, status=False):
+    """Per-step device time of sim.step() (events on the simulation stream), driver inputs untimed."""
+    import torch
+
+    times, iters, resid = [], [], []
+    for k in range(count):
+        driver.apply(first_step + k)
+        if flush is not None:
+            with torch.cuda.stream(sim.stream):
+                flush()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(sim.stream)
+        sim.step()
+        e1.record(sim.stream)
+        driver.read_result()
+        sim.stream.synchronize()
+        times.append(e0.elapsed_time(e1))
+        if status:
+            st = sim.solver_status()
+            iters.append(st.iterations)
+            resid.append(st.true_relative_residual if st.true_relative_residual >= 0 else st.relative_residual)
+    return times, iters, resid
+
+
+def run_e2e(sim, driver, first_step, count):
+    """Wall time per step through the ABI: host input -> H2D, step, result D2H, host read."""
+    t0 = time.perf_counter()
+    total = 0.0
+    for k in range(count):
+        host = driver.inputs_for(first_step + k)
+        driver.apply(first_step + k, host)
+        sim.step()
+        res = driver.read_result()
+        sim.stream.synchronize()
+        total += float(res[0])
+    return (time.perf_counter() - t0) * 1e3 / count, total
+
+
+def save_state(sim):
+    import torch
+
+    with torch.cuda.stream(sim.stream):
+        u, v, w = (t.clone() for t in sim.face_velocity(0))
+        d = sim.view(abi.VIEW_DENSITY).clone()
+        t_ = sim.view(abi.VIEW_TEMPERATURE).clone()
+    sim.stream.synchronize()
+    return u, v, w, d, t_
+
+
+def restore_state(sim, state):
+    import torch
+
+    u, v, w, d, t_ = state
+    with torch.cuda.stream(sim.stream):
+        sim.set_face_velocity(u, v, w)
+        sim.update_density(d)
+        sim.update_temperature(t_)
+    sim.stream.synchronize()
+
+
+def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5):
+    """Times the persistent solver kernel alone (smoke_b200_solve_pressure_cuda on the step's right-hand side) with
+    CUDA events on the context stream. Algorithmic bytes per iteration: 42 B/cell (reads p, x, r, s, w 4 B each +
+    code 2 B; writes p, x, r, s, w); setup 16 B/cell; refinement pass 10 B/cell."""
+    import torch
+
+    flush = L2Flush()
+    durs, iters = [], []
+    for _ in range(repeats):
+        with torch.cuda.stream(sim.stream):
+            flush()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(sim.stream)
+        sim.solve_pressure()
+        e1.record(sim.stream)
+        sim.stream.synchronize()
+        durs.append(e0.elapsed_time(e1))
+        st = sim.solver_status()
+        iters.append(st.iterations + 0.0 * st.passes)
+        passes = st.passes
+    ms = statistics.median(durs)
+    it = statistics.median(iters)
+    algo_bytes = n_cells * (42.0 * it + 16.0 + 10.0 * passes)
+    achieved = algo_bytes / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "pcg_kernel (persistent Chronopoulos-Gear PCG)", "achieved": round(achieved, 1), "peak": peak_gbs, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": round(achieved / peak_gbs, 3), "traffic": None, "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(ms, 4), "iterations": it,
+            "note": "working set (~9 vectors x 8 MiB) is L2-resident at 128^3; DRAM traffic per launch is in profiles/"}
+
+
+def cpu_baseline(sim, cfg, steps=2):
+    """The oracle (C restatement, FP32, OpenMP on all host cores) timed on the same state for a bounded sample."""
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    st = O.OracleState(cfg, 32)
+    u, v, w = (t.detach().cpu().numpy() for t in sim.face_velocity(0))
+    st.set("u", u)
+    st.set("v", v)
+    st.set("w", w)
+    for kind, name in ((abi.VIEW_DENSITY, "density"), (abi.VIEW_TEMPERATURE, "temperature"), (abi.VIEW_DENSITY_SOURCE, "density_source"),
+                       (abi.VIEW_TEMPERATURE_SOURCE, "temperature_source")):
+        st.set(name, sim.view(kind).cpu().numpy())
+    fx, fy, fz = sim.view(abi.VIEW_FORCE)
+    st.set("force_x", fx.cpu().numpy())
+    st.set("force_y", fy.cpu().numpy())
+    st.set("force_z", fz.cpu().numpy())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    its = []
+    for _ in range(steps):
+        s = st.step(0, 5, mode=1, max_iterations=500, tolerance=1e-5)
+        its.append(s.iterations)
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    return {"value": round(ms, 1), "unit": "ms/step", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{steps} full steps of the 128^3 plume from the GPU state after spin-up (FP32 oracle, Jacobi-PCG to 1e-5, {its} iterations)"}
+
+
+def build_sim(lib, cfg, stream):
+    import smoke_b200
+
+    return smoke_b200.Simulation(lib, cfg, stream)
+
+
+def bench_b200(args, rank, world, local):
+    import torch
+
+    import plume_scene
+    import smoke_b200
+
+    n = args.n
+    lib = smoke_b200.SmokeLibrary()
+    stream = torch.cuda.Stream()
+    cfg = plume_scene.plume_config(n, abi.MONOTONIC_CUBIC)
+    sim = smoke_b200.Simulation(lib, cfg, stream)
+    driver = plume_scene.PlumeDriver(sim, n, seed=1 + rank)
+    mixed = dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP64, max_iterations=500, tolerance=1e-5, refinement=2)
+    plain = dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP32, max_iterations=500, tolerance=1e-5, refinement=0)
+    sim.set_solver(**mixed)
+    flush = L2Flush()
+    # spin-up (untimed): the plume develops from rest
+    run_steps(sim, driver, 0, SPINUP_STEPS, None)
+    state = save_state(sim)
+    step0 = SPINUP_STEPS
+    # warm-up + timed, mixed form
+    run_steps(sim, driver, step0, args.warmup, flush)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        t_mixed, it_mixed, res_mixed = run_steps(sim, driver, step0 + args.warmup, args.steps, flush, status=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    # plain FP32 form from the same state
+    restore_state(sim, state)
+    sim.set_solver(**plain)
+    run_steps(sim, driver, step0, args.warmup, flush)
+    t_plain, it_plain, res_plain = run_steps(sim, driver, step0 + args.warmup, args.steps, flush, status=True)
+    # e2e through the ABI (mixed form), same state
+    restore_state(sim, state)
+    sim.set_solver(**mixed)
+    run_e2e(sim, driver, step0, args.warmup)
+    barrier(world)
+    e2e_ms, _ = run_e2e(sim, driver, step0 + args.warmup, args.steps)
+    barrier(world)
+    roof = solver_kernel_roofline(sim, n ** 3, *load_peaks())
+    ms_mixed = max_over_ranks(statistics.mean(t_mixed), world)
+    ms_plain = max_over_ranks(statistics.mean(t_plain), world)
+    e2e_ms = max_over_ranks(e2e_ms, world)
+    cpu = cpu_baseline(sim, cfg) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    sim.close()
+    if rank != 0:
+        return None
+    cells = n ** 3
+    line = {
+        "metric": METRIC, "value": round(ms_mixed, 4), "unit": "ms/step", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed, 4),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fp64 reductions)", "data": "synthetic (seeded plume scene)",
+        "config": {"workload": f"plume {n}^3 monotone-cubic, Jacobi-PCG to rel-res 1e-5 with FP64 dots and FP64 refinement", "grid": [n, n, n], "dt": 0.01,
+                   "source_box": "16x8x16 at x,z in [56,72), y in [0,8)" if n == 128 else "n/8 x n/16 x n/8", "spinup_steps": SPINUP_STEPS,
+                   "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}", "learned_preconditioner": "not used"},
+        "pcg_iterations": round(statistics.mean(it_mixed), 1), "true_rel_residual_max": max(res_mixed),
+        "cells_per_s": round(cells * world / (ms_mixed * 1e-3), 1),
+        "forms": {"mixed_fp64": {"ms_per_step": round(ms_mixed, 4), "pcg_iterations": round(statistics.mean(it_mixed), 1), "rel_residual_max": max(res_mixed)},
+                  "plain_fp32": {"ms_per_step": round(ms_plain, 4), "pcg_iterations": round(statistics.mean(it_plain), 1), "rel_residual_max": max(res_plain)}},
+        "roofline": roof,
+        "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": driver.h2d_bytes, "d2h_bytes_per_step": driver.d2h_bytes,
+                "includes": "per-step box inputs H2D, velocity/density/temperature views, source/force updates, step, total-density D2H, host sync"},
+        "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    return line
+
+
+def bench_reference(args, rank, world, local):
+    import torch
+
+    import plume_scene
+    import smoke_b200
+
+    if rank != 0:
+        return None
+    if not os.path.exists(REF_LIBRARY):
+        return {"impl": "reference", "unavailable": f"reference library not built ({REF_LIBRARY}); oracle/build_oracle.py builds it from the reference sources"}
+    n = args.n
+    lib = smoke_b200.SmokeLibrary(REF_LIBRARY, extensions=False)
+    stream = torch.cuda.Stream()
+    cfg = plume_scene.plume_config(n, abi.MONOTONIC_CUBIC, pressure_iterations=REFERENCE_CG_ITERATIONS)
+    sim = smoke_b200.Simulation(lib, cfg, stream)
+    driver = plume_scene.PlumeDriver(sim, n, seed=1)
+    flush = L2Flush()
+    run_steps(sim, driver, 0, SPINUP_STEPS + args.warmup, flush)
+    with ClockSampler(local) as clocks:
+        t, _, _ = run_steps(sim, driver, SPINUP_STEPS + args.warmup, args.steps, flush)
+    e2e_ms, _ = run_e2e(sim, driver, SPINUP_STEPS + args.warmup + args.steps, args.steps)
+    sim.close()
+    ms = statistics.mean(t)
+    sample = f"{args.steps} steps of the {n}^3 plume after {SPINUP_STEPS + args.warmup} untimed steps, reference CUDA/cuSPARSE build, {REFERENCE_CG_ITERATIONS} fixed CG iterations"
+    return {
+        "metric": METRIC, "impl": "reference", "value": round(ms, 4), "unit": "ms/step", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume scene)",
+        "config": {"workload": f"plume {n}^3 monotone-cubic, reference fixed CG x{REFERENCE_CG_ITERATIONS} (smallest count reaching rel-res 1e-5)", "grid": [n, n, n],
+                   "l2": "flushed between timed steps (256 MiB write)"},
+        "pcg_iterations": REFERENCE_CG_ITERATIONS,
+        "cpu_baseline": {"value": round(ms, 4), "unit": "ms/step", "cores": 1, "kind": "reference", "sample": sample,
+                         "where": "the reference has no CPU implementation; its own CUDA build runs on the same B200, driven by one host thread"},
+        "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": driver.h2d_bytes, "d2h_bytes_per_step": driver.d2h_bytes},
+        "clocks": clocks.summary(),
+    }
+
+
+def calibrate_reference(args):
+    """Fixed CG counts vs achieved relative residual ||b - A p|| / ||b|| of the reference on the plume scene."""
+    import torch
+
+    import plume_scene
+    import smoke_b200
+
+    lib = smoke_b200.SmokeLibrary(REF_LIBRARY, extensions=False)
+    out = {}
+    for iters in args.calibrate_counts:
+        stream = torch.cuda.Stream()
+        cfg = plume_scene.plume_config(args.n, abi.MONOTONIC_CUBIC, pressure_iterations=iters)
+        sim = smoke_b200.Simulation(lib, cfg, stream)
+        driver = plume_scene.PlumeDriver(sim, args.n, seed=1)
+        run_steps(sim, driver, 0, SPINUP_STEPS, None)
+        worst = 0.0
+        for k in range(10):
+            run_steps(sim, driver, SPINUP_STEPS + k, 1, None)
+            with torch.cuda.stream(stream):
+                p = sim.view(abi.VIEW_FLOW_PRESSURE).double()
+                b = sim.view(abi.VIEW_FLOW_PRESSURE_RHS).double()
+                worst = max(worst, float(plume_scene.closed_box_residual(p, b)))
+        sim.close()
+        out[iters] = worst
+        print(json.dumps({"reference_cg_iterations": iters, "max_rel_residual": worst}), flush=True)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--calibrate-reference", action="store_true")
+    ap.add_argument("--calibrate-counts", type=int, nargs="*", default=[200, 300, 400, 500, 600, 800, 1000])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_setup(args.gpus)
+    if args.calibrate_reference:
+        calibrate_reference(args)
+        return
+    line = bench_reference(args, rank, world, local) if args.impl == "reference" else bench_b200(args, rank, world, local)
+    barrier(world) if args.impl == "b200" else None
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,100 @@
+/*
+ * Additive extensions of libsmoke_b200.so. None of them changes a symbol of visual-simulation-of-smoke-3d.h;
+ * a caller that never calls them gets the reference's behaviour.
+ *
+ *  - solver selection: the reference runs exactly `pressure_iterations` iterations of unpreconditioned FP32 CG
+ *    from x0 = 0 (backend-cuda.cu:1788-1824) and that is this library's default. The extension selects a
+ *    Jacobi-preconditioned CG that stops at a relative residual, FP64 dot products, FP64 iterative
+ *    refinement of the true residual and warm starts;
+ *  - solver status: iterations, residuals and a status word of the last step's pressure solve (the reference
+ *    computes none of these);
+ *  - face-velocity access: the reference has no velocity setter (backend-cuda.cu:2085-2159), so a scene can
+ *    only be seeded from rest; the setter lets a test or a checkpoint restore an arbitrary MAC state;
+ *  - stage-wise stepping: runs the step's stages in order up to a given one, so each stage can be compared
+ *    with a CPU restatement on its own.
+ */
+#ifndef SMOKE_B200_EXT_H
+#define SMOKE_B200_EXT_H
+
+#include "visual-simulation-of-smoke-3d.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum SmokeB200SolverMode {
+    /* Reference semantics: unpreconditioned CG, x0 = 0, exactly config.pressure_iterations iterations,
+     * alpha/beta set to 0 when |denominator| <= 1e-20 (backend-cuda.cu:1414-1418, 1788-1824). */
+    SMOKE_B200_SOLVER_FIXED_CG = 0,
+    /* Jacobi-preconditioned CG that stops once ||r|| <= tolerance * ||b|| or after max_iterations. */
+    SMOKE_B200_SOLVER_JACOBI_PCG = 1,
+} SmokeB200SolverMode;
+
+typedef enum SmokeB200Reduction {
+    SMOKE_B200_REDUCTION_FP32 = 0, /* dot products accumulated and kept in FP32, as cublasSdot does */
+    SMOKE_B200_REDUCTION_FP64 = 1, /* dot products, alpha and beta in FP64; vectors stay FP32 */
+} SmokeB200Reduction;
+
+typedef struct SmokeB200SolverDesc {
+    uint32_t mode;           /* SmokeB200SolverMode */
+    uint32_t reduction;      /* SmokeB200Reduction */
+    int32_t max_iterations;  /* JACOBI_PCG: iteration cap per refinement pass (FIXED_CG uses pressure_iterations) */
+    float tolerance;         /* JACOBI_PCG: target ||b - A x||_2 / ||b||_2 */
+    uint32_t refinement;     /* number of extra passes allowed when the FP64 true residual misses tolerance */
+    uint32_t warm_start;     /* 1: start from the previous step's pressure instead of 0 */
+} SmokeB200SolverDesc;
+
+typedef enum SmokeB200SolveStatus {
+    SMOKE_B200_SOLVE_CONVERGED      = 0, /* reached tolerance (JACOBI_PCG) */
+    SMOKE_B200_SOLVE_ITERATION_CAP  = 1, /* ran all iterations (always the case for FIXED_CG) */
+    SMOKE_B200_SOLVE_BREAKDOWN      = 2, /* a CG denominator vanished before convergence */
+    SMOKE_B200_SOLVE_NOT_FINITE     = 3, /* NaN or Inf in a reduction */
+    SMOKE_B200_SOLVE_BARRIER_TIMEOUT = 4, /* a grid barrier of the persistent solver gave up waiting */
+    SMOKE_B200_SOLVE_NOT_RUN        = 5, /* no step has run yet */
+} SmokeB200SolveStatus;
+
+typedef struct SmokeB200SolverStatus {
+    int32_t iterations;             /* inner iterations of the last solve, all refinement passes */
+    int32_t passes;                 /* refinement passes run (1 = no refinement needed) */
+    uint32_t status;                /* SmokeB200SolveStatus */
+    uint32_t reserved;
+    double rhs_norm;                /* ||b||_2 */
+    double relative_residual;       /* recurrence residual ||r||/||b|| at exit */
+    double true_relative_residual;  /* ||b - A x||/||b|| recomputed in FP64 at exit, -1 if not computed */
+} SmokeB200SolverStatus;
+
+/* Selects the pressure solver for every later step; re-captures the step graph. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_set_solver_cuda(SmokeSimulationContext context, const SmokeB200SolverDesc* desc);
+
+/* Synchronises the context stream and reports the last step's pressure solve. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_get_solver_status_cuda(SmokeSimulationContext context, SmokeB200SolverStatus* out_status);
+
+/* Copies face velocities from device pointers: u has (nx+1)*ny*nz values, v nx*(ny+1)*nz, w nx*ny*(nz+1),
+ * x fastest, the reference's MAC layout (backend-cuda.cu:125-135). NULL means zero. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_set_face_velocity_cuda(SmokeSimulationContext context, const float* u, const float* v, const float* w);
+
+/* Borrowed device pointers to the face velocities. which = 0: the step's velocity; which = 1: the advected
+ * velocity before projection (the reference's temp_velocity_*). */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_get_face_velocity_cuda(SmokeSimulationContext context, uint32_t which, const float** out_u, const float** out_v, const float** out_w);
+
+typedef enum SmokeB200Stage {
+    SMOKE_B200_STAGE_FORCES          = 0, /* vorticity, buoyancy, confinement, face update, boundaries */
+    SMOKE_B200_STAGE_ADVECT_VELOCITY = 1, /* semi-Lagrangian velocity advection into the temp velocity */
+    SMOKE_B200_STAGE_PRESSURE        = 2, /* right-hand side and pressure solve */
+    SMOKE_B200_STAGE_PROJECT         = 3, /* gradient subtract, boundaries, temp velocity -> velocity */
+    SMOKE_B200_STAGE_SCALARS         = 4, /* temperature and density: source, advection, solid rules */
+} SmokeB200Stage;
+
+/* Runs the stages of one step from the first one through `last_stage` (eagerly, outside the step graph). */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimulationContext context, uint32_t last_stage);
+
+/* Solves the pressure system of the context's current right-hand side (the FLOW_PRESSURE_RHS view) into the
+ * pressure buffer with the selected solver: the step's pressure stage without the right-hand-side kernel. One
+ * kernel launch on the context stream; the outcome is read with smoke_b200_get_solver_status_cuda. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext context);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SMOKE_B200_EXT_H */

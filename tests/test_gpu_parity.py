@@ -1,0 +1,251 @@
+"""GPU parity of libsmoke_b200.so against the oracle (the C restatement of the reference step).
+
+Each stage is checked in isolation: the GPU state right before the stage is loaded into the oracle, the oracle
+runs that one stage, and the result must match the GPU's within FP32 rounding. Full steps are then checked end
+to end. Tolerances are normwise: max|gpu - oracle| / max|oracle| per field.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+import scenes
+import smoke_abi as abi
+import smoke_b200
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "closed16_linear": dict(boundary="closed", shape=(16, 16, 16), mode=abi.LINEAR, solids=False),
+    "closed_cubic_solids": dict(boundary="closed", shape=(12, 10, 8), mode=abi.MONOTONIC_CUBIC, solids=True),
+    "plume_cubic_solids": dict(boundary="plume", shape=(16, 12, 8), mode=abi.MONOTONIC_CUBIC, solids=True),
+    "mixed_linear_solids": dict(boundary="mixed", shape=(9, 11, 7), mode=abi.LINEAR, solids=True),
+    "slip_cubic_solids": dict(boundary="slip", shape=(10, 8, 12), mode=abi.MONOTONIC_CUBIC, solids=True),
+}
+
+# FP32 rounding: the GPU contracts a*b+c into FMAs, the oracle does not.
+STAGE_TOL = 2e-5
+REPORT = os.environ.get("SMOKE_PARITY_REPORT")
+
+
+def report(name, value):
+    if REPORT:
+        with open(REPORT, "a") as f:
+            f.write(json.dumps({"check": name, "value": value}) + "\n")
+
+
+def setup_case(lib, stream, name, seed=3, cfl=0.6):
+    c = CASES[name]
+    cfg = scenes.make_config(*c["shape"], boundary=c["boundary"], mode=c["mode"])
+    inp = scenes.random_inputs(cfg, seed=seed, solids=c["solids"], cfl=cfl)
+    return cfg, inp
+
+
+def gpu_after(lib, stream, cfg, inp, last_stage, tol=1e-7):
+    sim = smoke_b200.Simulation(lib, cfg, stream)
+    keep = scenes.load_gpu(sim, inp)
+    sim.set_solver(abi.SOLVER_JACOBI_PCG, abi.REDUCTION_FP64, max_iterations=4000, tolerance=tol, refinement=2)
+    with torch.cuda.stream(stream):
+        sim.step_stages(last_stage)
+    stream.synchronize()
+    del keep
+    return sim
+
+
+def faces(sim, which):
+    stream = sim.stream
+    with torch.cuda.stream(stream):
+        t = [x.clone() for x in sim.face_velocity(which)]
+    stream.synchronize()
+    return [x.cpu().numpy() for x in t]
+
+
+def cells(sim, kind):
+    with torch.cuda.stream(sim.stream):
+        v = sim.view(kind)
+        v = tuple(x.clone() for x in v) if isinstance(v, tuple) else v.clone()
+    sim.stream.synchronize()
+    return [x.cpu().numpy() for x in v] if isinstance(v, tuple) else v.cpu().numpy()
+
+
+def oracle_from(cfg, inp):
+    st = O.OracleState(cfg, 32)
+    scenes.load_oracle(st, inp)
+    return st
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_stage_forces(smoke_lib, cuda_stream, name):
+    cfg, inp = setup_case(smoke_lib, cuda_stream, name)
+    sim = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_FORCES)
+    gu, gv, gw = faces(sim, 2)
+    sim.close()
+    st = oracle_from(cfg, inp)
+    st.step(0, 0)
+    errs = [scenes.rel_err(g, st[k]) for g, k in zip((gu, gv, gw), ("u", "v", "w"))]
+    report(f"forces/{name}", errs)
+    assert max(errs) < STAGE_TOL, errs
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("cfl", [0.6, 3.5])
+def test_stage_advect_velocity(smoke_lib, cuda_stream, name, cfl):
+    cfg, inp = setup_case(smoke_lib, cuda_stream, name, cfl=cfl)
+    pre = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_FORCES)
+    bu, bv, bw = faces(pre, 2)
+    pre.close()
+    sim = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_ADVECT_VELOCITY)
+    cu, cv, cw = faces(sim, 1)
+    sim.close()
+    st = oracle_from(cfg, inp)
+    st.set("u", bu)
+    st.set("v", bv)
+    st.set("w", bw)
+    st.step(1, 1)
+    errs = [scenes.rel_err(g, st[k]) for g, k in zip((cu, cv, cw), ("temp_u", "temp_v", "temp_w"))]
+    report(f"advect/{name}/cfl{cfl}", errs)
+    assert max(errs) < STAGE_TOL, errs
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_stage_pressure(smoke_lib, cuda_stream, name):
+    cfg, inp = setup_case(smoke_lib, cuda_stream, name)
+    sim = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_PRESSURE)
+    cu, cv, cw = faces(sim, 1)
+    rhs = cells(sim, abi.VIEW_FLOW_PRESSURE_RHS)
+    p = cells(sim, abi.VIEW_FLOW_PRESSURE)
+    status = sim.solver_status()
+    sim.close()
+    st = oracle_from(cfg, inp)
+    st.set("temp_u", cu)
+    st.set("temp_v", cv)
+    st.set("temp_w", cw)
+    st.step(2, 2, mode=1, max_iterations=4000, tolerance=1e-7)
+    e_rhs = scenes.rel_err(rhs, st["pressure_rhs"])
+    res = O.relative_residual(cfg, inp["occupancy"], rhs, p)
+    truth, _ = O.solve_pressure(cfg, inp["occupancy"], rhs, bits=64, tolerance=1e-12)
+    e_p = scenes.rel_err(p, truth)
+    report(f"pressure/{name}", {"rhs": e_rhs, "true_residual": res, "p_vs_fp64": e_p, "iterations": status.iterations, "status": status.status,
+                                "reported_true_residual": status.true_relative_residual})
+    assert e_rhs < STAGE_TOL
+    assert status.status == abi.SOLVE_CONVERGED
+    assert res < 5e-7
+    assert abs(status.true_relative_residual - res) < 1e-7
+    assert e_p < 1e-4
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_stage_project(smoke_lib, cuda_stream, name):
+    cfg, inp = setup_case(smoke_lib, cuda_stream, name)
+    pre = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_PRESSURE)
+    cu, cv, cw = faces(pre, 1)
+    p = cells(pre, abi.VIEW_FLOW_PRESSURE)
+    pre.close()
+    sim = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_PROJECT)
+    au, av, aw = faces(sim, 0)
+    sim.close()
+    st = oracle_from(cfg, inp)
+    st.set("temp_u", cu)
+    st.set("temp_v", cv)
+    st.set("temp_w", cw)
+    st.set("pressure", p)
+    st.step(3, 3)
+    errs = [scenes.rel_err(g, st[k]) for g, k in zip((au, av, aw), ("u", "v", "w"))]
+    report(f"project/{name}", errs)
+    assert max(errs) < STAGE_TOL, errs
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("cfl", [0.6, 3.5])
+def test_stage_scalars(smoke_lib, cuda_stream, name, cfl):
+    cfg, inp = setup_case(smoke_lib, cuda_stream, name, cfl=cfl)
+    pre = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_PROJECT)
+    au, av, aw = faces(pre, 0)
+    pre.close()
+    sim = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_SCALARS)
+    d = cells(sim, abi.VIEW_DENSITY)
+    t = cells(sim, abi.VIEW_TEMPERATURE)
+    sim.close()
+    st = oracle_from(cfg, inp)
+    st.set("u", au)
+    st.set("v", av)
+    st.set("w", aw)
+    occ = inp["occupancy"] != 0
+    st.set("temperature", np.where(occ, inp["solid_temperature"], inp["temperature"]))  # step-start solid rule
+    st.step(4, 4)
+    errs = {"density": scenes.rel_err(d, st["density"]), "temperature": scenes.rel_err(t, st["temperature"])}
+    report(f"scalars/{name}/cfl{cfl}", errs)
+    assert max(errs.values()) < STAGE_TOL, errs
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_views_after_step(smoke_lib, cuda_stream, name):
+    cfg, inp = setup_case(smoke_lib, cuda_stream, name)
+    sim = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_SCALARS)
+    au, av, aw = faces(sim, 0)
+    snap = sim.snapshot([abi.VIEW_FLOW_VELOCITY, abi.VIEW_FLOW_VELOCITY_MAGNITUDE, abi.VIEW_FLOW_VORTICITY, abi.VIEW_FLOW_VORTICITY_MAGNITUDE, abi.VIEW_FLOW_DIVERGENCE,
+                         abi.VIEW_OCCUPANCY])
+    sim.close()
+    st = oracle_from(cfg, inp)
+    st.set("u", au)
+    st.set("v", av)
+    st.set("w", aw)
+    st.step(5, 5)
+    pairs = {"velocity_x": "centered_x", "velocity_y": "centered_y", "velocity_z": "centered_z", "velocity_magnitude": "velocity_magnitude", "vorticity_x": "vorticity_x",
+             "vorticity_y": "vorticity_y", "vorticity_z": "vorticity_z", "vorticity_magnitude": "vorticity_magnitude"}
+    errs = {k: scenes.rel_err(snap[k], st[v]) for k, v in pairs.items()}
+    # divergence after projection is ~0: compare on the scale of the velocity differences it is made of
+    scale = max(np.abs(au).max(), np.abs(av).max(), np.abs(aw).max()) / cfg.cell_size
+    errs["divergence_abs_over_scale"] = float(np.abs(snap["divergence"] - st["divergence"]).max() / scale)
+    errs["occupancy"] = scenes.rel_err(snap["occupancy"], inp["occupancy"].astype(np.float32))
+    report(f"views/{name}", errs)
+    assert max(errs.values()) < STAGE_TOL, errs
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_full_steps_against_oracle(smoke_lib, cuda_stream, name):
+    """Three graph-launched steps against three oracle steps, both solving to 1e-7."""
+    cfg, inp = setup_case(smoke_lib, cuda_stream, name, seed=11)
+    sim = smoke_b200.Simulation(smoke_lib, cfg, cuda_stream)
+    keep = scenes.load_gpu(sim, inp)
+    sim.set_solver(abi.SOLVER_JACOBI_PCG, abi.REDUCTION_FP64, max_iterations=4000, tolerance=1e-7, refinement=2)
+    st = oracle_from(cfg, inp)
+    worst = {}
+    for k in range(3):
+        with torch.cuda.stream(cuda_stream):
+            sim.step()
+        st.step(0, 5, mode=1, max_iterations=4000, tolerance=1e-7)
+        snap = sim.snapshot([abi.VIEW_DENSITY, abi.VIEW_TEMPERATURE, abi.VIEW_FLOW_VELOCITY, abi.VIEW_FLOW_PRESSURE])
+        for g, o in (("density", "density"), ("temperature", "temperature"), ("velocity_x", "centered_x"), ("velocity_y", "centered_y"), ("velocity_z", "centered_z"),
+                     ("pressure", "pressure")):
+            worst[g] = max(worst.get(g, 0.0), scenes.rel_err(snap[g], st[o]))
+    sim.close()
+    del keep
+    report(f"full3/{name}", worst)
+    assert max(worst.values()) < 2e-3, worst
+
+
+def test_fixed_cg_matches_reference_semantics(smoke_lib, cuda_stream):
+    """Default solver = the reference's fixed-count unpreconditioned CG from x0 = 0: after k iterations the GPU
+    pressure matches the oracle's restatement of backend-cuda.cu:1788-1824 for the same right-hand side."""
+    cfg, inp = setup_case(smoke_lib, cuda_stream, "closed_cubic_solids")
+    out = {}
+    for iters in (1, 5, 20, 200):
+        cfg.pressure_iterations = iters
+        sim = smoke_b200.Simulation(smoke_lib, cfg, cuda_stream)
+        keep = scenes.load_gpu(sim, inp)
+        with torch.cuda.stream(cuda_stream):
+            sim.step_stages(abi.STAGE_PRESSURE)
+        rhs = cells(sim, abi.VIEW_FLOW_PRESSURE_RHS)
+        p = cells(sim, abi.VIEW_FLOW_PRESSURE)
+        status = sim.solver_status()
+        sim.close()
+        del keep
+        x, _ = O.solve_pressure(cfg, inp["occupancy"], rhs, bits=64, mode=0)
+        out[iters] = scenes.rel_err(p, x)
+        assert status.iterations == iters and status.status == abi.SOLVE_ITERATION_CAP
+    report("fixed_cg", out)
+    assert out[1] < 1e-5 and out[5] < 1e-4 and out[20] < 1e-3 and out[200] < 1e-4, out

@@ -1,0 +1,481 @@
+// C ABI of libsmoke_b200.so: context lifetime, inputs, step, views (visual-simulation-of-smoke-3d.h) and the
+// extensions of smoke_b200_ext.h. Host code only; kernels are reached through launch.h.
+//
+// Reference behaviour: backend-cuda.cu:1833-2282. Design:
+//  - one device arena per context (256-byte aligned sub-buffers), so a context is one cudaMalloc;
+//  - three face-velocity sets: A (state), B (after forces), C (after advection); the projection writes A, so a
+//    step needs no device-to-device copies;
+//  - the step is captured once into a CUDA graph on a private stream and launched on the context stream;
+//  - derived views (centred velocity, |u|, vorticity, |w|, divergence) are computed on demand in get_view, and
+//    materialised before an occupancy or velocity change so they always reflect the state right after the step;
+//  - occupancy-derived data (pressure anchor, operator row codes, density fill list) is rebuilt only when
+//    occupancy changes.
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <nvtx3/nvtx3.hpp>
+
+#include "launch.h"
+#include "smoke_b200_ext.h"
+#include "visual-simulation-of-smoke-3d.h"
+
+static_assert(sizeof(SmokeSimulationFlowBoundaryFaceDesc) == 20);
+static_assert(sizeof(SmokeSimulationFlowBoundaryConfig) == 120);
+static_assert(sizeof(SmokeSimulationScalarBoundaryFaceDesc) == 8);
+static_assert(sizeof(SmokeSimulationScalarBoundaryConfig) == 48);
+static_assert(sizeof(SmokeSimulationConfig) == 44 + 120 + 48 + 48);
+static_assert(offsetof(SmokeSimulationConfig, flow_boundary) == 44);
+static_assert(offsetof(SmokeSimulationConfig, density_boundary) == 164);
+static_assert(offsetof(SmokeSimulationConfig, temperature_boundary) == 212);
+static_assert(sizeof(SmokeSimulationContextCreateDesc) == 280);
+static_assert(offsetof(SmokeSimulationContextCreateDesc, stream) == 264);
+static_assert(sizeof(SmokeSimulationViewRequest) == 16);
+static_assert(sizeof(SmokeSimulationView) == 56);
+static_assert(offsetof(SmokeSimulationView, row_stride_bytes) == 16);
+static_assert(offsetof(SmokeSimulationView, data0) == 32);
+static_assert(sizeof(SmokeB200SolverStatus) == sizeof(smoke_b200::PcgStatusDevice));
+
+namespace smoke_b200 {
+namespace {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+bool valid_flow_axis(const SmokeSimulationFlowBoundaryFaceDesc& a, const SmokeSimulationFlowBoundaryFaceDesc& b) {
+    auto ok = [](uint32_t t) { return t <= SMOKE_SIMULATION_FLOW_BOUNDARY_PERIODIC; };
+    if (!ok(a.type) || !ok(b.type)) return false;
+    return (a.type == SMOKE_SIMULATION_FLOW_BOUNDARY_PERIODIC) == (b.type == SMOKE_SIMULATION_FLOW_BOUNDARY_PERIODIC);
+}
+bool valid_scalar_axis(const SmokeSimulationScalarBoundaryFaceDesc& a, const SmokeSimulationScalarBoundaryFaceDesc& b) {
+    auto ok = [](uint32_t t) { return t <= SMOKE_SIMULATION_SCALAR_BOUNDARY_PERIODIC; };
+    if (!ok(a.type) || !ok(b.type)) return false;
+    return (a.type == SMOKE_SIMULATION_SCALAR_BOUNDARY_PERIODIC) == (b.type == SMOKE_SIMULATION_SCALAR_BOUNDARY_PERIODIC);
+}
+
+// The reference's create-time validation (backend-cuda.cu:1835-1863), plus the 32-bit index range this
+// library's kernels use.
+bool valid_config(const SmokeSimulationConfig& c) {
+    if (c.nx <= 0 || c.ny <= 0 || c.nz <= 0 || !(c.cell_size > 0.0f) || !(c.dt > 0.0f) || c.pressure_iterations <= 0) return false;
+    const auto& f = c.flow_boundary;
+    const auto& d = c.density_boundary;
+    const auto& t = c.temperature_boundary;
+    if (!valid_flow_axis(f.x_minus, f.x_plus) || !valid_flow_axis(f.y_minus, f.y_plus) || !valid_flow_axis(f.z_minus, f.z_plus)) return false;
+    if (!valid_scalar_axis(d.x_minus, d.x_plus) || !valid_scalar_axis(d.y_minus, d.y_plus) || !valid_scalar_axis(d.z_minus, d.z_plus)) return false;
+    if (!valid_scalar_axis(t.x_minus, t.x_plus) || !valid_scalar_axis(t.y_minus, t.y_plus) || !valid_scalar_axis(t.z_minus, t.z_plus)) return false;
+    const uint64_t nx = c.nx, ny = c.ny, nz = c.nz;
+    const uint64_t biggest = (nx + 1) * (ny + 1) * (nz + 1);
+    return biggest < (1ull << 31);
+}
+
+}  // namespace
+}  // namespace smoke_b200
+
+using namespace smoke_b200;
+
+struct SmokeSimulationContext_t {
+    SmokeSimulationConfig config{};
+    StepParams P{};
+    cudaStream_t stream = nullptr;
+    bool owns_stream = false;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    int fill_blocks = 0;
+
+    Faces A{}, B{}, C{};
+    float *density = nullptr, *density_tmp = nullptr, *density_source = nullptr;
+    float *temperature = nullptr, *temperature_tmp = nullptr, *temperature_source = nullptr;
+    float *force_x = nullptr, *force_y = nullptr, *force_z = nullptr;
+    float *solid_vx = nullptr, *solid_vy = nullptr, *solid_vz = nullptr, *solid_temperature = nullptr;
+    float* occupancy_float = nullptr;
+    float *pressure = nullptr, *rhs = nullptr;
+    float *cx = nullptr, *cy = nullptr, *cz = nullptr, *vmag = nullptr;
+    float *wx = nullptr, *wy = nullptr, *wz = nullptr, *wmag = nullptr, *divergence = nullptr;
+    float *fx = nullptr, *fy = nullptr, *fz = nullptr;
+    PcgWork pcg{};
+    uint16_t* codes = nullptr;
+    uint8_t* occupancy = nullptr;
+    FillEntry* fill_list = nullptr;
+    uint32_t* fill_count = nullptr;
+    int32_t* anchor = nullptr;
+    PcgControl* control = nullptr;
+
+    SmokeB200SolverDesc solver{SMOKE_B200_SOLVER_FIXED_CG, SMOKE_B200_REDUCTION_FP32, 500, 1.0e-5f, 0, 0};
+    PcgLaunchShape pcg_shape{};
+    bool views_stale = false;
+    bool stepped = false;
+
+    ~SmokeSimulationContext_t() { release(); }
+
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        if (arena) cudaFree(arena);
+        arena = nullptr;
+        if (capture_stream) cudaStreamDestroy(capture_stream);
+        capture_stream = nullptr;
+        if (owns_stream && stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+        owns_stream = false;
+    }
+
+    void allocate() {
+        const size_t n = P.n, nu = P.nu, nv = P.nv, nw = P.nw;
+        struct Slot {
+            void** ptr;
+            size_t bytes;
+        };
+        std::vector<Slot> slots;
+        auto f32 = [&](float** p, size_t count) { slots.push_back({reinterpret_cast<void**>(p), count * sizeof(float)}); };
+        for (Faces* f : {&A, &B, &C}) {
+            f32(&f->u, nu);
+            f32(&f->v, nv);
+            f32(&f->w, nw);
+        }
+        for (float** p : {&density, &density_tmp, &density_source, &temperature, &temperature_tmp, &temperature_source, &force_x, &force_y, &force_z, &solid_vx, &solid_vy, &solid_vz, &solid_temperature, &occupancy_float, &pressure, &rhs, &cx, &cy, &cz, &vmag, &wx, &wy, &wz, &wmag,
+                          &divergence, &fx, &fy, &fz, &pcg.r[0], &pcg.r[1], &pcg.s[0], &pcg.s[1], &pcg.w[0], &pcg.w[1], &pcg.p})
+            f32(p, n);
+        slots.push_back({reinterpret_cast<void**>(&codes), n * sizeof(uint16_t)});
+        slots.push_back({reinterpret_cast<void**>(&occupancy), n});
+        slots.push_back({reinterpret_cast<void**>(&fill_list), n * sizeof(FillEntry)});
+        slots.push_back({reinterpret_cast<void**>(&fill_count), sizeof(uint32_t)});
+        slots.push_back({reinterpret_cast<void**>(&anchor), sizeof(int32_t)});
+        slots.push_back({reinterpret_cast<void**>(&control), sizeof(PcgControl)});
+        auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
+        size_t total = 0;
+        for (const Slot& s : slots) total += align(s.bytes);
+        check(cudaMalloc(&arena, total), "cudaMalloc arena");
+        arena_bytes = total;
+        size_t off = 0;
+        for (const Slot& s : slots) {
+            *s.ptr = static_cast<char*>(arena) + off;
+            off += align(s.bytes);
+        }
+    }
+
+    // Occupancy-derived data: anchor, operator codes, density fill list, float occupancy view.
+    void rebuild_occupancy_data() {
+        check(launch_occupancy_float(P, occupancy, occupancy_float, stream), "occupancy view");
+        check(launch_anchor(P, occupancy, anchor, stream), "pressure anchor");
+        check(launch_stencil_codes(P, occupancy, anchor, codes, stream), "operator codes");
+        check(launch_fill_build(P, occupancy, anchor, fill_list, fill_count, stream), "density fill list");
+    }
+
+    PcgSettings pcg_settings() const {
+        PcgSettings S{};
+        const bool fixed = solver.mode == SMOKE_B200_SOLVER_FIXED_CG;
+        S.jacobi = fixed ? 0 : 1;
+        S.fp64 = solver.reduction == SMOKE_B200_REDUCTION_FP64;
+        S.fixed = fixed ? 1 : 0;
+        S.max_iterations = fixed ? config.pressure_iterations : solver.max_iterations;
+        S.tolerance = solver.tolerance;
+        S.refinement = fixed ? 0 : static_cast<int32_t>(solver.refinement);
+        S.warm_start = solver.warm_start ? 1 : 0;
+        return S;
+    }
+
+    // Stages of one step, in the reference's order (backend-cuda.cu:2000-2057, views excluded).
+    void enqueue_stages(cudaStream_t s, uint32_t last_stage) {
+        const ConstFaces solid{solid_vx, solid_vy, solid_vz};
+        check(launch_vorticity(P, as_const(A), occupancy, wx, wy, wz, wmag, s), "vorticity");
+        check(launch_cell_force(P, wx, wy, wz, wmag, density, temperature, force_x, force_y, force_z, occupancy, fx, fy, fz, s), "cell force");
+        check(launch_face_force(P, as_const(A), fx, fy, fz, occupancy, solid, B, s), "face force");
+        if (last_stage < SMOKE_B200_STAGE_ADVECT_VELOCITY) return;
+        check(launch_advect_velocity(P, as_const(B), occupancy, solid, C, s), "advect velocity");
+        if (last_stage < SMOKE_B200_STAGE_PRESSURE) return;
+        check(launch_rhs(P, as_const(C), occupancy, anchor, rhs, s), "pressure rhs");
+        check(launch_pcg(P, pcg_settings(), pcg_shape, codes, rhs, pressure, pcg, control, s), "pressure solve");
+        if (last_stage < SMOKE_B200_STAGE_PROJECT) return;
+        check(launch_project(P, as_const(C), pressure, occupancy, solid, A, s), "project");
+        if (last_stage < SMOKE_B200_STAGE_SCALARS) return;
+        check(launch_scalar_prep(P, temperature, temperature_source, density, density_source, occupancy, solid_temperature, temperature_tmp, density_tmp, s), "scalar sources");
+        check(launch_advect_scalars(P, as_const(A), occupancy, temperature_tmp, density_tmp, solid_temperature, temperature, density, s), "advect scalars");
+        check(launch_density_fill(fill_list, fill_count, density, fill_blocks, s), "density fill");
+    }
+
+    void capture_step_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        check(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal), "begin step capture");
+        try {
+            enqueue_stages(capture_stream, SMOKE_B200_STAGE_SCALARS);
+        } catch (...) {
+            cudaGraph_t broken = nullptr;
+            cudaStreamEndCapture(capture_stream, &broken);
+            if (broken) cudaGraphDestroy(broken);
+            throw;
+        }
+        check(cudaStreamEndCapture(capture_stream, &graph), "end step capture");
+        check(cudaGraphInstantiate(&exec, graph, 0), "instantiate step graph");
+    }
+
+    void materialise_views() {
+        if (!views_stale) return;
+        check(launch_views(P, as_const(A), occupancy, cx, cy, cz, vmag, wx, wy, wz, wmag, divergence, stream), "views");
+        views_stale = false;
+    }
+};
+
+namespace {
+
+SmokeSimulationResult ok_or_fail(cudaError_t e) { return e == cudaSuccess ? SMOKE_SIMULATION_RESULT_OK : SMOKE_SIMULATION_RESULT_BACKEND_FAILURE; }
+
+template <class F>
+SmokeSimulationResult guarded(F&& f) {
+    try {
+        return f();
+    } catch (const std::bad_alloc&) {
+        return SMOKE_SIMULATION_RESULT_OUT_OF_MEMORY;
+    } catch (...) {
+        return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    }
+}
+
+cudaError_t copy_or_zero(float* dst, const float* src, size_t count, cudaStream_t s) {
+    if (src == nullptr) return cudaMemsetAsync(dst, 0, count * sizeof(float), s);
+    return cudaMemcpyAsync(dst, src, count * sizeof(float), cudaMemcpyDeviceToDevice, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+SmokeSimulationResult smoke_simulation_create_context_cuda(const SmokeSimulationContextCreateDesc* desc, SmokeSimulationContext* out_context) {
+    nvtx3::scoped_range range("smoke_b200.create_context");
+    if (desc == nullptr || out_context == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (!valid_config(desc->config)) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    *out_context = nullptr;
+    std::unique_ptr<SmokeSimulationContext_t> ctx(new (std::nothrow) SmokeSimulationContext_t{});
+    if (!ctx) return SMOKE_SIMULATION_RESULT_OUT_OF_MEMORY;
+    const SmokeSimulationResult r = guarded([&] {
+        ctx->config = desc->config;
+        ctx->P = make_params(desc->config);
+        ctx->stream = static_cast<cudaStream_t>(desc->stream);
+        if (ctx->stream == nullptr) {
+            check(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "create stream");
+            ctx->owns_stream = true;
+        }
+        check(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking), "create capture stream");
+        int dev = 0, sms = 0;
+        check(cudaGetDevice(&dev), "device");
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+        ctx->fill_blocks = sms * 4;
+        check(pcg_launch_shape(&ctx->pcg_shape), "solver launch shape");
+        ctx->allocate();
+        cudaStream_t s = ctx->stream;
+        check(cudaMemsetAsync(ctx->arena, 0, ctx->arena_bytes, s), "zero arena");
+        check(launch_fill_value(ctx->density, desc->initial_density, ctx->P.n, s), "initial density");
+        check(launch_fill_value(ctx->temperature, desc->initial_temperature, ctx->P.n, s), "initial temperature");
+        check(launch_fill_value(ctx->solid_temperature, desc->config.ambient_temperature, ctx->P.n, s), "solid temperature");
+        ctx->rebuild_occupancy_data();
+        // the capture stream must not start before the arena is initialised
+        check(cudaStreamSynchronize(s), "initialise context");
+        ctx->capture_step_graph();
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+    if (r != SMOKE_SIMULATION_RESULT_OK) return r;
+    *out_context = ctx.release();
+    return SMOKE_SIMULATION_RESULT_OK;
+}
+
+SmokeSimulationResult smoke_simulation_destroy_context_cuda(SmokeSimulationContext context) {
+    nvtx3::scoped_range range("smoke_b200.destroy_context");
+    if (context == nullptr) return SMOKE_SIMULATION_RESULT_OK;
+    if (context->stream) cudaStreamSynchronize(context->stream);
+    delete context;
+    return SMOKE_SIMULATION_RESULT_OK;
+}
+
+SmokeSimulationResult smoke_simulation_update_density_cuda(SmokeSimulationContext c, const float* values) {
+    nvtx3::scoped_range range("smoke_b200.update_density");
+    return ok_or_fail(copy_or_zero(c->density, values, c->P.n, c->stream));
+}
+
+SmokeSimulationResult smoke_simulation_update_density_source_cuda(SmokeSimulationContext c, const float* values) {
+    nvtx3::scoped_range range("smoke_b200.update_density_source");
+    return ok_or_fail(copy_or_zero(c->density_source, values, c->P.n, c->stream));
+}
+
+SmokeSimulationResult smoke_simulation_update_temperature_cuda(SmokeSimulationContext c, const float* values) {
+    nvtx3::scoped_range range("smoke_b200.update_temperature");
+    return ok_or_fail(copy_or_zero(c->temperature, values, c->P.n, c->stream));
+}
+
+SmokeSimulationResult smoke_simulation_update_temperature_source_cuda(SmokeSimulationContext c, const float* values) {
+    nvtx3::scoped_range range("smoke_b200.update_temperature_source");
+    return ok_or_fail(copy_or_zero(c->temperature_source, values, c->P.n, c->stream));
+}
+
+SmokeSimulationResult smoke_simulation_update_force_cuda(SmokeSimulationContext c, const float* x, const float* y, const float* z) {
+    nvtx3::scoped_range range("smoke_b200.update_force");
+    if (copy_or_zero(c->force_x, x, c->P.n, c->stream) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (copy_or_zero(c->force_y, y, c->P.n, c->stream) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return ok_or_fail(copy_or_zero(c->force_z, z, c->P.n, c->stream));
+}
+
+SmokeSimulationResult smoke_simulation_update_occupancy_cuda(SmokeSimulationContext c, const uint8_t* values) {
+    nvtx3::scoped_range range("smoke_b200.update_occupancy");
+    return guarded([&] {
+        c->materialise_views();  // derived views keep showing the state right after the last step
+        if (values == nullptr) check(cudaMemsetAsync(c->occupancy, 0, c->P.n, c->stream), "clear occupancy");
+        else check(cudaMemcpyAsync(c->occupancy, values, c->P.n, cudaMemcpyDeviceToDevice, c->stream), "copy occupancy");
+        c->rebuild_occupancy_data();
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+SmokeSimulationResult smoke_simulation_update_solid_velocity_cuda(SmokeSimulationContext c, const float* x, const float* y, const float* z) {
+    nvtx3::scoped_range range("smoke_b200.update_solid_velocity");
+    if (copy_or_zero(c->solid_vx, x, c->P.n, c->stream) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (copy_or_zero(c->solid_vy, y, c->P.n, c->stream) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return ok_or_fail(copy_or_zero(c->solid_vz, z, c->P.n, c->stream));
+}
+
+SmokeSimulationResult smoke_simulation_update_solid_temperature_cuda(SmokeSimulationContext c, const float* values) {
+    nvtx3::scoped_range range("smoke_b200.update_solid_temperature");
+    if (values == nullptr) return ok_or_fail(launch_fill_value(c->solid_temperature, c->config.ambient_temperature, c->P.n, c->stream));
+    return ok_or_fail(cudaMemcpyAsync(c->solid_temperature, values, c->P.n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+}
+
+SmokeSimulationResult smoke_simulation_step_cuda(SmokeSimulationContext c) {
+    nvtx3::scoped_range range("smoke_b200.step");
+    if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (cudaGraphLaunch(c->exec, c->stream) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    c->views_stale = true;
+    c->stepped = true;
+    return SMOKE_SIMULATION_RESULT_OK;
+}
+
+SmokeSimulationResult smoke_simulation_get_view_cuda(SmokeSimulationContext c, const SmokeSimulationViewRequest* request, SmokeSimulationView* out) {
+    nvtx3::scoped_range range("smoke_b200.get_view");
+    if (c == nullptr || request == nullptr || out == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    *out = SmokeSimulationView{};
+    out->layout = SMOKE_SIMULATION_VIEW_LAYOUT_F32_3D;
+    out->nx = c->config.nx;
+    out->ny = c->config.ny;
+    out->nz = c->config.nz;
+    out->row_stride_bytes = static_cast<uint64_t>(c->config.nx) * sizeof(float);
+    out->slice_stride_bytes = static_cast<uint64_t>(c->config.nx) * static_cast<uint64_t>(c->config.ny) * sizeof(float);
+    auto one = [&](const float* p) { out->data0 = p; };
+    auto three = [&](const float* a, const float* b, const float* d) {
+        out->layout = SMOKE_SIMULATION_VIEW_LAYOUT_F32_3D_SOA3;
+        out->data0 = a;
+        out->data1 = b;
+        out->data2 = d;
+    };
+    const SmokeSimulationResult r = guarded([&] {
+        switch (request->kind) {
+        case SMOKE_SIMULATION_VIEW_DENSITY: one(c->density); break;
+        case SMOKE_SIMULATION_VIEW_DENSITY_SOURCE: one(c->density_source); break;
+        case SMOKE_SIMULATION_VIEW_TEMPERATURE: one(c->temperature); break;
+        case SMOKE_SIMULATION_VIEW_TEMPERATURE_SOURCE: one(c->temperature_source); break;
+        case SMOKE_SIMULATION_VIEW_FORCE: three(c->force_x, c->force_y, c->force_z); break;
+        case SMOKE_SIMULATION_VIEW_SOLID_VELOCITY: three(c->solid_vx, c->solid_vy, c->solid_vz); break;
+        case SMOKE_SIMULATION_VIEW_SOLID_TEMPERATURE: one(c->solid_temperature); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_VELOCITY: c->materialise_views(); three(c->cx, c->cy, c->cz); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_VELOCITY_MAGNITUDE: c->materialise_views(); one(c->vmag); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_PRESSURE: one(c->pressure); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_PRESSURE_RHS: one(c->rhs); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_DIVERGENCE: c->materialise_views(); one(c->divergence); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_VORTICITY: c->materialise_views(); three(c->wx, c->wy, c->wz); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_VORTICITY_MAGNITUDE: c->materialise_views(); one(c->wmag); break;
+        case SMOKE_SIMULATION_VIEW_OCCUPANCY: one(c->occupancy_float); break;
+        default: return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+        }
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+    if (r != SMOKE_SIMULATION_RESULT_OK) return r;
+    // order a foreign consumer stream after the context stream (backend-cuda.cu:2189-2205)
+    if (request->consumer_stream == nullptr) return SMOKE_SIMULATION_RESULT_OK;
+    auto consumer = static_cast<cudaStream_t>(request->consumer_stream);
+    if (consumer == c->stream) return SMOKE_SIMULATION_RESULT_OK;
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    const bool ok = cudaEventRecord(ev, c->stream) == cudaSuccess && cudaStreamWaitEvent(consumer, ev, 0) == cudaSuccess;
+    cudaEventDestroy(ev);
+    return ok ? SMOKE_SIMULATION_RESULT_OK : SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+}
+
+// ---------------------------------------------------------------------------------------------- extensions
+SmokeSimulationResult smoke_b200_set_solver_cuda(SmokeSimulationContext c, const SmokeB200SolverDesc* desc) {
+    if (c == nullptr || desc == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (desc->mode > SMOKE_B200_SOLVER_JACOBI_PCG || desc->reduction > SMOKE_B200_REDUCTION_FP64) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (desc->mode == SMOKE_B200_SOLVER_JACOBI_PCG && (desc->max_iterations <= 0 || !(desc->tolerance > 0.0f))) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        c->solver = *desc;
+        c->capture_step_graph();
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+SmokeSimulationResult smoke_b200_get_solver_status_cuda(SmokeSimulationContext c, SmokeB200SolverStatus* out) {
+    if (c == nullptr || out == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (!c->stepped) {
+        *out = SmokeB200SolverStatus{};
+        out->status = SMOKE_B200_SOLVE_NOT_RUN;
+        out->true_relative_residual = -1.0;
+        return SMOKE_SIMULATION_RESULT_OK;
+    }
+    PcgStatusDevice st{};
+    if (cudaMemcpyAsync(&st, &c->control->status, sizeof(st), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    std::memcpy(out, &st, sizeof(st));
+    return SMOKE_SIMULATION_RESULT_OK;
+}
+
+SmokeSimulationResult smoke_b200_set_face_velocity_cuda(SmokeSimulationContext c, const float* u, const float* v, const float* w) {
+    if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        c->materialise_views();
+        check(copy_or_zero(c->A.u, u, c->P.nu, c->stream), "set u");
+        check(copy_or_zero(c->A.v, v, c->P.nv, c->stream), "set v");
+        check(copy_or_zero(c->A.w, w, c->P.nw, c->stream), "set w");
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+SmokeSimulationResult smoke_b200_get_face_velocity_cuda(SmokeSimulationContext c, uint32_t which, const float** u, const float** v, const float** w) {
+    if (c == nullptr || u == nullptr || v == nullptr || w == nullptr || which > 2) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    const Faces& f = which == 0 ? c->A : (which == 1 ? c->C : c->B);
+    *u = f.u;
+    *v = f.v;
+    *w = f.w;
+    return SMOKE_SIMULATION_RESULT_OK;
+}
+
+SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimulationContext c, uint32_t last_stage) {
+    if (c == nullptr || last_stage > SMOKE_B200_STAGE_SCALARS) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        c->enqueue_stages(c->stream, last_stage);
+        c->views_stale = true;
+        c->stepped = true;
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext c) {
+    if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        check(launch_pcg(c->P, c->pcg_settings(), c->pcg_shape, c->codes, c->rhs, c->pressure, c->pcg, c->control, c->stream), "pressure solve");
+        c->stepped = true;
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,115 @@
+// Host-side launchers of the B200 smoke kernels. Plain pointers and sizes only; every launcher enqueues on
+// `stream` and returns the launch status.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "smoke_device.cuh"
+
+namespace smoke_b200 {
+
+// Face velocity triple (u: (nx+1)*ny*nz, v: nx*(ny+1)*nz, w: nx*ny*(nz+1)).
+struct Faces {
+    float* u;
+    float* v;
+    float* w;
+};
+struct ConstFaces {
+    const float* u;
+    const float* v;
+    const float* w;
+};
+inline ConstFaces as_const(const Faces& f) { return {f.u, f.v, f.w}; }
+
+// One entry of the density fill list: a solid cell and the fluid cell it copies (-1: none, value 0).
+struct FillEntry {
+    uint32_t cell;
+    int32_t source;
+};
+
+StepParams make_params(const SmokeSimulationConfig& cfg);
+
+// Forces: vorticity of the cell-centred velocity (writes the four vorticity buffers).
+cudaError_t launch_vorticity(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* wx, float* wy, float* wz, float* wmag, cudaStream_t s);
+// Forces: f = user force + buoyancy + vorticity confinement per cell.
+cudaError_t launch_cell_force(const StepParams& P, const float* wx, const float* wy, const float* wz, const float* wmag, const float* density, const float* temperature, const float* ufx, const float* ufy, const float* ufz, const uint8_t* occ, float* fx, float* fy, float* fz, cudaStream_t s);
+// Forces: out = settled(in + dt * face-average of f) (domain, solid and periodic face rules applied).
+cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* fx, const float* fy, const float* fz, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
+// Velocity self-advection: out = settled(semi-Lagrangian sample of in along in).
+cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
+// Pressure right-hand side from the advected velocity.
+cudaError_t launch_rhs(const StepParams& P, ConstFaces vel, const uint8_t* occ, const int32_t* anchor, float* rhs, cudaStream_t s);
+// Projection: out = settled(in - dt * grad p / h).
+cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
+// Scalars: source terms (and solid temperature) into the temporaries.
+cudaError_t launch_scalar_prep(const StepParams& P, const float* temperature, const float* temperature_source, const float* density, const float* density_source, const uint8_t* occ, const float* solid_temperature, float* t_tmp, float* d_tmp, cudaStream_t s);
+// Scalars: one shared back-trace per cell, sample both scalars, solid rules.
+cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, const uint8_t* occ, const float* t_tmp, const float* d_tmp, const float* solid_temperature, float* temperature, float* density, cudaStream_t s);
+// Scalars: solid cells copy their nearest fluid cell's density.
+cudaError_t launch_density_fill(const FillEntry* list, const uint32_t* count, float* density, int max_blocks, cudaStream_t s);
+// Derived views: centred velocity, |u|, vorticity, |w|, divergence of the step's final velocity.
+cudaError_t launch_views(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* cx, float* cy, float* cz, float* vmag, float* wx, float* wy, float* wz, float* wmag, float* div, cudaStream_t s);
+
+// Occupancy-derived data (run when occupancy changes).
+cudaError_t launch_occupancy_float(const StepParams& P, const uint8_t* occ, float* out, cudaStream_t s);
+cudaError_t launch_anchor(const StepParams& P, const uint8_t* occ, int32_t* anchor, cudaStream_t s);
+cudaError_t launch_stencil_codes(const StepParams& P, const uint8_t* occ, const int32_t* anchor, uint16_t* codes, cudaStream_t s);
+cudaError_t launch_fill_build(const StepParams& P, const uint8_t* occ, const int32_t* anchor, FillEntry* list, uint32_t* count, cudaStream_t s);
+
+cudaError_t launch_fill_value(float* dst, float value, uint64_t count, cudaStream_t s);
+
+// ------------------------------------------------------------------------------------------ pressure solve
+// Persistent, cooperative conjugate-gradient solver (pcg.cu). One launch solves A x = b for the masked
+// 7-point operator encoded in `codes` (bits 0-5: active neighbours -x,+x,-y,+y,-z,+z; bits 8-10: diagonal).
+struct PcgSettings {
+    int32_t jacobi;          // 0: M = I (reference CG), 1: M = diag(A)^-1
+    int32_t fp64;            // reductions in FP64 (1) or FP32 (0)
+    int32_t fixed;           // 1: run exactly max_iterations (reference semantics), 0: stop at tolerance
+    int32_t max_iterations;
+    float tolerance;
+    int32_t refinement;      // extra passes on the FP64 true residual
+    int32_t warm_start;      // start from x instead of 0
+    int32_t reserved;
+};
+
+struct PcgStatusDevice {
+    int32_t iterations;
+    int32_t passes;
+    uint32_t status;
+    uint32_t reserved;
+    double rhs_norm;
+    double relative_residual;
+    double true_relative_residual;
+};
+
+// Device-resident control block: grid barrier, abort flag, per-block partial sums (double-buffered by
+// iteration parity) and the status of the last solve.
+constexpr int kPcgMaxBlocks = 148 * 16;
+struct PcgControl {
+    unsigned int count;
+    unsigned int gen;
+    int abort;
+    int pad;
+    PcgStatusDevice status;
+    double partial[2][kPcgMaxBlocks][4];
+};
+
+struct PcgWork {
+    float* r[2];
+    float* s[2];
+    float* w[2];
+    float* p;
+};
+
+struct PcgLaunchShape {
+    int blocks;
+    int threads;
+};
+
+// Picks the persistent grid (all blocks co-resident) for the current device.
+cudaError_t pcg_launch_shape(PcgLaunchShape* out);
+// Enqueues: reset of the control header, then the cooperative solver launch.
+cudaError_t launch_pcg(const StepParams& P, const PcgSettings& S, const PcgLaunchShape& shape, const uint16_t* codes, const float* b, float* x, PcgWork work, PcgControl* ctl, cudaStream_t s);
+
+}  // namespace smoke_b200

@@ -1,0 +1,384 @@
+// Device-side building blocks of the B200 smoke step: launch parameters, index arithmetic, the reference's
+// boundary "ghost" rules, trilinear / monotone-cubic samplers and the RK2 back-trace.
+//
+// Behaviour follows the reference (backend-cuda.cu:121-838); the structure does not: every rule is
+// written once and specialised by template on the field kind, and each sampler first tests whether its whole
+// tap box lies inside the array, in which case it gathers without any boundary logic (the common case).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "visual-simulation-of-smoke-3d.h"
+
+namespace smoke_b200 {
+
+constexpr uint32_t kFlowNoSlip = SMOKE_SIMULATION_FLOW_BOUNDARY_NO_SLIP_WALL;
+constexpr uint32_t kFlowFreeSlip = SMOKE_SIMULATION_FLOW_BOUNDARY_FREE_SLIP_WALL;
+constexpr uint32_t kFlowOutflow = SMOKE_SIMULATION_FLOW_BOUNDARY_OUTFLOW;
+constexpr uint32_t kFlowPeriodic = SMOKE_SIMULATION_FLOW_BOUNDARY_PERIODIC;
+constexpr uint32_t kScalarFixed = SMOKE_SIMULATION_SCALAR_BOUNDARY_FIXED_VALUE;
+constexpr uint32_t kScalarZeroFlux = SMOKE_SIMULATION_SCALAR_BOUNDARY_ZERO_FLUX;
+constexpr uint32_t kScalarPeriodic = SMOKE_SIMULATION_SCALAR_BOUNDARY_PERIODIC;
+
+// Unsigned division by a runtime constant d >= 1, exact for every 32-bit numerator
+// (Granlund & Montgomery 1994, "round-up" multiplier with the add-and-shift fix-up).
+struct FastDiv {
+    uint32_t d = 1, m = 0, s = 0;
+    FastDiv() = default;
+    explicit FastDiv(uint32_t divisor) : d(divisor) {
+        uint32_t l = 0;
+        while ((1ull << l) < d) ++l;
+        m = static_cast<uint32_t>(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+        s = l;
+    }
+#if defined(__CUDACC__)
+    __device__ __forceinline__ uint32_t div(uint32_t n) const {
+        if (d == 1) return n;
+        const uint32_t t = __umulhi(n, m);
+        return (t + ((n - t) >> 1)) >> (s - 1);
+    }
+#endif
+};
+
+// Everything a step kernel needs, passed by value (__grid_constant__) to every launch.
+struct StepParams {
+    int nx, ny, nz;
+    float h, dt;
+    float ambient, alpha, beta, epsilon;
+    int cubic;          // scalar_advection_mode == MONOTONIC_CUBIC (applies to velocity and scalars)
+    int fper[3];        // flow periodic per axis
+    int dper[3];        // density periodic per axis
+    int tper[3];        // temperature periodic per axis
+    SmokeSimulationFlowBoundaryFaceDesc flow[6];   // x-, x+, y-, y+, z-, z+
+    SmokeSimulationScalarBoundaryFaceDesc den[6];
+    SmokeSimulationScalarBoundaryFaceDesc tem[6];
+    uint32_t n, nu, nv, nw; // cell and face counts
+    FastDiv div_nx, div_ny, div_slab;            // cells: x fastest
+    FastDiv div_fx[3], div_fy[3];                // faces of axis a: row length and rows per slab
+};
+
+#if defined(__CUDACC__)
+
+__device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
+__device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return imin(imax(v, lo), hi); }
+__device__ __forceinline__ int wrapi(int v, int n) {
+    v %= n;
+    return v < 0 ? v + n : v;
+}
+
+// Cell (x,y,z) -> linear index, x fastest.
+__device__ __forceinline__ uint32_t cidx(const StepParams& P, int x, int y, int z) {
+    return (static_cast<uint32_t>(z) * P.ny + y) * P.nx + x;
+}
+// Face of axis A: extents (nx + [A==0]) x (ny + [A==1]) x (nz + [A==2]).
+template <int A>
+__device__ __forceinline__ int fsx(const StepParams& P) { return P.nx + (A == 0); }
+template <int A>
+__device__ __forceinline__ int fsy(const StepParams& P) { return P.ny + (A == 1); }
+template <int A>
+__device__ __forceinline__ int fsz(const StepParams& P) { return P.nz + (A == 2); }
+template <int A>
+__device__ __forceinline__ uint32_t fidx(const StepParams& P, int i, int j, int k) {
+    return (static_cast<uint32_t>(k) * fsy<A>(P) + j) * fsx<A>(P) + i;
+}
+
+__device__ __forceinline__ float face_comp(const SmokeSimulationFlowBoundaryFaceDesc& f, int c) {
+    return c == 0 ? f.velocity_x : (c == 1 ? f.velocity_y : f.velocity_z);
+}
+
+__device__ __forceinline__ int axis_n(const StepParams& P, int a) { return a == 0 ? P.nx : (a == 1 ? P.ny : P.nz); }
+
+// ---------------------------------------------------------------------------------------------- taps
+// Face component A at integer index (i,j,k), with the reference's ghost rule outside the array
+// (backend-cuda.cu:276-376): along A, OUTFLOW -> interior, otherwise 2*wall - interior; across A,
+// OUTFLOW and FREE_SLIP -> interior, otherwise 2*wall - interior; periodic axes wrap. Axes are resolved
+// in x, y, z order and the interior sample clamps the remaining coordinates.
+template <int A>
+__device__ inline float face_tap_slow(const float* __restrict__ f, int i, int j, int k, const StepParams& P) {
+    int c[3] = {i, j, k};
+    const int ext[3] = {fsx<A>(P) - 1, fsy<A>(P) - 1, fsz<A>(P) - 1};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (c[a] < 0 || c[a] > ext[a]) {
+            if (P.fper[a]) {
+                c[a] = wrapi(c[a], axis_n(P, a));
+            } else {
+                const SmokeSimulationFlowBoundaryFaceDesc face = P.flow[2 * a + (c[a] < 0 ? 0 : 1)];
+                int q[3];
+#pragma unroll
+                for (int b = 0; b < 3; ++b) q[b] = (b == a) ? (c[a] < 0 ? 0 : ext[a]) : clampi(c[b], 0, ext[b]);
+                const float interior = f[fidx<A>(P, q[0], q[1], q[2])];
+                if (face.type == kFlowOutflow) return interior;
+                if (a != A && face.type == kFlowFreeSlip) return interior;
+                return 2.0f * face_comp(face, A) - interior;
+            }
+        }
+    }
+    return f[fidx<A>(P, c[0], c[1], c[2])];
+}
+
+// Cell-centred scalar tap with the scalar rule (backend-cuda.cu:166-200): PERIODIC wraps, ZERO_FLUX clamps,
+// FIXED_VALUE returns the face value.
+__device__ inline float scalar_tap_slow(const float* __restrict__ f, int x, int y, int z, const StepParams& P, const SmokeSimulationScalarBoundaryFaceDesc* bc, const int* per) {
+    int c[3] = {x, y, z};
+    const int n[3] = {P.nx, P.ny, P.nz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (c[a] < 0 || c[a] >= n[a]) {
+            const SmokeSimulationScalarBoundaryFaceDesc face = bc[2 * a + (c[a] < 0 ? 0 : 1)];
+            if (per[a]) c[a] = wrapi(c[a], n[a]);
+            else if (face.type == kScalarZeroFlux) c[a] = c[a] < 0 ? 0 : n[a] - 1;
+            else return face.value;
+        }
+    }
+    return f[cidx(P, c[0], c[1], c[2])];
+}
+
+// ---------------------------------------------------------------------------------------------- samplers
+// Hermite cubic with central slopes, slopes zeroed where they disagree in sign with the secant or the secant
+// is below 1e-6 (backend-cuda.cu:378-392).
+__device__ __forceinline__ float mono_cubic(float p0, float p1, float p2, float p3, float t) {
+    const float delta = p2 - p1;
+    float m1 = 0.5f * (p2 - p0);
+    float m2 = 0.5f * (p3 - p1);
+    if (fabsf(delta) < 1.0e-6f) {
+        m1 = 0.0f;
+        m2 = 0.0f;
+    } else {
+        if (m1 * delta <= 0.0f) m1 = 0.0f;
+        if (m2 * delta <= 0.0f) m2 = 0.0f;
+    }
+    const float t2 = t * t;
+    const float t3 = t2 * t;
+    return (2.0f * t3 - 3.0f * t2 + 1.0f) * p1 + (t3 - 2.0f * t2 + t) * m1 + (-2.0f * t3 + 3.0f * t2) * p2 + (t3 - t2) * m2;
+}
+
+__device__ __forceinline__ float wrap_pos(float p, int n, float h) {
+    const float extent = static_cast<float>(n) * h;
+    p = fmodf(p, extent);
+    if (p < 0.0f) p += extent;
+    return p;
+}
+
+// Field kinds: 0,1,2 = MAC face component of that axis; 3 = density; 4 = temperature.
+template <int KIND>
+struct FieldTraits {
+    static constexpr bool kFace = KIND < 3;
+};
+
+template <int KIND>
+__device__ __forceinline__ float tap(const float* __restrict__ f, int i, int j, int k, const StepParams& P) {
+    if constexpr (KIND < 3) return face_tap_slow<KIND>(f, i, j, k, P);
+    else if constexpr (KIND == 3) return scalar_tap_slow(f, i, j, k, P, P.den, P.dper);
+    else return scalar_tap_slow(f, i, j, k, P, P.tem, P.tper);
+}
+
+template <int KIND>
+__device__ __forceinline__ bool periodic_axis(const StepParams& P, int a) {
+    if constexpr (KIND < 3) return P.fper[a] != 0;
+    else if constexpr (KIND == 3) return P.dper[a] != 0;
+    else return P.tper[a] != 0;
+}
+
+template <int KIND>
+__device__ __forceinline__ uint32_t lin(const StepParams& P, int i, int j, int k) {
+    if constexpr (KIND < 3) return fidx<KIND>(P, i, j, k);
+    else return cidx(P, i, j, k);
+}
+
+// Samples field KIND at world position (x,y,z): periodic wrap of the position, conversion to grid coordinates
+// (cell-centred axes offset by -0.5, backend-cuda.cu:413-415, 505-507), then trilinear (8 taps) or tensor
+// monotone cubic (64 taps). When the tap box is inside the array the taps are plain loads.
+template <int KIND, bool CUBIC>
+__device__ inline float sample(const float* __restrict__ f, float x, float y, float z, const StepParams& P) {
+    if (periodic_axis<KIND>(P, 0)) x = wrap_pos(x, P.nx, P.h);
+    if (periodic_axis<KIND>(P, 1)) y = wrap_pos(y, P.ny, P.h);
+    if (periodic_axis<KIND>(P, 2)) z = wrap_pos(z, P.nz, P.h);
+    const float gx = KIND == 0 ? x / P.h : x / P.h - 0.5f;
+    const float gy = KIND == 1 ? y / P.h : y / P.h - 0.5f;
+    const float gz = KIND == 2 ? z / P.h : z / P.h - 0.5f;
+    const int x0 = static_cast<int>(floorf(gx));
+    const int y0 = static_cast<int>(floorf(gy));
+    const int z0 = static_cast<int>(floorf(gz));
+    const float tx = gx - static_cast<float>(x0);
+    const float ty = gy - static_cast<float>(y0);
+    const float tz = gz - static_cast<float>(z0);
+    const int ex = P.nx + (KIND == 0) - 1, ey = P.ny + (KIND == 1) - 1, ez = P.nz + (KIND == 2) - 1;
+    if constexpr (!CUBIC) {
+        float c[8];
+        // written so that saturated conversions (huge or infinite positions) cannot overflow the test
+        if (x0 >= 0 && x0 < ex && y0 >= 0 && y0 < ey && z0 >= 0 && z0 < ez) {
+            const uint32_t b = lin<KIND>(P, x0, y0, z0);
+            const uint32_t sy = static_cast<uint32_t>(ex + 1);
+            const uint32_t sz = sy * static_cast<uint32_t>(ey + 1);
+            c[0] = __ldg(f + b);
+            c[1] = __ldg(f + b + 1);
+            c[2] = __ldg(f + b + sy);
+            c[3] = __ldg(f + b + sy + 1);
+            c[4] = __ldg(f + b + sz);
+            c[5] = __ldg(f + b + sz + 1);
+            c[6] = __ldg(f + b + sz + sy);
+            c[7] = __ldg(f + b + sz + sy + 1);
+        } else {
+            c[0] = tap<KIND>(f, x0, y0, z0, P);
+            c[1] = tap<KIND>(f, x0 + 1, y0, z0, P);
+            c[2] = tap<KIND>(f, x0, y0 + 1, z0, P);
+            c[3] = tap<KIND>(f, x0 + 1, y0 + 1, z0, P);
+            c[4] = tap<KIND>(f, x0, y0, z0 + 1, P);
+            c[5] = tap<KIND>(f, x0 + 1, y0, z0 + 1, P);
+            c[6] = tap<KIND>(f, x0, y0 + 1, z0 + 1, P);
+            c[7] = tap<KIND>(f, x0 + 1, y0 + 1, z0 + 1, P);
+        }
+        const float c00 = c[0] + (c[1] - c[0]) * tx;
+        const float c10 = c[2] + (c[3] - c[2]) * tx;
+        const float c01 = c[4] + (c[5] - c[4]) * tx;
+        const float c11 = c[6] + (c[7] - c[6]) * tx;
+        const float c0 = c00 + (c10 - c00) * ty;
+        const float c1 = c01 + (c11 - c01) * ty;
+        return c0 + (c1 - c0) * tz;
+    } else {
+        const bool inside = x0 >= 1 && x0 <= ex - 2 && y0 >= 1 && y0 <= ey - 2 && z0 >= 1 && z0 <= ez - 2;
+        const uint32_t sy = static_cast<uint32_t>(ex + 1);
+        const uint32_t sz = sy * static_cast<uint32_t>(ey + 1);
+        float zs[4];
+#pragma unroll
+        for (int dz = 0; dz < 4; ++dz) {
+            float ys[4];
+#pragma unroll
+            for (int dy = 0; dy < 4; ++dy) {
+                float p[4];
+                if (inside) {
+                    const uint32_t b = lin<KIND>(P, x0 - 1, y0 + dy - 1, z0 + dz - 1);
+                    p[0] = __ldg(f + b);
+                    p[1] = __ldg(f + b + 1);
+                    p[2] = __ldg(f + b + 2);
+                    p[3] = __ldg(f + b + 3);
+                } else {
+#pragma unroll
+                    for (int dx = 0; dx < 4; ++dx) p[dx] = tap<KIND>(f, x0 + dx - 1, y0 + dy - 1, z0 + dz - 1, P);
+                }
+                ys[dy] = mono_cubic(p[0], p[1], p[2], p[3], tx);
+            }
+            zs[dz] = mono_cubic(ys[0], ys[1], ys[2], ys[3], ty);
+        }
+        (void)sz;
+        return mono_cubic(zs[0], zs[1], zs[2], zs[3], tz);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------- trace
+// End-point / probe test of the back-trace (backend-cuda.cu:781-812): outside [0, n*h] on a non-periodic
+// axis, or inside a solid cell.
+__device__ __forceinline__ bool blocked(float x, float y, float z, const uint8_t* __restrict__ occ, const StepParams& P) {
+    if (P.fper[0]) x = wrap_pos(x, P.nx, P.h);
+    if (P.fper[1]) y = wrap_pos(y, P.ny, P.h);
+    if (P.fper[2]) z = wrap_pos(z, P.nz, P.h);
+    if (x < 0.0f || x > static_cast<float>(P.nx) * P.h || y < 0.0f || y > static_cast<float>(P.ny) * P.h || z < 0.0f || z > static_cast<float>(P.nz) * P.h) return true;
+    int cx = static_cast<int>(floorf(x / P.h));
+    int cy = static_cast<int>(floorf(y / P.h));
+    int cz = static_cast<int>(floorf(z / P.h));
+    if (cx == P.nx) cx = P.nx - 1;
+    if (cy == P.ny) cy = P.ny - 1;
+    if (cz == P.nz) cz = P.nz - 1;
+    if (cx < 0 || cx >= P.nx || cy < 0 || cy >= P.ny || cz < 0 || cz >= P.nz) return true;
+    return occ[cidx(P, cx, cy, cz)] != 0;
+}
+
+// Midpoint RK2 back-trace through the face velocities (u,v,w), trilinear samples; a blocked end point is
+// pulled back towards the start by 10 bisection steps (backend-cuda.cu:760-838).
+__device__ inline float3 trace_rk2(float sx, float sy, float sz, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const StepParams& P) {
+    const float dt = P.dt;
+    const float a0 = sample<0, false>(u, sx, sy, sz, P);
+    const float b0 = sample<1, false>(v, sx, sy, sz, P);
+    const float c0 = sample<2, false>(w, sx, sy, sz, P);
+    const float mx = sx - 0.5f * dt * a0, my = sy - 0.5f * dt * b0, mz = sz - 0.5f * dt * c0;
+    const float a1 = sample<0, false>(u, mx, my, mz, P);
+    const float b1 = sample<1, false>(v, mx, my, mz, P);
+    const float c1 = sample<2, false>(w, mx, my, mz, P);
+    const float tx = sx - dt * a1, ty = sy - dt * b1, tz = sz - dt * c1;
+    if (!blocked(tx, ty, tz, occ, P)) return make_float3(tx, ty, tz);
+    float lo = 0.0f, hi = 1.0f;
+    for (int it = 0; it < 10; ++it) {
+        const float mid = 0.5f * (lo + hi);
+        if (blocked(sx + (tx - sx) * mid, sy + (ty - sy) * mid, sz + (tz - sz) * mid, occ, P)) hi = mid;
+        else lo = mid;
+    }
+    return make_float3(sx + (tx - sx) * lo, sy + (ty - sy) * lo, sz + (tz - sz) * lo);
+}
+
+// ---------------------------------------------------------------------------------------------- centred velocity
+// Face -> cell average of component C at an in-range cell (backend-cuda.cu:859-868).
+template <int C>
+__device__ __forceinline__ float centred(const float* __restrict__ f, int x, int y, int z, const StepParams& P) {
+    const uint32_t a = fidx<C>(P, x, y, z);
+    const uint32_t step = C == 0 ? 1u : (C == 1 ? static_cast<uint32_t>(P.nx) : static_cast<uint32_t>(P.nx) * P.ny);
+    return 0.5f * (__ldg(f + a) + __ldg(f + a + step));
+}
+
+// Centred component C at any cell index, with the ghost rule of backend-cuda.cu:228-274: across a wall,
+// 2*wall - interior; OUTFLOW and FREE_SLIP-tangential -> interior; periodic wraps.
+template <int C>
+__device__ inline float centred_tap(const float* __restrict__ f, int x, int y, int z, const StepParams& P) {
+    int c[3] = {x, y, z};
+    const int n[3] = {P.nx, P.ny, P.nz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (c[a] < 0 || c[a] >= n[a]) {
+            if (P.fper[a]) {
+                c[a] = wrapi(c[a], n[a]);
+            } else {
+                int q[3];
+#pragma unroll
+                for (int b = 0; b < 3; ++b) q[b] = (b == a) ? (c[a] < 0 ? 0 : n[a] - 1) : clampi(c[b], 0, n[b] - 1);
+                const float interior = centred<C>(f, q[0], q[1], q[2], P);
+                const SmokeSimulationFlowBoundaryFaceDesc face = P.flow[2 * a + (c[a] < 0 ? 0 : 1)];
+                if (face.type == kFlowOutflow) return interior;
+                if (face.type == kFlowFreeSlip && C != a) return interior;
+                return 2.0f * face_comp(face, C) - interior;
+            }
+        }
+    }
+    return centred<C>(f, c[0], c[1], c[2], P);
+}
+
+// Vorticity of the centred velocity at an in-range fluid cell: central differences / h (backend-cuda.cu:885-900).
+__device__ __forceinline__ float4 vorticity_at(const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, int x, int y, int z, const StepParams& P) {
+    const float h = P.h;
+    const float dvz_dy = 0.5f * (centred_tap<2>(w, x, y + 1, z, P) - centred_tap<2>(w, x, y - 1, z, P)) / h;
+    const float dvy_dz = 0.5f * (centred_tap<1>(v, x, y, z + 1, P) - centred_tap<1>(v, x, y, z - 1, P)) / h;
+    const float dvx_dz = 0.5f * (centred_tap<0>(u, x, y, z + 1, P) - centred_tap<0>(u, x, y, z - 1, P)) / h;
+    const float dvz_dx = 0.5f * (centred_tap<2>(w, x + 1, y, z, P) - centred_tap<2>(w, x - 1, y, z, P)) / h;
+    const float dvy_dx = 0.5f * (centred_tap<1>(v, x + 1, y, z, P) - centred_tap<1>(v, x - 1, y, z, P)) / h;
+    const float dvx_dy = 0.5f * (centred_tap<0>(u, x, y + 1, z, P) - centred_tap<0>(u, x, y - 1, z, P)) / h;
+    const float wx = dvz_dy - dvy_dz;
+    const float wy = dvx_dz - dvz_dx;
+    const float wz = dvy_dx - dvx_dy;
+    return make_float4(wx, wy, wz, sqrtf(wx * wx + wy * wy + wz * wz));
+}
+
+// Cell coordinates of linear cell index q.
+__device__ __forceinline__ void cell_xyz(const StepParams& P, uint32_t q, int& x, int& y, int& z) {
+    const uint32_t zz = P.div_slab.div(q);
+    const uint32_t rem = q - zz * static_cast<uint32_t>(P.nx) * P.ny;
+    const uint32_t yy = P.div_nx.div(rem);
+    x = static_cast<int>(rem - yy * P.nx);
+    y = static_cast<int>(yy);
+    z = static_cast<int>(zz);
+}
+
+// Face coordinates of linear face index q of axis A.
+template <int A>
+__device__ __forceinline__ void face_ijk(const StepParams& P, uint32_t q, int& i, int& j, int& k) {
+    const uint32_t sx = fsx<A>(P), sy = fsy<A>(P);
+    const uint32_t row = P.div_fx[A].div(q);
+    const uint32_t kk = P.div_fy[A].div(row);
+    i = static_cast<int>(q - row * sx);
+    j = static_cast<int>(row - kk * sy);
+    k = static_cast<int>(kk);
+}
+
+#endif  // __CUDACC__
+
+}  // namespace smoke_b200

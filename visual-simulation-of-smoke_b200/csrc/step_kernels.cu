@@ -1,0 +1,569 @@
+// Step kernels of the B200 smoke library (everything except the pressure solve, which is in pcg.cu).
+//
+// Reference behaviour: backend-cuda.cu:840-1609 and the step order of :2000-2057. Design differences:
+//  - every face kernel produces the SETTLED face value in one pass: the reference's update kernel, its three
+//    enforce_*_boundaries passes and its periodic sync become one read-only-input kernel writing a separate
+//    output buffer (no in-place races, no D2D copies). A non-periodic domain face copies the settled value of
+//    its interior neighbour for OUTFLOW (backend-cuda.cu:1023-1024), a face touching a solid cell takes the
+//    mean solid velocity (:1036-1063), and face n of a periodic axis equals face 0 (:1170-1189);
+//  - the three face axes run in one launch (block ranges per axis);
+//  - temperature and density share one back-trace per cell;
+//  - the density fill of solid cells is a precomputed (cell, nearest fluid cell) list built when occupancy
+//    changes, instead of a per-step Chebyshev-shell search (:1243-1290).
+#include "launch.h"
+
+namespace smoke_b200 {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned blocks_for(uint64_t count, int threads = kThreads) { return static_cast<unsigned>((count + threads - 1) / threads); }
+
+// Flow-resolved cell lookup: wraps periodic axes, false when outside a non-periodic domain (:146-151).
+__device__ __forceinline__ bool resolve_flow(const StepParams& P, int& x, int& y, int& z) {
+    if (P.fper[0]) x = wrapi(x, P.nx);
+    if (P.fper[1]) y = wrapi(y, P.ny);
+    if (P.fper[2]) z = wrapi(z, P.nz);
+    return x >= 0 && x < P.nx && y >= 0 && y < P.ny && z >= 0 && z < P.nz;
+}
+
+// Mean solid velocity of the solid cells on either side of face (i,j,k) of axis A, if any (:1036-1063).
+template <int A>
+__device__ __forceinline__ bool solid_face(const StepParams& P, int i, int j, int k, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float& out) {
+    int l[3] = {i, j, k};
+    int r[3] = {i, j, k};
+    l[A] -= 1;
+    const bool hl = resolve_flow(P, l[0], l[1], l[2]);
+    const bool hr = resolve_flow(P, r[0], r[1], r[2]);
+    const uint32_t li = hl ? cidx(P, l[0], l[1], l[2]) : 0u;
+    const uint32_t ri = hr ? cidx(P, r[0], r[1], r[2]) : 0u;
+    const bool ol = hl && occ[li] != 0;
+    const bool orr = hr && occ[ri] != 0;
+    if (!ol && !orr) return false;
+    float value = 0.0f, weight = 0.0f;
+    if (ol) {
+        value += solid[li];
+        weight += 1.0f;
+    }
+    if (orr) {
+        value += solid[ri];
+        weight += 1.0f;
+    }
+    out = value / weight;
+    return true;
+}
+
+// Settled value of face (i,j,k) of axis A: domain-face rule, periodic duplicate, solid rule, else the
+// stage's own interior value `inner(i,j,k)`.
+template <int A, class Inner>
+__device__ __forceinline__ float settle(const StepParams& P, int i, int j, int k, const uint8_t* __restrict__ occ, const float* __restrict__ solid, Inner&& inner) {
+    int c[3] = {i, j, k};
+    const int n = axis_n(P, A);
+    const SmokeSimulationFlowBoundaryFaceDesc lo = P.flow[2 * A], hi = P.flow[2 * A + 1];
+    if (!P.fper[A]) {
+        if (c[A] == 0) {
+            if (!(lo.type == kFlowOutflow && n > 0)) return face_comp(lo, A);
+            c[A] = 1;
+        } else if (c[A] == n) {
+            if (hi.type != kFlowOutflow) return face_comp(hi, A);
+            c[A] = n - 1;
+        }
+    } else if (c[A] == n) {
+        c[A] = 0;
+    }
+    // an index that is itself a domain face (possible only when n == 1) takes no solid rule
+    const bool domain_index = !P.fper[A] && (c[A] == 0 || c[A] == n);
+    float v;
+    if (!domain_index && solid_face<A>(P, c[0], c[1], c[2], occ, solid, v)) return v;
+    return inner(c[0], c[1], c[2]);
+}
+
+template <int A>
+__device__ __forceinline__ const float* pick(const float* a, const float* b, const float* c) {
+    return A == 0 ? a : (A == 1 ? b : c);
+}
+template <int A>
+__device__ __forceinline__ float* pick(float* a, float* b, float* c) {
+    return A == 0 ? a : (A == 1 ? b : c);
+}
+
+// ------------------------------------------------------------------------------------------ forces
+__global__ void __launch_bounds__(kThreads) vorticity_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, float* __restrict__ wx, float* __restrict__ wy, float* __restrict__ wz, float* __restrict__ wm) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n) return;
+    int x, y, z;
+    cell_xyz(P, q, x, y, z);
+    if (occ[q] != 0) {
+        wx[q] = wy[q] = wz[q] = wm[q] = 0.0f;
+        return;
+    }
+    const float4 o = vorticity_at(u, v, w, x, y, z, P);
+    wx[q] = o.x;
+    wy[q] = o.y;
+    wz[q] = o.z;
+    wm[q] = o.w;
+}
+
+// |w| lookup with clamp (or wrap on periodic axes), no occupancy test (load_flow_cell, :202-226).
+__device__ __forceinline__ float flow_cell(const float* __restrict__ f, int x, int y, int z, const StepParams& P) {
+    if (x < 0 || x >= P.nx) x = P.fper[0] ? wrapi(x, P.nx) : (x < 0 ? 0 : P.nx - 1);
+    if (y < 0 || y >= P.ny) y = P.fper[1] ? wrapi(y, P.ny) : (y < 0 ? 0 : P.ny - 1);
+    if (z < 0 || z >= P.nz) z = P.fper[2] ? wrapi(z, P.nz) : (z < 0 ? 0 : P.nz - 1);
+    return __ldg(f + cidx(P, x, y, z));
+}
+
+// f = user force; fluid cells add buoyancy (:910-918) and confinement eps*h*(N x w) (:920-948).
+__global__ void __launch_bounds__(kThreads) cell_force_kernel(const __grid_constant__ StepParams P, const float* __restrict__ wx, const float* __restrict__ wy, const float* __restrict__ wz, const float* __restrict__ wm, const float* __restrict__ density, const float* __restrict__ temperature, const float* __restrict__ ufx,
+                                                               const float* __restrict__ ufy, const float* __restrict__ ufz, const uint8_t* __restrict__ occ, float* __restrict__ fx, float* __restrict__ fy, float* __restrict__ fz) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n) return;
+    float ax = ufx[q], ay = ufy[q], az = ufz[q];
+    if (occ[q] == 0) {
+        int x, y, z;
+        cell_xyz(P, q, x, y, z);
+        ay += -P.alpha * density[q] + P.beta * (temperature[q] - P.ambient);
+        const float h = P.h;
+        const float gx = 0.5f * (flow_cell(wm, x + 1, y, z, P) - flow_cell(wm, x - 1, y, z, P)) / h;
+        const float gy = 0.5f * (flow_cell(wm, x, y + 1, z, P) - flow_cell(wm, x, y - 1, z, P)) / h;
+        const float gz = 0.5f * (flow_cell(wm, x, y, z + 1, P) - flow_cell(wm, x, y, z - 1, P)) / h;
+        const float gmag = sqrtf(gx * gx + gy * gy + gz * gz);
+        if (!(gmag < 1.0e-6f)) {
+            const float inv = 1.0f / gmag;
+            const float nxv = gx * inv, nyv = gy * inv, nzv = gz * inv;
+            const float ox = wx[q], oy = wy[q], oz = wz[q];
+            ax += P.epsilon * h * (nyv * oz - nzv * oy);
+            ay += P.epsilon * h * (nzv * ox - nxv * oz);
+            az += P.epsilon * h * (nxv * oy - nyv * ox);
+        }
+    }
+    fx[q] = ax;
+    fy[q] = ay;
+    fz[q] = az;
+}
+
+template <int A>
+__device__ __forceinline__ void face_force_one(const StepParams& P, uint32_t q, const float* __restrict__ in, const float* __restrict__ f, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
+    int i, j, k;
+    face_ijk<A>(P, q, i, j, k);
+    const int n = axis_n(P, A);
+    out[q] = settle<A>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
+        const int s = A == 0 ? a : (A == 1 ? b : c);
+        float sum = 0.0f, weight = 0.0f;
+        int lc[3] = {a, b, c};
+        if (s > 0) {
+            lc[A] = s - 1;
+            sum += f[cidx(P, lc[0], lc[1], lc[2])];
+            weight += 1.0f;
+        }
+        if (s < n) {
+            lc[A] = s;
+            sum += f[cidx(P, lc[0], lc[1], lc[2])];
+            weight += 1.0f;
+        }
+        const float base = in[fidx<A>(P, a, b, c)];
+        return weight > 0.0f ? base + P.dt * (sum / weight) : base;
+    });
+}
+
+// Block ranges: [0, bu) -> x faces, [bu, bu+bv) -> y faces, rest -> z faces.
+__global__ void __launch_bounds__(kThreads) face_force_kernel(const __grid_constant__ StepParams P, const float* __restrict__ iu, const float* __restrict__ iv, const float* __restrict__ iw, const float* __restrict__ fx, const float* __restrict__ fy, const float* __restrict__ fz, const uint8_t* __restrict__ occ, const float* __restrict__ su,
+                                                               const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou, float* __restrict__ ov, float* __restrict__ ow, unsigned bu, unsigned bv) {
+    const unsigned b = blockIdx.x;
+    if (b < bu) {
+        const uint32_t q = b * kThreads + threadIdx.x;
+        if (q < P.nu) face_force_one<0>(P, q, iu, fx, occ, su, ou);
+    } else if (b < bu + bv) {
+        const uint32_t q = (b - bu) * kThreads + threadIdx.x;
+        if (q < P.nv) face_force_one<1>(P, q, iv, fy, occ, sv, ov);
+    } else {
+        const uint32_t q = (b - bu - bv) * kThreads + threadIdx.x;
+        if (q < P.nw) face_force_one<2>(P, q, iw, fz, occ, sw, ow);
+    }
+}
+
+// ------------------------------------------------------------------------------------------ velocity advection
+template <int A>
+__device__ __forceinline__ void advect_face_one(const StepParams& P, uint32_t q, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
+    int i, j, k;
+    face_ijk<A>(P, q, i, j, k);
+    const float* src = pick<A>(u, v, w);
+    out[q] = settle<A>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
+        const float h = P.h;
+        const float px = A == 0 ? static_cast<float>(a) * h : (static_cast<float>(a) + 0.5f) * h;
+        const float py = A == 1 ? static_cast<float>(b) * h : (static_cast<float>(b) + 0.5f) * h;
+        const float pz = A == 2 ? static_cast<float>(c) * h : (static_cast<float>(c) + 0.5f) * h;
+        const float3 p = trace_rk2(px, py, pz, u, v, w, occ, P);
+        return P.cubic ? sample<A, true>(src, p.x, p.y, p.z, P) : sample<A, false>(src, p.x, p.y, p.z, P);
+    });
+}
+
+__global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou,
+                                                                    float* __restrict__ ov, float* __restrict__ ow, unsigned bu, unsigned bv) {
+    const unsigned b = blockIdx.x;
+    if (b < bu) {
+        const uint32_t q = b * kThreads + threadIdx.x;
+        if (q < P.nu) advect_face_one<0>(P, q, u, v, w, occ, su, ou);
+    } else if (b < bu + bv) {
+        const uint32_t q = (b - bu) * kThreads + threadIdx.x;
+        if (q < P.nv) advect_face_one<1>(P, q, u, v, w, occ, sv, ov);
+    } else {
+        const uint32_t q = (b - bu - bv) * kThreads + threadIdx.x;
+        if (q < P.nw) advect_face_one<2>(P, q, u, v, w, occ, sw, ow);
+    }
+}
+
+// ------------------------------------------------------------------------------------------ pressure rhs
+// b = -(h^2/dt) div u* + sum of OUTFLOW face pressures; 0 at solid cells and at the anchor (:1304-1328).
+__global__ void __launch_bounds__(kThreads) rhs_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const int32_t* __restrict__ anchor, float* __restrict__ rhs) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n) return;
+    if (static_cast<int32_t>(q) == *anchor || occ[q] != 0) {
+        rhs[q] = 0.0f;
+        return;
+    }
+    int x, y, z;
+    cell_xyz(P, q, x, y, z);
+    const float h = P.h;
+    const float div = (u[fidx<0>(P, x + 1, y, z)] - u[fidx<0>(P, x, y, z)] + v[fidx<1>(P, x, y + 1, z)] - v[fidx<1>(P, x, y, z)] + w[fidx<2>(P, x, y, z + 1)] - w[fidx<2>(P, x, y, z)]) / h;
+    float bsum = 0.0f;
+    if (x == 0 && P.flow[0].type == kFlowOutflow) bsum += P.flow[0].pressure;
+    if (x == P.nx - 1 && P.flow[1].type == kFlowOutflow) bsum += P.flow[1].pressure;
+    if (y == 0 && P.flow[2].type == kFlowOutflow) bsum += P.flow[2].pressure;
+    if (y == P.ny - 1 && P.flow[3].type == kFlowOutflow) bsum += P.flow[3].pressure;
+    if (z == 0 && P.flow[4].type == kFlowOutflow) bsum += P.flow[4].pressure;
+    if (z == P.nz - 1 && P.flow[5].type == kFlowOutflow) bsum += P.flow[5].pressure;
+    rhs[q] = -(h * h / P.dt) * div + bsum;
+}
+
+// ------------------------------------------------------------------------------------------ projection
+template <int A>
+__device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, const float* __restrict__ in, const float* __restrict__ p, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
+    int i, j, k;
+    face_ijk<A>(P, q, i, j, k);
+    out[q] = settle<A>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
+        int l[3] = {a, b, c};
+        int r[3] = {a, b, c};
+        l[A] -= 1;
+        const bool hl = resolve_flow(P, l[0], l[1], l[2]);
+        const bool hr = resolve_flow(P, r[0], r[1], r[2]);
+        const float base = in[fidx<A>(P, a, b, c)];
+        if (!(hl && hr)) return base;
+        const float pr = p[cidx(P, r[0], r[1], r[2])];
+        const float pl = p[cidx(P, l[0], l[1], l[2])];
+        return base - P.dt * (pr - pl) / P.h;
+    });
+}
+
+__global__ void __launch_bounds__(kThreads) project_kernel(const __grid_constant__ StepParams P, const float* __restrict__ iu, const float* __restrict__ iv, const float* __restrict__ iw, const float* __restrict__ p, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou,
+                                                            float* __restrict__ ov, float* __restrict__ ow, unsigned bu, unsigned bv) {
+    const unsigned b = blockIdx.x;
+    if (b < bu) {
+        const uint32_t q = b * kThreads + threadIdx.x;
+        if (q < P.nu) project_one<0>(P, q, iu, p, occ, su, ou);
+    } else if (b < bu + bv) {
+        const uint32_t q = (b - bu) * kThreads + threadIdx.x;
+        if (q < P.nv) project_one<1>(P, q, iv, p, occ, sv, ov);
+    } else {
+        const uint32_t q = (b - bu - bv) * kThreads + threadIdx.x;
+        if (q < P.nw) project_one<2>(P, q, iw, p, occ, sw, ow);
+    }
+}
+
+// ------------------------------------------------------------------------------------------ scalars
+// t_tmp = T' + dt*src_T where T' is T with solid cells set to the solid temperature (the step-start
+// apply_solid_temperature of :2001 folded in); d_tmp = rho + dt*src_rho (add_source, :852-857).
+__global__ void __launch_bounds__(kThreads) scalar_prep_kernel(const __grid_constant__ StepParams P, const float* __restrict__ t, const float* __restrict__ ts, const float* __restrict__ d, const float* __restrict__ ds, const uint8_t* __restrict__ occ, const float* __restrict__ solid_t, float* __restrict__ t_tmp,
+                                                                float* __restrict__ d_tmp) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n) return;
+    const float tv = occ[q] != 0 ? solid_t[q] : t[q];
+    t_tmp[q] = tv + P.dt * ts[q];
+    d_tmp[q] = d[q] + P.dt * ds[q];
+}
+
+// Fluid cells: one back-trace, then both scalars sampled with their own boundary rules (:1221-1233).
+// Solid cells: temperature = solid temperature (:1235-1241), density = 0 until the fill pass.
+template <bool CUBIC>
+__global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const float* __restrict__ t_tmp, const float* __restrict__ d_tmp, const float* __restrict__ solid_t, float* __restrict__ t,
+                                                                   float* __restrict__ d) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n) return;
+    if (occ[q] != 0) {
+        t[q] = solid_t[q];
+        d[q] = 0.0f;
+        return;
+    }
+    int x, y, z;
+    cell_xyz(P, q, x, y, z);
+    const float h = P.h;
+    const float3 p = trace_rk2((static_cast<float>(x) + 0.5f) * h, (static_cast<float>(y) + 0.5f) * h, (static_cast<float>(z) + 0.5f) * h, u, v, w, occ, P);
+    t[q] = sample<4, CUBIC>(t_tmp, p.x, p.y, p.z, P);
+    d[q] = sample<3, CUBIC>(d_tmp, p.x, p.y, p.z, P);
+}
+
+__global__ void density_fill_kernel(const FillEntry* __restrict__ list, const uint32_t* __restrict__ count, float* __restrict__ d) {
+    const uint32_t n = *count;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const FillEntry e = list[t];
+        d[e.cell] = e.source >= 0 ? d[e.source] : 0.0f;
+    }
+}
+
+// ------------------------------------------------------------------------------------------ views
+__global__ void __launch_bounds__(kThreads) views_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, float* __restrict__ cx, float* __restrict__ cy, float* __restrict__ cz, float* __restrict__ vm, float* __restrict__ wx, float* __restrict__ wy,
+                                                          float* __restrict__ wz, float* __restrict__ wm, float* __restrict__ div) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n) return;
+    int x, y, z;
+    cell_xyz(P, q, x, y, z);
+    const float a = centred<0>(u, x, y, z, P);
+    const float b = centred<1>(v, x, y, z, P);
+    const float c = centred<2>(w, x, y, z, P);
+    cx[q] = a;
+    cy[q] = b;
+    cz[q] = c;
+    vm[q] = sqrtf(a * a + b * b + c * c);
+    if (occ[q] != 0) {
+        wx[q] = wy[q] = wz[q] = wm[q] = 0.0f;
+        div[q] = 0.0f;
+        return;
+    }
+    const float4 o = vorticity_at(u, v, w, x, y, z, P);
+    wx[q] = o.x;
+    wy[q] = o.y;
+    wz[q] = o.z;
+    wm[q] = o.w;
+    div[q] = (u[fidx<0>(P, x + 1, y, z)] - u[fidx<0>(P, x, y, z)] + v[fidx<1>(P, x, y + 1, z)] - v[fidx<1>(P, x, y, z)] + w[fidx<2>(P, x, y, z + 1)] - w[fidx<2>(P, x, y, z)]) / P.h;
+}
+
+// ------------------------------------------------------------------------------------------ occupancy-derived
+__global__ void occupancy_float_kernel(uint32_t n, const uint8_t* __restrict__ occ, float* __restrict__ out) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) out[q] = static_cast<float>(occ[q]);
+}
+
+__global__ void set_int_kernel(int32_t* p, int32_t v) { *p = v; }
+
+// anchor = smallest fluid cell index (:1292-1302); warp minimum first, one atomic per warp.
+__global__ void anchor_kernel(uint32_t n, const uint8_t* __restrict__ occ, int32_t* anchor) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t v = (q < n && occ[q] == 0) ? static_cast<int32_t>(q) : 0x7fffffff;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0 && v != 0x7fffffff) atomicMin(anchor, v);
+}
+
+// Row code of the Poisson operator (:1343-1412): solid or anchor rows are identity (diag 1, no neighbours);
+// a fluid row's diagonal counts fluid neighbours (anchor included, periodic wrap, repeats counted) plus OUTFLOW
+// domain faces, at least 1; neighbour bits mark distinct fluid non-anchor neighbours other than the cell itself.
+__global__ void __launch_bounds__(kThreads) stencil_code_kernel(const __grid_constant__ StepParams P, const uint8_t* __restrict__ occ, const int32_t* __restrict__ anchor_ptr, uint16_t* __restrict__ codes) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n) return;
+    const int32_t anchor = *anchor_ptr;
+    if (occ[q] != 0 || static_cast<int32_t>(q) == anchor) {
+        codes[q] = static_cast<uint16_t>(1u << 8);
+        return;
+    }
+    int c[3];
+    cell_xyz(P, q, c[0], c[1], c[2]);
+    const int n[3] = {P.nx, P.ny, P.nz};
+    uint32_t diag = 0, mask = 0;
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+        const int a = e >> 1;
+        int d[3] = {c[0], c[1], c[2]};
+        d[a] += (e & 1) ? 1 : -1;
+        if (d[a] < 0 || d[a] >= n[a]) {
+            if (!P.fper[a]) {
+                if (P.flow[e].type == kFlowOutflow) ++diag;
+                continue;
+            }
+            d[a] = wrapi(d[a], n[a]);
+        }
+        const uint32_t nb = cidx(P, d[0], d[1], d[2]);
+        if (occ[nb] != 0) continue;
+        ++diag;
+        if (static_cast<int32_t>(nb) == anchor || nb == q) continue;
+        if ((e & 1) && n[a] == 2 && P.fper[a]) continue;  // same cell as the -a neighbour, kept once
+        mask |= 1u << e;
+    }
+    if (diag == 0) diag = 1;
+    codes[q] = static_cast<uint16_t>(mask | (diag << 8));
+}
+
+// Nearest-fluid source of each solid cell (:1243-1290): first Chebyshev shell (radius 1, 2, ...) holding a fluid
+// cell, smallest squared distance in it, first in (dz, dy, dx) scan order on ties, density periodicity. Only the
+// shell surface is enumerated, in the same order as a full-cube scan.
+__global__ void __launch_bounds__(kThreads) fill_build_kernel(const __grid_constant__ StepParams P, const uint8_t* __restrict__ occ, const int32_t* __restrict__ anchor_ptr, FillEntry* __restrict__ list, uint32_t* __restrict__ count) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.n || occ[q] == 0) return;
+    int32_t best = -1;
+    if (*anchor_ptr < static_cast<int32_t>(P.n)) {  // at least one fluid cell exists
+        int x, y, z;
+        cell_xyz(P, q, x, y, z);
+        const int max_radius = imax(P.nx, imax(P.ny, P.nz));
+        for (int r = 1; r <= max_radius && best < 0; ++r) {
+            int best_d2 = 0x7fffffff;
+            for (int dz = -r; dz <= r; ++dz) {
+                for (int dy = -r; dy <= r; ++dy) {
+                    const bool full_row = (dz == -r || dz == r || dy == -r || dy == r);
+                    const int step = full_row ? 1 : 2 * r;
+                    for (int dx = -r; dx <= r; dx += step) {
+                        int c[3] = {x + dx, y + dy, z + dz};
+                        const int nn[3] = {P.nx, P.ny, P.nz};
+                        bool ok = true;
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            if (P.dper[a]) c[a] = wrapi(c[a], nn[a]);
+                            ok = ok && c[a] >= 0 && c[a] < nn[a];
+                        }
+                        if (!ok) continue;
+                        const uint32_t nb = cidx(P, c[0], c[1], c[2]);
+                        if (occ[nb] != 0) continue;
+                        const int d2 = dx * dx + dy * dy + dz * dz;
+                        if (d2 < best_d2) {
+                            best_d2 = d2;
+                            best = static_cast<int32_t>(nb);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    const uint32_t slot = atomicAdd(count, 1u);
+    list[slot] = FillEntry{q, best};
+}
+
+__global__ void fill_value_kernel(float* __restrict__ dst, float value, uint64_t count) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < count; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) dst[i] = value;
+}
+
+}  // namespace
+
+StepParams make_params(const SmokeSimulationConfig& cfg) {
+    StepParams P{};
+    P.nx = cfg.nx;
+    P.ny = cfg.ny;
+    P.nz = cfg.nz;
+    P.h = cfg.cell_size;
+    P.dt = cfg.dt;
+    P.ambient = cfg.ambient_temperature;
+    P.alpha = cfg.buoyancy_density_factor;
+    P.beta = cfg.buoyancy_temperature_factor;
+    P.epsilon = cfg.vorticity_confinement;
+    P.cubic = cfg.scalar_advection_mode == SMOKE_SIMULATION_SCALAR_ADVECTION_MONOTONIC_CUBIC;
+    const SmokeSimulationFlowBoundaryFaceDesc* fb = &cfg.flow_boundary.x_minus;
+    const SmokeSimulationScalarBoundaryFaceDesc* db = &cfg.density_boundary.x_minus;
+    const SmokeSimulationScalarBoundaryFaceDesc* tb = &cfg.temperature_boundary.x_minus;
+    for (int e = 0; e < 6; ++e) {
+        P.flow[e] = fb[e];
+        P.den[e] = db[e];
+        P.tem[e] = tb[e];
+    }
+    for (int a = 0; a < 3; ++a) {
+        P.fper[a] = fb[2 * a].type == kFlowPeriodic && fb[2 * a + 1].type == kFlowPeriodic;
+        P.dper[a] = db[2 * a].type == kScalarPeriodic && db[2 * a + 1].type == kScalarPeriodic;
+        P.tper[a] = tb[2 * a].type == kScalarPeriodic && tb[2 * a + 1].type == kScalarPeriodic;
+    }
+    const uint32_t nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
+    P.n = nx * ny * nz;
+    P.nu = (nx + 1) * ny * nz;
+    P.nv = nx * (ny + 1) * nz;
+    P.nw = nx * ny * (nz + 1);
+    P.div_nx = FastDiv(nx);
+    P.div_ny = FastDiv(ny);
+    P.div_slab = FastDiv(nx * ny);
+    for (int a = 0; a < 3; ++a) {
+        P.div_fx[a] = FastDiv(nx + (a == 0));
+        P.div_fy[a] = FastDiv(ny + (a == 1));
+    }
+    return P;
+}
+
+cudaError_t launch_vorticity(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* wx, float* wy, float* wz, float* wmag, cudaStream_t s) {
+    vorticity_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, vel.u, vel.v, vel.w, occ, wx, wy, wz, wmag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_force(const StepParams& P, const float* wx, const float* wy, const float* wz, const float* wmag, const float* density, const float* temperature, const float* ufx, const float* ufy, const float* ufz, const uint8_t* occ, float* fx, float* fy, float* fz, cudaStream_t s) {
+    cell_force_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, wx, wy, wz, wmag, density, temperature, ufx, ufy, ufz, occ, fx, fy, fz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* fx, const float* fy, const float* fz, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
+    const unsigned bu = blocks_for(P.nu), bv = blocks_for(P.nv), bw = blocks_for(P.nw);
+    face_force_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, fx, fy, fz, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
+    const unsigned bu = blocks_for(P.nu), bv = blocks_for(P.nv), bw = blocks_for(P.nw);
+    advect_velocity_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rhs(const StepParams& P, ConstFaces vel, const uint8_t* occ, const int32_t* anchor, float* rhs, cudaStream_t s) {
+    rhs_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, vel.u, vel.v, vel.w, occ, anchor, rhs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
+    const unsigned bu = blocks_for(P.nu), bv = blocks_for(P.nv), bw = blocks_for(P.nw);
+    project_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, pressure, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scalar_prep(const StepParams& P, const float* temperature, const float* temperature_source, const float* density, const float* density_source, const uint8_t* occ, const float* solid_temperature, float* t_tmp, float* d_tmp, cudaStream_t s) {
+    scalar_prep_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, temperature, temperature_source, density, density_source, occ, solid_temperature, t_tmp, d_tmp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, const uint8_t* occ, const float* t_tmp, const float* d_tmp, const float* solid_temperature, float* temperature, float* density, cudaStream_t s) {
+    if (P.cubic) advect_scalars_kernel<true><<<blocks_for(P.n), kThreads, 0, s>>>(P, vel.u, vel.v, vel.w, occ, t_tmp, d_tmp, solid_temperature, temperature, density);
+    else advect_scalars_kernel<false><<<blocks_for(P.n), kThreads, 0, s>>>(P, vel.u, vel.v, vel.w, occ, t_tmp, d_tmp, solid_temperature, temperature, density);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_density_fill(const FillEntry* list, const uint32_t* count, float* density, int max_blocks, cudaStream_t s) {
+    density_fill_kernel<<<max_blocks, kThreads, 0, s>>>(list, count, density);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_views(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* cx, float* cy, float* cz, float* vmag, float* wx, float* wy, float* wz, float* wmag, float* div, cudaStream_t s) {
+    views_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, vel.u, vel.v, vel.w, occ, cx, cy, cz, vmag, wx, wy, wz, wmag, div);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_occupancy_float(const StepParams& P, const uint8_t* occ, float* out, cudaStream_t s) {
+    occupancy_float_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P.n, occ, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_anchor(const StepParams& P, const uint8_t* occ, int32_t* anchor, cudaStream_t s) {
+    set_int_kernel<<<1, 1, 0, s>>>(anchor, static_cast<int32_t>(P.n));
+    anchor_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P.n, occ, anchor);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stencil_codes(const StepParams& P, const uint8_t* occ, const int32_t* anchor, uint16_t* codes, cudaStream_t s) {
+    stencil_code_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, occ, anchor, codes);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_build(const StepParams& P, const uint8_t* occ, const int32_t* anchor, FillEntry* list, uint32_t* count, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    fill_build_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, occ, anchor, list, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_value(float* dst, float value, uint64_t count, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    const uint64_t want = (count + kThreads - 1) / kThreads;
+    const unsigned grid = static_cast<unsigned>(want < 4096 ? want : 4096);
+    fill_value_kernel<<<grid, kThreads, 0, s>>>(dst, value, count);
+    return cudaGetLastError();
+}
+
+}  // namespace smoke_b200
