@@ -458,12 +458,17 @@ static real solid_velocity_value(const real* sv, const uint8_t* occ, int x, int 
 
 /* enforce_velocity_{x,y,z}_boundaries_kernel :1014-1168 and sync_periodic_velocity_* :1170-1189, for the
  * face component normal to `axis`. Interior faces touching a solid cell take the mean solid velocity of the
- * solid neighbours; then non-periodic domain faces take the prescribed normal velocity, or for OUTFLOW the
- * (settled) value of the adjacent interior face; then on periodic axes face n copies face 0. */
+ * solid neighbours; non-periodic domain faces take the prescribed normal velocity, or for OUTFLOW the value the
+ * adjacent interior face had when the kernel started (:1023-1024, :1030-1031: in the reference the copy and the
+ * neighbour's solid rule run in the same kernel, and on B200 the copying thread reads first); then on periodic
+ * axes face n copies face 0. */
 static void enforce(const Ctx* c, real* f, int axis, const uint8_t* occ, const real* solid_v) {
     const Grid* g = &c->g;
     const int nx = g->nx, ny = g->ny, nz = g->nz;
     const int sx = nx + (axis == 0), sy = ny + (axis == 1), sz = nz + (axis == 2);
+    const size_t total = (size_t)sx * sy * sz;
+    real* before = (real*)malloc(total * sizeof(real));
+    memcpy(before, f, total * sizeof(real));
     const int n_axis = axis == 0 ? nx : (axis == 1 ? ny : nz);
     const FlowFace lo = axis == 0 ? g->fb.x_minus : (axis == 1 ? g->fb.y_minus : g->fb.z_minus);
     const FlowFace hi = axis == 0 ? g->fb.x_plus : (axis == 1 ? g->fb.y_plus : g->fb.z_plus);
@@ -493,7 +498,7 @@ static void enforce(const Ctx* c, real* f, int axis, const uint8_t* occ, const r
                 }
                 f[((size_t)k * sy + j) * sx + i] = weight > K(0.0) ? value / weight : K(0.0);
             }
-    /* domain faces, read from the settled interior neighbour (both ends read before either is written) */
+    /* domain faces: OUTFLOW copies the adjacent face's value from before this pass */
 #pragma omp parallel for schedule(static)
     for (int k = 0; k < sz; ++k)
         for (int j = 0; j < sy; ++j)
@@ -504,12 +509,13 @@ static void enforce(const Ctx* c, real* f, int axis, const uint8_t* occ, const r
                 const size_t base = ((size_t)k * sy + j) * sx + i;
                 const size_t first = base, last = base + (size_t)n_axis * stride;
                 real v_lo = f[first], v_hi = f[last];
-                if (lo.type != FLOW_PERIODIC) v_lo = (lo.type == FLOW_OUTFLOW && n_axis > 0) ? f[first + stride] : face_component(lo, axis);
-                if (hi.type != FLOW_PERIODIC) v_hi = (hi.type == FLOW_OUTFLOW && n_axis > 0) ? f[last - stride] : face_component(hi, axis);
+                if (lo.type != FLOW_PERIODIC) v_lo = (lo.type == FLOW_OUTFLOW && n_axis > 0) ? before[first + stride] : face_component(lo, axis);
+                if (hi.type != FLOW_PERIODIC) v_hi = (hi.type == FLOW_OUTFLOW && n_axis > 0) ? before[last - stride] : face_component(hi, axis);
                 f[first] = v_lo;
                 f[last] = v_hi;
                 if (periodic) f[last] = f[first];
             }
+    free(before);
 }
 
 /* Forces, backend-cuda.cu:2001-2018 (apply_solid_temperature, centre velocity, vorticity, seed_force,

@@ -56,18 +56,25 @@ __device__ __forceinline__ bool solid_face(const StepParams& P, int i, int j, in
 
 // Settled value of face (i,j,k) of axis A: domain-face rule, periodic duplicate, solid rule, else the
 // stage's own interior value `inner(i,j,k)`.
-template <int A, class Inner>
+// An OUTFLOW domain face copies its interior neighbour. In the reference that copy and the neighbour's solid rule
+// run in the same enforce kernel and the copy reads first (observed on B200, :1023-1024 vs :1036-1063), so after
+// the force and advection stages the copy does NOT see the neighbour's solid rule. The projection kernel applies
+// the solid rule itself before its enforce pass (:1465-1475), so there the copy does see it: OUTFLOW_SEES_SOLID.
+template <int A, bool OUTFLOW_SEES_SOLID, class Inner>
 __device__ __forceinline__ float settle(const StepParams& P, int i, int j, int k, const uint8_t* __restrict__ occ, const float* __restrict__ solid, Inner&& inner) {
     int c[3] = {i, j, k};
     const int n = axis_n(P, A);
     const SmokeSimulationFlowBoundaryFaceDesc lo = P.flow[2 * A], hi = P.flow[2 * A + 1];
+    bool outflow_copy = false;
     if (!P.fper[A]) {
         if (c[A] == 0) {
             if (!(lo.type == kFlowOutflow && n > 0)) return face_comp(lo, A);
             c[A] = 1;
+            outflow_copy = true;
         } else if (c[A] == n) {
             if (hi.type != kFlowOutflow) return face_comp(hi, A);
             c[A] = n - 1;
+            outflow_copy = true;
         }
     } else if (c[A] == n) {
         c[A] = 0;
@@ -75,7 +82,7 @@ __device__ __forceinline__ float settle(const StepParams& P, int i, int j, int k
     // an index that is itself a domain face (possible only when n == 1) takes no solid rule
     const bool domain_index = !P.fper[A] && (c[A] == 0 || c[A] == n);
     float v;
-    if (!domain_index && solid_face<A>(P, c[0], c[1], c[2], occ, solid, v)) return v;
+    if ((OUTFLOW_SEES_SOLID || !outflow_copy) && !domain_index && solid_face<A>(P, c[0], c[1], c[2], occ, solid, v)) return v;
     return inner(c[0], c[1], c[2]);
 }
 
@@ -147,7 +154,7 @@ __device__ __forceinline__ void face_force_one(const StepParams& P, uint32_t q, 
     int i, j, k;
     face_ijk<A>(P, q, i, j, k);
     const int n = axis_n(P, A);
-    out[q] = settle<A>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
+    out[q] = settle<A, false>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
         const int s = A == 0 ? a : (A == 1 ? b : c);
         float sum = 0.0f, weight = 0.0f;
         int lc[3] = {a, b, c};
@@ -188,7 +195,7 @@ __device__ __forceinline__ void advect_face_one(const StepParams& P, uint32_t q,
     int i, j, k;
     face_ijk<A>(P, q, i, j, k);
     const float* src = pick<A>(u, v, w);
-    out[q] = settle<A>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
+    out[q] = settle<A, false>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
         const float h = P.h;
         const float px = A == 0 ? static_cast<float>(a) * h : (static_cast<float>(a) + 0.5f) * h;
         const float py = A == 1 ? static_cast<float>(b) * h : (static_cast<float>(b) + 0.5f) * h;
@@ -241,7 +248,7 @@ template <int A>
 __device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, const float* __restrict__ in, const float* __restrict__ p, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
     int i, j, k;
     face_ijk<A>(P, q, i, j, k);
-    out[q] = settle<A>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
+    out[q] = settle<A, true>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
         int l[3] = {a, b, c};
         int r[3] = {a, b, c};
         l[A] -= 1;

@@ -169,15 +169,15 @@ class Simulation:
         import torch
 
         out = {}
-        for kind in kinds if kinds is not None else range(15):
-            v = self.view(kind)
-            name = abi.VIEW_NAMES[kind]
-            if isinstance(v, tuple):
-                for ax, t in zip(abi.AXES, v):
-                    out[f"{name}_{ax}"] = t.clone()
-            else:
-                out[name] = v.clone()
-        torch.cuda.current_stream().synchronize()
+        with torch.cuda.stream(self.stream):  # copies ordered after the library's work on its stream
+            for kind in kinds if kinds is not None else range(15):
+                v = self.view(kind)
+                name = abi.VIEW_NAMES[kind]
+                if isinstance(v, tuple):
+                    for ax, t in zip(abi.AXES, v):
+                        out[f"{name}_{ax}"] = t.clone()
+                else:
+                    out[name] = v.clone()
         self.stream.synchronize()
         return {k: t.cpu().numpy() for k, t in out.items()}
 
@@ -199,6 +199,15 @@ class Simulation:
         _check(self.lib.smoke_b200_get_face_velocity_cuda(self.handle, which, C.byref(pu), C.byref(pv), C.byref(pw)), "get_face_velocity")
         su, sv, sw = abi.face_shapes(self.config)
         return device_view(pu.value, su), device_view(pv.value, sv), device_view(pw.value, sw)
+
+    def face_velocity_host(self, which: int = 0):
+        """Host numpy copies of the face velocities (ordered after the library's work)."""
+        import torch
+
+        with torch.cuda.stream(self.stream):
+            t = [x.clone() for x in self.face_velocity(which)]
+        self.stream.synchronize()
+        return [x.cpu().numpy() for x in t]
 
     def step_stages(self, last_stage: int):
         _check(self.lib.smoke_b200_step_stages_cuda(self.handle, last_stage), "step_stages")
