@@ -147,8 +147,9 @@ struct SmokeSimulationContext_t {
             f32(&f->w, nw);
         }
         for (float** p : {&density, &density_tmp, &density_source, &temperature, &temperature_tmp, &temperature_source, &force_x, &force_y, &force_z, &solid_vx, &solid_vy, &solid_vz, &solid_temperature, &occupancy_float, &pressure, &rhs, &cx, &cy, &cz, &vmag, &wx, &wy, &wz, &wmag,
-                          &divergence, &fx, &fy, &fz, &pcg.r[0], &pcg.r[1], &pcg.s[0], &pcg.s[1], &pcg.w[0], &pcg.w[1], &pcg.p})
+                          &divergence, &fx, &fy, &fz, &pcg.r[0], &pcg.r[1], &pcg.s[0], &pcg.s[1], &pcg.w[0], &pcg.w[1], &pcg.p, &pcg.e})
             f32(p, n);
+        slots.push_back({reinterpret_cast<void**>(&pcg.x64), n * sizeof(double)});
         slots.push_back({reinterpret_cast<void**>(&codes), n * sizeof(uint16_t)});
         slots.push_back({reinterpret_cast<void**>(&occupancy), n});
         slots.push_back({reinterpret_cast<void**>(&fill_list), n * sizeof(FillEntry)});
@@ -200,7 +201,9 @@ struct SmokeSimulationContext_t {
         check(launch_rhs(P, as_const(C), occupancy, anchor, rhs, s), "pressure rhs");
         check(launch_pcg(P, pcg_settings(), pcg_shape, codes, rhs, pressure, pcg, control, s), "pressure solve");
         if (last_stage < SMOKE_B200_STAGE_PROJECT) return;
-        check(launch_project(P, as_const(C), pressure, occupancy, solid, A, s), "project");
+        const PcgSettings S = pcg_settings();
+        const double* p64 = (!S.fixed && S.refinement > 0) ? pcg.x64 : nullptr;
+        check(launch_project(P, as_const(C), pressure, p64, occupancy, solid, A, s), "project");
         if (last_stage < SMOKE_B200_STAGE_SCALARS) return;
         check(launch_scalar_prep(P, temperature, temperature_source, density, density_source, occupancy, solid_temperature, temperature_tmp, density_tmp, s), "scalar sources");
         check(launch_advect_scalars(P, as_const(A), occupancy, temperature_tmp, density_tmp, solid_temperature, temperature, density, s), "advect scalars");

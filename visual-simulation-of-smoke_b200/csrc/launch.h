@@ -40,8 +40,8 @@ cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* f
 cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
 // Pressure right-hand side from the advected velocity.
 cudaError_t launch_rhs(const StepParams& P, ConstFaces vel, const uint8_t* occ, const int32_t* anchor, float* rhs, cudaStream_t s);
-// Projection: out = settled(in - dt * grad p / h).
-cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
+// Projection: out = settled(in - dt * grad p / h); pressure64 (optional) is the FP64 solution of a refined solve.
+cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const double* pressure64, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
 // Scalars: source terms (and solid temperature) into the temporaries.
 cudaError_t launch_scalar_prep(const StepParams& P, const float* temperature, const float* temperature_source, const float* density, const float* density_source, const uint8_t* occ, const float* solid_temperature, float* t_tmp, float* d_tmp, cudaStream_t s);
 // Scalars: one shared back-trace per cell, sample both scalars, solid rules.
@@ -100,6 +100,8 @@ struct PcgWork {
     float* s[2];
     float* w[2];
     float* p;
+    float* e;      // FP32 correction iterate of a refinement pass
+    double* x64;   // FP64 solution accumulator (refinement); kept between steps as the warm start
 };
 
 struct PcgLaunchShape {

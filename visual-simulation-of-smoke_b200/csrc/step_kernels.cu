@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kThreads) rhs_kernel(const __grid_constant__ S
 
 // ------------------------------------------------------------------------------------------ projection
 template <int A>
-__device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, const float* __restrict__ in, const float* __restrict__ p, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
+__device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, const float* __restrict__ in, const float* __restrict__ p, const double* __restrict__ p64, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
     int i, j, k;
     face_ijk<A>(P, q, i, j, k);
     out[q] = settle<A, true>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
@@ -256,24 +256,28 @@ __device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, con
         const bool hr = resolve_flow(P, r[0], r[1], r[2]);
         const float base = in[fidx<A>(P, a, b, c)];
         if (!(hl && hr)) return base;
+        if (p64 != nullptr) {  // FP64 solution of a refined solve: the gradient keeps its precision
+            const double g = static_cast<double>(P.dt) * (p64[cidx(P, r[0], r[1], r[2])] - p64[cidx(P, l[0], l[1], l[2])]) / static_cast<double>(P.h);
+            return base - static_cast<float>(g);
+        }
         const float pr = p[cidx(P, r[0], r[1], r[2])];
         const float pl = p[cidx(P, l[0], l[1], l[2])];
         return base - P.dt * (pr - pl) / P.h;
     });
 }
 
-__global__ void __launch_bounds__(kThreads) project_kernel(const __grid_constant__ StepParams P, const float* __restrict__ iu, const float* __restrict__ iv, const float* __restrict__ iw, const float* __restrict__ p, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou,
+__global__ void __launch_bounds__(kThreads) project_kernel(const __grid_constant__ StepParams P, const float* __restrict__ iu, const float* __restrict__ iv, const float* __restrict__ iw, const float* __restrict__ p, const double* __restrict__ p64, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou,
                                                             float* __restrict__ ov, float* __restrict__ ow, unsigned bu, unsigned bv) {
     const unsigned b = blockIdx.x;
     if (b < bu) {
         const uint32_t q = b * kThreads + threadIdx.x;
-        if (q < P.nu) project_one<0>(P, q, iu, p, occ, su, ou);
+        if (q < P.nu) project_one<0>(P, q, iu, p, p64, occ, su, ou);
     } else if (b < bu + bv) {
         const uint32_t q = (b - bu) * kThreads + threadIdx.x;
-        if (q < P.nv) project_one<1>(P, q, iv, p, occ, sv, ov);
+        if (q < P.nv) project_one<1>(P, q, iv, p, p64, occ, sv, ov);
     } else {
         const uint32_t q = (b - bu - bv) * kThreads + threadIdx.x;
-        if (q < P.nw) project_one<2>(P, q, iw, p, occ, sw, ow);
+        if (q < P.nw) project_one<2>(P, q, iw, p, p64, occ, sw, ow);
     }
 }
 
@@ -515,9 +519,9 @@ cudaError_t launch_rhs(const StepParams& P, ConstFaces vel, const uint8_t* occ, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
+cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const double* pressure64, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
     const unsigned bu = blocks_for(P.nu), bv = blocks_for(P.nv), bw = blocks_for(P.nw);
-    project_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, pressure, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
+    project_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, pressure, pressure64, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
     return cudaGetLastError();
 }
 
