@@ -93,6 +93,38 @@ SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimu
  * kernel launch on the context stream; the outcome is read with smoke_b200_get_solver_status_cuda. */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext context);
 
+/* Pressure solve that allocates nothing. No counterpart in the reference (which has no standalone solve and
+ * allocates all its buffers with cudaMalloc when a context is created).
+ *
+ * For callers that cannot call cudaMalloc while they run: a renderer or engine that reserves its GPU memory up
+ * front and forbids allocations in its frame loop (cudaMalloc can synchronise the device and stall a frame), or
+ * a plug-in that lives inside another application's memory budget. The solver's scratch memory is one device
+ * array inside the library image, so the call allocates no memory, neither directly nor through a library.
+ *
+ * Solves the system of the step's pressure stage for `config`, `occupancy` (nx*ny*nz bytes on the device, nonzero =
+ * solid; NULL = no solids) and the right-hand side `rhs` (nx*ny*nz floats on the device) into `pressure` (device,
+ * nx*ny*nz floats), on `stream`, with `solver` (NULL = the reference's fixed-count CG; warm_start is ignored).
+ * The result equals smoke_b200_solve_pressure_cuda on a context holding the same occupancy and right-hand side.
+ *
+ * Limits and rules:
+ *  - at most smoke_b200_noalloc_max_cells() = 64^3 = 262,144 cells; a larger grid returns BACKEND_FAILURE and
+ *    smoke_b200_last_error() says why. The scratch array (about 11 MB) is held on every GPU that loads the library
+ *    until the process exits;
+ *  - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that device
+ *    current; make that first call before capturing any stream into a CUDA graph;
+ *  - every call shares the one array: calls that overlap on the GPU (different streams, or several host threads)
+ *    race and corrupt each other. Serialise them on one stream. The array keeps the last call's contents; the
+ *    call itself clears whatever must start at zero;
+ *  - out_status (optional) synchronises `stream` and reports like smoke_b200_get_solver_status_cuda. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_noalloc_cuda(const SmokeSimulationConfig* config, const uint8_t* occupancy, const float* rhs, float* pressure,
+                                                                                 const SmokeB200SolverDesc* solver, void* stream, SmokeB200SolverStatus* out_status);
+
+/* Largest grid (cells) smoke_b200_solve_pressure_noalloc_cuda accepts. */
+SMOKE_SIMULATION_API unsigned long long smoke_b200_noalloc_max_cells(void);
+
+/* Reason of the last failure of smoke_b200_solve_pressure_noalloc_cuda on this host thread ("" if none). */
+SMOKE_SIMULATION_API const char* smoke_b200_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
