@@ -207,14 +207,23 @@ def restore_state(sim, state):
     sim.stream.synchronize()
 
 
-def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5):
+# Algorithmic bytes per cell and iteration of the solver kernels (each operand counted once):
+#  - Jacobi/CG (pcg_kernel): reads p, x, r, s, w (4 B each) + code (2 B); writes p, x, r, s, w -> 42 B;
+#  - multigrid FCG (mgfcg_kernel), level 0: restriction reads r, code, writes z (10 B); prolongation reads z, writes
+#    t (8 B); smoothing reads t, r, code, q, writes z (18 B); p/q pass reads z, p, code, r, writes p, q (22 B);
+#    update pass reads e, p, r, q, writes e, r (24 B) -> 82 B, plus ~1/7 of that on the coarser levels -> 94 B.
+JACOBI_BYTES_PER_CELL_ITERATION = 42.0
+MG_BYTES_PER_CELL_ITERATION = 94.0
+
+
+def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5, bytes_per_iteration=JACOBI_BYTES_PER_CELL_ITERATION, kernel="pcg_kernel"):
     """Times the persistent solver kernel alone (smoke_b200_solve_pressure_cuda on the step's right-hand side) with
-    CUDA events on the context stream. Algorithmic bytes per iteration: 42 B/cell (reads p, x, r, s, w 4 B each +
-    code 2 B; writes p, x, r, s, w); setup 16 B/cell; refinement pass 10 B/cell."""
+    CUDA events on the context stream; algorithmic bytes = cells x (bytes per iteration x iterations + setup)."""
     import torch
 
     flush = L2Flush()
     durs, iters = [], []
+    passes = 1
     for _ in range(repeats):
         with torch.cuda.stream(sim.stream):
             flush()
@@ -226,15 +235,16 @@ def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5):
         sim.stream.synchronize()
         durs.append(e0.elapsed_time(e1))
         st = sim.solver_status()
-        iters.append(st.iterations + 0.0 * st.passes)
+        iters.append(st.iterations)
         passes = st.passes
     ms = statistics.median(durs)
     it = statistics.median(iters)
-    algo_bytes = n_cells * (42.0 * it + 16.0 + 10.0 * passes)
+    algo_bytes = n_cells * (bytes_per_iteration * it + 16.0 + 26.0 * passes)
     achieved = algo_bytes / (ms * 1e-3) / 1e9
-    return {"bound": "hbm", "kernel": "pcg_kernel (persistent Chronopoulos-Gear PCG)", "achieved": round(achieved, 1), "peak": peak_gbs, "peak_kind": peak_kind, "unit": "GB/s",
+    return {"bound": "hbm", "kernel": kernel, "achieved": round(achieved, 1), "peak": peak_gbs, "peak_kind": peak_kind, "unit": "GB/s",
             "frac": round(achieved / peak_gbs, 3), "traffic": None, "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(ms, 4), "iterations": it,
-            "note": "working set (~9 vectors x 8 MiB) is L2-resident at 128^3; DRAM traffic per launch is in profiles/"}
+            "bytes_per_cell_iteration": bytes_per_iteration,
+            "note": "the solver's working set is L2-resident at 128^3; DRAM traffic per launch is in profiles/"}
 
 
 def cpu_baseline(sim, cfg, steps=2):
@@ -271,6 +281,15 @@ def build_sim(lib, cfg, stream):
     return smoke_b200.Simulation(lib, cfg, stream)
 
 
+# Solver forms measured on the same plume states. The headline ("value") is the first one.
+FORMS = {
+    "multigrid_fp64": dict(mode=abi.SOLVER_MG_FCG, reduction=abi.REDUCTION_FP64, max_iterations=500, tolerance=1e-5, refinement=3),
+    "jacobi_fp64": dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP64, max_iterations=3000, tolerance=1e-5, refinement=3),
+    "plain_fp32": dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP32, max_iterations=1500, tolerance=1e-5, refinement=0),
+}
+HEADLINE = "multigrid_fp64"
+
+
 def bench_b200(args, rank, world, local):
     import torch
 
@@ -283,58 +302,58 @@ def bench_b200(args, rank, world, local):
     cfg = plume_scene.plume_config(n, abi.MONOTONIC_CUBIC)
     sim = smoke_b200.Simulation(lib, cfg, stream)
     driver = plume_scene.PlumeDriver(sim, n, seed=1 + rank)
-    mixed = dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP64, max_iterations=3000, tolerance=1e-5, refinement=3)
-    plain = dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP32, max_iterations=1500, tolerance=1e-5, refinement=0)
-    sim.set_solver(**mixed)
+    sim.set_solver(**FORMS[HEADLINE])
     flush = L2Flush()
     # spin-up (untimed): the plume develops from rest
     run_steps(sim, driver, 0, SPINUP_STEPS, None)
     state = save_state(sim)
     step0 = SPINUP_STEPS
-    # warm-up + timed, mixed form
-    run_steps(sim, driver, step0, args.warmup, flush)
-    barrier(world)
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        t_mixed, it_mixed, res_mixed = run_steps(sim, driver, step0 + args.warmup, args.steps, flush, status=True)
-    torch.cuda.synchronize()
-    barrier(world)
-    # plain FP32 form from the same state
+    results = {}
+    clocks = None
+    for name, form in FORMS.items():
+        restore_state(sim, state)
+        sim.set_solver(**form)
+        run_steps(sim, driver, step0, args.warmup, flush)
+        barrier(world)
+        torch.cuda.synchronize()
+        if name == HEADLINE:
+            with ClockSampler(local) as clocks:
+                t, its, res = run_steps(sim, driver, step0 + args.warmup, args.steps, flush, status=True)
+        else:
+            t, its, res = run_steps(sim, driver, step0 + args.warmup, args.steps, flush, status=True)
+        torch.cuda.synchronize()
+        barrier(world)
+        results[name] = (max_over_ranks(statistics.mean(t), world), statistics.mean(its), max(res))
+    # e2e through the ABI (headline form), same state
     restore_state(sim, state)
-    sim.set_solver(**plain)
-    run_steps(sim, driver, step0, args.warmup, flush)
-    t_plain, it_plain, res_plain = run_steps(sim, driver, step0 + args.warmup, args.steps, flush, status=True)
-    # e2e through the ABI (mixed form), same state
-    restore_state(sim, state)
-    sim.set_solver(**mixed)
+    sim.set_solver(**FORMS[HEADLINE])
     run_e2e(sim, driver, step0, args.warmup)
     barrier(world)
     e2e_ms, _ = run_e2e(sim, driver, step0 + args.warmup, args.steps)
     barrier(world)
-    roof = solver_kernel_roofline(sim, n ** 3, *load_peaks())
-    ms_mixed = max_over_ranks(statistics.mean(t_mixed), world)
-    ms_plain = max_over_ranks(statistics.mean(t_plain), world)
     e2e_ms = max_over_ranks(e2e_ms, world)
+    roof = solver_kernel_roofline(sim, n ** 3, *load_peaks(), bytes_per_iteration=MG_BYTES_PER_CELL_ITERATION, kernel="mgfcg_kernel (persistent multigrid-preconditioned FCG)")
     cpu = cpu_baseline(sim, cfg) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     sim.close()
     if rank != 0:
         return None
     cells = n ** 3
+    ms, its, res = results[HEADLINE]
     line = {
-        "metric": METRIC, "value": round(ms_mixed, 4), "unit": "ms/step", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_mixed, 4),
+        "metric": METRIC, "value": round(ms, 4), "unit": "ms/step", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fp64 reductions)", "data": "synthetic (seeded plume scene)",
-        "config": {"workload": f"plume {n}^3 monotone-cubic, Jacobi-PCG to rel-res 1e-5 with FP64 dots and FP64 refinement", "grid": [n, n, n], "dt": 0.01,
+        "config": {"workload": f"plume {n}^3 monotone-cubic; pressure to rel-res 1e-5: multigrid-preconditioned FCG, FP64 dots, FP64 refinement", "grid": [n, n, n], "dt": 0.01,
                    "source_box": "16x8x16 at x,z in [56,72), y in [0,8)" if n == 128 else "n/8 x n/16 x n/8", "spinup_steps": SPINUP_STEPS,
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}", "learned_preconditioner": "not used"},
-        "pcg_iterations": round(statistics.mean(it_mixed), 1), "true_rel_residual_max": max(res_mixed),
-        "cells_per_s": round(cells * world / (ms_mixed * 1e-3), 1),
-        "forms": {"mixed_fp64": {"ms_per_step": round(ms_mixed, 4), "pcg_iterations": round(statistics.mean(it_mixed), 1), "rel_residual_max": max(res_mixed)},
-                  "plain_fp32": {"ms_per_step": round(ms_plain, 4), "pcg_iterations": round(statistics.mean(it_plain), 1), "rel_residual_max": max(res_plain)}},
+        "pcg_iterations": round(its, 1), "true_rel_residual_max": res,
+        "cells_per_s": round(cells * world / (ms * 1e-3), 1),
+        "forms": {k: {"ms_per_step": round(v[0], 4), "pcg_iterations": round(v[1], 1), "rel_residual_max": v[2]} for k, v in results.items()},
+        "speedup_vs_plain_fp32": round(results["plain_fp32"][0] / ms, 2),
         "roofline": roof,
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": driver.h2d_bytes, "d2h_bytes_per_step": driver.d2h_bytes,
                 "includes": "per-step box inputs H2D, velocity/density/temperature views, source/force updates, step, total-density D2H, host sync"},
         "gpu_launches": KERNELS_PER_STEP * args.steps,
-        "clocks": clocks.summary(),
+        "clocks": clocks.summary() if clocks is not None else None,
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu

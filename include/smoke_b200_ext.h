@@ -28,6 +28,8 @@ typedef enum SmokeB200SolverMode {
     SMOKE_B200_SOLVER_FIXED_CG = 0,
     /* Jacobi-preconditioned CG that stops once ||r|| <= tolerance * ||b|| or after max_iterations. */
     SMOKE_B200_SOLVER_JACOBI_PCG = 1,
+    /* Flexible CG preconditioned by one geometric multigrid V(1,1) cycle; same stopping rule as JACOBI_PCG. */
+    SMOKE_B200_SOLVER_MG_FCG = 2,
 } SmokeB200SolverMode;
 
 typedef enum SmokeB200Reduction {

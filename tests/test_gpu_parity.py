@@ -44,10 +44,10 @@ def setup_case(lib, stream, name, seed=3, cfl=0.6):
     return cfg, inp
 
 
-def gpu_after(lib, stream, cfg, inp, last_stage, tol=1e-7):
+def gpu_after(lib, stream, cfg, inp, last_stage, tol=1e-7, mode=abi.SOLVER_JACOBI_PCG):
     sim = smoke_b200.Simulation(lib, cfg, stream)
     keep = scenes.load_gpu(sim, inp)
-    sim.set_solver(abi.SOLVER_JACOBI_PCG, abi.REDUCTION_FP64, max_iterations=4000, tolerance=tol, refinement=2)
+    sim.set_solver(mode, abi.REDUCTION_FP64, max_iterations=4000, tolerance=tol, refinement=2)
     with torch.cuda.stream(stream):
         sim.step_stages(last_stage)
     stream.synchronize()
@@ -110,10 +110,11 @@ def test_stage_advect_velocity(smoke_lib, cuda_stream, name, cfl):
     assert max(errs) < STAGE_TOL, errs
 
 
+@pytest.mark.parametrize("mode", [abi.SOLVER_JACOBI_PCG, abi.SOLVER_MG_FCG], ids=["jacobi", "multigrid"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_stage_pressure(smoke_lib, cuda_stream, name):
+def test_stage_pressure(smoke_lib, cuda_stream, name, mode):
     cfg, inp = setup_case(smoke_lib, cuda_stream, name)
-    sim = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_PRESSURE)
+    sim = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_PRESSURE, mode=mode)
     cu, cv, cw = faces(sim, 1)
     rhs = cells(sim, abi.VIEW_FLOW_PRESSURE_RHS)
     p = cells(sim, abi.VIEW_FLOW_PRESSURE)
@@ -128,7 +129,7 @@ def test_stage_pressure(smoke_lib, cuda_stream, name):
     res = O.relative_residual(cfg, inp["occupancy"], rhs, p)
     truth, _ = O.solve_pressure(cfg, inp["occupancy"], rhs, bits=64, tolerance=1e-12)
     e_p = scenes.rel_err(p, truth)
-    report(f"pressure/{name}", {"rhs": e_rhs, "true_residual": res, "p_vs_fp64": e_p, "iterations": status.iterations, "status": status.status,
+    report(f"pressure/{name}/mode{mode}", {"rhs": e_rhs, "true_residual": res, "p_vs_fp64": e_p, "iterations": status.iterations, "status": status.status,
                                 "reported_true_residual": status.true_relative_residual})
     assert e_rhs < STAGE_TOL
     assert status.status == abi.SOLVE_CONVERGED
@@ -205,13 +206,14 @@ def test_views_after_step(smoke_lib, cuda_stream, name):
     assert max(errs.values()) < STAGE_TOL, errs
 
 
+@pytest.mark.parametrize("mode", [abi.SOLVER_JACOBI_PCG, abi.SOLVER_MG_FCG], ids=["jacobi", "multigrid"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_full_steps_against_oracle(smoke_lib, cuda_stream, name):
+def test_full_steps_against_oracle(smoke_lib, cuda_stream, name, mode):
     """Three graph-launched steps against three oracle steps, both solving to 1e-7."""
     cfg, inp = setup_case(smoke_lib, cuda_stream, name, seed=11)
     sim = smoke_b200.Simulation(smoke_lib, cfg, cuda_stream)
     keep = scenes.load_gpu(sim, inp)
-    sim.set_solver(abi.SOLVER_JACOBI_PCG, abi.REDUCTION_FP64, max_iterations=4000, tolerance=1e-7, refinement=2)
+    sim.set_solver(mode, abi.REDUCTION_FP64, max_iterations=4000, tolerance=1e-7, refinement=2)
     st = oracle_from(cfg, inp)
     worst = {}
     for k in range(3):
@@ -224,7 +226,7 @@ def test_full_steps_against_oracle(smoke_lib, cuda_stream, name):
             worst[g] = max(worst.get(g, 0.0), scenes.rel_err(snap[g], st[o]))
     sim.close()
     del keep
-    report(f"full3/{name}", worst)
+    report(f"full3/{name}/mode{mode}", worst)
     assert max(worst.values()) < 2e-3, worst
 
 

@@ -111,6 +111,8 @@ struct SmokeSimulationContext_t {
     uint32_t* fill_count = nullptr;
     int32_t* anchor = nullptr;
     PcgControl* control = nullptr;
+    MgHierarchy mg{};
+    MgWork mg_work{};
 
     SmokeB200SolverDesc solver{SMOKE_B200_SOLVER_FIXED_CG, SMOKE_B200_REDUCTION_FP32, 500, 1.0e-5f, 0, 0};
     PcgLaunchShape pcg_shape{};
@@ -156,6 +158,31 @@ struct SmokeSimulationContext_t {
         slots.push_back({reinterpret_cast<void**>(&fill_count), sizeof(uint32_t)});
         slots.push_back({reinterpret_cast<void**>(&anchor), sizeof(int32_t)});
         slots.push_back({reinterpret_cast<void**>(&control), sizeof(PcgControl)});
+        // multigrid levels: level 0 shares the Jacobi solver's vectors; coarser levels get their own arrays
+        mg.levels = mg_level_count(P.nx, P.ny, P.nz);
+        for (int a = 0; a < 3; ++a) mg.fper[a] = P.fper[a];
+        int lx = P.nx, ly = P.ny, lz = P.nz;
+        mg.grid_levels = 0;
+        for (int l = 0; l < mg.levels; ++l) {
+            MgLevel& L = mg.L[l];
+            L.nx = lx;
+            L.ny = ly;
+            L.nz = lz;
+            L.n = static_cast<uint32_t>(lx) * ly * lz;
+            L.div_nx = FastDiv(lx);
+            L.div_slab = FastDiv(static_cast<uint32_t>(lx) * ly);
+            if (L.n > kMgBlockLevelCells) mg.grid_levels = l + 1;
+            slots.push_back({reinterpret_cast<void**>(&L.fluid), L.n});
+            if (l > 0) {
+                slots.push_back({reinterpret_cast<void**>(&L.code), L.n * sizeof(uint16_t)});
+                for (float** p : {&L.r, &L.zp, &L.t}) slots.push_back({reinterpret_cast<void**>(p), L.n * sizeof(float)});
+            }
+            lx = (lx + 1) / 2;
+            ly = (ly + 1) / 2;
+            lz = (lz + 1) / 2;
+        }
+        if (mg.grid_levels < 1) mg.grid_levels = 1;
+        if (mg.grid_levels > mg.levels - 1) mg.grid_levels = mg.levels - 1;
         auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
         size_t total = 0;
         for (const Slot& s : slots) total += align(s.bytes);
@@ -166,6 +193,16 @@ struct SmokeSimulationContext_t {
             *s.ptr = static_cast<char*>(arena) + off;
             off += align(s.bytes);
         }
+        MgLevel& L0 = mg.L[0];
+        L0.code = codes;
+        L0.r = pcg.r[0];
+        L0.zp = pcg.r[1];
+        L0.t = pcg.w[0];
+        mg_work.p[0] = pcg.s[0];
+        mg_work.p[1] = pcg.s[1];
+        mg_work.q = pcg.w[1];
+        mg_work.e = pcg.e;
+        mg_work.x64 = pcg.x64;
     }
 
     // Occupancy-derived data: anchor, operator codes, density fill list, float occupancy view.
@@ -174,6 +211,14 @@ struct SmokeSimulationContext_t {
         check(launch_anchor(P, occupancy, anchor, stream), "pressure anchor");
         check(launch_stencil_codes(P, occupancy, anchor, codes, stream), "operator codes");
         check(launch_fill_build(P, occupancy, anchor, fill_list, fill_count, stream), "density fill list");
+        check(launch_mg_setup(P, mg, occupancy, stream), "multigrid levels");
+    }
+
+    // The pressure solve of the selected mode on the context's right-hand side.
+    void enqueue_solve(cudaStream_t s) {
+        const PcgSettings S = pcg_settings();
+        if (solver.mode == SMOKE_B200_SOLVER_MG_FCG) check(launch_mgfcg(P, S, mg, rhs, pressure, mg_work, anchor, control, s), "pressure solve (multigrid FCG)");
+        else check(launch_pcg(P, S, pcg_shape, codes, rhs, pressure, pcg, control, s), "pressure solve");
     }
 
     PcgSettings pcg_settings() const {
@@ -199,7 +244,7 @@ struct SmokeSimulationContext_t {
         check(launch_advect_velocity(P, as_const(B), occupancy, solid, C, s), "advect velocity");
         if (last_stage < SMOKE_B200_STAGE_PRESSURE) return;
         check(launch_rhs(P, as_const(C), occupancy, anchor, rhs, s), "pressure rhs");
-        check(launch_pcg(P, pcg_settings(), pcg_shape, codes, rhs, pressure, pcg, control, s), "pressure solve");
+        enqueue_solve(s);
         if (last_stage < SMOKE_B200_STAGE_PROJECT) return;
         const PcgSettings S = pcg_settings();
         const double* p64 = (!S.fixed && S.refinement > 0) ? pcg.x64 : nullptr;
@@ -418,8 +463,8 @@ SmokeSimulationResult smoke_simulation_get_view_cuda(SmokeSimulationContext c, c
 // ---------------------------------------------------------------------------------------------- extensions
 SmokeSimulationResult smoke_b200_set_solver_cuda(SmokeSimulationContext c, const SmokeB200SolverDesc* desc) {
     if (c == nullptr || desc == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-    if (desc->mode > SMOKE_B200_SOLVER_JACOBI_PCG || desc->reduction > SMOKE_B200_REDUCTION_FP64) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-    if (desc->mode == SMOKE_B200_SOLVER_JACOBI_PCG && (desc->max_iterations <= 0 || !(desc->tolerance > 0.0f))) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (desc->mode > SMOKE_B200_SOLVER_MG_FCG || desc->reduction > SMOKE_B200_REDUCTION_FP64) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (desc->mode != SMOKE_B200_SOLVER_FIXED_CG && (desc->max_iterations <= 0 || !(desc->tolerance > 0.0f))) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return guarded([&] {
         c->solver = *desc;
         c->capture_step_graph();
@@ -475,7 +520,7 @@ SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimulationContext c, uint
 SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext c) {
     if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return guarded([&] {
-        check(launch_pcg(c->P, c->pcg_settings(), c->pcg_shape, c->codes, c->rhs, c->pressure, c->pcg, c->control, c->stream), "pressure solve");
+        c->enqueue_solve(c->stream);
         c->stepped = true;
         return SMOKE_SIMULATION_RESULT_OK;
     });

@@ -2,6 +2,7 @@
 // `stream` and returns the launch status.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -83,17 +84,21 @@ struct PcgStatusDevice {
     double true_relative_residual;
 };
 
-// Device-resident control block: grid barrier, abort flag, per-block partial sums (double-buffered by
-// iteration parity) and the status of the last solve.
+// Device-resident control block: grid barrier counter (its top bit flips once every block has arrived), abort flag,
+// a ring of three all-reduce slots (each spread over kPcgSumCopies cache lines so that concurrent atomic adds
+// contend less) and the status of the last solve. Zeroed (up to `status`) before every launch.
 constexpr int kPcgMaxBlocks = 148 * 16;
+constexpr int kPcgSumCopies = 8;
 struct PcgControl {
-    unsigned int count;
-    unsigned int gen;
+    unsigned int bar;
+    unsigned int pad0;
     int abort;
-    int pad;
+    int pad1;
+    unsigned int pad2[28];
+    double totals[3][kPcgSumCopies][16];  // 4 sums per copy, one 128-byte line per copy
     PcgStatusDevice status;
-    double partial[2][kPcgMaxBlocks][4];
 };
+constexpr size_t kPcgControlResetBytes = offsetof(PcgControl, status);
 
 struct PcgWork {
     float* r[2];
@@ -108,6 +113,41 @@ struct PcgLaunchShape {
     int blocks;
     int threads;
 };
+
+// ------------------------------------------------------------------------------------------ multigrid hierarchy
+// Geometric multigrid for the pressure operator (mgpcg.cu). Level 0 is the grid itself; level l+1 halves every
+// extent (rounding up). A coarse cell is fluid when any of its children is; every level's operator is the masked
+// 7-point stencil of its fluid cells (the fine rules without the anchor).
+constexpr int kMgMaxLevels = 12;
+constexpr uint32_t kMgBlockLevelCells = 4096;  // levels this small run inside one block
+struct MgLevel {
+    int nx, ny, nz;
+    uint32_t n;
+    FastDiv div_nx, div_slab;
+    uint16_t* code;   // row codes (level 0: the fine operator's codes)
+    uint8_t* fluid;   // 1 = fluid cell
+    float* r;         // right-hand side / residual of the level (level 0: the solver residual)
+    float* zp;        // correction (level 0: the preconditioned residual z)
+    float* t;         // scratch of the level
+};
+struct MgHierarchy {
+    int levels;       // >= 2
+    int grid_levels;  // levels [0, grid_levels) run on the whole grid; coarser ones inside one block
+    int fper[3];
+    MgLevel L[kMgMaxLevels];
+};
+struct MgWork {
+    float* p[2];
+    float* q;
+    float* e;
+    double* x64;
+};
+// Level extents and the number of grid-wide levels for a fine grid.
+int mg_level_count(int nx, int ny, int nz);
+// Builds level fluid masks and codes from the occupancy (after the fine codes and anchor exist).
+cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uint8_t* occ, cudaStream_t s);
+// Enqueues the control reset and the cooperative multigrid-preconditioned FCG solve of A x = b.
+cudaError_t launch_mgfcg(const StepParams& P, const PcgSettings& S, const MgHierarchy& H, const float* b, float* x, MgWork work, const int32_t* anchor, PcgControl* ctl, cudaStream_t s);
 
 // Picks the persistent grid (all blocks co-resident) for the current device.
 cudaError_t pcg_launch_shape(PcgLaunchShape* out);

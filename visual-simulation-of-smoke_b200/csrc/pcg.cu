@@ -4,21 +4,23 @@
 // (backend-cuda.cu:1343-1412, 1788-1824) by ONE cooperative launch that runs every iteration:
 //  - the operator is the masked 7-point stencil encoded per cell in a 16-bit code (neighbour bits + diagonal),
 //    with the reference's matrix values (stencil_code_kernel in step_kernels.cu);
-//  - each block owns fixed 32x8x8 bricks of cells; per iteration it stages r, s, w and the codes of a brick plus a
-//    one-cell halo in shared memory (halo cells across a periodic edge are fetched from the opposite side), so
-//    every value is read from L2/HBM once per brick instead of once per neighbour;
+//  - work is split into 32x8-cell columns marched in z ("2.5D" stencil): every thread owns one (x, y) cell of a
+//    column, so a plane step costs one address add; the +-z neighbours stay in registers and only the thin in-plane
+//    halo goes through a three-plane ring in shared memory. Loads of plane z+2 are issued before plane z is
+//    computed. Each block owns a fixed, balanced range of column-planes;
 //  - the iteration is the Chronopoulos-Gear form of (P)CG: both dot products of an iteration are reduced together,
 //    so there is ONE grid barrier per iteration. r, s and w are double-buffered: a block recomputes its halo's new
 //    residuals from the old buffers while other blocks write the new ones;
-//  - reductions: every block publishes its partial sums; the last block to arrive at the barrier adds all of them
-//    in block order (the same order whichever block is last) and publishes the totals, so every block takes the
-//    same deterministic scalar decisions;
+//  - the barrier (grid_sync.cuh) is one atomic per block on a flip-bit counter; its all-reduce adds FP64 partials
+//    atomically into copies spread over cache lines, so every block reads the same totals and takes the same scalar
+//    decisions (the summation order of the block partials is not fixed);
 //  - FIXED mode reproduces the reference: M = I, x0 = 0, exactly N iterations, alpha/beta = 0 when the denominator
 //    magnitude is <= 1e-20. Tolerance mode stops at ||r|| <= tol ||b||. With refinement, the solution is accumulated
 //    in FP64 (x64 += e after each FP32 inner solve of A e = r) and r = b - A x64 is recomputed in FP64, so the
 //    residual can go below the FP32 floor of the pressure itself;
 //  - every grid barrier waits at most kBarrierTimeoutNs, then raises an abort flag that makes all blocks leave; the
 //    host reads the outcome from the status block.
+#include "grid_sync.cuh"
 #include "launch.h"
 #include "smoke_b200_ext.h"
 
@@ -26,195 +28,180 @@ namespace smoke_b200 {
 
 namespace {
 
-constexpr int kThreads = 512;
-constexpr int BX = 32, BY = 8, BZ = 8;
-constexpr int TX = BX + 2, TY = BY + 2, TZ = BZ + 2;
-constexpr int kTile = TX * TY * TZ;
-constexpr int kBrick = BX * BY * BZ;
-constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
-constexpr unsigned kBarrierMaxSpins = 1u << 26;
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
+constexpr int kThreads = 256;
+constexpr int CX = 32, CY = 8;
+constexpr int PX = CX + 2, PY = CY + 2;
+constexpr int kPlane = PX * PY;
+constexpr int kHaloSlots = kPlane - CX * CY;
+static_assert(kHaloSlots <= kThreads, "one halo slot per thread at most");
+using gsync::global_ns;
+using gsync::warp_sum;
 
 template <typename T>
-__device__ __forceinline__ T warp_sum(T v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
+__device__ __forceinline__ bool barrier_allreduce(PcgControl* ctl, unsigned& phase, T local[4], T out[4], bool reduce = true) {
+    return gsync::barrier_allreduce<kThreads, T>(ctl, phase, local, out, reduce);
 }
 
-// Block sum of 4 values in a fixed order; the result is valid in thread 0.
-template <typename T>
-__device__ void block_sum4(T v[4], T (*scratch)[kThreads / 32]) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = warp_sum(v[k]);
-    if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) scratch[k][warp] = v[k];
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) v[k] = warp_sum(lane < kThreads / 32 ? scratch[k][lane] : T(0));
-    }
-    __syncthreads();
-}
-
-// Grid barrier fused with a deterministic all-reduce of 4 sums. Returns false if the solve was aborted.
-template <typename T>
-__device__ bool barrier_allreduce(PcgControl* ctl, int parity, T local[4], T out[4]) {
-    __shared__ T scratch[4][kThreads / 32];
-    __shared__ int s_last, s_ok;
-    block_sum4(local, scratch);
-    unsigned gen = 0;
-    if (threadIdx.x == 0) {
-        double* slot = ctl->partial[0][blockIdx.x];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) slot[k] = static_cast<double>(local[k]);
-        // read the generation before arriving: it cannot advance until this block has arrived
-        gen = *static_cast<volatile unsigned*>(&ctl->gen);
-        __threadfence();
-        const unsigned arrived = atomicAdd(&ctl->count, 1u);
-        s_last = arrived == gridDim.x - 1;
-    }
-    __syncthreads();
-    int ok = 1;
-    if (s_last) {
-        // the last block adds every block's partials in block order
-        T v[4] = {0, 0, 0, 0};
-        for (unsigned b = threadIdx.x; b < gridDim.x; b += kThreads) {
-            const double* slot = ctl->partial[0][b];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) v[k] += static_cast<T>(__ldcg(slot + k));
-        }
-        block_sum4(v, scratch);
-        if (threadIdx.x == 0) {
-            double* tot = ctl->partial[1][parity];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) tot[k] = static_cast<double>(v[k]);
-            atomicExch(&ctl->count, 0u);
-            __threadfence();
-            atomicAdd(&ctl->gen, 1u);
-        }
-    } else if (threadIdx.x == 0) {
-        volatile unsigned* vgen = &ctl->gen;
-        volatile int* vabort = &ctl->abort;
-        const unsigned long long t0 = global_ns();
-        unsigned spins = 0;
-        while (*vgen == gen) {
-            if (*vabort) {
-                ok = 0;
-                break;
-            }
-            ++spins;
-            if (spins >= kBarrierMaxSpins || ((spins & 63u) == 0 && global_ns() - t0 > kBarrierTimeoutNs)) {
-                atomicExch(&ctl->abort, 1);
-                ok = 0;
-                break;
-            }
-        }
-    }
-    if (threadIdx.x == 0) {
-        __threadfence();
-        if (*static_cast<volatile int*>(&ctl->abort)) ok = 0;
-        s_ok = ok;
-    }
-    __syncthreads();
-    const double* tot = ctl->partial[1][parity];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) out[k] = static_cast<T>(__ldcg(tot + k));
-    __syncthreads();
-    return s_ok != 0;
-}
-
-struct Bricks {
-    int nbx, nby, count;
+struct Columns {
+    int ncx, ncy;
+    uint32_t total;  // column-planes: ncx * ncy * nz
 };
 
-__device__ __forceinline__ void brick_origin(const Bricks& B, int b, int& x0, int& y0, int& z0) {
-    const int bx = b % B.nbx;
-    const int t = b / B.nbx;
-    const int by = t % B.nby;
-    const int bz = t / B.nby;
-    x0 = bx * BX;
-    y0 = by * BY;
-    z0 = bz * BZ;
-}
-
-// Global cell of tile slot t (halo included), wrapped across periodic edges; false outside the domain.
-__device__ __forceinline__ bool tile_cell(const StepParams& P, int x0, int y0, int z0, int t, uint32_t& q) {
-    int gx = x0 + t % TX - 1;
-    int gy = y0 + (t / TX) % TY - 1;
-    int gz = z0 + t / (TX * TY) - 1;
-    if (gx < 0 || gx >= P.nx) {
-        if (!P.fper[0]) return false;
-        gx = wrapi(gx, P.nx);
-    }
-    if (gy < 0 || gy >= P.ny) {
-        if (!P.fper[1]) return false;
-        gy = wrapi(gy, P.ny);
-    }
-    if (gz < 0 || gz >= P.nz) {
-        if (!P.fper[2]) return false;
-        gz = wrapi(gz, P.nz);
-    }
-    q = cidx(P, gx, gy, gz);
+__device__ __forceinline__ bool wrap_axis(int& v, int n, int periodic) {
+    if (v >= 0 && v < n) return true;
+    if (!periodic) return false;
+    v = wrapi(v, n);
     return true;
 }
 
-// Own cell c (0..kBrick) of a brick: tile slot and global index; false outside the domain.
-__device__ __forceinline__ bool own_cell(const StepParams& P, int x0, int y0, int z0, int c, int& slot, uint32_t& q) {
-    const int bx = c % BX, by = (c / BX) % BY, bz = c / (BX * BY);
-    const int gx = x0 + bx, gy = y0 + by, gz = z0 + bz;
-    slot = ((bz + 1) * TY + (by + 1)) * TX + (bx + 1);
-    if (gx >= P.nx || gy >= P.ny || gz >= P.nz) return false;
-    q = cidx(P, gx, gy, gz);
+// Per-thread geometry of one column: the thread's own slot, and (threads < kHaloSlots) one halo slot of the ring.
+struct ColumnGeo {
+    uint32_t own_off, halo_off;  // in-plane offsets (y * nx + x) of the cells loaded into the slots
+    int own_slot, halo_slot;
+    bool own_out;                // the own cell is inside the domain and produces output
+    bool own_load, halo_load;    // the slot maps to a cell (possibly across a periodic edge)
+};
+
+__device__ __forceinline__ ColumnGeo column_geo(const StepParams& P, int x0, int y0) {
+    ColumnGeo g;
+    const int tx = threadIdx.x % CX, ty = threadIdx.x / CX;
+    int gx = x0 + tx, gy = y0 + ty;
+    g.own_slot = (ty + 1) * PX + tx + 1;
+    g.own_out = gx < P.nx && gy < P.ny;
+    g.own_load = wrap_axis(gx, P.nx, P.fper[0]) && wrap_axis(gy, P.ny, P.fper[1]);
+    g.own_off = g.own_load ? static_cast<uint32_t>(gy) * P.nx + gx : 0u;
+    g.halo_load = false;
+    g.halo_slot = 0;
+    g.halo_off = 0;
+    if (threadIdx.x < kHaloSlots) {
+        const int h = threadIdx.x;
+        int hx, hy;
+        if (h < PX) {
+            hx = h - 1;
+            hy = -1;
+        } else if (h < 2 * PX) {
+            hx = h - PX - 1;
+            hy = CY;
+        } else if (h < 2 * PX + CY) {
+            hx = -1;
+            hy = h - 2 * PX;
+        } else {
+            hx = CX;
+            hy = h - 2 * PX - CY;
+        }
+        g.halo_slot = (hy + 1) * PX + hx + 1;
+        int lx = x0 + hx, ly = y0 + hy;
+        g.halo_load = wrap_axis(lx, P.nx, P.fper[0]) && wrap_axis(ly, P.ny, P.fper[1]);
+        g.halo_off = g.halo_load ? static_cast<uint32_t>(ly) * P.nx + lx : 0u;
+    }
+    return g;
+}
+
+// Offset of plane z (wrapped across a periodic edge); false outside the domain.
+__device__ __forceinline__ bool plane_base(const StepParams& P, int z, uint32_t& base) {
+    if (!wrap_axis(z, P.nz, P.fper[2])) return false;
+    base = static_cast<uint32_t>(z) * static_cast<uint32_t>(P.nx) * P.ny;
     return true;
+}
+
+// March over every column segment of this block. For each plane z of a segment [za, zb):
+//   load(ok, q, own) -> Data       loads one slot's inputs (zero Data when !ok)
+//   ufn(Data) -> V                 the value whose stencil is taken
+//   own(q, Data, um1, u0, u1, plane, slot)   the own cell's work at plane z (um1/u1: its -z/+z values)
+// Planes of the ring are (z mod 3). One __syncthreads per plane step.
+template <typename V, typename Data, class Load, class UFn, class Own>
+__device__ __forceinline__ void march(const StepParams& P, const Columns& C, V (*ring)[kPlane], Load&& load, UFn&& ufn, Own&& own) {
+    const uint32_t a = static_cast<uint32_t>((static_cast<uint64_t>(blockIdx.x) * C.total) / gridDim.x);
+    const uint32_t b = static_cast<uint32_t>((static_cast<uint64_t>(blockIdx.x + 1) * C.total) / gridDim.x);
+    const int nz = P.nz;
+    uint32_t L = a;
+    while (L < b) {
+        const int col = static_cast<int>(L / static_cast<uint32_t>(nz));
+        const int za = static_cast<int>(L - static_cast<uint32_t>(col) * nz);
+        const int zb = za + static_cast<int>(min(static_cast<uint32_t>(nz - za), b - L));
+        L += static_cast<uint32_t>(zb - za);
+        const ColumnGeo g = column_geo(P, (col % C.ncx) * CX, (col / C.ncx) * CY);
+        const bool halo = threadIdx.x < kHaloSlots;
+        auto fetch = [&](int z, Data& own_d, Data& halo_d) {
+            uint32_t base = 0;
+            const bool pz = plane_base(P, z, base);
+            own_d = load(pz && g.own_load, base + g.own_off, true);
+            if (halo) halo_d = load(pz && g.halo_load, base + g.halo_off, false);
+        };
+        Data om1, o0, o1, o2, h0, h1, h2, hm1;
+        fetch(za - 1, om1, hm1);
+        fetch(za, o0, h0);
+        fetch(za + 1, o1, h1);
+        V um1 = ufn(om1);
+        V u0 = ufn(o0);
+        ring[za % 3][g.own_slot] = u0;
+        if (halo) ring[za % 3][g.halo_slot] = ufn(h0);
+        for (int z = za; z < zb; ++z) {
+            if (z + 2 <= zb) fetch(z + 2, o2, h2);
+            const V u1 = ufn(o1);
+            ring[(z + 1) % 3][g.own_slot] = u1;
+            if (halo) ring[(z + 1) % 3][g.halo_slot] = ufn(h1);
+            __syncthreads();
+            if (g.own_out) {
+                uint32_t base = 0;
+                plane_base(P, z, base);
+                own(base + g.own_off, o0, um1, u0, u1, ring[z % 3], g.own_slot);
+            }
+            um1 = u0;
+            u0 = u1;
+            o0 = o1;
+            o1 = o2;
+            h1 = h2;
+        }
+        __syncthreads();
+    }
 }
 
 template <bool JACOBI>
 __device__ __forceinline__ float inv_diag(uint16_t code) {
-    if constexpr (JACOBI) return __frcp_rn(static_cast<float>((code >> 8) & 7u));
+    if constexpr (JACOBI) return code ? __frcp_rn(static_cast<float>((code >> 8) & 7u)) : 0.0f;
     else return 1.0f;
 }
 __device__ __forceinline__ float diag_of(uint16_t code) { return static_cast<float>((code >> 8) & 7u); }
 
-// Masked 7-point stencil on a tile array: diag * v[slot] - sum of active neighbours.
+// diag * u0 - active neighbours; in-plane ones from the ring plane, -z/+z from registers.
 template <typename V>
-__device__ __forceinline__ V stencil(const V* tile, int slot, uint16_t code) {
-    V acc = static_cast<V>(diag_of(code)) * tile[slot];
-    if (code & 1u) acc -= tile[slot - 1];
-    if (code & 2u) acc -= tile[slot + 1];
-    if (code & 4u) acc -= tile[slot - TX];
-    if (code & 8u) acc -= tile[slot + TX];
-    if (code & 16u) acc -= tile[slot - TX * TY];
-    if (code & 32u) acc -= tile[slot + TX * TY];
+__device__ __forceinline__ V stencil(uint16_t code, V u0, V um1, V u1, const V* plane, int slot) {
+    V acc = static_cast<V>(diag_of(code)) * u0;
+    if (code & 1u) acc -= plane[slot - 1];
+    if (code & 2u) acc -= plane[slot + 1];
+    if (code & 4u) acc -= plane[slot - PX];
+    if (code & 8u) acc -= plane[slot + PX];
+    if (code & 16u) acc -= um1;
+    if (code & 32u) acc -= u1;
     return acc;
 }
 
-struct Smem {
-    float r[kTile];
-    float s[kTile];
-    float w[kTile];
-    float u[kTile];
-    uint16_t code[kTile];
+struct IterData {
+    float r, s, w, p, e;
+    uint16_t code;
+};
+struct SrcData {
+    float v;
+    uint16_t code;
+};
+struct X64Data {
+    double v;
+    uint16_t code;
 };
 
 template <typename T>
 __device__ __forceinline__ bool finite_all(T a, T b, T c) { return isfinite(a) && isfinite(b) && isfinite(c); }
 
 template <bool JACOBI, typename T>
-__global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const __grid_constant__ StepParams P, const PcgSettings S, const Bricks B, const uint16_t* __restrict__ codes, const float* __restrict__ b, float* x, PcgWork W, PcgControl* ctl) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+__global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ StepParams P, const PcgSettings S, const Columns C, const uint16_t* __restrict__ codes, const float* __restrict__ b, float* x, PcgWork W, PcgControl* ctl) {
+    __shared__ __align__(16) double ring_raw[3][kPlane];
+    float(*ring_f)[kPlane] = reinterpret_cast<float(*)[kPlane]>(ring_raw);
+    double(*ring_d)[kPlane] = ring_raw;
     const bool ir = !S.fixed && S.refinement > 0;  // FP64 accumulation + true-residual passes
     float* e = ir ? W.e : x;                         // the FP32 iterate
     const T guard = static_cast<T>(1.0e-20);
-    int parity = 0;
+    unsigned phase = 0;
     int cur = 0;
     uint32_t status = SMOKE_B200_SOLVE_ITERATION_CAP;
     double true_rel = -1.0;
@@ -222,51 +209,41 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const __grid_constant_
     bool aborted = false;
 
     auto sync_sums = [&](T local[4], T out[4]) -> bool {
-        const bool ok = barrier_allreduce<T>(ctl, parity, local, out);
-        parity ^= 1;
+        const bool ok = barrier_allreduce<T>(ctl, phase, local, out);
         if (!ok) aborted = true;
         return ok;
     };
 
-    // ------------------------------------------------------------ pass start: R[cur] = r0 given; W[cur] = A M r0
-    // src: the residual to start from; from_b: r0 = b (cold start, nothing else written yet)
-    auto start_pass = [&](const float* src, bool zero_x, T sums[4]) -> bool {
+    // ------------------------------------------------------------ pass start: R[cur] = src, W[cur] = A M src
+    auto start_pass = [&](const float* src, bool zero_e, T sums[4]) -> bool {
         T loc[4] = {0, 0, 0, 0};
-        for (int br = blockIdx.x; br < B.count; br += gridDim.x) {
-            int x0, y0, z0;
-            brick_origin(B, br, x0, y0, z0);
-            for (int t = threadIdx.x; t < kTile; t += kThreads) {
-                uint32_t q;
-                float rv = 0.0f;
-                uint16_t cd = 0;
-                if (tile_cell(P, x0, y0, z0, t, q)) {
-                    rv = __ldcg(src + q);
-                    cd = __ldg(codes + q);
+        float* Rc = W.r[cur];
+        float* Wc = W.w[cur];
+        float* Sc = W.s[cur];
+        march<float, SrcData>(
+            P, C, ring_f,
+            [&](bool ok, uint32_t q, bool) {
+                SrcData d{0.0f, 0};
+                if (ok) {
+                    d.v = __ldcg(src + q);
+                    d.code = __ldg(codes + q);
                 }
-                sm.u[t] = rv * inv_diag<JACOBI>(cd);
-                sm.code[t] = cd;
-            }
-            __syncthreads();
-            for (int c = threadIdx.x; c < kBrick; c += kThreads) {
-                int slot;
-                uint32_t q;
-                if (!own_cell(P, x0, y0, z0, c, slot, q)) continue;
-                const uint16_t cd = sm.code[slot];
-                const float r = __ldcg(src + q);
-                const float u = sm.u[slot];
-                const float w = stencil(sm.u, slot, cd);
-                W.r[cur][q] = r;
-                W.w[cur][q] = w;
-                W.s[cur][q] = 0.0f;
+                return d;
+            },
+            [&](const SrcData& d) { return d.v * inv_diag<JACOBI>(d.code); },
+            [&](uint32_t q, const SrcData& d, float um1, float u0, float u1, const float* plane, int slot) {
+                const float w = stencil(d.code, u0, um1, u1, plane, slot);
+                Rc[q] = d.v;
+                Wc[q] = w;
+                Sc[q] = 0.0f;
                 W.p[q] = 0.0f;
-                if (zero_x) e[q] = 0.0f;
-                loc[0] += static_cast<T>(r) * static_cast<T>(u);
-                loc[1] += static_cast<T>(w) * static_cast<T>(u);
-                loc[2] += static_cast<T>(r) * static_cast<T>(r);
-                loc[3] += static_cast<T>(__ldg(b + q)) * static_cast<T>(__ldg(b + q));
-            }
-            __syncthreads();
-        }
+                if (zero_e) e[q] = 0.0f;
+                const float bv = __ldg(b + q);
+                loc[0] += static_cast<T>(d.v) * static_cast<T>(u0);
+                loc[1] += static_cast<T>(w) * static_cast<T>(u0);
+                loc[2] += static_cast<T>(d.v) * static_cast<T>(d.v);
+                loc[3] += static_cast<T>(bv) * static_cast<T>(bv);
+            });
         return sync_sums(loc, sums);
     };
 
@@ -279,99 +256,72 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const __grid_constant_
         float* Sn = W.s[cur ^ 1];
         float* Wn = W.w[cur ^ 1];
         T loc[4] = {0, 0, 0, 0};
-        for (int br = blockIdx.x; br < B.count; br += gridDim.x) {
-            int x0, y0, z0;
-            brick_origin(B, br, x0, y0, z0);
-            for (int t = threadIdx.x; t < kTile; t += kThreads) {
-                uint32_t q;
-                float r = 0.0f, s = 0.0f, w = 0.0f;
-                uint16_t cd = 0;
-                if (tile_cell(P, x0, y0, z0, t, q)) {
-                    r = __ldcg(Rc + q);
-                    s = __ldcg(Sc + q);
-                    w = __ldcg(Wc + q);
-                    cd = __ldg(codes + q);
+        march<float, IterData>(
+            P, C, ring_f,
+            [&](bool ok, uint32_t q, bool own) {
+                IterData d{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0};
+                if (ok) {
+                    d.r = __ldcg(Rc + q);
+                    d.s = __ldcg(Sc + q);
+                    d.w = __ldcg(Wc + q);
+                    d.code = __ldg(codes + q);
+                    if (own) {
+                        d.p = __ldcg(W.p + q);
+                        d.e = __ldcg(e + q);
+                    }
                 }
-                sm.r[t] = r;
-                sm.s[t] = s;
-                sm.w[t] = w;
-                sm.code[t] = cd;
-                const float sn = w + fb * s;    // s_i
-                const float rn = r - fa * sn;   // r_{i+1}
-                sm.u[t] = rn * inv_diag<JACOBI>(cd);  // u_{i+1} = M r_{i+1}
-            }
-            __syncthreads();
-            for (int c = threadIdx.x; c < kBrick; c += kThreads) {
-                int slot;
-                uint32_t q;
-                if (!own_cell(P, x0, y0, z0, c, slot, q)) continue;
-                const uint16_t cd = sm.code[slot];
-                const float inv = inv_diag<JACOBI>(cd);
-                const float r = sm.r[slot], s = sm.s[slot], w = sm.w[slot];
-                const float pv = r * inv + fb * __ldcg(W.p + q);  // p_i = u_i + beta p_{i-1}
-                const float sn = w + fb * s;
-                const float rn = r - fa * sn;
-                const float un = sm.u[slot];
-                const float wn = stencil(sm.u, slot, cd);  // w_{i+1} = A u_{i+1}
+                return d;
+            },
+            [&](const IterData& d) {
+                const float sn = d.w + fb * d.s;  // s_i
+                const float rn = d.r - fa * sn;   // r_{i+1}
+                return rn * inv_diag<JACOBI>(d.code);  // u_{i+1} = M r_{i+1}
+            },
+            [&](uint32_t q, const IterData& d, float um1, float u0, float u1, const float* plane, int slot) {
+                const float pv = d.r * inv_diag<JACOBI>(d.code) + fb * d.p;  // p_i = u_i + beta p_{i-1}
+                const float sn = d.w + fb * d.s;
+                const float rn = d.r - fa * sn;
+                const float wn = stencil(d.code, u0, um1, u1, plane, slot);  // w_{i+1} = A u_{i+1}
                 W.p[q] = pv;
-                e[q] = __ldcg(e + q) + fa * pv;
+                e[q] = d.e + fa * pv;
                 Rn[q] = rn;
                 Sn[q] = sn;
                 Wn[q] = wn;
-                loc[0] += static_cast<T>(rn) * static_cast<T>(un);
-                loc[1] += static_cast<T>(wn) * static_cast<T>(un);
+                loc[0] += static_cast<T>(rn) * static_cast<T>(u0);
+                loc[1] += static_cast<T>(wn) * static_cast<T>(u0);
                 loc[2] += static_cast<T>(rn) * static_cast<T>(rn);
-            }
-            __syncthreads();
-        }
+            });
         const bool ok = sync_sums(loc, sums);
         cur ^= 1;
         return ok;
     };
 
     // ------------------------------------------------------------ FP64 accumulation and true residual
-    auto accumulate = [&]() {  // x64 (+)= e, e = 0
-        for (int br = blockIdx.x; br < B.count; br += gridDim.x) {
-            int x0, y0, z0;
-            brick_origin(B, br, x0, y0, z0);
-            for (int c = threadIdx.x; c < kBrick; c += kThreads) {
-                int slot;
-                uint32_t q;
-                if (!own_cell(P, x0, y0, z0, c, slot, q)) continue;
-                W.x64[q] = (passes == 1 && !S.warm_start ? 0.0 : W.x64[q]) + static_cast<double>(__ldcg(e + q));
-            }
-        }
+    const uint32_t gtid = blockIdx.x * kThreads + threadIdx.x, gstride = gridDim.x * kThreads;
+    auto accumulate = [&]() {  // x64 (+)= e
+        const bool fresh = passes == 1 && !S.warm_start;
+        for (uint32_t q = gtid; q < P.n; q += gstride) W.x64[q] = (fresh ? 0.0 : W.x64[q]) + static_cast<double>(__ldcg(e + q));
     };
-    auto true_residual = [&](double sums[4]) -> bool {  // R[cur] = b - A x64 (FP64), returns ||r||^2
-        double* tile = reinterpret_cast<double*>(smem_raw);  // kTile doubles fit in the r/s/w arrays
+    auto true_residual = [&](double sums[4]) -> bool {  // R[cur] = b - A x64 (FP64)
         double loc[4] = {0, 0, 0, 0};
-        for (int br = blockIdx.x; br < B.count; br += gridDim.x) {
-            int x0, y0, z0;
-            brick_origin(B, br, x0, y0, z0);
-            for (int t = threadIdx.x; t < kTile; t += kThreads) {
-                uint32_t q;
-                double v = 0.0;
-                uint16_t cd = 0;
-                if (tile_cell(P, x0, y0, z0, t, q)) {
-                    v = __ldcg(W.x64 + q);
-                    cd = __ldg(codes + q);
+        float* Rc = W.r[cur];
+        march<double, X64Data>(
+            P, C, ring_d,
+            [&](bool ok, uint32_t q, bool) {
+                X64Data d{0.0, 0};
+                if (ok) {
+                    d.v = __ldcg(W.x64 + q);
+                    d.code = __ldg(codes + q);
                 }
-                tile[t] = v;
-                sm.code[t] = cd;
-            }
-            __syncthreads();
-            for (int c = threadIdx.x; c < kBrick; c += kThreads) {
-                int slot;
-                uint32_t q;
-                if (!own_cell(P, x0, y0, z0, c, slot, q)) continue;
-                const double rv = static_cast<double>(__ldg(b + q)) - stencil(tile, slot, sm.code[slot]);
-                W.r[cur][q] = static_cast<float>(rv);
+                return d;
+            },
+            [&](const X64Data& d) { return d.v; },
+            [&](uint32_t q, const X64Data& d, double um1, double u0, double u1, const double* plane, int slot) {
+                const double rv = static_cast<double>(__ldg(b + q)) - stencil(d.code, u0, um1, u1, plane, slot);
+                Rc[q] = static_cast<float>(rv);
                 loc[0] += rv * rv;
-            }
-            __syncthreads();
-        }
-        const bool ok = barrier_allreduce<double>(ctl, parity, loc, sums);
-        parity ^= 1;
+            });
+        const bool ok = barrier_allreduce<double>(ctl, phase, loc, sums);
         if (!ok) aborted = true;
         return ok;
     };
@@ -379,8 +329,8 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const __grid_constant_
     // ------------------------------------------------------------ setup
     T sums[4] = {0, 0, 0, 0};
     if (S.warm_start && ir) {
-        // x64 was seeded by the host (from the previous pressure); e = 0, r0 = b - A x64
-        for (uint32_t q = blockIdx.x * kThreads + threadIdx.x; q < P.n; q += gridDim.x * kThreads) e[q] = 0.0f;
+        // x64 holds the previous solution: e = 0, r0 = b - A x64
+        for (uint32_t q = gtid; q < P.n; q += gstride) e[q] = 0.0f;
         double ds[4];
         if (true_residual(ds)) start_pass(W.r[cur], false, sums);
     } else {
@@ -394,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const __grid_constant_
         status = SMOKE_B200_SOLVE_BARRIER_TIMEOUT;
     } else if (!(bb > T(0))) {
         // b = 0: the solution is 0
-        for (uint32_t q = blockIdx.x * kThreads + threadIdx.x; q < P.n; q += gridDim.x * kThreads) {
+        for (uint32_t q = gtid; q < P.n; q += gstride) {
             x[q] = 0.0f;
             if (ir) W.x64[q] = 0.0;
         }
@@ -472,7 +422,10 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const __grid_constant_
             // FP64: x64 += e, then r = b - A x64
             accumulate();
             T none[4] = {0, 0, 0, 0}, dummy[4];
-            if (!sync_sums(none, dummy)) break;
+            if (!barrier_allreduce<T>(ctl, phase, none, dummy, false)) {
+                aborted = true;
+                break;
+            }
             double ds[4];
             if (!true_residual(ds)) break;
             true_rel = sqrt(ds[0] / static_cast<double>(bb));
@@ -493,8 +446,8 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const __grid_constant_
         }
         if (aborted) status = SMOKE_B200_SOLVE_BARRIER_TIMEOUT;
         if (ir && !aborted) {
-            // the FP32 pressure is the rounded FP64 solution
-            for (uint32_t q = blockIdx.x * kThreads + threadIdx.x; q < P.n; q += gridDim.x * kThreads) x[q] = static_cast<float>(W.x64[q]);
+            // the FP32 pressure is the rounded FP64 solution (x64 is complete: the last barrier followed its writes)
+            for (uint32_t q = gtid; q < P.n; q += gstride) x[q] = static_cast<float>(W.x64[q]);
         }
     }
 
@@ -514,37 +467,37 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(const __grid_constant_
 template <bool J, typename T>
 cudaError_t launch_one(const StepParams& P, const PcgSettings& S, const uint16_t* codes, const float* b, float* x, PcgWork work, PcgControl* ctl, cudaStream_t s) {
     static int max_blocks = 0;
-    const size_t smem = sizeof(Smem);
     if (max_blocks == 0) {
         int dev = 0, sms = 0, per_sm = 0;
-        cudaError_t e = cudaFuncSetAttribute(pcg_kernel<J, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        if (e == cudaSuccess) e = cudaGetDevice(&dev);
+        cudaError_t e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<J, T>, kThreads, smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<J, T>, kThreads, 0);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) return cudaErrorLaunchOutOfResources;
         max_blocks = sms * per_sm;
         if (max_blocks > kPcgMaxBlocks) max_blocks = kPcgMaxBlocks;
     }
-    Bricks B{};
-    B.nbx = (P.nx + BX - 1) / BX;
-    B.nby = (P.ny + BY - 1) / BY;
-    const int nbz = (P.nz + BZ - 1) / BZ;
-    B.count = B.nbx * B.nby * nbz;
-    const int blocks = B.count < max_blocks ? B.count : max_blocks;
-    cudaError_t e = cudaMemsetAsync(ctl, 0, 4 * sizeof(unsigned int), s);
+    Columns C{};
+    C.ncx = (P.nx + CX - 1) / CX;
+    C.ncy = (P.ny + CY - 1) / CY;
+    C.total = static_cast<uint32_t>(C.ncx) * C.ncy * P.nz;
+    // at least ~8 planes per block, so the two-plane prologue of a segment stays a small share of its work
+    uint32_t want = C.total / 8u;
+    if (want < 1u) want = 1u;
+    const int blocks = static_cast<int>(want < static_cast<uint32_t>(max_blocks) ? want : static_cast<uint32_t>(max_blocks));
+    cudaError_t e = cudaMemsetAsync(ctl, 0, kPcgControlResetBytes, s);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(blocks);
     cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = smem;
+    cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, pcg_kernel<J, T>, P, S, B, codes, b, x, work, ctl);
+    return cudaLaunchKernelEx(&cfg, pcg_kernel<J, T>, P, S, C, codes, b, x, work, ctl);
 }
 
 }  // namespace

@@ -57,6 +57,7 @@ LAYOUT_F32_3D_SOA3 = 1
 # extension enums (smoke_b200_ext.h)
 SOLVER_FIXED_CG = 0
 SOLVER_JACOBI_PCG = 1
+SOLVER_MG_FCG = 2
 REDUCTION_FP32 = 0
 REDUCTION_FP64 = 1
 SOLVE_CONVERGED = 0
