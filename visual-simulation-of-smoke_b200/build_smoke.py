@@ -18,7 +18,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CU_SOURCES = ["step_kernels.cu", "pcg.cu", "mgpcg.cu", "noalloc.cu"]
 CPP_SOURCES = ["context.cpp"]
-HEADERS = ["smoke_device.cuh", "launch.h", "grid_sync.cuh"]
+HEADERS = ["smoke_device.cuh", "launch.h", "grid_sync.cuh", "march.cuh"]
 INCLUDES = [os.path.join(ROOT, "include"), CSRC]
 
 NVCC_FLAGS = [

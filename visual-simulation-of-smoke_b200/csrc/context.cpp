@@ -116,6 +116,7 @@ struct SmokeSimulationContext_t {
 
     SmokeB200SolverDesc solver{SMOKE_B200_SOLVER_FIXED_CG, SMOKE_B200_REDUCTION_FP32, 500, 1.0e-5f, 0, 0};
     PcgLaunchShape pcg_shape{};
+    bool profile_solver = false;
     bool views_stale = false;
     bool stepped = false;
 
@@ -202,6 +203,7 @@ struct SmokeSimulationContext_t {
         mg_work.p[1] = pcg.s[1];
         mg_work.q = pcg.w[1];
         mg_work.e = pcg.e;
+        mg_work.r_alt = pcg.p;
         mg_work.x64 = pcg.x64;
     }
 
@@ -231,6 +233,7 @@ struct SmokeSimulationContext_t {
         S.tolerance = solver.tolerance;
         S.refinement = fixed ? 0 : static_cast<int32_t>(solver.refinement);
         S.warm_start = solver.warm_start ? 1 : 0;
+        S.profile = profile_solver ? 1 : 0;
         return S;
     }
 
@@ -522,6 +525,24 @@ SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext c) {
     return guarded([&] {
         c->enqueue_solve(c->stream);
         c->stepped = true;
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+SmokeSimulationResult smoke_b200_profile_solver_cuda(SmokeSimulationContext c, uint32_t enable, uint64_t* out_phase_ns, uint32_t count) {
+    if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        if (out_phase_ns != nullptr && count > 0) {
+            unsigned long long ns[kSolverPhases] = {};
+            check(cudaMemcpyAsync(ns, c->control->phase_ns, sizeof(ns), cudaMemcpyDeviceToHost, c->stream), "read solver profile");
+            check(cudaStreamSynchronize(c->stream), "read solver profile");
+            for (uint32_t k = 0; k < count && k < static_cast<uint32_t>(kSolverPhases); ++k) out_phase_ns[k] = ns[k];
+        }
+        const bool want = enable != 0;
+        if (want != c->profile_solver) {
+            c->profile_solver = want;
+            c->capture_step_graph();
+        }
         return SMOKE_SIMULATION_RESULT_OK;
     });
 }

@@ -71,7 +71,7 @@ struct PcgSettings {
     float tolerance;
     int32_t refinement;      // extra passes on the FP64 true residual
     int32_t warm_start;      // start from x instead of 0
-    int32_t reserved;
+    int32_t profile;         // 1: record wall time per solver phase in PcgControl::phase_ns
 };
 
 struct PcgStatusDevice {
@@ -89,6 +89,7 @@ struct PcgStatusDevice {
 // contend less) and the status of the last solve. Zeroed (up to `status`) before every launch.
 constexpr int kPcgMaxBlocks = 148 * 16;
 constexpr int kPcgSumCopies = 8;
+constexpr int kSolverPhases = 8;
 struct PcgControl {
     unsigned int bar;
     unsigned int pad0;
@@ -97,6 +98,7 @@ struct PcgControl {
     unsigned int pad2[28];
     double totals[3][kPcgSumCopies][16];  // 4 sums per copy, one 128-byte line per copy
     PcgStatusDevice status;
+    unsigned long long phase_ns[kSolverPhases];  // wall time per solver phase (when profiling is on)
 };
 constexpr size_t kPcgControlResetBytes = offsetof(PcgControl, status);
 
@@ -140,6 +142,7 @@ struct MgWork {
     float* p[2];
     float* q;
     float* e;
+    float* r_alt;  // second residual buffer: the update pass reads one and writes the other
     double* x64;
 };
 // Level extents and the number of grid-wide levels for a fine grid.

@@ -18,6 +18,7 @@
 // restart from the FP64 residual b - A x64, as in pcg.cu.
 #include "grid_sync.cuh"
 #include "launch.h"
+#include "march.cuh"
 #include "smoke_b200_ext.h"
 
 namespace smoke_b200 {
@@ -75,6 +76,18 @@ __device__ __forceinline__ float apply_stencil(const MgLevel& L, uint32_t q, uin
     return acc;
 }
 
+// Masked stencil on the march's ring plane: in-plane neighbours from the plane, -z/+z from registers.
+__device__ __forceinline__ float zstencil(uint16_t code, float u0, float um1, float u1, const float* plane, int slot) {
+    float acc = diagf(code) * u0;
+    if (code & 1u) acc -= plane[slot - 1];
+    if (code & 2u) acc -= plane[slot + 1];
+    if (code & 4u) acc -= plane[slot - zmarch::PX];
+    if (code & 8u) acc -= plane[slot + zmarch::PX];
+    if (code & 16u) acc -= um1;
+    if (code & 32u) acc -= u1;
+    return acc;
+}
+
 __device__ __forceinline__ bool wrap_c(int& v, int n, int per) {
     if (v >= 0 && v < n) return true;
     if (!per) return false;
@@ -83,11 +96,11 @@ __device__ __forceinline__ bool wrap_c(int& v, int n, int per) {
     return true;
 }
 
-// Cell-centred trilinear prolongation of coarse level C's correction zp at fine cell (x, y, z).
+// Cell-centred trilinear prolongation of coarse level C's final correction (C.t) at fine cell (x, y, z).
 __device__ __forceinline__ float prolong(const MgLevel& C, const int* fper, int x, int y, int z) {
     const int X = x >> 1, Y = y >> 1, Z = z >> 1;
     const int sx = (x & 1) ? 1 : -1, sy = (y & 1) ? 1 : -1, sz = (z & 1) ? 1 : -1;
-    const float parent = C.zp[lidx(C, X, Y, Z)];
+    const float parent = C.t[lidx(C, X, Y, Z)];
     float acc = 0.0f;
 #pragma unroll
     for (int k = 0; k < 2; ++k)
@@ -101,7 +114,7 @@ __device__ __forceinline__ float prolong(const MgLevel& C, const int* fper, int 
                     int cx = X + i * sx, cy = Y + j * sy, cz = Z + k * sz;
                     if (wrap_c(cx, C.nx, fper[0]) && wrap_c(cy, C.ny, fper[1]) && wrap_c(cz, C.nz, fper[2])) {
                         const uint32_t cq = lidx(C, cx, cy, cz);
-                        if (C.fluid[cq]) v = C.zp[cq];
+                        if (C.fluid[cq]) v = C.t[cq];
                     }
                 }
                 acc += w * v;
@@ -138,75 +151,87 @@ __device__ void restrict_pass(const MgHierarchy& H, int l, uint32_t first, uint3
     }
 }
 
-// Up, part 1: t = zp + P(z_coarse) on level l (zero on non-fluid cells; on level 0 also on the anchor).
-__device__ void prolong_pass(const MgHierarchy& H, int l, int32_t anchor, uint32_t first, uint32_t stride) {
+// Block-level up pass on level l (block 0 only): zp += P(t_{l+1}), then t = zp + w D^-1 (r - A zp).
+__device__ void block_up(const MgHierarchy& H, int l) {
     const MgLevel& F = H.L[l];
     const MgLevel& C = H.L[l + 1];
-    for (uint32_t q = first; q < F.n; q += stride) {
+    for (uint32_t q = threadIdx.x; q < F.n; q += zmarch::kThreads) {
         float v = 0.0f;
-        if (F.fluid[q] && !(l == 0 && static_cast<int32_t>(q) == anchor)) {
+        if (F.fluid[q]) {
             int x, y, z;
             lxyz(F, q, x, y, z);
             v = F.zp[q] + prolong(C, H.fper, x, y, z);
         }
+        F.zp[q] = v;
+    }
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < F.n; q += zmarch::kThreads) {
+        float v = 0.0f;
+        if (F.fluid[q]) {
+            const uint16_t code = F.code[q];
+            const float s0 = F.zp[q];
+            v = s0 + kOmega * (F.r[q] - apply_stencil(F, q, code, s0, [&](uint32_t nb) { return F.zp[nb]; })) / diagf(code);
+        }
         F.t[q] = v;
     }
+    __syncthreads();
 }
 
-// Up, part 2: post-smooth zp = t + w D^-1 (r - A t) on level l. On level 0 the result is the preconditioned residual,
-// and the partial sums (z, r) and (z, q) are accumulated.
-template <typename T>
-__device__ void smooth_pass(const MgHierarchy& H, int l, int32_t anchor, const float* q_prev, uint32_t first, uint32_t stride, T& zr, T& zq) {
-    const MgLevel& F = H.L[l];
-    for (uint32_t q = first; q < F.n; q += stride) {
-        float v = 0.0f;
-        if (F.fluid[q] && !(l == 0 && static_cast<int32_t>(q) == anchor)) {
-            const uint16_t code = F.code[q];
-            const float tq = F.t[q];
-            const float at = apply_stencil(F, q, code, tq, [&](uint32_t nb) { return F.t[nb]; });
-            v = tq + kOmega * (F.r[q] - at) / diagf(code);
-        }
-        F.zp[q] = v;
-        if (l == 0) {
-            zr += static_cast<T>(v) * static_cast<T>(F.r[q]);
-            zq += static_cast<T>(v) * static_cast<T>(q_prev[q]);
-        }
-    }
-}
-
-// Coarsest level: Jacobi sweeps from zero, ping-pong between zp and t, result in zp.
-__device__ void coarsest_solve(const MgLevel& L, uint32_t first, uint32_t stride, bool block_only) {
-    for (uint32_t q = first; q < L.n; q += stride) L.zp[q] = L.fluid[q] ? kOmega * L.r[q] / diagf(L.code[q]) : 0.0f;
+// Coarsest level (block 0 only): Jacobi sweeps from zero, ping-pong between zp and t, result in t.
+__device__ void coarsest_solve(const MgLevel& L) {
+    for (uint32_t q = threadIdx.x; q < L.n; q += zmarch::kThreads) L.t[q] = L.fluid[q] ? kOmega * L.r[q] / diagf(L.code[q]) : 0.0f;
     for (int sweep = 0; sweep < kCoarsestSweeps; ++sweep) {
-        if (block_only) __syncthreads();
-        float* src = (sweep & 1) ? L.t : L.zp;
-        float* dst = (sweep & 1) ? L.zp : L.t;
-        for (uint32_t q = first; q < L.n; q += stride) {
+        __syncthreads();
+        float* src = (sweep & 1) ? L.zp : L.t;
+        float* dst = (sweep & 1) ? L.t : L.zp;
+        for (uint32_t q = threadIdx.x; q < L.n; q += zmarch::kThreads) {
             float v = 0.0f;
             if (L.fluid[q]) {
                 const uint16_t code = L.code[q];
-                const float s = src[q];
-                v = s + kOmega * (L.r[q] - apply_stencil(L, q, code, s, [&](uint32_t nb) { return src[nb]; })) / diagf(code);
+                const float s0 = src[q];
+                v = s0 + kOmega * (L.r[q] - apply_stencil(L, q, code, s0, [&](uint32_t nb) { return src[nb]; })) / diagf(code);
             }
             dst[q] = v;
         }
     }
-    if (block_only) __syncthreads();
+    __syncthreads();  // kCoarsestSweeps is even: the result is in t
 }
+static_assert(kCoarsestSweeps % 2 == 0, "the coarsest sweeps must end in t");
+
+__device__ __forceinline__ float diag_safe(uint16_t code) {
+    const float d = diagf(code);
+    return d > 0.0f ? d : 1.0f;
+}
+
+struct UpdData {  // level-0 update + restriction pass
+    float r, q, p, e;
+    uint16_t code;
+};
+struct ProData {  // prolongation + smoothing pass
+    float t, r, qp;
+    uint16_t code;
+};
+struct PqData {  // p / q pass
+    float z, p, r;
+    uint16_t code;
+};
 
 template <typename T>
 __device__ __forceinline__ bool finite3(T a, T b, T c) { return isfinite(a) && isfinite(b) && isfinite(c); }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 2) mgfcg_kernel(const __grid_constant__ StepParams P, const PcgSettings S, const __grid_constant__ MgHierarchy H, const float* __restrict__ b, float* x, MgWork W, const int32_t* anchor_ptr, PcgControl* ctl) {
+__global__ void __launch_bounds__(zmarch::kThreads, 2) mgfcg_kernel(const __grid_constant__ StepParams P, const PcgSettings S, const __grid_constant__ MgHierarchy H, const float* __restrict__ b, float* x, MgWork W, const int32_t* anchor_ptr, PcgControl* ctl) {
+    __shared__ __align__(16) float ring[3][zmarch::kPlane];
     const MgLevel& L0 = H.L[0];
+    const MgLevel& L1 = H.L[1];
     const uint32_t n = L0.n;
-    const uint32_t gfirst = blockIdx.x * kThreads + threadIdx.x, gstride = gridDim.x * kThreads;
+    const uint32_t gfirst = blockIdx.x * zmarch::kThreads + threadIdx.x, gstride = gridDim.x * zmarch::kThreads;
     const int32_t anchor = *anchor_ptr;
     const bool ir = !S.fixed && S.refinement > 0;
     float* e = ir ? W.e : x;
-    float* r = L0.r;
-    float* z = L0.zp;
+    float* rb[2] = {L0.r, W.r_alt};  // residual, double-buffered across the update pass
+    int rc = 0;
+    float* Z = L0.t;  // the preconditioned residual
     unsigned phase = 0;
     int cur = 0;
     uint32_t status = SMOKE_B200_SOLVE_ITERATION_CAP;
@@ -214,55 +239,166 @@ __global__ void __launch_bounds__(kThreads, 2) mgfcg_kernel(const __grid_constan
     int it = 0, passes = 1;
     bool aborted = false;
     T none[4] = {0, 0, 0, 0}, dummy[4];
-
-    auto grid_barrier = [&]() -> bool {
-        if (!barrier_allreduce<T>(ctl, phase, none, dummy, false)) aborted = true;
-        return !aborted;
+    const int g = H.grid_levels;
+    // phase timing (block 0's timeline; blocks move in lock step between grid barriers)
+    const bool prof = S.profile && blockIdx.x == 0 && threadIdx.x == 0;
+    unsigned long long prof_acc[kSolverPhases] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long prof_last = prof ? global_ns() : 0;
+    auto mark = [&](int k) {
+        if (prof) {
+            const unsigned long long t = global_ns();
+            prof_acc[k] += t - prof_last;
+            prof_last = t;
+        }
     };
 
-    // One V-cycle on r -> z; returns the reduced (z, r) and (z, q_prev).
-    auto vcycle = [&](const float* q_prev, T& zr_out, T& zq_out) -> bool {
-        const int g = H.grid_levels;  // levels [0, g) are grid-wide; level g is the first with <= kMgBlockLevelCells
-        for (int l = 0; l < g; ++l) {
+    auto level_geom = [&](int l) { return zmarch::geom_of(H.L[l].nx, H.L[l].ny, H.L[l].nz, H.fper); };
+    auto level_cols = [&](int l) {
+        zmarch::Columns C{};
+        C.ncx = (H.L[l].nx + zmarch::CX - 1) / zmarch::CX;
+        C.ncy = (H.L[l].ny + zmarch::CY - 1) / zmarch::CY;
+        C.total = static_cast<uint32_t>(C.ncx) * C.ncy * H.L[l].nz;
+        return C;
+    };
+    auto grid_barrier = [&]() -> bool {
+        if (!gsync::barrier_allreduce<zmarch::kThreads, T>(ctl, phase, none, dummy, false)) aborted = true;
+        return !aborted;
+    };
+    auto reduce = [&](T loc[4], T out[4]) -> bool {
+        if (!gsync::barrier_allreduce<zmarch::kThreads, T>(ctl, phase, loc, out, true)) aborted = true;
+        return !aborted;
+    };
+    auto zero_l1r = [&]() {
+        for (uint32_t q = gfirst; q < L1.n; q += gstride) L1.r[q] = 0.0f;
+    };
+
+    // Level 0, pass 1: r -= alpha q, e += alpha p, pre-smooth (zp = w D^-1 r) and restrict the residual into L1.r
+    // (atomic adds of 1/2 res); partial ||r||^2.
+    auto update_restrict = [&](float fa, T& rr) {
+        const zmarch::MarchGeom G = level_geom(0);
+        const zmarch::Columns C = level_cols(0);
+        const float* pc = W.p[cur];
+        const float* r = rb[rc];
+        float* rn_out = rb[rc ^ 1];
+        zmarch::march<float, UpdData>(
+            G, C, ring,
+            [&](bool ok, uint32_t q, bool own, int, int, int) {
+                UpdData d{0.0f, 0.0f, 0.0f, 0.0f, 0};
+                if (ok) {
+                    d.r = r[q];
+                    d.q = W.q[q];
+                    d.code = L0.code[q];
+                    if (own) {
+                        d.p = pc[q];
+                        d.e = e[q];
+                    }
+                }
+                return d;
+            },
+            [&](const UpdData& d) { return kOmega * (d.r - fa * d.q) / diag_safe(d.code); },
+            [&](uint32_t q, const UpdData& d, float um1, float u0, float u1, const float* plane, int slot, int cx, int cy, int cz) {
+                const float rn = d.r - fa * d.q;
+                const float res = rn - zstencil(d.code, u0, um1, u1, plane, slot);
+                rn_out[q] = rn;
+                L0.zp[q] = u0;
+                e[q] = d.e + fa * d.p;
+                atomicAdd(L1.r + lidx(L1, cx >> 1, cy >> 1, cz >> 1), 0.5f * res);
+                rr += static_cast<T>(rn) * static_cast<T>(rn);
+            });
+        rc ^= 1;
+    };
+
+    // Level l: t = zp + P(t_{l+1}) (0 on non-fluid cells and the anchor), then out = t + w D^-1 (r - A t).
+    // Level 0 writes Z and accumulates (Z, r), (Z, q_prev); coarser levels write their t... through `dst`.
+    auto prolong_smooth = [&](int l, float* dst, T& zr, T& zq) {
+        const MgLevel& F = H.L[l];
+        const MgLevel& Cn = H.L[l + 1];
+        const float* rsrc = l == 0 ? rb[rc] : F.r;
+        const zmarch::MarchGeom G = level_geom(l);
+        const zmarch::Columns C = level_cols(l);
+        zmarch::march<float, ProData>(
+            G, C, ring,
+            [&](bool ok, uint32_t q, bool own, int cx, int cy, int cz) {
+                ProData d{0.0f, 0.0f, 0.0f, 0};
+                if (ok && F.fluid[q] && !(l == 0 && static_cast<int32_t>(q) == anchor)) {
+                    d.t = F.zp[q] + prolong(Cn, H.fper, cx, cy, cz);
+                    d.code = F.code[q];
+                    if (own) {
+                        d.r = rsrc[q];
+                        if (l == 0) d.qp = W.q[q];
+                    }
+                }
+                return d;
+            },
+            [&](const ProData& d) { return d.t; },
+            [&](uint32_t q, const ProData& d, float um1, float u0, float u1, const float* plane, int slot, int, int, int) {
+                const float v = d.code ? u0 + kOmega * (d.r - zstencil(d.code, u0, um1, u1, plane, slot)) / diagf(d.code) : 0.0f;
+                dst[q] = v;
+                if (l == 0) {
+                    zr += static_cast<T>(v) * static_cast<T>(d.r);
+                    zq += static_cast<T>(v) * static_cast<T>(d.qp);
+                }
+            });
+    };
+
+    // Level 0, pass 3: p = Z + beta p_old, q = A p; partials (p, q), (p, r). Clears L1.r for the next restriction.
+    auto pq_pass = [&](float fb, T& pq, T& pr) {
+        const zmarch::MarchGeom G = level_geom(0);
+        const zmarch::Columns C = level_cols(0);
+        const float* po = W.p[cur];
+        float* pn = W.p[cur ^ 1];
+        zmarch::march<float, PqData>(
+            G, C, ring,
+            [&](bool ok, uint32_t q, bool own, int, int, int) {
+                PqData d{0.0f, 0.0f, 0.0f, 0};
+                if (ok) {
+                    d.z = Z[q];
+                    d.p = po[q];
+                    d.code = L0.code[q];
+                    if (own) d.r = rb[rc][q];
+                }
+                return d;
+            },
+            [&](const PqData& d) { return d.z + fb * d.p; },
+            [&](uint32_t q, const PqData& d, float um1, float u0, float u1, const float* plane, int slot, int, int, int) {
+                const float qv = zstencil(d.code, u0, um1, u1, plane, slot);
+                pn[q] = u0;
+                W.q[q] = qv;
+                pq += static_cast<T>(u0) * static_cast<T>(qv);
+                pr += static_cast<T>(u0) * static_cast<T>(d.r);
+            });
+        zero_l1r();
+    };
+
+    // The coarse part of a V-cycle: levels 1 .. coarsest, given L1.r; leaves L1.t.
+    auto coarse_cycle = [&]() -> bool {
+        for (int l = 1; l < g; ++l) {
             restrict_pass(H, l, gfirst, gstride);
             if (!grid_barrier()) return false;
         }
-        // levels g .. coarsest: block 0 only
+        mark(1);
         if (blockIdx.x == 0) {
             const int lc = H.levels - 1;
-            for (int l = g; l < lc; ++l) {
-                restrict_pass(H, l, threadIdx.x, kThreads);
+            for (int l = (g > 1 ? g : 1); l < lc; ++l) {
+                restrict_pass(H, l, threadIdx.x, zmarch::kThreads);
                 __syncthreads();
             }
-            coarsest_solve(H.L[lc], threadIdx.x, kThreads, true);
-            for (int l = lc - 1; l >= g; --l) {
-                prolong_pass(H, l, anchor, threadIdx.x, kThreads);
-                __syncthreads();
-                T a = 0, c = 0;
-                smooth_pass<T>(H, l, anchor, q_prev, threadIdx.x, kThreads, a, c);
-                __syncthreads();
-            }
+            coarsest_solve(H.L[lc]);
+            for (int l = lc - 1; l >= (g > 1 ? g : 1); --l) block_up(H, l);
         }
         if (!grid_barrier()) return false;
-        T zr = 0, zq = 0;
-        for (int l = g - 1; l >= 0; --l) {
-            prolong_pass(H, l, anchor, gfirst, gstride);
+        mark(2);
+        for (int l = g - 1; l >= 1; --l) {
+            T a = 0, c = 0;
+            prolong_smooth(l, H.L[l].t, a, c);
             if (!grid_barrier()) return false;
-            smooth_pass<T>(H, l, anchor, q_prev, gfirst, gstride, zr, zq);
-            if (l > 0 && !grid_barrier()) return false;
         }
-        T loc[4] = {zr, zq, 0, 0}, tot[4];
-        if (!barrier_allreduce<T>(ctl, phase, loc, tot)) {
-            aborted = true;
-            return false;
-        }
-        zr_out = tot[0];
-        zq_out = tot[1];
+        mark(3);
         return true;
     };
 
-    // ------------------------------------------------------------ setup: r = b (or b - A x64), e = 0, q = p = 0
-    T bb = 0, rr0 = 0;
+    // ------------------------------------------------------------ setup: r = b, e = q = p = 0, L1.r = 0
+    T bb = 0;
     {
         T loc[4] = {0, 0, 0, 0}, tot[4];
         for (uint32_t q = gfirst; q < n; q += gstride) {
@@ -272,36 +408,12 @@ __global__ void __launch_bounds__(kThreads, 2) mgfcg_kernel(const __grid_constan
             W.q[q] = 0.0f;
             W.p[0][q] = 0.0f;
             W.p[1][q] = 0.0f;
-            if (!(S.warm_start && ir)) r[q] = bv;
+            rb[0][q] = bv;
         }
-        if (barrier_allreduce<T>(ctl, phase, loc, tot)) bb = tot[0];
-        else aborted = true;
-        if (!aborted && S.warm_start && ir) {
-            T l2[4] = {0, 0, 0, 0};
-            for (uint32_t q = gfirst; q < n; q += gstride) {
-                const uint16_t code = L0.code[q];
-                const double ax = static_cast<double>(diagf(code)) * W.x64[q] - [&]() {
-                    double s = 0.0;
-                    const uint32_t mask = code & 63u;
-                    if (mask) {
-                        int cx, cy, cz;
-                        lxyz(L0, q, cx, cy, cz);
-                        for (int k = 0; k < 6; ++k)
-                            if (mask & (1u << k)) s += W.x64[lnbr(L0, q, cx, cy, cz, k)];
-                    }
-                    return s;
-                }();
-                const double rv = static_cast<double>(__ldg(b + q)) - ax;
-                r[q] = static_cast<float>(rv);
-                l2[0] += static_cast<T>(rv * rv);
-            }
-            if (barrier_allreduce<T>(ctl, phase, l2, tot)) rr0 = tot[0];
-            else aborted = true;
-        } else {
-            rr0 = bb;
-        }
+        zero_l1r();
+        if (reduce(loc, tot)) bb = tot[0];
     }
-    T rnorm2 = rr0;
+    T rnorm2 = bb;
 
     if (aborted) {
         status = SMOKE_B200_SOLVE_BARRIER_TIMEOUT;
@@ -311,12 +423,11 @@ __global__ void __launch_bounds__(kThreads, 2) mgfcg_kernel(const __grid_constan
             if (ir) W.x64[q] = 0.0;
         }
         rnorm2 = 0;
-        status = SMOKE_B200_SOLVE_CONVERGED;
-        if (!isfinite(bb)) status = SMOKE_B200_SOLVE_NOT_FINITE;
+        status = isfinite(bb) ? SMOKE_B200_SOLVE_CONVERGED : SMOKE_B200_SOLVE_NOT_FINITE;
         if (ir) true_rel = 0.0;
     } else {
         const T tol2 = static_cast<T>(S.tolerance) * static_cast<T>(S.tolerance) * bb;
-        T pass_rr0 = rr0;
+        T pass_rr0 = bb;
         for (;;) {  // refinement passes
             T target2 = tol2;
             if (ir) {
@@ -326,57 +437,16 @@ __global__ void __launch_bounds__(kThreads, 2) mgfcg_kernel(const __grid_constan
             }
             bool first = true;
             T alpha = 0, pq_prev = 1;
-            if (rnorm2 <= target2) status = SMOKE_B200_SOLVE_CONVERGED;
-            while (!(rnorm2 <= target2)) {
-                T zr, zq;
-                if (!vcycle(W.q, zr, zq)) break;
-                const T beta = first ? T(0) : -zq / pq_prev;
-                if (!isfinite(beta) || !isfinite(zr)) {
-                    status = SMOKE_B200_SOLVE_NOT_FINITE;
-                    break;
-                }
-                // pass A: p = z + beta p_old, q = A p, partials (p, q), (p, r)
-                const float fb = static_cast<float>(beta);
-                const float* po = W.p[cur];
-                float* pn = W.p[cur ^ 1];
-                T loc[4] = {0, 0, 0, 0}, tot[4];
-                for (uint32_t q = gfirst; q < n; q += gstride) {
-                    const uint16_t code = L0.code[q];
-                    const float pv = z[q] + fb * po[q];
-                    const float qv = apply_stencil(L0, q, code, pv, [&](uint32_t nb) { return z[nb] + fb * po[nb]; });
-                    pn[q] = pv;
-                    W.q[q] = qv;
-                    loc[0] += static_cast<T>(pv) * static_cast<T>(qv);
-                    loc[1] += static_cast<T>(pv) * static_cast<T>(r[q]);
-                }
-                if (!barrier_allreduce<T>(ctl, phase, loc, tot)) {
-                    aborted = true;
-                    break;
-                }
-                const T pq = tot[0], pr = tot[1];
-                if (!(pq > T(0)) || !isfinite(pr)) {
-                    status = isfinite(pq) ? SMOKE_B200_SOLVE_BREAKDOWN : SMOKE_B200_SOLVE_NOT_FINITE;
-                    break;
-                }
-                alpha = pr / pq;
-                const float fa = static_cast<float>(alpha);
-                // pass B: e += alpha p, r -= alpha q
-                T l2[4] = {0, 0, 0, 0};
-                for (uint32_t q = gfirst; q < n; q += gstride) {
-                    e[q] += fa * pn[q];
-                    const float rv = r[q] - fa * W.q[q];
-                    r[q] = rv;
-                    l2[0] += static_cast<T>(rv) * static_cast<T>(rv);
-                }
-                if (!barrier_allreduce<T>(ctl, phase, l2, tot)) {
-                    aborted = true;
-                    break;
-                }
+            for (;;) {
+                // pass 1 (alpha = 0 on the first round: only the pre-smoothing and restriction of r)
+                mark(6);
+                T rr = 0;
+                update_restrict(static_cast<float>(alpha), rr);
+                T loc[4] = {rr, 0, 0, 0}, tot[4];
+                if (!reduce(loc, tot)) break;
+                mark(0);
                 rnorm2 = tot[0];
-                ++it;
-                cur ^= 1;
-                pq_prev = pq;
-                first = false;
+                if (!first) ++it;
                 if (!isfinite(rnorm2)) {
                     status = SMOKE_B200_SOLVE_NOT_FINITE;
                     break;
@@ -389,9 +459,39 @@ __global__ void __launch_bounds__(kThreads, 2) mgfcg_kernel(const __grid_constan
                     status = SMOKE_B200_SOLVE_ITERATION_CAP;
                     break;
                 }
+                // V-cycle: coarse levels, then level 0's prolongation and post-smoothing into Z
+                if (!coarse_cycle()) break;
+                T zr = 0, zq = 0;
+                prolong_smooth(0, Z, zr, zq);
+                T l2[4] = {zr, zq, 0, 0};
+                if (!reduce(l2, tot)) break;
+                mark(4);
+                zr = tot[0];
+                zq = tot[1];
+                const T beta = first ? T(0) : -zq / pq_prev;
+                if (!isfinite(beta) || !isfinite(zr)) {
+                    status = SMOKE_B200_SOLVE_NOT_FINITE;
+                    break;
+                }
+                // pass 3: p, q
+                T pq = 0, pr = 0;
+                pq_pass(static_cast<float>(beta), pq, pr);
+                T l3[4] = {pq, pr, 0, 0};
+                if (!reduce(l3, tot)) break;
+                mark(5);
+                pq = tot[0];
+                pr = tot[1];
+                cur ^= 1;
+                if (!(pq > T(0)) || !isfinite(pr)) {
+                    status = isfinite(pq) ? SMOKE_B200_SOLVE_BREAKDOWN : SMOKE_B200_SOLVE_NOT_FINITE;
+                    break;
+                }
+                alpha = pr / pq;
+                pq_prev = pq;
+                first = false;
             }
             if (aborted || !ir) break;
-            // FP64: x64 += e, r = b - A x64
+            // FP64: x64 += e, r = b - A x64, e = q = 0, L1.r = 0
             const bool fresh = passes == 1 && !S.warm_start;
             for (uint32_t q = gfirst; q < n; q += gstride) W.x64[q] = (fresh ? 0.0 : W.x64[q]) + static_cast<double>(e[q]);
             if (!grid_barrier()) break;
@@ -407,11 +507,13 @@ __global__ void __launch_bounds__(kThreads, 2) mgfcg_kernel(const __grid_constan
                         if (mask & (1u << k)) ax -= W.x64[lnbr(L0, q, cx, cy, cz, k)];
                 }
                 const double rv = static_cast<double>(__ldg(b + q)) - ax;
-                r[q] = static_cast<float>(rv);
+                rb[rc][q] = static_cast<float>(rv);
                 e[q] = 0.0f;
+                W.q[q] = 0.0f;
                 dl[0] += rv * rv;
             }
-            if (!gsync::barrier_allreduce<kThreads, double>(ctl, phase, dl, dt)) {
+            zero_l1r();
+            if (!gsync::barrier_allreduce<zmarch::kThreads, double>(ctl, phase, dl, dt)) {
                 aborted = true;
                 break;
             }
@@ -433,6 +535,9 @@ __global__ void __launch_bounds__(kThreads, 2) mgfcg_kernel(const __grid_constan
             for (uint32_t q = gfirst; q < n; q += gstride) x[q] = static_cast<float>(W.x64[q]);
     }
 
+    mark(7);
+    if (prof)
+        for (int k = 0; k < kSolverPhases; ++k) ctl->phase_ns[k] = prof_acc[k];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         PcgStatusDevice st{};
         st.iterations = it;
@@ -513,7 +618,9 @@ cudaError_t launch_mg_one(const StepParams& P, const PcgSettings& S, const MgHie
         max_blocks = sms * per_sm;
         if (max_blocks > kPcgMaxBlocks) max_blocks = kPcgMaxBlocks;
     }
-    uint32_t want = (H.L[0].n + kThreads * 4 - 1) / (kThreads * 4);
+    // at least ~8 column-planes of level 0 per block (see march.cuh)
+    const uint32_t planes = zmarch::column_planes(zmarch::geom_of(H.L[0].nx, H.L[0].ny, H.L[0].nz, H.fper));
+    uint32_t want = planes / 8u;
     if (want < 1u) want = 1u;
     const int blocks = static_cast<int>(want < static_cast<uint32_t>(max_blocks) ? want : static_cast<uint32_t>(max_blocks));
     cudaError_t e = cudaMemsetAsync(ctl, 0, kPcgControlResetBytes, s);

@@ -21,6 +21,7 @@
 //  - every grid barrier waits at most kBarrierTimeoutNs, then raises an abort flag that makes all blocks leave; the
 //    host reads the outcome from the status block.
 #include "grid_sync.cuh"
+#include "march.cuh"
 #include "launch.h"
 #include "smoke_b200_ext.h"
 
@@ -28,133 +29,20 @@ namespace smoke_b200 {
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int CX = 32, CY = 8;
-constexpr int PX = CX + 2, PY = CY + 2;
-constexpr int kPlane = PX * PY;
-constexpr int kHaloSlots = kPlane - CX * CY;
-static_assert(kHaloSlots <= kThreads, "one halo slot per thread at most");
+using zmarch::kThreads;
+using zmarch::CX;
+using zmarch::CY;
+using zmarch::PX;
+using zmarch::kPlane;
+using zmarch::Columns;
+using zmarch::MarchGeom;
+using zmarch::march;
 using gsync::global_ns;
 using gsync::warp_sum;
 
 template <typename T>
 __device__ __forceinline__ bool barrier_allreduce(PcgControl* ctl, unsigned& phase, T local[4], T out[4], bool reduce = true) {
     return gsync::barrier_allreduce<kThreads, T>(ctl, phase, local, out, reduce);
-}
-
-struct Columns {
-    int ncx, ncy;
-    uint32_t total;  // column-planes: ncx * ncy * nz
-};
-
-__device__ __forceinline__ bool wrap_axis(int& v, int n, int periodic) {
-    if (v >= 0 && v < n) return true;
-    if (!periodic) return false;
-    v = wrapi(v, n);
-    return true;
-}
-
-// Per-thread geometry of one column: the thread's own slot, and (threads < kHaloSlots) one halo slot of the ring.
-struct ColumnGeo {
-    uint32_t own_off, halo_off;  // in-plane offsets (y * nx + x) of the cells loaded into the slots
-    int own_slot, halo_slot;
-    bool own_out;                // the own cell is inside the domain and produces output
-    bool own_load, halo_load;    // the slot maps to a cell (possibly across a periodic edge)
-};
-
-__device__ __forceinline__ ColumnGeo column_geo(const StepParams& P, int x0, int y0) {
-    ColumnGeo g;
-    const int tx = threadIdx.x % CX, ty = threadIdx.x / CX;
-    int gx = x0 + tx, gy = y0 + ty;
-    g.own_slot = (ty + 1) * PX + tx + 1;
-    g.own_out = gx < P.nx && gy < P.ny;
-    g.own_load = wrap_axis(gx, P.nx, P.fper[0]) && wrap_axis(gy, P.ny, P.fper[1]);
-    g.own_off = g.own_load ? static_cast<uint32_t>(gy) * P.nx + gx : 0u;
-    g.halo_load = false;
-    g.halo_slot = 0;
-    g.halo_off = 0;
-    if (threadIdx.x < kHaloSlots) {
-        const int h = threadIdx.x;
-        int hx, hy;
-        if (h < PX) {
-            hx = h - 1;
-            hy = -1;
-        } else if (h < 2 * PX) {
-            hx = h - PX - 1;
-            hy = CY;
-        } else if (h < 2 * PX + CY) {
-            hx = -1;
-            hy = h - 2 * PX;
-        } else {
-            hx = CX;
-            hy = h - 2 * PX - CY;
-        }
-        g.halo_slot = (hy + 1) * PX + hx + 1;
-        int lx = x0 + hx, ly = y0 + hy;
-        g.halo_load = wrap_axis(lx, P.nx, P.fper[0]) && wrap_axis(ly, P.ny, P.fper[1]);
-        g.halo_off = g.halo_load ? static_cast<uint32_t>(ly) * P.nx + lx : 0u;
-    }
-    return g;
-}
-
-// Offset of plane z (wrapped across a periodic edge); false outside the domain.
-__device__ __forceinline__ bool plane_base(const StepParams& P, int z, uint32_t& base) {
-    if (!wrap_axis(z, P.nz, P.fper[2])) return false;
-    base = static_cast<uint32_t>(z) * static_cast<uint32_t>(P.nx) * P.ny;
-    return true;
-}
-
-// March over every column segment of this block. For each plane z of a segment [za, zb):
-//   load(ok, q, own) -> Data       loads one slot's inputs (zero Data when !ok)
-//   ufn(Data) -> V                 the value whose stencil is taken
-//   own(q, Data, um1, u0, u1, plane, slot)   the own cell's work at plane z (um1/u1: its -z/+z values)
-// Planes of the ring are (z mod 3). One __syncthreads per plane step.
-template <typename V, typename Data, class Load, class UFn, class Own>
-__device__ __forceinline__ void march(const StepParams& P, const Columns& C, V (*ring)[kPlane], Load&& load, UFn&& ufn, Own&& own) {
-    const uint32_t a = static_cast<uint32_t>((static_cast<uint64_t>(blockIdx.x) * C.total) / gridDim.x);
-    const uint32_t b = static_cast<uint32_t>((static_cast<uint64_t>(blockIdx.x + 1) * C.total) / gridDim.x);
-    const int nz = P.nz;
-    uint32_t L = a;
-    while (L < b) {
-        const int col = static_cast<int>(L / static_cast<uint32_t>(nz));
-        const int za = static_cast<int>(L - static_cast<uint32_t>(col) * nz);
-        const int zb = za + static_cast<int>(min(static_cast<uint32_t>(nz - za), b - L));
-        L += static_cast<uint32_t>(zb - za);
-        const ColumnGeo g = column_geo(P, (col % C.ncx) * CX, (col / C.ncx) * CY);
-        const bool halo = threadIdx.x < kHaloSlots;
-        auto fetch = [&](int z, Data& own_d, Data& halo_d) {
-            uint32_t base = 0;
-            const bool pz = plane_base(P, z, base);
-            own_d = load(pz && g.own_load, base + g.own_off, true);
-            if (halo) halo_d = load(pz && g.halo_load, base + g.halo_off, false);
-        };
-        Data om1, o0, o1, o2, h0, h1, h2, hm1;
-        fetch(za - 1, om1, hm1);
-        fetch(za, o0, h0);
-        fetch(za + 1, o1, h1);
-        V um1 = ufn(om1);
-        V u0 = ufn(o0);
-        ring[za % 3][g.own_slot] = u0;
-        if (halo) ring[za % 3][g.halo_slot] = ufn(h0);
-        for (int z = za; z < zb; ++z) {
-            if (z + 2 <= zb) fetch(z + 2, o2, h2);
-            const V u1 = ufn(o1);
-            ring[(z + 1) % 3][g.own_slot] = u1;
-            if (halo) ring[(z + 1) % 3][g.halo_slot] = ufn(h1);
-            __syncthreads();
-            if (g.own_out) {
-                uint32_t base = 0;
-                plane_base(P, z, base);
-                own(base + g.own_off, o0, um1, u0, u1, ring[z % 3], g.own_slot);
-            }
-            um1 = u0;
-            u0 = u1;
-            o0 = o1;
-            o1 = o2;
-            h1 = h2;
-        }
-        __syncthreads();
-    }
 }
 
 template <bool JACOBI>
@@ -196,6 +84,7 @@ __device__ __forceinline__ bool finite_all(T a, T b, T c) { return isfinite(a) &
 template <bool JACOBI, typename T>
 __global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ StepParams P, const PcgSettings S, const Columns C, const uint16_t* __restrict__ codes, const float* __restrict__ b, float* x, PcgWork W, PcgControl* ctl) {
     __shared__ __align__(16) double ring_raw[3][kPlane];
+    const MarchGeom G = zmarch::geom_of(P.nx, P.ny, P.nz, P.fper);
     float(*ring_f)[kPlane] = reinterpret_cast<float(*)[kPlane]>(ring_raw);
     double(*ring_d)[kPlane] = ring_raw;
     const bool ir = !S.fixed && S.refinement > 0;  // FP64 accumulation + true-residual passes
@@ -221,8 +110,8 @@ __global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ S
         float* Wc = W.w[cur];
         float* Sc = W.s[cur];
         march<float, SrcData>(
-            P, C, ring_f,
-            [&](bool ok, uint32_t q, bool) {
+            G, C, ring_f,
+            [&](bool ok, uint32_t q, bool, int, int, int) {
                 SrcData d{0.0f, 0};
                 if (ok) {
                     d.v = __ldcg(src + q);
@@ -231,7 +120,7 @@ __global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ S
                 return d;
             },
             [&](const SrcData& d) { return d.v * inv_diag<JACOBI>(d.code); },
-            [&](uint32_t q, const SrcData& d, float um1, float u0, float u1, const float* plane, int slot) {
+            [&](uint32_t q, const SrcData& d, float um1, float u0, float u1, const float* plane, int slot, int, int, int) {
                 const float w = stencil(d.code, u0, um1, u1, plane, slot);
                 Rc[q] = d.v;
                 Wc[q] = w;
@@ -257,8 +146,8 @@ __global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ S
         float* Wn = W.w[cur ^ 1];
         T loc[4] = {0, 0, 0, 0};
         march<float, IterData>(
-            P, C, ring_f,
-            [&](bool ok, uint32_t q, bool own) {
+            G, C, ring_f,
+            [&](bool ok, uint32_t q, bool own, int, int, int) {
                 IterData d{0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0};
                 if (ok) {
                     d.r = __ldcg(Rc + q);
@@ -277,7 +166,7 @@ __global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ S
                 const float rn = d.r - fa * sn;   // r_{i+1}
                 return rn * inv_diag<JACOBI>(d.code);  // u_{i+1} = M r_{i+1}
             },
-            [&](uint32_t q, const IterData& d, float um1, float u0, float u1, const float* plane, int slot) {
+            [&](uint32_t q, const IterData& d, float um1, float u0, float u1, const float* plane, int slot, int, int, int) {
                 const float pv = d.r * inv_diag<JACOBI>(d.code) + fb * d.p;  // p_i = u_i + beta p_{i-1}
                 const float sn = d.w + fb * d.s;
                 const float rn = d.r - fa * sn;
@@ -306,8 +195,8 @@ __global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ S
         double loc[4] = {0, 0, 0, 0};
         float* Rc = W.r[cur];
         march<double, X64Data>(
-            P, C, ring_d,
-            [&](bool ok, uint32_t q, bool) {
+            G, C, ring_d,
+            [&](bool ok, uint32_t q, bool, int, int, int) {
                 X64Data d{0.0, 0};
                 if (ok) {
                     d.v = __ldcg(W.x64 + q);
@@ -316,7 +205,7 @@ __global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ S
                 return d;
             },
             [&](const X64Data& d) { return d.v; },
-            [&](uint32_t q, const X64Data& d, double um1, double u0, double u1, const double* plane, int slot) {
+            [&](uint32_t q, const X64Data& d, double um1, double u0, double u1, const double* plane, int slot, int, int, int) {
                 const double rv = static_cast<double>(__ldg(b + q)) - stencil(d.code, u0, um1, u1, plane, slot);
                 Rc[q] = static_cast<float>(rv);
                 loc[0] += rv * rv;

@@ -188,11 +188,53 @@ __device__ __forceinline__ uint32_t lin(const StepParams& P, int i, int j, int k
     else return cidx(P, i, j, k);
 }
 
+// Boundary-aware taps and interpolation with a runtime field kind. Only reached when some tap of a sample lies
+// outside the array (near the domain edge), so it is kept out of line: inlining the ghost rules into every tap of
+// every sampler made the advection kernels miss in the instruction cache.
+__device__ __noinline__ inline float tap_rt(const float* __restrict__ f, int kind, int i, int j, int k, const StepParams& P) {
+    switch (kind) {
+    case 0: return face_tap_slow<0>(f, i, j, k, P);
+    case 1: return face_tap_slow<1>(f, i, j, k, P);
+    case 2: return face_tap_slow<2>(f, i, j, k, P);
+    case 3: return scalar_tap_slow(f, i, j, k, P, P.den, P.dper);
+    default: return scalar_tap_slow(f, i, j, k, P, P.tem, P.tper);
+    }
+}
+
+__device__ __noinline__ inline float sample_edge(const float* __restrict__ f, int kind, int cubic, int x0, int y0, int z0, float tx, float ty, float tz, const StepParams& P) {
+    if (!cubic) {
+        const float c000 = tap_rt(f, kind, x0, y0, z0, P), c100 = tap_rt(f, kind, x0 + 1, y0, z0, P);
+        const float c010 = tap_rt(f, kind, x0, y0 + 1, z0, P), c110 = tap_rt(f, kind, x0 + 1, y0 + 1, z0, P);
+        const float c001 = tap_rt(f, kind, x0, y0, z0 + 1, P), c101 = tap_rt(f, kind, x0 + 1, y0, z0 + 1, P);
+        const float c011 = tap_rt(f, kind, x0, y0 + 1, z0 + 1, P), c111 = tap_rt(f, kind, x0 + 1, y0 + 1, z0 + 1, P);
+        const float c00 = c000 + (c100 - c000) * tx;
+        const float c10 = c010 + (c110 - c010) * tx;
+        const float c01 = c001 + (c101 - c001) * tx;
+        const float c11 = c011 + (c111 - c011) * tx;
+        const float c0 = c00 + (c10 - c00) * ty;
+        const float c1 = c01 + (c11 - c01) * ty;
+        return c0 + (c1 - c0) * tz;
+    }
+    float zs[4];
+#pragma unroll 1
+    for (int dz = 0; dz < 4; ++dz) {
+        float ys[4];
+#pragma unroll 1
+        for (int dy = 0; dy < 4; ++dy) {
+            const int yy = y0 + dy - 1, zz = z0 + dz - 1;
+            ys[dy] = mono_cubic(tap_rt(f, kind, x0 - 1, yy, zz, P), tap_rt(f, kind, x0, yy, zz, P), tap_rt(f, kind, x0 + 1, yy, zz, P), tap_rt(f, kind, x0 + 2, yy, zz, P), tx);
+        }
+        zs[dz] = mono_cubic(ys[0], ys[1], ys[2], ys[3], ty);
+    }
+    return mono_cubic(zs[0], zs[1], zs[2], zs[3], tz);
+}
+
 // Samples field KIND at world position (x,y,z): periodic wrap of the position, conversion to grid coordinates
 // (cell-centred axes offset by -0.5, backend-cuda.cu:413-415, 505-507), then trilinear (8 taps) or tensor
-// monotone cubic (64 taps). When the tap box is inside the array the taps are plain loads.
+// monotone cubic (64 taps). When the tap box is inside the array the taps are plain loads (inline); otherwise
+// sample_edge applies the boundary rules.
 template <int KIND, bool CUBIC>
-__device__ inline float sample(const float* __restrict__ f, float x, float y, float z, const StepParams& P) {
+__device__ __forceinline__ float sample(const float* __restrict__ f, float x, float y, float z, const StepParams& P) {
     if (periodic_axis<KIND>(P, 0)) x = wrap_pos(x, P.nx, P.h);
     if (periodic_axis<KIND>(P, 1)) y = wrap_pos(y, P.ny, P.h);
     if (periodic_axis<KIND>(P, 2)) z = wrap_pos(z, P.nz, P.h);
@@ -206,64 +248,37 @@ __device__ inline float sample(const float* __restrict__ f, float x, float y, fl
     const float ty = gy - static_cast<float>(y0);
     const float tz = gz - static_cast<float>(z0);
     const int ex = P.nx + (KIND == 0) - 1, ey = P.ny + (KIND == 1) - 1, ez = P.nz + (KIND == 2) - 1;
+    const uint32_t sy = static_cast<uint32_t>(ex + 1);
+    const uint32_t sz = sy * static_cast<uint32_t>(ey + 1);
     if constexpr (!CUBIC) {
-        float c[8];
         // written so that saturated conversions (huge or infinite positions) cannot overflow the test
-        if (x0 >= 0 && x0 < ex && y0 >= 0 && y0 < ey && z0 >= 0 && z0 < ez) {
-            const uint32_t b = lin<KIND>(P, x0, y0, z0);
-            const uint32_t sy = static_cast<uint32_t>(ex + 1);
-            const uint32_t sz = sy * static_cast<uint32_t>(ey + 1);
-            c[0] = __ldg(f + b);
-            c[1] = __ldg(f + b + 1);
-            c[2] = __ldg(f + b + sy);
-            c[3] = __ldg(f + b + sy + 1);
-            c[4] = __ldg(f + b + sz);
-            c[5] = __ldg(f + b + sz + 1);
-            c[6] = __ldg(f + b + sz + sy);
-            c[7] = __ldg(f + b + sz + sy + 1);
-        } else {
-            c[0] = tap<KIND>(f, x0, y0, z0, P);
-            c[1] = tap<KIND>(f, x0 + 1, y0, z0, P);
-            c[2] = tap<KIND>(f, x0, y0 + 1, z0, P);
-            c[3] = tap<KIND>(f, x0 + 1, y0 + 1, z0, P);
-            c[4] = tap<KIND>(f, x0, y0, z0 + 1, P);
-            c[5] = tap<KIND>(f, x0 + 1, y0, z0 + 1, P);
-            c[6] = tap<KIND>(f, x0, y0 + 1, z0 + 1, P);
-            c[7] = tap<KIND>(f, x0 + 1, y0 + 1, z0 + 1, P);
-        }
-        const float c00 = c[0] + (c[1] - c[0]) * tx;
-        const float c10 = c[2] + (c[3] - c[2]) * tx;
-        const float c01 = c[4] + (c[5] - c[4]) * tx;
-        const float c11 = c[6] + (c[7] - c[6]) * tx;
+        if (!(x0 >= 0 && x0 < ex && y0 >= 0 && y0 < ey && z0 >= 0 && z0 < ez)) return sample_edge(f, KIND, 0, x0, y0, z0, tx, ty, tz, P);
+        const uint32_t b = lin<KIND>(P, x0, y0, z0);
+        const float c000 = __ldg(f + b), c100 = __ldg(f + b + 1);
+        const float c010 = __ldg(f + b + sy), c110 = __ldg(f + b + sy + 1);
+        const float c001 = __ldg(f + b + sz), c101 = __ldg(f + b + sz + 1);
+        const float c011 = __ldg(f + b + sz + sy), c111 = __ldg(f + b + sz + sy + 1);
+        const float c00 = c000 + (c100 - c000) * tx;
+        const float c10 = c010 + (c110 - c010) * tx;
+        const float c01 = c001 + (c101 - c001) * tx;
+        const float c11 = c011 + (c111 - c011) * tx;
         const float c0 = c00 + (c10 - c00) * ty;
         const float c1 = c01 + (c11 - c01) * ty;
         return c0 + (c1 - c0) * tz;
     } else {
-        const bool inside = x0 >= 1 && x0 <= ex - 2 && y0 >= 1 && y0 <= ey - 2 && z0 >= 1 && z0 <= ez - 2;
-        const uint32_t sy = static_cast<uint32_t>(ex + 1);
-        const uint32_t sz = sy * static_cast<uint32_t>(ey + 1);
+        if (!(x0 >= 1 && x0 <= ex - 2 && y0 >= 1 && y0 <= ey - 2 && z0 >= 1 && z0 <= ez - 2)) return sample_edge(f, KIND, 1, x0, y0, z0, tx, ty, tz, P);
+        const uint32_t base = lin<KIND>(P, x0 - 1, y0 - 1, z0 - 1);
         float zs[4];
 #pragma unroll
         for (int dz = 0; dz < 4; ++dz) {
             float ys[4];
 #pragma unroll
             for (int dy = 0; dy < 4; ++dy) {
-                float p[4];
-                if (inside) {
-                    const uint32_t b = lin<KIND>(P, x0 - 1, y0 + dy - 1, z0 + dz - 1);
-                    p[0] = __ldg(f + b);
-                    p[1] = __ldg(f + b + 1);
-                    p[2] = __ldg(f + b + 2);
-                    p[3] = __ldg(f + b + 3);
-                } else {
-#pragma unroll
-                    for (int dx = 0; dx < 4; ++dx) p[dx] = tap<KIND>(f, x0 + dx - 1, y0 + dy - 1, z0 + dz - 1, P);
-                }
-                ys[dy] = mono_cubic(p[0], p[1], p[2], p[3], tx);
+                const uint32_t b = base + dz * sz + dy * sy;
+                ys[dy] = mono_cubic(__ldg(f + b), __ldg(f + b + 1), __ldg(f + b + 2), __ldg(f + b + 3), tx);
             }
             zs[dz] = mono_cubic(ys[0], ys[1], ys[2], ys[3], ty);
         }
-        (void)sz;
         return mono_cubic(zs[0], zs[1], zs[2], zs[3], tz);
     }
 }
@@ -288,7 +303,7 @@ __device__ __forceinline__ bool blocked(float x, float y, float z, const uint8_t
 
 // Midpoint RK2 back-trace through the face velocities (u,v,w), trilinear samples; a blocked end point is
 // pulled back towards the start by 10 bisection steps (backend-cuda.cu:760-838).
-__device__ inline float3 trace_rk2(float sx, float sy, float sz, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const StepParams& P) {
+__device__ __noinline__ inline float3 trace_rk2(float sx, float sy, float sz, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const StepParams& P) {
     const float dt = P.dt;
     const float a0 = sample<0, false>(u, sx, sy, sz, P);
     const float b0 = sample<1, false>(v, sx, sy, sz, P);
