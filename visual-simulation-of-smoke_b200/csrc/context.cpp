@@ -153,7 +153,7 @@ struct SmokeSimulationContext_t {
                           &divergence, &fx, &fy, &fz, &pcg.r[0], &pcg.r[1], &pcg.s[0], &pcg.s[1], &pcg.w[0], &pcg.w[1], &pcg.p, &pcg.e})
             f32(p, n);
         slots.push_back({reinterpret_cast<void**>(&pcg.x64), n * sizeof(double)});
-        slots.push_back({reinterpret_cast<void**>(&codes), n * sizeof(uint16_t)});
+        slots.push_back({reinterpret_cast<void**>(&codes), (n + 2) * sizeof(uint16_t)});
         slots.push_back({reinterpret_cast<void**>(&occupancy), n});
         slots.push_back({reinterpret_cast<void**>(&fill_list), n * sizeof(FillEntry)});
         slots.push_back({reinterpret_cast<void**>(&fill_count), sizeof(uint32_t)});
@@ -163,7 +163,6 @@ struct SmokeSimulationContext_t {
         mg.levels = mg_level_count(P.nx, P.ny, P.nz);
         for (int a = 0; a < 3; ++a) mg.fper[a] = P.fper[a];
         int lx = P.nx, ly = P.ny, lz = P.nz;
-        mg.grid_levels = 0;
         for (int l = 0; l < mg.levels; ++l) {
             MgLevel& L = mg.L[l];
             L.nx = lx;
@@ -172,18 +171,23 @@ struct SmokeSimulationContext_t {
             L.n = static_cast<uint32_t>(lx) * ly * lz;
             L.div_nx = FastDiv(lx);
             L.div_slab = FastDiv(static_cast<uint32_t>(lx) * ly);
-            if (L.n > kMgBlockLevelCells) mg.grid_levels = l + 1;
             slots.push_back({reinterpret_cast<void**>(&L.fluid), L.n});
             if (l > 0) {
-                slots.push_back({reinterpret_cast<void**>(&L.code), L.n * sizeof(uint16_t)});
+                slots.push_back({reinterpret_cast<void**>(&L.code), (L.n + 2) * sizeof(uint16_t)});
                 for (float** p : {&L.r, &L.zp, &L.t}) slots.push_back({reinterpret_cast<void**>(p), L.n * sizeof(float)});
             }
             lx = (lx + 1) / 2;
             ly = (ly + 1) / 2;
             lz = (lz + 1) / 2;
         }
-        if (mg.grid_levels < 1) mg.grid_levels = 1;
-        if (mg.grid_levels > mg.levels - 1) mg.grid_levels = mg.levels - 1;
+        // block levels: the coarsest levels of at most kMgBlockLevelCells cells whose arrays fit kMgBlockBytes
+        mg.grid_levels = mg.levels - 1;
+        uint32_t block_words = 0;
+        for (int l = mg.levels - 1; l >= 1; --l) {
+            block_words += mg_block_words(mg.L[l].n);
+            if (mg.L[l].n > kMgBlockLevelCells || block_words * 4u > kMgBlockBytes) break;
+            mg.grid_levels = l;
+        }
         auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
         size_t total = 0;
         for (const Slot& s : slots) total += align(s.bytes);
@@ -219,7 +223,7 @@ struct SmokeSimulationContext_t {
     // The pressure solve of the selected mode on the context's right-hand side.
     void enqueue_solve(cudaStream_t s) {
         const PcgSettings S = pcg_settings();
-        if (solver.mode == SMOKE_B200_SOLVER_MG_FCG) check(launch_mgfcg(P, S, mg, rhs, pressure, mg_work, anchor, control, s), "pressure solve (multigrid FCG)");
+        if (solver.mode == SMOKE_B200_SOLVER_MG_FCG) check(launch_mgfcg(P, S, mg, rhs, pressure, mg_work, control, s), "pressure solve (multigrid FCG)");
         else check(launch_pcg(P, S, pcg_shape, codes, rhs, pressure, pcg, control, s), "pressure solve");
     }
 

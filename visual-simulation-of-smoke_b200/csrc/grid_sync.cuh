@@ -51,7 +51,8 @@ template <int THREADS, typename T>
 __device__ bool barrier_allreduce(PcgControl* ctl, unsigned& phase, T local[4], T out[4], bool reduce = true) {
     __shared__ T scratch[4][THREADS / 32];
     __shared__ int s_ok;
-    if (reduce) block_sum4<THREADS>(local, scratch);
+    if (reduce) block_sum4<THREADS>(local, scratch);  // its __syncthreads orders the block's earlier writes
+    else __syncthreads();
     const int slot = static_cast<int>(phase % 3u);
     if (threadIdx.x == 0) {
         if (reduce) {

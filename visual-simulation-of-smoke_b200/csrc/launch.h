@@ -121,12 +121,17 @@ struct PcgLaunchShape {
 // extent (rounding up). A coarse cell is fluid when any of its children is; every level's operator is the masked
 // 7-point stencil of its fluid cells (the fine rules without the anchor).
 constexpr int kMgMaxLevels = 12;
-constexpr uint32_t kMgBlockLevelCells = 4096;  // levels this small run inside one block
+constexpr uint32_t kMgBlockLevelCells = 512;   // levels this small may run inside one block, in shared memory
+constexpr uint32_t kMgBlockBytes = 16 * 1024;  // shared memory for those levels (3 floats + 1 code per cell)
+// Shared-memory words of one block-level level of n cells: r, zp, t and the 16-bit codes (padded pairs).
+__host__ __device__ constexpr uint32_t mg_block_words(uint32_t n) { return 3u * n + (n + 2u) / 2u; }
+// Bit of the operator code that marks a cell whose unknown is solved for (fluid; at level 0 also not the anchor).
+constexpr uint16_t kCodeActive = 1u << 12;
 struct MgLevel {
     int nx, ny, nz;
     uint32_t n;
     FastDiv div_nx, div_slab;
-    uint16_t* code;   // row codes (level 0: the fine operator's codes)
+    uint16_t* code;   // row codes (level 0: the fine operator's codes); arrays hold n + 2 entries
     uint8_t* fluid;   // 1 = fluid cell
     float* r;         // right-hand side / residual of the level (level 0: the solver residual)
     float* zp;        // correction (level 0: the preconditioned residual z)
@@ -134,7 +139,7 @@ struct MgLevel {
 };
 struct MgHierarchy {
     int levels;       // >= 2
-    int grid_levels;  // levels [0, grid_levels) run on the whole grid; coarser ones inside one block
+    int grid_levels;  // levels [0, grid_levels) run on the whole grid; coarser ones inside block 0's shared memory
     int fper[3];
     MgLevel L[kMgMaxLevels];
 };
@@ -150,7 +155,7 @@ int mg_level_count(int nx, int ny, int nz);
 // Builds level fluid masks and codes from the occupancy (after the fine codes and anchor exist).
 cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uint8_t* occ, cudaStream_t s);
 // Enqueues the control reset and the cooperative multigrid-preconditioned FCG solve of A x = b.
-cudaError_t launch_mgfcg(const StepParams& P, const PcgSettings& S, const MgHierarchy& H, const float* b, float* x, MgWork work, const int32_t* anchor, PcgControl* ctl, cudaStream_t s);
+cudaError_t launch_mgfcg(const StepParams& P, const PcgSettings& S, const MgHierarchy& H, const float* b, float* x, MgWork work, PcgControl* ctl, cudaStream_t s);
 
 // Picks the persistent grid (all blocks co-resident) for the current device.
 cudaError_t pcg_launch_shape(PcgLaunchShape* out);

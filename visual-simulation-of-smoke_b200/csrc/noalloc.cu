@@ -24,7 +24,7 @@ constexpr uint64_t align256(uint64_t v) { return (v + 255) & ~uint64_t(255); }
 // Scratch layout: operator codes, anchor, occupancy (used when the caller passes none), 8 FP32 CG vectors,
 // the FP64 solution accumulator, the solver control block.
 constexpr uint64_t kOffCodes = 0;
-constexpr uint64_t kOffAnchor = kOffCodes + align256(kNoAllocMaxCells * sizeof(uint16_t));
+constexpr uint64_t kOffAnchor = kOffCodes + align256((kNoAllocMaxCells + 2) * sizeof(uint16_t));  // codes carry 2 spare entries
 constexpr uint64_t kOffOcc = kOffAnchor + 256;
 constexpr uint64_t kOffVectors = kOffOcc + align256(kNoAllocMaxCells);
 constexpr uint64_t kVectorBytes = align256(kNoAllocMaxCells * sizeof(float));

@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(kThreads) stencil_code_kernel(const __grid_con
         mask |= 1u << e;
     }
     if (diag == 0) diag = 1;
-    codes[q] = static_cast<uint16_t>(mask | (diag << 8));
+    codes[q] = static_cast<uint16_t>(mask | (diag << 8) | kCodeActive);
 }
 
 // Nearest-fluid source of each solid cell (:1243-1290): first Chebyshev shell (radius 1, 2, ...) holding a fluid
