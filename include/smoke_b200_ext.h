@@ -95,13 +95,6 @@ SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimu
  * kernel launch on the context stream; the outcome is read with smoke_b200_get_solver_status_cuda. */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext context);
 
-/* Solver phase timing. enable = 1 makes every later solve record its wall time per phase (block 0's timeline
- * between grid barriers, nanoseconds); out_phase_ns (optional, `count` entries, up to 8) receives the phases of the
- * last solve (synchronises the context stream). Multigrid FCG phases: 0 residual update + level-0 restriction,
- * 1 coarse restrictions, 2 block-level coarse cycle, 3 coarse prolongation + smoothing, 4 level-0 prolongation +
- * smoothing, 5 search-direction pass, 6 refinement and setup, 7 exit. Re-captures the step graph when the flag changes. */
-SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_profile_solver_cuda(SmokeSimulationContext context, uint32_t enable, uint64_t* out_phase_ns, uint32_t count);
-
 /* Pressure solve that allocates nothing. No counterpart in the reference (which has no standalone solve and
  * allocates all its buffers with cudaMalloc when a context is created).
  *

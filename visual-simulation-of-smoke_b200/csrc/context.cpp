@@ -88,8 +88,10 @@ struct SmokeSimulationContext_t {
     cudaStream_t stream = nullptr;
     bool owns_stream = false;
     cudaStream_t capture_stream = nullptr;
+    cudaStream_t body_stream = nullptr;      // captures the bodies of the solver's graph loops
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t solve_exec = nullptr;    // the multigrid solve alone (solve_pressure / eager stages)
     void* arena = nullptr;
     size_t arena_bytes = 0;
     int fill_blocks = 0;
@@ -113,10 +115,10 @@ struct SmokeSimulationContext_t {
     PcgControl* control = nullptr;
     MgHierarchy mg{};
     MgWork mg_work{};
+    MgState* mg_state = nullptr;
 
     SmokeB200SolverDesc solver{SMOKE_B200_SOLVER_FIXED_CG, SMOKE_B200_REDUCTION_FP32, 500, 1.0e-5f, 0, 0};
     PcgLaunchShape pcg_shape{};
-    bool profile_solver = false;
     bool views_stale = false;
     bool stepped = false;
 
@@ -125,12 +127,16 @@ struct SmokeSimulationContext_t {
     void release() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        if (solve_exec) cudaGraphExecDestroy(solve_exec);
         exec = nullptr;
         graph = nullptr;
+        solve_exec = nullptr;
         if (arena) cudaFree(arena);
         arena = nullptr;
         if (capture_stream) cudaStreamDestroy(capture_stream);
         capture_stream = nullptr;
+        if (body_stream) cudaStreamDestroy(body_stream);
+        body_stream = nullptr;
         if (owns_stream && stream) cudaStreamDestroy(stream);
         stream = nullptr;
         owns_stream = false;
@@ -159,6 +165,7 @@ struct SmokeSimulationContext_t {
         slots.push_back({reinterpret_cast<void**>(&fill_count), sizeof(uint32_t)});
         slots.push_back({reinterpret_cast<void**>(&anchor), sizeof(int32_t)});
         slots.push_back({reinterpret_cast<void**>(&control), sizeof(PcgControl)});
+        slots.push_back({reinterpret_cast<void**>(&mg_state), sizeof(MgState)});
         // multigrid levels: level 0 shares the Jacobi solver's vectors; coarser levels get their own arrays
         mg.levels = mg_level_count(P.nx, P.ny, P.nz);
         for (int a = 0; a < 3; ++a) mg.fper[a] = P.fper[a];
@@ -203,11 +210,12 @@ struct SmokeSimulationContext_t {
         L0.r = pcg.r[0];
         L0.zp = pcg.r[1];
         L0.t = pcg.w[0];
+        mg_work.r[0] = pcg.r[0];
+        mg_work.r[1] = pcg.p;
         mg_work.p[0] = pcg.s[0];
         mg_work.p[1] = pcg.s[1];
         mg_work.q = pcg.w[1];
         mg_work.e = pcg.e;
-        mg_work.r_alt = pcg.p;
         mg_work.x64 = pcg.x64;
     }
 
@@ -220,11 +228,31 @@ struct SmokeSimulationContext_t {
         check(launch_mg_setup(P, mg, occupancy, stream), "multigrid levels");
     }
 
-    // The pressure solve of the selected mode on the context's right-hand side.
-    void enqueue_solve(cudaStream_t s) {
+    // The pressure solve of the selected mode on the context's right-hand side. The multigrid solve is a graph:
+    // recorded into the capture when `s` is capturing, else launched as the prebuilt solve graph.
+    void enqueue_solve(cudaStream_t s, bool capturing) {
         const PcgSettings S = pcg_settings();
-        if (solver.mode == SMOKE_B200_SOLVER_MG_FCG) check(launch_mgfcg(P, S, mg, rhs, pressure, mg_work, control, s), "pressure solve (multigrid FCG)");
-        else check(launch_pcg(P, S, pcg_shape, codes, rhs, pressure, pcg, control, s), "pressure solve");
+        if (solver.mode != SMOKE_B200_SOLVER_MG_FCG) {
+            check(launch_pcg(P, S, pcg_shape, codes, rhs, pressure, pcg, control, s), "pressure solve");
+            return;
+        }
+        if (!capturing) {
+            check(cudaGraphLaunch(solve_exec, s), "pressure solve (multigrid FCG graph)");
+            return;
+        }
+        MgSolveArgs A{};
+        A.H = mg;
+        A.W = mg_work;
+        A.b = rhs;
+        A.x = pressure;
+        A.ir = S.refinement > 0 ? 1 : 0;
+        A.e = A.ir ? mg_work.e : pressure;
+        A.st = mg_state;
+        A.warm = A.ir && S.warm_start ? 1 : 0;
+        A.max_iterations = S.max_iterations;
+        A.refinement = S.refinement < mg_max_refinement() ? S.refinement : mg_max_refinement();
+        A.tol = S.tolerance;
+        check(enqueue_mg_solve(A, S.fp64 != 0, &control->status, s, body_stream), "pressure solve (multigrid FCG)");
     }
 
     PcgSettings pcg_settings() const {
@@ -237,12 +265,11 @@ struct SmokeSimulationContext_t {
         S.tolerance = solver.tolerance;
         S.refinement = fixed ? 0 : static_cast<int32_t>(solver.refinement);
         S.warm_start = solver.warm_start ? 1 : 0;
-        S.profile = profile_solver ? 1 : 0;
         return S;
     }
 
     // Stages of one step, in the reference's order (backend-cuda.cu:2000-2057, views excluded).
-    void enqueue_stages(cudaStream_t s, uint32_t last_stage) {
+    void enqueue_stages(cudaStream_t s, uint32_t last_stage, bool capturing) {
         const ConstFaces solid{solid_vx, solid_vy, solid_vz};
         check(launch_vorticity(P, as_const(A), occupancy, wx, wy, wz, wmag, s), "vorticity");
         check(launch_cell_force(P, wx, wy, wz, wmag, density, temperature, force_x, force_y, force_z, occupancy, fx, fy, fz, s), "cell force");
@@ -251,7 +278,7 @@ struct SmokeSimulationContext_t {
         check(launch_advect_velocity(P, as_const(B), occupancy, solid, C, s), "advect velocity");
         if (last_stage < SMOKE_B200_STAGE_PRESSURE) return;
         check(launch_rhs(P, as_const(C), occupancy, anchor, rhs, s), "pressure rhs");
-        enqueue_solve(s);
+        enqueue_solve(s, capturing);
         if (last_stage < SMOKE_B200_STAGE_PROJECT) return;
         const PcgSettings S = pcg_settings();
         const double* p64 = (!S.fixed && S.refinement > 0) ? pcg.x64 : nullptr;
@@ -269,7 +296,7 @@ struct SmokeSimulationContext_t {
         graph = nullptr;
         check(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal), "begin step capture");
         try {
-            enqueue_stages(capture_stream, SMOKE_B200_STAGE_SCALARS);
+            enqueue_stages(capture_stream, SMOKE_B200_STAGE_SCALARS, true);
         } catch (...) {
             cudaGraph_t broken = nullptr;
             cudaStreamEndCapture(capture_stream, &broken);
@@ -278,6 +305,23 @@ struct SmokeSimulationContext_t {
         }
         check(cudaStreamEndCapture(capture_stream, &graph), "end step capture");
         check(cudaGraphInstantiate(&exec, graph, 0), "instantiate step graph");
+        if (solve_exec) cudaGraphExecDestroy(solve_exec);
+        solve_exec = nullptr;
+        if (solver.mode != SMOKE_B200_SOLVER_MG_FCG) return;
+        cudaGraph_t solve_graph = nullptr;
+        check(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal), "begin solve capture");
+        try {
+            enqueue_solve(capture_stream, true);
+        } catch (...) {
+            cudaGraph_t broken = nullptr;
+            cudaStreamEndCapture(capture_stream, &broken);
+            if (broken) cudaGraphDestroy(broken);
+            throw;
+        }
+        check(cudaStreamEndCapture(capture_stream, &solve_graph), "end solve capture");
+        const cudaError_t e = cudaGraphInstantiate(&solve_exec, solve_graph, 0);
+        cudaGraphDestroy(solve_graph);
+        check(e, "instantiate solve graph");
     }
 
     void materialise_views() {
@@ -327,6 +371,7 @@ SmokeSimulationResult smoke_simulation_create_context_cuda(const SmokeSimulation
             ctx->owns_stream = true;
         }
         check(cudaStreamCreateWithFlags(&ctx->capture_stream, cudaStreamNonBlocking), "create capture stream");
+        check(cudaStreamCreateWithFlags(&ctx->body_stream, cudaStreamNonBlocking), "create graph body stream");
         int dev = 0, sms = 0;
         check(cudaGetDevice(&dev), "device");
         check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
@@ -517,7 +562,7 @@ SmokeSimulationResult smoke_b200_get_face_velocity_cuda(SmokeSimulationContext c
 SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimulationContext c, uint32_t last_stage) {
     if (c == nullptr || last_stage > SMOKE_B200_STAGE_SCALARS) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return guarded([&] {
-        c->enqueue_stages(c->stream, last_stage);
+        c->enqueue_stages(c->stream, last_stage, false);
         c->views_stale = true;
         c->stepped = true;
         return SMOKE_SIMULATION_RESULT_OK;
@@ -527,26 +572,8 @@ SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimulationContext c, uint
 SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext c) {
     if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return guarded([&] {
-        c->enqueue_solve(c->stream);
+        c->enqueue_solve(c->stream, false);
         c->stepped = true;
-        return SMOKE_SIMULATION_RESULT_OK;
-    });
-}
-
-SmokeSimulationResult smoke_b200_profile_solver_cuda(SmokeSimulationContext c, uint32_t enable, uint64_t* out_phase_ns, uint32_t count) {
-    if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-    return guarded([&] {
-        if (out_phase_ns != nullptr && count > 0) {
-            unsigned long long ns[kSolverPhases] = {};
-            check(cudaMemcpyAsync(ns, c->control->phase_ns, sizeof(ns), cudaMemcpyDeviceToHost, c->stream), "read solver profile");
-            check(cudaStreamSynchronize(c->stream), "read solver profile");
-            for (uint32_t k = 0; k < count && k < static_cast<uint32_t>(kSolverPhases); ++k) out_phase_ns[k] = ns[k];
-        }
-        const bool want = enable != 0;
-        if (want != c->profile_solver) {
-            c->profile_solver = want;
-            c->capture_step_graph();
-        }
         return SMOKE_SIMULATION_RESULT_OK;
     });
 }

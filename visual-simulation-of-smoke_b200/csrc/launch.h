@@ -71,7 +71,7 @@ struct PcgSettings {
     float tolerance;
     int32_t refinement;      // extra passes on the FP64 true residual
     int32_t warm_start;      // start from x instead of 0
-    int32_t profile;         // 1: record wall time per solver phase in PcgControl::phase_ns
+    int32_t reserved;
 };
 
 struct PcgStatusDevice {
@@ -89,7 +89,6 @@ struct PcgStatusDevice {
 // contend less) and the status of the last solve. Zeroed (up to `status`) before every launch.
 constexpr int kPcgMaxBlocks = 148 * 16;
 constexpr int kPcgSumCopies = 8;
-constexpr int kSolverPhases = 8;
 struct PcgControl {
     unsigned int bar;
     unsigned int pad0;
@@ -98,7 +97,6 @@ struct PcgControl {
     unsigned int pad2[28];
     double totals[3][kPcgSumCopies][16];  // 4 sums per copy, one 128-byte line per copy
     PcgStatusDevice status;
-    unsigned long long phase_ns[kSolverPhases];  // wall time per solver phase (when profiling is on)
 };
 constexpr size_t kPcgControlResetBytes = offsetof(PcgControl, status);
 
@@ -143,19 +141,45 @@ struct MgHierarchy {
     int fper[3];
     MgLevel L[kMgMaxLevels];
 };
+// Level-0 vectors of the multigrid FCG solve (the residual and search direction are double-buffered: a pass reads
+// one buffer and writes the other, and the device-side parity picks which).
 struct MgWork {
+    float* r[2];
     float* p[2];
     float* q;
-    float* e;
-    float* r_alt;  // second residual buffer: the update pass reads one and writes the other
-    double* x64;
+    float* e;      // FP32 correction iterate of a refinement pass
+    double* x64;   // FP64 solution accumulator (refinement); kept between steps as the warm start
+};
+// Device-side scalars of one multigrid solve (reset at the start of every solve).
+constexpr int kMgSlots = 32;  // addresses each FP64 dot-product accumulator is spread over
+enum MgAccumulator { kAccBB = 0, kAccRR, kAccZR, kAccZQ, kAccPQ, kAccPR, kAccCount };
+struct MgState {
+    double acc[kAccCount][kMgSlots];
+    double bb, rnorm2, pq_prev, target2, pass_rr0, true_rel;
+    float alpha, beta;     // step sizes, computed by the last block of the kernel that completes their sums
+    unsigned int done[5];  // last-block election counters
+    int parity, first_iter, it, passes;
+    uint32_t status, fail, halt, zero_solution;
+};
+struct MgSolveArgs {
+    MgHierarchy H;
+    MgWork W;
+    const float* b;
+    float* x;
+    float* e;  // the FP32 iterate: x itself without refinement, else W.e
+    MgState* st;
+    int ir, warm, max_iterations, refinement;
+    float tol;
 };
 // Level extents and the number of grid-wide levels for a fine grid.
 int mg_level_count(int nx, int ny, int nz);
+// Largest refinement count the multigrid solve honours (the graph unrolls refinement + 1 passes).
+int mg_max_refinement();
 // Builds level fluid masks and codes from the occupancy (after the fine codes and anchor exist).
 cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uint8_t* occ, cudaStream_t s);
-// Enqueues the control reset and the cooperative multigrid-preconditioned FCG solve of A x = b.
-cudaError_t launch_mgfcg(const StepParams& P, const PcgSettings& S, const MgHierarchy& H, const float* b, float* x, MgWork work, PcgControl* ctl, cudaStream_t s);
+// Records the multigrid-preconditioned FCG solve of A x = b into the graph being captured on `s` (kernels, and
+// one `while` node per pass whose body is captured on `body_stream`); the outcome lands in *status_out.
+cudaError_t enqueue_mg_solve(const MgSolveArgs& args, bool fp64, PcgStatusDevice* status_out, cudaStream_t s, cudaStream_t body_stream);
 
 // Picks the persistent grid (all blocks co-resident) for the current device.
 cudaError_t pcg_launch_shape(PcgLaunchShape* out);

@@ -1,0 +1,904 @@
+// Multigrid-preconditioned flexible conjugate gradients for the pressure system, driven by a CUDA graph.
+//
+// No reference counterpart: the reference solves with unpreconditioned CG (backend-cuda.cu:1788-1824), which at
+// 128^3 needs ~900 iterations and stalls near relative residual 2.5e-5 in FP32. Here the preconditioner is one
+// geometric multigrid V(1,1) cycle:
+//  - levels: level l+1 halves every extent of level l (rounding up) down to <= 4 cells per axis; a coarse cell is
+//    active (fluid) when any child is; each level's operator is the masked 7-point stencil of its active cells,
+//    built with the fine rules (periodic wrap, OUTFLOW faces on the diagonal) but without the anchor;
+//  - smoothing: damped Jacobi, weight kOmega; the pre-smoothing sweep starts from zero;
+//  - restriction: r_{l+1}(C) = 1/2 * sum of the residuals of C's (up to 8) children after pre-smoothing; with the
+//    trilinear prolongation below this is the Petrov-Galerkin scaling of the 7-point operator (R A P ~ 2 A_coarse);
+//  - prolongation: cell-centred trilinear (weights 3/4 and 1/4 per axis); a corner outside the domain or on an
+//    inactive coarse cell takes the parent's value (inactive coarse cells carry the bit pattern kTag in t);
+//  - the coarsest levels (at most kMgBlockLevelCells cells, kMgBlockBytes in all) run in one block from shared
+//    memory; every other level pass is one kernel with one thread per cell at full occupancy.
+// The outer iteration is flexible CG (Notay 2000: beta_k = -(z_k, q_{k-1}) / (p_{k-1}, q_{k-1})), which stays
+// valid when the preconditioner is not exactly symmetric. Refinement passes accumulate the solution in FP64 and
+// restart from the FP64 residual b - A x64, as in pcg.cu.
+//
+// Execution: the solve is a graph (enqueue_mg_solve is called while the stream is being captured). Per iteration
+// the body of a graph `while` node runs: coarse restrictions, the block-level cycle, coarse prolongation +
+// smoothing, level-0 prolongation, level-0 smoothing with (z, r) (z, q), p/q with (p, q) (p, r), and the level-0
+// update r -= alpha q, e += alpha p with pre-smoothing, restriction and ||r||^2. The last block of the update
+// kernel tests convergence and sets the loop condition (cudaGraphSetConditional), so the host never waits.
+// Dot products: block sums, then FP64 atomic adds spread over kMgSlots addresses, summed in slot order.
+// Each restriction block covers whole 2x2x2 parents and writes the coarse right-hand side directly.
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "launch.h"
+#include "smoke_b200_ext.h"
+
+namespace smoke_b200 {
+
+namespace {
+
+constexpr int TX = 32, TY = 4, TZ = 2;  // cells of one block; even extents, so blocks hold whole parents
+constexpr int kThreads = TX * TY * TZ;
+constexpr int kBlockLevelThreads = 512;
+constexpr float kOmega = 0.8f;
+constexpr int kCoarsestSweeps = 16;
+constexpr uint32_t kTag = 0x7fc0feedu;  // t of an inactive coarse cell (a NaN payload arithmetic never produces)
+constexpr int kMaxPasses = 8;           // refinement passes in the graph (refinement is clamped to kMaxPasses - 1)
+
+__device__ __forceinline__ bool active(uint16_t code) { return (code & kCodeActive) != 0; }
+__device__ __forceinline__ float diagf(uint16_t code) { return static_cast<float>((code >> 8) & 7u); }
+__device__ __forceinline__ bool is_tag(float v) { return __float_as_uint(v) == kTag; }
+// Damped Jacobi step size w / diag (the preconditioner needs no correctly rounded quotient).
+__device__ __forceinline__ float wdiag(uint16_t code) { return __fdividef(kOmega, diagf(code)); }
+
+__device__ __forceinline__ void lxyz(const MgLevel& L, uint32_t q, int& x, int& y, int& z) {
+    const uint32_t zz = L.div_slab.div(q);
+    const uint32_t rem = q - zz * static_cast<uint32_t>(L.nx) * L.ny;
+    const uint32_t yy = L.div_nx.div(rem);
+    x = static_cast<int>(rem - yy * L.nx);
+    y = static_cast<int>(yy);
+    z = static_cast<int>(zz);
+}
+__device__ __forceinline__ uint32_t lidx(const MgLevel& L, int x, int y, int z) { return (static_cast<uint32_t>(z) * L.ny + y) * L.nx + x; }
+
+// Neighbour e (0..5 = -x +x -y +y -z +z) of an active stencil bit: in range, or across a periodic edge.
+__device__ __forceinline__ uint32_t lnbr(const MgLevel& L, uint32_t q, int x, int y, int z, int e) {
+    const uint32_t nx = L.nx, slab = static_cast<uint32_t>(L.nx) * L.ny;
+    switch (e) {
+    case 0: return x > 0 ? q - 1 : q + (nx - 1);
+    case 1: return x < L.nx - 1 ? q + 1 : q - (nx - 1);
+    case 2: return y > 0 ? q - nx : q + (L.ny - 1) * nx;
+    case 3: return y < L.ny - 1 ? q + nx : q - (L.ny - 1) * nx;
+    case 4: return z > 0 ? q - slab : q + (L.nz - 1) * slab;
+    default: return z < L.nz - 1 ? q + slab : q - (L.nz - 1) * slab;
+    }
+}
+// diag * v0 - sum of v over the active neighbours of (q; x, y, z); v(index) supplies the values.
+template <typename R, class V>
+__device__ __forceinline__ R stencil_xyz(const MgLevel& L, uint32_t q, int x, int y, int z, uint16_t code, R v0, V&& v) {
+    R acc = static_cast<R>(diagf(code)) * v0;
+#pragma unroll
+    for (int e = 0; e < 6; ++e)
+        if (code & (1u << e)) acc -= v(lnbr(L, q, x, y, z, e));
+    return acc;
+}
+
+// Masked 7-point stencil from preloaded values: diag * v0 - sum of vn[e] over the code's active neighbour bits.
+__device__ __forceinline__ float masked_stencil(uint16_t code, float v0, const float vn[6]) {
+    float acc = diagf(code) * v0;
+#pragma unroll
+    for (int e = 0; e < 6; ++e)
+        if (code & (1u << e)) acc -= vn[e];
+    return acc;
+}
+
+// v in [-1, n]: wraps one step across a periodic edge; false when v is outside a non-periodic axis.
+__device__ __forceinline__ bool wrap_c(int& v, int n, int per) {
+    if (v < 0) {
+        v += n;
+        return per != 0;
+    }
+    if (v >= n) {
+        v -= n;
+        return per != 0;
+    }
+    return true;
+}
+
+// Coarse index pair of one axis for fine coordinate v: the parent p = v >> 1 and its neighbour toward v's side
+// (wrapped across a periodic edge, clamped to p at a wall, where the corner takes the parent's value).
+__device__ __forceinline__ void corner_axis(int v, int n, int per, int& p, int& s) {
+    p = v >> 1;
+    s = (v & 1) ? p + 1 : p - 1;
+    if (s < 0) s = per ? s + n : p;
+    else if (s >= n) s = per ? s - n : p;
+}
+
+// Trilinear prolongation of C.t at fine cell (x, y, z); a corner on an inactive coarse cell (kTag) or beyond a
+// wall takes the parent's value.
+__device__ __forceinline__ float prolong_tagged(const MgLevel& C, const int* fper, int x, int y, int z) {
+    int x0, x1, y0, y1, z0, z1;
+    corner_axis(x, C.nx, fper[0], x0, x1);
+    corner_axis(y, C.ny, fper[1], y0, y1);
+    corner_axis(z, C.nz, fper[2], z0, z1);
+    const uint32_t nx = C.nx;
+    const uint32_t r00 = (static_cast<uint32_t>(z0) * C.ny + y0) * nx, r01 = (static_cast<uint32_t>(z0) * C.ny + y1) * nx;
+    const uint32_t r10 = (static_cast<uint32_t>(z1) * C.ny + y0) * nx, r11 = (static_cast<uint32_t>(z1) * C.ny + y1) * nx;
+    const bool wx = x1 == x0, wy = y1 == y0, wz = z1 == z0;  // clamped at a wall (or a 1-cell periodic axis)
+    const float* t = C.t;
+    const float c0 = t[r00 + x0], c1 = t[r00 + x1], c2 = t[r01 + x0], c3 = t[r01 + x1];
+    const float c4 = t[r10 + x0], c5 = t[r10 + x1], c6 = t[r11 + x0], c7 = t[r11 + x1];
+    const float parent = is_tag(c0) ? 0.0f : c0;
+    auto v = [&](float c, bool wall) { return (wall || is_tag(c)) ? parent : c; };
+    // weights (3/4 or 1/4 per axis): 27/64 parent, 9/64 edge, 3/64 face-diagonal, 1/64 opposite corner
+    const float near = 0.421875f * parent + 0.140625f * (v(c1, wx) + v(c2, wy) + v(c4, wz));
+    const float far = 0.046875f * (v(c3, wx || wy) + v(c5, wx || wz) + v(c6, wy || wz)) + 0.015625f * v(c7, wx || wy || wz);
+    return near + far;
+}
+
+// ---------------------------------------------------------------------------------------------- block helpers
+// Level kernels: one thread per cell of a TX x TY x TZ tile; block (bx, by, bz) walks the tiles (bx, by, k) for k in
+// its share of the z range, so that a wave of resident blocks covers the level and z-neighbours come from L1.
+struct Cell {
+    int x, y, z;     // coordinates
+    int bx, by, bz;  // tile
+    uint32_t q;
+    bool in;
+};
+__device__ __forceinline__ int tiles_z(const MgLevel& L) { return (L.nz + TZ - 1) / TZ; }
+template <class F>
+__device__ __forceinline__ void for_tiles(const MgLevel& L, F&& f) {
+    const int nzt = tiles_z(L);
+    const int share = (nzt + gridDim.z - 1) / gridDim.z;
+    const int k0 = blockIdx.z * share, k1 = min(nzt, k0 + share);
+    Cell c;
+    c.bx = blockIdx.x;
+    c.by = blockIdx.y;
+    c.x = c.bx * TX + threadIdx.x;
+    c.y = c.by * TY + threadIdx.y;
+    const bool in_xy = c.x < L.nx && c.y < L.ny;
+    for (int k = k0; k < k1; ++k) {
+        c.bz = k;
+        c.z = k * TZ + threadIdx.z;
+        c.in = in_xy && c.z < L.nz;
+        c.q = c.in ? lidx(L, c.x, c.y, c.z) : 0u;
+        f(c);
+    }
+}
+__device__ __forceinline__ uint32_t block_linear() { return (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x; }
+__device__ __forceinline__ uint32_t grid_blocks() { return gridDim.x * gridDim.y * gridDim.z; }
+__device__ __forceinline__ int tid() { return (threadIdx.z * TY + threadIdx.y) * TX + threadIdx.x; }
+
+// Indices of the 6 neighbours of an in-domain cell, computed from its coordinates alone (wrapped across periodic
+// edges, the cell itself where a non-periodic boundary cuts the stencil), so that every load of a stencil can be
+// issued before the operator code arrives; the code's bits then pick the terms.
+__device__ __forceinline__ void nbr_all(const MgLevel& L, const int* per, const Cell& c, uint32_t nb[6]) {
+    const uint32_t nx = L.nx, slab = nx * L.ny, q = c.q;
+    nb[0] = c.x > 0 ? q - 1 : (per[0] ? q + (nx - 1) : q);
+    nb[1] = c.x < L.nx - 1 ? q + 1 : (per[0] ? q - (nx - 1) : q);
+    nb[2] = c.y > 0 ? q - nx : (per[1] ? q + (L.ny - 1) * nx : q);
+    nb[3] = c.y < L.ny - 1 ? q + nx : (per[1] ? q - (L.ny - 1) * nx : q);
+    nb[4] = c.z > 0 ? q - slab : (per[2] ? q + (L.nz - 1) * slab : q);
+    nb[5] = c.z < L.nz - 1 ? q + slab : (per[2] ? q - (L.nz - 1) * slab : q);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block sums of a and b added (FP64) into accumulators ka and kb (kb < 0: only a), in slot block % kMgSlots.
+template <typename T>
+__device__ __forceinline__ void block_accumulate(MgState* st, int ka, T a, int kb, T b) {
+    __shared__ T part[2][kThreads / 32];
+    const int t = tid(), lane = t & 31, warp = t >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) {
+        part[0][warp] = a;
+        part[1][warp] = b;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        a = warp_sum(lane < kThreads / 32 ? part[0][lane] : T(0));
+        b = warp_sum(lane < kThreads / 32 ? part[1][lane] : T(0));
+        if (lane == 0) {
+            const uint32_t slot = block_linear() % kMgSlots;
+            atomicAdd(&st->acc[ka][slot], static_cast<double>(a));
+            if (kb >= 0) atomicAdd(&st->acc[kb][slot], static_cast<double>(b));
+        }
+    }
+}
+
+// Sum of accumulator k in slot order (read through L2).
+__device__ __forceinline__ double total(const MgState* st, int k) {
+    double s = 0.0;
+#pragma unroll 8
+    for (int i = 0; i < kMgSlots; ++i) s += __ldcg(&st->acc[k][i]);
+    return s;
+}
+__device__ __forceinline__ void zero_acc(MgState* st, int k) {
+    for (int i = 0; i < kMgSlots; ++i) st->acc[k][i] = 0.0;
+}
+
+// The 2x2x2 child sums of a tile's cells written into the coarse level's right-hand side (whole block calls it).
+__device__ __forceinline__ void restrict_tile(float c, const MgLevel& C, const Cell& cell) {
+    __shared__ float sm[TZ][TY][TX];
+    sm[threadIdx.z][threadIdx.y][threadIdx.x] = c;
+    __syncthreads();
+    const int t = tid();
+    if (t < (TX / 2) * (TY / 2)) {
+        const int cx = t % (TX / 2), cy = t / (TX / 2);
+        const float s = (sm[0][2 * cy][2 * cx] + sm[0][2 * cy][2 * cx + 1]) + (sm[0][2 * cy + 1][2 * cx] + sm[0][2 * cy + 1][2 * cx + 1]) +
+                        (sm[1][2 * cy][2 * cx] + sm[1][2 * cy][2 * cx + 1]) + (sm[1][2 * cy + 1][2 * cx] + sm[1][2 * cy + 1][2 * cx + 1]);
+        const int X = cell.bx * (TX / 2) + cx, Y = cell.by * (TY / 2) + cy, Z = cell.bz;
+        if (X < C.nx && Y < C.ny && Z < C.nz) C.r[lidx(C, X, Y, Z)] = s;
+    }
+    __syncthreads();
+}
+
+// Last-block election: true in thread 0 of the block that finishes last, after every block's earlier writes and
+// atomics are visible to it. The counter returns to 0.
+__device__ __forceinline__ bool last_block(unsigned int* counter) {
+    __shared__ bool s_last;
+    __syncthreads();
+    if (tid() == 0) {
+        __threadfence();
+        const unsigned int ticket = atomicAdd(counter, 1u);
+        s_last = ticket == grid_blocks() - 1;
+        if (s_last) {
+            *counter = 0;
+            __threadfence();
+        }
+    }
+    __syncthreads();
+    return s_last && tid() == 0;
+}
+
+// ---------------------------------------------------------------------------------------------- kernels
+// Solve set-up on level 0: r = b (or b - A x64 for a warm start), e = q = p = 0; ||b||^2 and ||r0||^2. The last
+// block initialises the solve's scalars.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) mg_setup_kernel(const __grid_constant__ MgSolveArgs A) {
+    const MgLevel& L0 = A.H.L[0];
+    MgState* st = A.st;
+    T bb = 0, rr = 0;
+    for_tiles(L0, [&](const Cell& c) {
+        if (!c.in) return;
+        const float bv = A.b[c.q];
+        bb += static_cast<T>(bv) * static_cast<T>(bv);
+        A.W.p[0][c.q] = 0.0f;
+        A.W.p[1][c.q] = 0.0f;
+        A.W.q[c.q] = 0.0f;
+        A.e[c.q] = 0.0f;
+        if (A.warm) {
+            const uint16_t code = L0.code[c.q];
+            double rv = 0.0;
+            if (active(code)) rv = static_cast<double>(bv) - stencil_xyz<double>(L0, c.q, c.x, c.y, c.z, code, A.W.x64[c.q], [&](uint32_t nb) { return A.W.x64[nb]; });
+            A.W.r[0][c.q] = static_cast<float>(rv);
+            rr += static_cast<T>(rv * rv);
+        } else {
+            A.W.r[0][c.q] = bv;
+            rr += static_cast<T>(bv) * static_cast<T>(bv);
+        }
+    });
+    block_accumulate<T>(st, kAccBB, bb, kAccRR, rr);
+    if (!last_block(&st->done[0])) return;
+    const double btot = total(st, kAccBB), rtot = total(st, kAccRR);
+    st->bb = btot;
+    st->rnorm2 = rtot;
+    st->pass_rr0 = rtot;
+    st->parity = 0;
+    st->first_iter = 1;
+    st->it = 0;
+    st->passes = 1;
+    st->alpha = 0.0f;
+    st->beta = 0.0f;
+    st->status = SMOKE_B200_SOLVE_ITERATION_CAP;
+    const double tol2 = static_cast<double>(A.tol) * A.tol * btot;
+    st->target2 = A.ir ? fmax(0.09 * tol2, 9e-8 * rtot) : tol2;
+    if (!(btot > 0.0)) {  // b = 0 (solution 0) or not finite
+        st->status = isfinite(btot) ? SMOKE_B200_SOLVE_CONVERGED : SMOKE_B200_SOLVE_NOT_FINITE;
+        st->halt = 1;
+        st->zero_solution = 1;
+        st->rnorm2 = 0.0;
+    }
+    zero_acc(st, kAccRR);
+}
+
+// Level-0 update: r' = r - alpha q, e += alpha p, zp = w D^-1 r', restriction of r' - A zp into level 1, ||r'||^2.
+// initial = 1: the pass's first round (alpha = 0, no iteration counted). The last block tests convergence, flips
+// the buffer parity and sets the loop condition `cond`.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_constant__ MgSolveArgs A, int initial, cudaGraphConditionalHandle cond) {
+    const MgLevel& L0 = A.H.L[0];
+    MgState* st = A.st;
+    const bool skip = st->halt || st->fail;  // uniform over the grid
+    const int par = st->parity;
+    const float a = initial ? 0.0f : st->alpha;
+    T rr = 0;
+    if (!skip) {
+        const float* r = A.W.r[par];
+        float* rn_out = A.W.r[par ^ 1];
+        const float* pn = A.W.p[par ^ 1];
+        for_tiles(L0, [&](const Cell& c) {
+            float res = 0.0f;
+            if (c.in) {
+                uint32_t nb[6];
+                nbr_all(L0, A.H.fper, c, nb);
+                const uint16_t code = L0.code[c.q];
+                const float rq = r[c.q], qq = A.W.q[c.q];
+                const float pq = initial ? 0.0f : pn[c.q], eq = initial ? 0.0f : A.e[c.q];
+                float un[6];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) un[k] = wdiag(L0.code[nb[k]]) * (r[nb[k]] - a * A.W.q[nb[k]]);
+                const float rn = rq - a * qq;
+                float zp = 0.0f;
+                if (active(code)) {
+                    zp = wdiag(code) * rn;
+                    res = 0.5f * (rn - masked_stencil(code, zp, un));
+                }
+                rn_out[c.q] = rn;
+                L0.zp[c.q] = zp;
+                if (!initial) A.e[c.q] = eq + a * pq;
+                rr += static_cast<T>(rn) * static_cast<T>(rn);
+            }
+            restrict_tile(res, A.H.L[1], c);
+        });
+        block_accumulate<T>(st, kAccRR, rr, -1, T(0));
+    }
+    if (!last_block(&st->done[1])) return;
+    if (st->halt) {
+        cudaGraphSetConditional(cond, 0);
+        return;
+    }
+    int stop = 0;
+    if (st->fail) {
+        st->status = st->fail;
+        stop = 1;
+    } else {
+        const double rn2 = total(st, kAccRR);
+        if (!initial) st->it += 1;
+        st->rnorm2 = rn2;
+        if (!isfinite(rn2)) {
+            st->status = SMOKE_B200_SOLVE_NOT_FINITE;
+            stop = 1;
+        } else if (rn2 <= st->target2) {
+            st->status = SMOKE_B200_SOLVE_CONVERGED;
+            stop = 1;
+        } else if (st->it >= A.max_iterations) {
+            st->status = SMOKE_B200_SOLVE_ITERATION_CAP;
+            stop = 1;
+        }
+    }
+    if (!initial) st->first_iter = 0;
+    st->parity ^= 1;
+    for (int k = kAccRR; k < kAccCount; ++k) zero_acc(st, k);
+    __threadfence();
+    cudaGraphSetConditional(cond, stop ? 0u : 1u);
+}
+
+// Level l >= 1: zp = w D^-1 r (pre-smoothing from zero), restriction of r - A zp into level l + 1.
+__global__ void __launch_bounds__(kThreads) mg_restrict_kernel(const __grid_constant__ MgHierarchy H, int l) {
+    const MgLevel& F = H.L[l];
+    for_tiles(F, [&](const Cell& c) {
+        float res = 0.0f;
+        if (c.in) {
+            uint32_t nb[6];
+            nbr_all(F, H.fper, c, nb);
+            const uint16_t code = F.code[c.q];
+            const float rv = F.r[c.q];
+            float un[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) un[k] = wdiag(F.code[nb[k]]) * F.r[nb[k]];
+            float zp = 0.0f;
+            if (active(code)) {
+                zp = wdiag(code) * rv;
+                res = 0.5f * (rv - masked_stencil(code, zp, un));
+            }
+            F.zp[c.q] = zp;
+        }
+        restrict_tile(res, H.L[l + 1], c);
+    });
+}
+
+// Level l: zp += P(t_{l+1}) on active cells (in place; pointwise).
+__global__ void __launch_bounds__(kThreads) mg_prolong_kernel(const __grid_constant__ MgHierarchy H, int l) {
+    const MgLevel& F = H.L[l];
+    const MgLevel& C = H.L[l + 1];
+    for_tiles(F, [&](const Cell& c) {
+        if (!c.in) return;
+        const uint16_t code = F.code[c.q];
+        const float zp = F.zp[c.q];
+        const float p = prolong_tagged(C, H.fper, c.x, c.y, c.z);
+        if (active(code)) F.zp[c.q] = zp + p;
+    });
+}
+
+// Level l post-smoothing: t = zp + w D^-1 (r - A zp) on active cells; inactive cells get kTag (coarse levels) or 0
+// (level 0, whose t is the preconditioned residual z). Level 0 also accumulates (z, r) and (z, q), and its last
+// block computes beta (0 on a pass's first iteration).
+template <bool LEVEL0, typename T>
+__global__ void __launch_bounds__(kThreads) mg_smooth_kernel(const __grid_constant__ MgSolveArgs A, int l) {
+    const MgLevel& F = A.H.L[LEVEL0 ? 0 : l];
+    MgState* st = A.st;
+    const float* r = LEVEL0 ? A.W.r[st->parity] : F.r;
+    const float inactive_value = LEVEL0 ? 0.0f : __uint_as_float(kTag);
+    T zr = 0, zq = 0;
+    for_tiles(F, [&](const Cell& c) {
+        if (!c.in) return;
+        uint32_t nb[6];
+        nbr_all(F, A.H.fper, c, nb);
+        const uint16_t code = F.code[c.q];
+        const float s0 = F.zp[c.q], rv = r[c.q];
+        const float qv = LEVEL0 ? A.W.q[c.q] : 0.0f;
+        float sn[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sn[k] = F.zp[nb[k]];
+        float z = inactive_value;
+        if (active(code)) {
+            z = s0 + wdiag(code) * (rv - masked_stencil(code, s0, sn));
+            if (LEVEL0) {
+                zr += static_cast<T>(z) * static_cast<T>(rv);
+                zq += static_cast<T>(z) * static_cast<T>(qv);
+            }
+        }
+        F.t[c.q] = z;
+    });
+    if (!LEVEL0) return;
+    block_accumulate<T>(st, kAccZR, zr, kAccZQ, zq);
+    if (!last_block(&st->done[3])) return;
+    const double beta = st->first_iter ? 0.0 : -total(st, kAccZQ) / st->pq_prev;
+    if (!isfinite(beta) || !isfinite(total(st, kAccZR))) st->fail = SMOKE_B200_SOLVE_NOT_FINITE;
+    st->beta = static_cast<float>(beta);
+}
+
+// p' = z + beta p, q = A p'; (p', q) and (p', r). The last block computes alpha = (p', r) / (p', q).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) mg_pq_kernel(const __grid_constant__ MgSolveArgs A) {
+    const MgLevel& F = A.H.L[0];
+    MgState* st = A.st;
+    const bool skip = st->fail;  // uniform over the grid
+    const int par = st->parity;
+    const float fb = st->beta;
+    T pq = 0, pr = 0;
+    if (!skip) {
+        const float* Z = F.t;
+        const float* po = A.W.p[par];
+        float* pn = A.W.p[par ^ 1];
+        const float* r = A.W.r[par];
+        for_tiles(F, [&](const Cell& c) {
+            if (!c.in) return;
+            uint32_t nb[6];
+            nbr_all(F, A.H.fper, c, nb);
+            const uint16_t code = F.code[c.q];
+            const float pv = Z[c.q] + fb * po[c.q];
+            float pnb[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) pnb[k] = Z[nb[k]] + fb * po[nb[k]];
+            const float qv = masked_stencil(code, pv, pnb);
+            pn[c.q] = pv;
+            A.W.q[c.q] = qv;
+            pq += static_cast<T>(pv) * static_cast<T>(qv);
+            pr += static_cast<T>(pv) * static_cast<T>(r[c.q]);
+        });
+        block_accumulate<T>(st, kAccPQ, pq, kAccPR, pr);
+    }
+    if (!last_block(&st->done[4]) || skip) return;
+    const double pqt = total(st, kAccPQ), prt = total(st, kAccPR);
+    if (!(pqt > 0.0) || !isfinite(prt)) {
+        st->fail = isfinite(pqt) ? SMOKE_B200_SOLVE_BREAKDOWN : SMOKE_B200_SOLVE_NOT_FINITE;
+        return;
+    }
+    st->alpha = static_cast<float>(prt / pqt);
+    st->pq_prev = pqt;
+}
+
+// Block-level part of the V-cycle (one block): see block_cycle.
+template <int THREADS>
+__device__ MgLevel smem_level(const MgHierarchy& H, float* area, int l) {
+    uint32_t off = 0;
+    for (int k = H.grid_levels; k < l; ++k) off += mg_block_words(H.L[k].n);
+    MgLevel S = H.L[l];
+    S.r = area + off;
+    S.zp = S.r + S.n;
+    S.t = S.zp + S.n;
+    S.code = reinterpret_cast<uint16_t*>(S.t + S.n);
+    S.fluid = nullptr;
+    return S;
+}
+
+template <typename R, class V>
+__device__ __forceinline__ R stencil_q(const MgLevel& L, uint32_t q, uint16_t code, R v0, V&& v) {
+    if (!(code & 63u)) return static_cast<R>(diagf(code)) * v0;
+    int x, y, z;
+    lxyz(L, q, x, y, z);
+    return stencil_xyz<R>(L, q, x, y, z, code, v0, v);
+}
+
+// Trilinear prolongation of C.t (shared memory) at fine cell (x, y, z), C's codes marking its active cells.
+__device__ __forceinline__ float prolong_codes(const MgLevel& C, const int* fper, int x, int y, int z) {
+    const int X = x >> 1, Y = y >> 1, Z = z >> 1;
+    const int sx = (x & 1) ? 1 : -1, sy = (y & 1) ? 1 : -1, sz = (z & 1) ? 1 : -1;
+    const float parent = C.t[lidx(C, X, Y, Z)];
+    float acc = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const float w = ((m & 1) ? 0.25f : 0.75f) * ((m & 2) ? 0.25f : 0.75f) * ((m & 4) ? 0.25f : 0.75f);
+        float v = parent;
+        if (m) {
+            int cx = X + ((m & 1) ? sx : 0), cy = Y + ((m & 2) ? sy : 0), cz = Z + ((m & 4) ? sz : 0);
+            if (wrap_c(cx, C.nx, fper[0]) && wrap_c(cy, C.ny, fper[1]) && wrap_c(cz, C.nz, fper[2])) {
+                const uint32_t cq = lidx(C, cx, cy, cz);
+                if (active(C.code[cq])) v = C.t[cq];
+            }
+        }
+        acc += w * v;
+    }
+    return acc;
+}
+
+// The coarse part of the V-cycle below the grid levels, in one block: reads r of level g (global), runs the
+// pre-smoothing and restriction, the coarsest Jacobi sweeps and the up passes in shared memory, and writes t of
+// level g (kTag on inactive cells).
+__global__ void __launch_bounds__(kBlockLevelThreads) mg_block_kernel(const __grid_constant__ MgHierarchy H) {
+    extern __shared__ __align__(16) float area[];
+    constexpr int NT = kBlockLevelThreads;
+    const int g = H.grid_levels, lc = H.levels - 1;
+    const int t = threadIdx.x;
+    for (int l = g; l <= lc; ++l) {  // codes as aligned pairs (the arrays carry two spare entries)
+        const MgLevel S = smem_level<NT>(H, area, l);
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(H.L[l].code);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(S.code);
+        for (uint32_t i = t; i < (S.n + 1) / 2; i += NT) dst[i] = src[i];
+    }
+    {
+        const MgLevel S = smem_level<NT>(H, area, g);
+        for (uint32_t q = t; q < S.n; q += NT) S.r[q] = H.L[g].r[q];
+    }
+    __syncthreads();
+    for (int l = g; l < lc; ++l) {
+        const MgLevel F = smem_level<NT>(H, area, l);
+        const MgLevel C = smem_level<NT>(H, area, l + 1);
+        for (uint32_t q = t; q < C.n; q += NT) C.r[q] = 0.0f;
+        for (uint32_t q = t; q < F.n; q += NT) {
+            const uint16_t code = F.code[q];
+            F.zp[q] = active(code) ? wdiag(code) * F.r[q] : 0.0f;
+        }
+        __syncthreads();
+        for (uint32_t q = t; q < F.n; q += NT) {
+            const uint16_t code = F.code[q];
+            if (!active(code)) continue;
+            const float res = F.r[q] - stencil_q<float>(F, q, code, F.zp[q], [&](uint32_t nb) { return F.zp[nb]; });
+            int x, y, z;
+            lxyz(F, q, x, y, z);
+            atomicAdd(C.r + lidx(C, x >> 1, y >> 1, z >> 1), 0.5f * res);
+        }
+        __syncthreads();
+    }
+    {  // coarsest level: Jacobi sweeps from zero, ping-pong between t and zp, result in t
+        const MgLevel L = smem_level<NT>(H, area, lc);
+        for (uint32_t q = t; q < L.n; q += NT) {
+            const uint16_t code = L.code[q];
+            L.t[q] = active(code) ? wdiag(code) * L.r[q] : 0.0f;
+        }
+        for (int sweep = 0; sweep < kCoarsestSweeps; ++sweep) {
+            __syncthreads();
+            float* src = (sweep & 1) ? L.zp : L.t;
+            float* dst = (sweep & 1) ? L.t : L.zp;
+            for (uint32_t q = t; q < L.n; q += NT) {
+                const uint16_t code = L.code[q];
+                float v = 0.0f;
+                if (active(code)) {
+                    const float s0 = src[q];
+                    v = s0 + wdiag(code) * (L.r[q] - stencil_q<float>(L, q, code, s0, [&](uint32_t nb) { return src[nb]; }));
+                }
+                dst[q] = v;
+            }
+        }
+        __syncthreads();
+    }
+    static_assert(kCoarsestSweeps % 2 == 0, "the coarsest sweeps end in t");
+    for (int l = lc - 1; l >= g; --l) {
+        const MgLevel F = smem_level<NT>(H, area, l);
+        const MgLevel C = smem_level<NT>(H, area, l + 1);
+        for (uint32_t q = t; q < F.n; q += NT) {
+            if (!active(F.code[q])) continue;
+            int x, y, z;
+            lxyz(F, q, x, y, z);
+            F.zp[q] += prolong_codes(C, H.fper, x, y, z);
+        }
+        __syncthreads();
+        for (uint32_t q = t; q < F.n; q += NT) {
+            const uint16_t code = F.code[q];
+            float v = 0.0f;
+            if (active(code)) {
+                const float s0 = F.zp[q];
+                v = s0 + wdiag(code) * (F.r[q] - stencil_q<float>(F, q, code, s0, [&](uint32_t nb) { return F.zp[nb]; }));
+            }
+            F.t[q] = v;
+        }
+        __syncthreads();
+    }
+    const MgLevel S = smem_level<NT>(H, area, g);
+    for (uint32_t q = t; q < S.n; q += NT) H.L[g].t[q] = active(S.code[q]) ? S.t[q] : __uint_as_float(kTag);
+}
+
+// Refinement: x64 = (first pass of a cold start ? 0 : x64) + e.
+__global__ void __launch_bounds__(kThreads) mg_accumulate_kernel(const __grid_constant__ MgSolveArgs A) {
+    const MgState* st = A.st;
+    if (st->halt) return;
+    const bool fresh = st->passes == 1 && !A.warm;
+    const MgLevel& L0 = A.H.L[0];
+    for_tiles(L0, [&](const Cell& c) {
+        if (c.in) A.W.x64[c.q] = (fresh ? 0.0 : A.W.x64[c.q]) + static_cast<double>(A.e[c.q]);
+    });
+}
+
+// Refinement: r = b - A x64 (FP64) into the current residual buffer, e = q = 0, ||r||^2. The last block decides
+// between another pass and the end of the solve.
+__global__ void __launch_bounds__(kThreads) mg_residual_kernel(const __grid_constant__ MgSolveArgs A) {
+    const MgLevel& L0 = A.H.L[0];
+    MgState* st = A.st;
+    if (st->halt) return;  // uniform: no block reaches the election
+    float* r = A.W.r[st->parity];
+    double rr = 0.0;
+    for_tiles(L0, [&](const Cell& c) {
+        if (!c.in) return;
+        const uint16_t code = L0.code[c.q];
+        double rv = 0.0;
+        if (active(code)) rv = static_cast<double>(A.b[c.q]) - stencil_xyz<double>(L0, c.q, c.x, c.y, c.z, code, A.W.x64[c.q], [&](uint32_t nb) { return A.W.x64[nb]; });
+        r[c.q] = static_cast<float>(rv);
+        A.e[c.q] = 0.0f;
+        A.W.q[c.q] = 0.0f;
+        rr += rv * rv;
+    });
+    block_accumulate<double>(st, kAccRR, rr, -1, 0.0);
+    if (!last_block(&st->done[2])) return;
+    const double rtot = total(st, kAccRR);
+    const double true_rel = sqrt(rtot / st->bb);
+    st->true_rel = true_rel;
+    if (true_rel <= static_cast<double>(A.tol)) {
+        st->status = SMOKE_B200_SOLVE_CONVERGED;
+        st->halt = 1;
+    } else if (st->passes > A.refinement || st->it >= A.max_iterations || st->status != SMOKE_B200_SOLVE_CONVERGED) {
+        if (st->status == SMOKE_B200_SOLVE_CONVERGED) st->status = SMOKE_B200_SOLVE_ITERATION_CAP;
+        st->halt = 1;
+    } else {
+        st->passes += 1;
+        st->rnorm2 = rtot;
+        st->pass_rr0 = rtot;
+        const double tol2 = static_cast<double>(A.tol) * A.tol * st->bb;
+        st->target2 = fmax(0.09 * tol2, 9e-8 * rtot);
+        st->first_iter = 1;
+        st->status = SMOKE_B200_SOLVE_ITERATION_CAP;
+    }
+    zero_acc(st, kAccRR);
+}
+
+// Solution write-back and status record.
+__global__ void __launch_bounds__(kThreads) mg_finalize_kernel(const __grid_constant__ MgSolveArgs A, PcgStatusDevice* out) {
+    const MgState* st = A.st;
+    const MgLevel& L0 = A.H.L[0];
+    if (st->zero_solution || A.ir) {
+        for_tiles(L0, [&](const Cell& c) {
+            if (!c.in) return;
+            if (st->zero_solution) {
+                A.x[c.q] = 0.0f;
+                if (A.ir) A.W.x64[c.q] = 0.0;
+            } else {
+                A.x[c.q] = static_cast<float>(A.W.x64[c.q]);
+            }
+        });
+    }
+    if (block_linear() != 0 || tid() != 0) return;
+    PcgStatusDevice s{};
+    s.iterations = st->it;
+    s.passes = st->passes;
+    s.status = st->status;
+    s.rhs_norm = sqrt(st->bb);
+    s.relative_residual = st->bb > 0.0 ? sqrt(st->rnorm2 / st->bb) : 0.0;
+    s.true_relative_residual = A.ir ? (st->zero_solution ? 0.0 : st->true_rel) : -1.0;
+    *out = s;
+}
+
+// ---------------------------------------------------------------------------------------------- host side
+const dim3 kBlock(TX, TY, TZ);
+
+// Grid of one wave for `kernel` on level L: the level's tile columns (x, y), and as many z shares as the resident
+// blocks (per SM x SMs, cached per kernel and device) allow.
+template <class K>
+dim3 wave(K kernel, const MgLevel& L) {
+    static std::mutex lock;
+    static std::map<std::pair<const void*, int>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int resident = 0;
+    {
+        std::lock_guard<std::mutex> guard(lock);
+        const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+        auto it = cache.find(key);
+        if (it == cache.end()) {
+            int sms = 0, per_sm = 0;
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+            it = cache.emplace(key, sms * per_sm).first;
+        }
+        resident = it->second;
+    }
+    const int tx = (L.nx + TX - 1) / TX, ty = (L.ny + TY - 1) / TY, tz = (L.nz + TZ - 1) / TZ;
+    int gz = resident / (tx * ty);
+    if (gz < 1) gz = 1;
+    if (gz > tz) gz = tz;
+    gz = (tz + ((tz + gz - 1) / gz) - 1) / ((tz + gz - 1) / gz);  // no empty z shares
+    return dim3(tx, ty, gz);
+}
+
+// Adds a `while` node after the capture's current dependencies and captures `body` into it on `body_stream`.
+template <class Body>
+cudaError_t add_while(cudaStream_t s, cudaStream_t body_stream, cudaGraphConditionalHandle h, Body&& body) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, &deps, &ndeps);
+    if (e != cudaSuccess) return e;
+    if (cs != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    e = cudaGraphAddNode(&node, graph, deps, ndeps, &np);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamBeginCaptureToGraph(body_stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    body(body_stream);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t eb = cudaGetLastError();
+    e = cudaStreamEndCapture(body_stream, &captured);
+    if (eb != cudaSuccess) return eb;
+    if (e != cudaSuccess) return e;
+    return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+template <typename T>
+cudaError_t enqueue_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream_t s, cudaStream_t body_stream) {
+    const MgHierarchy& H = A.H;
+    const MgLevel& L0 = H.L[0];
+    const int g = H.grid_levels;
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, nullptr, nullptr);
+    if (e != cudaSuccess) return e;
+    if (cs != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureImplicit;
+    uint32_t block_bytes = 0;
+    for (int l = g; l < H.levels; ++l) block_bytes += 4u * mg_block_words(H.L[l].n);
+
+    e = cudaMemsetAsync(A.st, 0, sizeof(MgState), s);
+    if (e != cudaSuccess) return e;
+    mg_setup_kernel<T><<<wave(mg_setup_kernel<T>, L0), kBlock, 0, s>>>(A);
+    const int passes = A.ir ? A.refinement + 1 : 1;
+    for (int pass = 0; pass < passes; ++pass) {
+        cudaGraphConditionalHandle h;
+        e = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) return e;
+        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, s>>>(A, 1, h);
+        e = add_while(s, body_stream, h, [&](cudaStream_t bs) {
+            for (int l = 1; l < g; ++l) mg_restrict_kernel<<<wave(mg_restrict_kernel, H.L[l]), kBlock, 0, bs>>>(H, l);
+            mg_block_kernel<<<1, kBlockLevelThreads, block_bytes, bs>>>(H);
+            for (int l = g - 1; l >= 1; --l) {
+                mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[l]), kBlock, 0, bs>>>(H, l);
+                mg_smooth_kernel<false, T><<<wave(mg_smooth_kernel<false, T>, H.L[l]), kBlock, 0, bs>>>(A, l);
+            }
+            mg_prolong_kernel<<<wave(mg_prolong_kernel, L0), kBlock, 0, bs>>>(H, 0);
+            mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0), kBlock, 0, bs>>>(A, 0);
+            mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0), kBlock, 0, bs>>>(A);
+            mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, bs>>>(A, 0, h);
+        });
+        if (e != cudaSuccess) return e;
+        if (A.ir) {
+            mg_accumulate_kernel<<<wave(mg_accumulate_kernel, L0), kBlock, 0, s>>>(A);
+            mg_residual_kernel<<<wave(mg_residual_kernel, L0), kBlock, 0, s>>>(A);
+        }
+    }
+    mg_finalize_kernel<<<wave(mg_finalize_kernel, L0), kBlock, 0, s>>>(A, out);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------- hierarchy setup
+__global__ void mg_fluid0_kernel(uint32_t n, const uint8_t* __restrict__ occ, uint8_t* __restrict__ fluid) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) fluid[q] = occ[q] == 0 ? 1 : 0;
+}
+
+__global__ void mg_coarsen_kernel(const MgLevel F, const MgLevel C) {
+    const uint32_t cq = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cq >= C.n) return;
+    int X, Y, Z;
+    lxyz(C, cq, X, Y, Z);
+    uint8_t any = 0;
+    for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
+                if (x < F.nx && y < F.ny && z < F.nz) any |= F.fluid[lidx(F, x, y, z)];
+            }
+    C.fluid[cq] = any;
+}
+
+// Operator codes of a coarse level: the fine rules (stencil_code_kernel) without the anchor. The two spare
+// entries past the end are zero (inactive).
+__global__ void mg_code_kernel(const MgLevel L, const __grid_constant__ StepParams P) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= L.n + 2) return;
+    if (q >= L.n) {
+        L.code[q] = 0;
+        return;
+    }
+    if (!L.fluid[q]) {
+        L.code[q] = static_cast<uint16_t>(1u << 8);
+        return;
+    }
+    int c[3];
+    lxyz(L, q, c[0], c[1], c[2]);
+    const int nn[3] = {L.nx, L.ny, L.nz};
+    uint32_t diag = 0, mask = 0;
+    for (int e = 0; e < 6; ++e) {
+        const int a = e >> 1;
+        int d[3] = {c[0], c[1], c[2]};
+        d[a] += (e & 1) ? 1 : -1;
+        if (d[a] < 0 || d[a] >= nn[a]) {
+            if (!P.fper[a]) {
+                if (P.flow[e].type == kFlowOutflow) ++diag;
+                continue;
+            }
+            d[a] = wrapi(d[a], nn[a]);
+        }
+        const uint32_t nb = lidx(L, d[0], d[1], d[2]);
+        if (!L.fluid[nb]) continue;
+        ++diag;
+        if (nb == q) continue;
+        if ((e & 1) && nn[a] == 2 && P.fper[a]) continue;
+        mask |= 1u << e;
+    }
+    if (diag == 0) diag = 1;
+    L.code[q] = static_cast<uint16_t>(mask | (diag << 8) | kCodeActive);
+}
+
+// Zeroes the two spare entries past the level-0 codes.
+__global__ void mg_code_tail_kernel(uint16_t* code, uint32_t n) {
+    if (threadIdx.x < 2) code[n + threadIdx.x] = 0;
+}
+
+}  // namespace
+
+int mg_level_count(int nx, int ny, int nz) {
+    int levels = 1;
+    while ((nx > 4 || ny > 4 || nz > 4) && levels < kMgMaxLevels) {
+        nx = (nx + 1) / 2;
+        ny = (ny + 1) / 2;
+        nz = (nz + 1) / 2;
+        ++levels;
+    }
+    return levels < 2 ? 2 : levels;
+}
+
+int mg_max_refinement() { return kMaxPasses - 1; }
+
+cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uint8_t* occ, cudaStream_t s) {
+    mg_fluid0_kernel<<<(H.L[0].n + 255) / 256, 256, 0, s>>>(H.L[0].n, occ, H.L[0].fluid);
+    mg_code_tail_kernel<<<1, 32, 0, s>>>(H.L[0].code, H.L[0].n);
+    for (int l = 1; l < H.levels; ++l) {
+        mg_coarsen_kernel<<<(H.L[l].n + 255) / 256, 256, 0, s>>>(H.L[l - 1], H.L[l]);
+        mg_code_kernel<<<(H.L[l].n + 2 + 255) / 256, 256, 0, s>>>(H.L[l], P);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_mg_solve(const MgSolveArgs& args, bool fp64, PcgStatusDevice* status_out, cudaStream_t s, cudaStream_t body_stream) {
+    return fp64 ? enqueue_typed<double>(args, status_out, s, body_stream) : enqueue_typed<float>(args, status_out, s, body_stream);
+}
+
+}  // namespace smoke_b200

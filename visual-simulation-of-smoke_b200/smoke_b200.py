@@ -51,7 +51,6 @@ class SmokeLibrary:
         ("smoke_b200_get_face_velocity_cuda", [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
         ("smoke_b200_step_stages_cuda", [C.c_void_p, C.c_uint32]),
         ("smoke_b200_solve_pressure_cuda", [C.c_void_p]),
-        ("smoke_b200_profile_solver_cuda", [C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64), C.c_uint32]),
     ]
 
     def __init__(self, path: str = DEFAULT_LIBRARY, extensions: bool = True):
@@ -215,9 +214,3 @@ class Simulation:
 
     def solve_pressure(self):
         _check(self.lib.smoke_b200_solve_pressure_cuda(self.handle), "solve_pressure")
-
-    def profile_solver(self, enable: bool = True):
-        """Turns solver phase timing on/off and returns the last solve's phase times in microseconds."""
-        buf = (C.c_uint64 * 8)()
-        _check(self.lib.smoke_b200_profile_solver_cuda(self.handle, 1 if enable else 0, buf, 8), "profile_solver")
-        return [v / 1000.0 for v in buf]
