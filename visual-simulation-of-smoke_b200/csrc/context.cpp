@@ -106,6 +106,8 @@ struct SmokeSimulationContext_t {
     float *cx = nullptr, *cy = nullptr, *cz = nullptr, *vmag = nullptr;
     float *wx = nullptr, *wy = nullptr, *wz = nullptr, *wmag = nullptr, *divergence = nullptr;
     float *fx = nullptr, *fy = nullptr, *fz = nullptr;
+    Faces pad{};                                       // padded copies of the velocity being sampled
+    float *pad_t = nullptr, *pad_d = nullptr;          // padded copies of the scalar sources
     PcgWork pcg{};
     uint16_t* codes = nullptr;
     uint8_t* occupancy = nullptr;
@@ -159,6 +161,11 @@ struct SmokeSimulationContext_t {
                           &divergence, &fx, &fy, &fz, &pcg.r[0], &pcg.r[1], &pcg.s[0], &pcg.s[1], &pcg.w[0], &pcg.w[1], &pcg.p, &pcg.e})
             f32(p, n);
         slots.push_back({reinterpret_cast<void**>(&pcg.x64), n * sizeof(double)});
+        f32(&pad.u, pad_count(P, 0));
+        f32(&pad.v, pad_count(P, 1));
+        f32(&pad.w, pad_count(P, 2));
+        f32(&pad_t, pad_count(P, 4));
+        f32(&pad_d, pad_count(P, 3));
         slots.push_back({reinterpret_cast<void**>(&codes), (n + 2) * sizeof(uint16_t)});
         slots.push_back({reinterpret_cast<void**>(&occupancy), n});
         slots.push_back({reinterpret_cast<void**>(&fill_list), n * sizeof(FillEntry)});
@@ -275,7 +282,10 @@ struct SmokeSimulationContext_t {
         check(launch_cell_force(P, wx, wy, wz, wmag, density, temperature, force_x, force_y, force_z, occupancy, fx, fy, fz, s), "cell force");
         check(launch_face_force(P, as_const(A), fx, fy, fz, occupancy, solid, B, s), "face force");
         if (last_stage < SMOKE_B200_STAGE_ADVECT_VELOCITY) return;
-        check(launch_advect_velocity(P, as_const(B), occupancy, solid, C, s), "advect velocity");
+        check(launch_pad(P, 0, B.u, pad.u, s), "pad u");
+        check(launch_pad(P, 1, B.v, pad.v, s), "pad v");
+        check(launch_pad(P, 2, B.w, pad.w, s), "pad w");
+        check(launch_advect_velocity(P, as_const(B), as_const(pad), occupancy, solid, C, s), "advect velocity");
         if (last_stage < SMOKE_B200_STAGE_PRESSURE) return;
         check(launch_rhs(P, as_const(C), occupancy, anchor, rhs, s), "pressure rhs");
         enqueue_solve(s, capturing);
@@ -285,7 +295,12 @@ struct SmokeSimulationContext_t {
         check(launch_project(P, as_const(C), pressure, p64, occupancy, solid, A, s), "project");
         if (last_stage < SMOKE_B200_STAGE_SCALARS) return;
         check(launch_scalar_prep(P, temperature, temperature_source, density, density_source, occupancy, solid_temperature, temperature_tmp, density_tmp, s), "scalar sources");
-        check(launch_advect_scalars(P, as_const(A), occupancy, temperature_tmp, density_tmp, solid_temperature, temperature, density, s), "advect scalars");
+        check(launch_pad(P, 0, A.u, pad.u, s), "pad u");
+        check(launch_pad(P, 1, A.v, pad.v, s), "pad v");
+        check(launch_pad(P, 2, A.w, pad.w, s), "pad w");
+        check(launch_pad(P, 4, temperature_tmp, pad_t, s), "pad temperature");
+        check(launch_pad(P, 3, density_tmp, pad_d, s), "pad density");
+        check(launch_advect_scalars(P, as_const(A), as_const(pad), occupancy, temperature_tmp, pad_t, density_tmp, pad_d, solid_temperature, temperature, density, s), "advect scalars");
         check(launch_density_fill(fill_list, fill_count, density, fill_blocks, s), "density fill");
     }
 

@@ -37,16 +37,20 @@ cudaError_t launch_vorticity(const StepParams& P, ConstFaces vel, const uint8_t*
 cudaError_t launch_cell_force(const StepParams& P, const float* wx, const float* wy, const float* wz, const float* wmag, const float* density, const float* temperature, const float* ufx, const float* ufy, const float* ufz, const uint8_t* occ, float* fx, float* fy, float* fz, cudaStream_t s);
 // Forces: out = settled(in + dt * face-average of f) (domain, solid and periodic face rules applied).
 cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* fx, const float* fy, const float* fz, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
-// Velocity self-advection: out = settled(semi-Lagrangian sample of in along in).
-cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
+// Padded copies (PadField): element count of the copy of field kind (0-2 face components, 3 density, 4
+// temperature), and the kernel that fills it from f.
+size_t pad_count(const StepParams& P, int kind);
+cudaError_t launch_pad(const StepParams& P, int kind, const float* f, float* pad, cudaStream_t s);
+// Velocity self-advection: out = settled(semi-Lagrangian sample of in along in); pad holds the padded copies of in.
+cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, ConstFaces pad, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
 // Pressure right-hand side from the advected velocity.
 cudaError_t launch_rhs(const StepParams& P, ConstFaces vel, const uint8_t* occ, const int32_t* anchor, float* rhs, cudaStream_t s);
 // Projection: out = settled(in - dt * grad p / h); pressure64 (optional) is the FP64 solution of a refined solve.
 cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const double* pressure64, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
 // Scalars: source terms (and solid temperature) into the temporaries.
 cudaError_t launch_scalar_prep(const StepParams& P, const float* temperature, const float* temperature_source, const float* density, const float* density_source, const uint8_t* occ, const float* solid_temperature, float* t_tmp, float* d_tmp, cudaStream_t s);
-// Scalars: one shared back-trace per cell, sample both scalars, solid rules.
-cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, const uint8_t* occ, const float* t_tmp, const float* d_tmp, const float* solid_temperature, float* temperature, float* density, cudaStream_t s);
+// Scalars: one shared back-trace per cell, sample both scalars, solid rules (vel_pad, t_pad, d_pad: padded copies).
+cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, ConstFaces vel_pad, const uint8_t* occ, const float* t_tmp, const float* t_pad, const float* d_tmp, const float* d_pad, const float* solid_temperature, float* temperature, float* density, cudaStream_t s);
 // Scalars: solid cells copy their nearest fluid cell's density.
 cudaError_t launch_density_fill(const FillEntry* list, const uint32_t* count, float* density, int max_blocks, cudaStream_t s);
 // Derived views: centred velocity, |u|, vorticity, |w|, divergence of the step's final velocity.

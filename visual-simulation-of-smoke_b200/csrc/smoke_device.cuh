@@ -283,6 +283,78 @@ __device__ __forceinline__ float sample(const float* __restrict__ f, float x, fl
     }
 }
 
+// ---------------------------------------------------------------------------------------------- padded fields
+// A sampled field copied with kPad ghost cells on every side, each ghost cell holding exactly the boundary tap of
+// its index (face_tap_slow / scalar_tap_slow), so that a sample whose taps all lie within kPad cells of the array
+// is one plain tensor of loads with no per-tap test. Samples of points inside the domain always qualify; `raw` (the
+// unpadded field) serves the rare sample reaching further out, through sample_edge.
+constexpr int kPad = 2;
+struct PadField {
+    const float* p;    // padded array, index (k + kPad) * pxy + (j + kPad) * px + (i + kPad)
+    const float* raw;  // the field itself
+    uint32_t px, pxy;  // padded row and slab pitch
+};
+
+template <int KIND, bool CUBIC>
+__device__ __forceinline__ float sample_pad(const PadField& F, float x, float y, float z, const StepParams& P) {
+    if (periodic_axis<KIND>(P, 0)) x = wrap_pos(x, P.nx, P.h);
+    if (periodic_axis<KIND>(P, 1)) y = wrap_pos(y, P.ny, P.h);
+    if (periodic_axis<KIND>(P, 2)) z = wrap_pos(z, P.nz, P.h);
+    const float gx = KIND == 0 ? x / P.h : x / P.h - 0.5f;
+    const float gy = KIND == 1 ? y / P.h : y / P.h - 0.5f;
+    const float gz = KIND == 2 ? z / P.h : z / P.h - 0.5f;
+    const int x0 = static_cast<int>(floorf(gx));
+    const int y0 = static_cast<int>(floorf(gy));
+    const int z0 = static_cast<int>(floorf(gz));
+    const float tx = gx - static_cast<float>(x0);
+    const float ty = gy - static_cast<float>(y0);
+    const float tz = gz - static_cast<float>(z0);
+    const int ex = P.nx + (KIND == 0) - 1, ey = P.ny + (KIND == 1) - 1, ez = P.nz + (KIND == 2) - 1;  // last indices
+    const uint32_t sy = F.px, sz = F.pxy;
+    if constexpr (!CUBIC) {
+        // taps x0 .. x0+1 within [-kPad, ex+kPad]; written so that saturated conversions cannot overflow the test
+        if (!(x0 >= -kPad && x0 < ex + kPad && y0 >= -kPad && y0 < ey + kPad && z0 >= -kPad && z0 < ez + kPad)) return sample_edge(F.raw, KIND, 0, x0, y0, z0, tx, ty, tz, P);
+        const uint32_t b = static_cast<uint32_t>(z0 + kPad) * sz + static_cast<uint32_t>(y0 + kPad) * sy + static_cast<uint32_t>(x0 + kPad);
+        const float* f = F.p;
+        const float c000 = __ldg(f + b), c100 = __ldg(f + b + 1);
+        const float c010 = __ldg(f + b + sy), c110 = __ldg(f + b + sy + 1);
+        const float c001 = __ldg(f + b + sz), c101 = __ldg(f + b + sz + 1);
+        const float c011 = __ldg(f + b + sz + sy), c111 = __ldg(f + b + sz + sy + 1);
+        const float c00 = c000 + (c100 - c000) * tx;
+        const float c10 = c010 + (c110 - c010) * tx;
+        const float c01 = c001 + (c101 - c001) * tx;
+        const float c11 = c011 + (c111 - c011) * tx;
+        const float c0 = c00 + (c10 - c00) * ty;
+        const float c1 = c01 + (c11 - c01) * ty;
+        return c0 + (c1 - c0) * tz;
+    } else {
+        // taps x0-1 .. x0+2 within [-kPad, ex+kPad]
+        if (!(x0 >= 1 - kPad && x0 <= ex + kPad - 2 && y0 >= 1 - kPad && y0 <= ey + kPad - 2 && z0 >= 1 - kPad && z0 <= ez + kPad - 2)) return sample_edge(F.raw, KIND, 1, x0, y0, z0, tx, ty, tz, P);
+        const uint32_t base = static_cast<uint32_t>(z0 - 1 + kPad) * sz + static_cast<uint32_t>(y0 - 1 + kPad) * sy + static_cast<uint32_t>(x0 - 1 + kPad);
+        const float* f = F.p;
+        float zs[4];
+#pragma unroll
+        for (int dz = 0; dz < 4; ++dz) {
+            float ys[4];
+#pragma unroll
+            for (int dy = 0; dy < 4; ++dy) {
+                const uint32_t b = base + dz * sz + dy * sy;
+                ys[dy] = mono_cubic(__ldg(f + b), __ldg(f + b + 1), __ldg(f + b + 2), __ldg(f + b + 3), tx);
+            }
+            zs[dz] = mono_cubic(ys[0], ys[1], ys[2], ys[3], ty);
+        }
+        return mono_cubic(zs[0], zs[1], zs[2], zs[3], tz);
+    }
+}
+
+// The boundary tap of field KIND at any integer index (the value a ghost cell of the padded copy holds).
+template <int KIND>
+__device__ __forceinline__ float boundary_tap(const float* __restrict__ f, int i, int j, int k, const StepParams& P) {
+    if constexpr (KIND < 3) return face_tap_slow<KIND>(f, i, j, k, P);
+    else if constexpr (KIND == 3) return scalar_tap_slow(f, i, j, k, P, P.den, P.dper);
+    else return scalar_tap_slow(f, i, j, k, P, P.tem, P.tper);
+}
+
 // ---------------------------------------------------------------------------------------------- trace
 // End-point / probe test of the back-trace (backend-cuda.cu:781-812): outside [0, n*h] on a non-periodic
 // axis, or inside a solid cell.
@@ -301,19 +373,8 @@ __device__ __forceinline__ bool blocked(float x, float y, float z, const uint8_t
     return occ[cidx(P, cx, cy, cz)] != 0;
 }
 
-// Midpoint RK2 back-trace through the face velocities (u,v,w), trilinear samples; a blocked end point is
-// pulled back towards the start by 10 bisection steps (backend-cuda.cu:760-838).
-__device__ __noinline__ inline float3 trace_rk2(float sx, float sy, float sz, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const StepParams& P) {
-    const float dt = P.dt;
-    const float a0 = sample<0, false>(u, sx, sy, sz, P);
-    const float b0 = sample<1, false>(v, sx, sy, sz, P);
-    const float c0 = sample<2, false>(w, sx, sy, sz, P);
-    const float mx = sx - 0.5f * dt * a0, my = sy - 0.5f * dt * b0, mz = sz - 0.5f * dt * c0;
-    const float a1 = sample<0, false>(u, mx, my, mz, P);
-    const float b1 = sample<1, false>(v, mx, my, mz, P);
-    const float c1 = sample<2, false>(w, mx, my, mz, P);
-    const float tx = sx - dt * a1, ty = sy - dt * b1, tz = sz - dt * c1;
-    if (!blocked(tx, ty, tz, occ, P)) return make_float3(tx, ty, tz);
+// Bisection of a blocked back-trace end point towards the start, 10 steps (backend-cuda.cu:760-838).
+__device__ __noinline__ inline float3 bisect_blocked(float sx, float sy, float sz, float tx, float ty, float tz, const uint8_t* __restrict__ occ, const StepParams& P) {
     float lo = 0.0f, hi = 1.0f;
     for (int it = 0; it < 10; ++it) {
         const float mid = 0.5f * (lo + hi);
@@ -321,6 +382,22 @@ __device__ __noinline__ inline float3 trace_rk2(float sx, float sy, float sz, co
         else lo = mid;
     }
     return make_float3(sx + (tx - sx) * lo, sy + (ty - sy) * lo, sz + (tz - sz) * lo);
+}
+
+// Midpoint RK2 back-trace through the face velocities (padded copies of u, v, w), trilinear samples; a blocked end
+// point is pulled back towards the start by bisection (backend-cuda.cu:760-838).
+__device__ __forceinline__ float3 trace_rk2(float sx, float sy, float sz, const PadField& u, const PadField& v, const PadField& w, const uint8_t* __restrict__ occ, const StepParams& P) {
+    const float dt = P.dt;
+    const float a0 = sample_pad<0, false>(u, sx, sy, sz, P);
+    const float b0 = sample_pad<1, false>(v, sx, sy, sz, P);
+    const float c0 = sample_pad<2, false>(w, sx, sy, sz, P);
+    const float mx = sx - 0.5f * dt * a0, my = sy - 0.5f * dt * b0, mz = sz - 0.5f * dt * c0;
+    const float a1 = sample_pad<0, false>(u, mx, my, mz, P);
+    const float b1 = sample_pad<1, false>(v, mx, my, mz, P);
+    const float c1 = sample_pad<2, false>(w, mx, my, mz, P);
+    const float tx = sx - dt * a1, ty = sy - dt * b1, tz = sz - dt * c1;
+    if (!blocked(tx, ty, tz, occ, P)) return make_float3(tx, ty, tz);
+    return bisect_blocked(sx, sy, sz, tx, ty, tz, occ, P);
 }
 
 // ---------------------------------------------------------------------------------------------- centred velocity

@@ -190,34 +190,49 @@ __global__ void __launch_bounds__(kThreads) face_force_kernel(const __grid_const
 }
 
 // ------------------------------------------------------------------------------------------ velocity advection
-template <int A>
-__device__ __forceinline__ void advect_face_one(const StepParams& P, uint32_t q, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
+template <int A, bool CUBIC>
+__device__ __forceinline__ void advect_face_one(const StepParams& P, uint32_t q, const PadField& u, const PadField& v, const PadField& w, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
     int i, j, k;
     face_ijk<A>(P, q, i, j, k);
-    const float* src = pick<A>(u, v, w);
+    const PadField& src = A == 0 ? u : (A == 1 ? v : w);
     out[q] = settle<A, false>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
         const float h = P.h;
         const float px = A == 0 ? static_cast<float>(a) * h : (static_cast<float>(a) + 0.5f) * h;
         const float py = A == 1 ? static_cast<float>(b) * h : (static_cast<float>(b) + 0.5f) * h;
         const float pz = A == 2 ? static_cast<float>(c) * h : (static_cast<float>(c) + 0.5f) * h;
         const float3 p = trace_rk2(px, py, pz, u, v, w, occ, P);
-        return P.cubic ? sample<A, true>(src, p.x, p.y, p.z, P) : sample<A, false>(src, p.x, p.y, p.z, P);
+        return sample_pad<A, CUBIC>(src, p.x, p.y, p.z, P);
     });
 }
 
-__global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou,
-                                                                    float* __restrict__ ov, float* __restrict__ ow, unsigned bu, unsigned bv) {
+// Samples and traces read the padded copies of the velocity (ghost cells hold the boundary taps).
+template <bool CUBIC>
+__global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ StepParams P, const PadField u, const PadField v, const PadField w, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou, float* __restrict__ ov,
+                                                                    float* __restrict__ ow, unsigned bu, unsigned bv) {
     const unsigned b = blockIdx.x;
     if (b < bu) {
         const uint32_t q = b * kThreads + threadIdx.x;
-        if (q < P.nu) advect_face_one<0>(P, q, u, v, w, occ, su, ou);
+        if (q < P.nu) advect_face_one<0, CUBIC>(P, q, u, v, w, occ, su, ou);
     } else if (b < bu + bv) {
         const uint32_t q = (b - bu) * kThreads + threadIdx.x;
-        if (q < P.nv) advect_face_one<1>(P, q, u, v, w, occ, sv, ov);
+        if (q < P.nv) advect_face_one<1, CUBIC>(P, q, u, v, w, occ, sv, ov);
     } else {
         const uint32_t q = (b - bu - bv) * kThreads + threadIdx.x;
-        if (q < P.nw) advect_face_one<2>(P, q, u, v, w, occ, sw, ow);
+        if (q < P.nw) advect_face_one<2, CUBIC>(P, q, u, v, w, occ, sw, ow);
     }
+}
+
+// Padded copy of field KIND (see PadField): one thread per padded cell.
+template <int KIND>
+__global__ void __launch_bounds__(kThreads) pad_kernel(const __grid_constant__ StepParams P, const float* __restrict__ f, float* __restrict__ out) {
+    const int fx = P.nx + (KIND == 0), fy = P.ny + (KIND == 1), fz = P.nz + (KIND == 2);
+    const uint32_t px = fx + 2 * kPad, py = fy + 2 * kPad, pz = fz + 2 * kPad;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= px * py * pz) return;
+    const uint32_t row = t / px, slab = row / py;
+    const int i = static_cast<int>(t - row * px) - kPad, j = static_cast<int>(row - slab * py) - kPad, k = static_cast<int>(slab) - kPad;
+    const bool in = i >= 0 && i < fx && j >= 0 && j < fy && k >= 0 && k < fz;
+    out[t] = in ? f[(static_cast<uint32_t>(k) * fy + j) * fx + i] : boundary_tap<KIND>(f, i, j, k, P);
 }
 
 // ------------------------------------------------------------------------------------------ pressure rhs
@@ -296,8 +311,7 @@ __global__ void __launch_bounds__(kThreads) scalar_prep_kernel(const __grid_cons
 // Fluid cells: one back-trace, then both scalars sampled with their own boundary rules (:1221-1233).
 // Solid cells: temperature = solid temperature (:1235-1241), density = 0 until the fill pass.
 template <bool CUBIC>
-__global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const float* __restrict__ t_tmp, const float* __restrict__ d_tmp, const float* __restrict__ solid_t, float* __restrict__ t,
-                                                                   float* __restrict__ d) {
+__global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ StepParams P, const PadField u, const PadField v, const PadField w, const uint8_t* __restrict__ occ, const PadField t_tmp, const PadField d_tmp, const float* __restrict__ solid_t, float* __restrict__ t, float* __restrict__ d) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.n) return;
     if (occ[q] != 0) {
@@ -309,8 +323,8 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_c
     cell_xyz(P, q, x, y, z);
     const float h = P.h;
     const float3 p = trace_rk2((static_cast<float>(x) + 0.5f) * h, (static_cast<float>(y) + 0.5f) * h, (static_cast<float>(z) + 0.5f) * h, u, v, w, occ, P);
-    t[q] = sample<4, CUBIC>(t_tmp, p.x, p.y, p.z, P);
-    d[q] = sample<3, CUBIC>(d_tmp, p.x, p.y, p.z, P);
+    t[q] = sample_pad<4, CUBIC>(t_tmp, p.x, p.y, p.z, P);
+    d[q] = sample_pad<3, CUBIC>(d_tmp, p.x, p.y, p.z, P);
 }
 
 __global__ void density_fill_kernel(const FillEntry* __restrict__ list, const uint32_t* __restrict__ count, float* __restrict__ d) {
@@ -508,9 +522,38 @@ cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* f
     return cudaGetLastError();
 }
 
-cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
+// Padded copy descriptor of field KIND stored at `pad`.
+PadField pad_field(const StepParams& P, int kind, const float* raw, const float* pad) {
+    const uint32_t fx = P.nx + (kind == 0), fy = P.ny + (kind == 1);
+    PadField F{};
+    F.p = pad;
+    F.raw = raw;
+    F.px = fx + 2 * kPad;
+    F.pxy = F.px * (fy + 2 * kPad);
+    return F;
+}
+
+size_t pad_count(const StepParams& P, int kind) {
+    return static_cast<size_t>(P.nx + (kind == 0) + 2 * kPad) * (P.ny + (kind == 1) + 2 * kPad) * (P.nz + (kind == 2) + 2 * kPad);
+}
+
+cudaError_t launch_pad(const StepParams& P, int kind, const float* f, float* pad, cudaStream_t s) {
+    const unsigned grid = static_cast<unsigned>((pad_count(P, kind) + kThreads - 1) / kThreads);
+    switch (kind) {
+    case 0: pad_kernel<0><<<grid, kThreads, 0, s>>>(P, f, pad); break;
+    case 1: pad_kernel<1><<<grid, kThreads, 0, s>>>(P, f, pad); break;
+    case 2: pad_kernel<2><<<grid, kThreads, 0, s>>>(P, f, pad); break;
+    case 3: pad_kernel<3><<<grid, kThreads, 0, s>>>(P, f, pad); break;
+    default: pad_kernel<4><<<grid, kThreads, 0, s>>>(P, f, pad); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, ConstFaces pad, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
     const unsigned bu = blocks_for(P.nu), bv = blocks_for(P.nv), bw = blocks_for(P.nw);
-    advect_velocity_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
+    const PadField u = pad_field(P, 0, in.u, pad.u), v = pad_field(P, 1, in.v, pad.v), w = pad_field(P, 2, in.w, pad.w);
+    if (P.cubic) advect_velocity_kernel<true><<<bu + bv + bw, kThreads, 0, s>>>(P, u, v, w, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
+    else advect_velocity_kernel<false><<<bu + bv + bw, kThreads, 0, s>>>(P, u, v, w, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
     return cudaGetLastError();
 }
 
@@ -530,9 +573,11 @@ cudaError_t launch_scalar_prep(const StepParams& P, const float* temperature, co
     return cudaGetLastError();
 }
 
-cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, const uint8_t* occ, const float* t_tmp, const float* d_tmp, const float* solid_temperature, float* temperature, float* density, cudaStream_t s) {
-    if (P.cubic) advect_scalars_kernel<true><<<blocks_for(P.n), kThreads, 0, s>>>(P, vel.u, vel.v, vel.w, occ, t_tmp, d_tmp, solid_temperature, temperature, density);
-    else advect_scalars_kernel<false><<<blocks_for(P.n), kThreads, 0, s>>>(P, vel.u, vel.v, vel.w, occ, t_tmp, d_tmp, solid_temperature, temperature, density);
+cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, ConstFaces vel_pad, const uint8_t* occ, const float* t_tmp, const float* t_pad, const float* d_tmp, const float* d_pad, const float* solid_temperature, float* temperature, float* density, cudaStream_t s) {
+    const PadField u = pad_field(P, 0, vel.u, vel_pad.u), v = pad_field(P, 1, vel.v, vel_pad.v), w = pad_field(P, 2, vel.w, vel_pad.w);
+    const PadField t = pad_field(P, 4, t_tmp, t_pad), d = pad_field(P, 3, d_tmp, d_pad);
+    if (P.cubic) advect_scalars_kernel<true><<<blocks_for(P.n), kThreads, 0, s>>>(P, u, v, w, occ, t, d, solid_temperature, temperature, density);
+    else advect_scalars_kernel<false><<<blocks_for(P.n), kThreads, 0, s>>>(P, u, v, w, occ, t, d, solid_temperature, temperature, density);
     return cudaGetLastError();
 }
 
