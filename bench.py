@@ -2,14 +2,14 @@
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--n 128]
 
-One JSON line on rank 0. "value" is the device time of one step of the mixed-precision form (FP32 stencils,
-Jacobi-PCG with FP64 dot products and an FP64 true-residual refinement, to 1e-5) with every input resident in
-HBM and L2 flushed between timed steps; "e2e" is the same step driven through the C ABI with the step's host input
-copied in from pinned memory and its result (total density) read back, per step. The plain-FP32 form (FP32
-reductions, no refinement) runs on the same states and is reported beside it. `--impl reference` runs the
-reference's own CUDA library (compiled from its sources into oracle/_ref) on the same scene through the same ABI,
-with the fixed CG iteration count that reaches 1e-5 on this scene. Several GPUs run independent replicas (the step
-does not shard); timing is the max over ranks.
+One JSON line on rank 0. "value" is the device time of one step of the headline form (FP32 stencils, multigrid-
+preconditioned FCG with FP64 dot products and an FP64 true-residual refinement, to 1e-5) with every input resident
+in HBM and L2 flushed between timed steps; "e2e" is the same step driven through the C ABI with the step's host
+input copied in from pinned memory and its result (total density) read back, per step. The Jacobi-PCG and plain-
+FP32 forms run on the same states and are reported beside it. `--impl reference` runs the reference's own CUDA
+library (compiled from its sources into oracle/_ref) on the same scene through the same ABI, with the fixed CG
+iteration count that reaches its FP32 residual floor on this scene. Several GPUs run independent replicas (the
+step does not shard); timing is the max over ranks. `--profile` runs a profiling workload instead (no JSON line).
 """
 from __future__ import annotations
 
@@ -31,11 +31,40 @@ import smoke_abi as abi  # noqa: E402
 
 METRIC = "ms/step and PCG iters at 128³ to rel-res 1e-5: learned+mixed vs plain FP32"
 REF_LIBRARY = os.path.join(ROOT, "oracle", "_ref", "libvisual-simulation-of-smoke.so")
-# Smallest fixed CG iteration count with which the reference reaches relative residual <= 1e-5 on every step of
-# the 128^3 plume (after the spin-up); measured on a B200 with `bench.py --calibrate-reference`.
-REFERENCE_CG_ITERATIONS = 600
+# Fixed CG iteration count of the reference on the 128^3 plume: its FP32 CG stalls near relative residual 2.5e-5
+# (it never reaches 1e-5), and 900 is the smallest count that reaches that floor on every step after the spin-up
+# (measured on a B200 with `bench.py --calibrate-reference`).
+REFERENCE_CG_ITERATIONS = 900
 SPINUP_STEPS = 30
-KERNELS_PER_STEP = 10  # vorticity, cell force, face force, advect velocity, rhs, solver, project, scalar prep, advect scalars, density fill
+# Kernels of one step outside the pressure solve: vorticity, cell force, face force, 3 velocity pads, advect velocity,
+# rhs, project, scalar prep, 5 pads (velocity + 2 scalars), advect scalars, density fill.
+STEP_KERNELS = 17
+
+
+def mg_grid_levels(n):
+    """Levels of the multigrid hierarchy of an n^3 grid and how many run grid-wide (mirrors context.cpp)."""
+    dims, (x, y, z) = [], (n, n, n)
+    dims.append((x, y, z))
+    while (x > 4 or y > 4 or z > 4) and len(dims) < 12:
+        x, y, z = (x + 1) // 2, (y + 1) // 2, (z + 1) // 2
+        dims.append((x, y, z))
+    cells = [a * b * c for a, b, c in dims]
+    grid, words = len(dims) - 1, 0
+    for l in range(len(dims) - 1, 0, -1):
+        words += 3 * cells[l] + (cells[l] + 2) // 2
+        if cells[l] > 512 or words * 4 > 16 * 1024:
+            break
+        grid = l
+    return len(dims), grid
+
+
+def solver_launches(n, iterations, refinement):
+    """Kernels the multigrid solve graph launches: set-up and write-back, per refinement pass the first update, the
+    accumulation and the FP64 residual, and per iteration the loop body (restriction, prolongation and smoothing of
+    every grid level below 0, the block-level cycle, level-0 prolongation, smoothing, p/q and update)."""
+    _, g = mg_grid_levels(n)
+    per_iteration = 3 * (g - 1) + 5
+    return 2 + 3 * (refinement + 1) + per_iteration * iterations
 
 
 def load_peaks():
@@ -207,18 +236,20 @@ def restore_state(sim, state):
     sim.stream.synchronize()
 
 
-# Algorithmic bytes per cell and iteration of the solver kernels (each operand counted once):
+# Algorithmic bytes per cell and iteration of the solver kernels (each operand counted once per kernel):
 #  - Jacobi/CG (pcg_kernel): reads p, x, r, s, w (4 B each) + code (2 B); writes p, x, r, s, w -> 42 B;
-#  - multigrid FCG (mgfcg_kernel), level 0: restriction reads r, code, writes z (10 B); prolongation reads z, writes
-#    t (8 B); smoothing reads t, r, code, q, writes z (18 B); p/q pass reads z, p, code, r, writes p, q (22 B);
-#    update pass reads e, p, r, q, writes e, r (24 B) -> 82 B, plus ~1/7 of that on the coarser levels -> 94 B.
+#  - multigrid FCG graph, level 0: update reads r, q, p, e, code, writes r', zp, e (30 B); prolongation reads code,
+#    zp, writes zp (10 B); smoothing reads code, zp, r, q, writes z (18 B); p/q reads code, z, p, r, writes p', q
+#    (22 B) -> 80 B; the coarser levels add 1/8 + 1/64 + ... of their 34 B (restriction 10, prolongation 10,
+#    smoothing 14) plus the restricted right-hand sides -> 85 B per fine cell and iteration.
 JACOBI_BYTES_PER_CELL_ITERATION = 42.0
-MG_BYTES_PER_CELL_ITERATION = 94.0
+MG_BYTES_PER_CELL_ITERATION = 85.0
 
 
 def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5, bytes_per_iteration=JACOBI_BYTES_PER_CELL_ITERATION, kernel="pcg_kernel"):
-    """Times the persistent solver kernel alone (smoke_b200_solve_pressure_cuda on the step's right-hand side) with
-    CUDA events on the context stream; algorithmic bytes = cells x (bytes per iteration x iterations + setup)."""
+    """Times the pressure solve alone (smoke_b200_solve_pressure_cuda on the step's right-hand side: one graph launch
+    on the context stream) with CUDA events on that stream; algorithmic bytes = cells x (bytes per iteration x
+    iterations + set-up 24 B + 46 B per refinement pass)."""
     import torch
 
     flush = L2Flush()
@@ -239,12 +270,12 @@ def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5, bytes_p
         passes = st.passes
     ms = statistics.median(durs)
     it = statistics.median(iters)
-    algo_bytes = n_cells * (bytes_per_iteration * it + 16.0 + 26.0 * passes)
+    algo_bytes = n_cells * (bytes_per_iteration * it + 24.0 + 46.0 * passes)
     achieved = algo_bytes / (ms * 1e-3) / 1e9
     return {"bound": "hbm", "kernel": kernel, "achieved": round(achieved, 1), "peak": peak_gbs, "peak_kind": peak_kind, "unit": "GB/s",
             "frac": round(achieved / peak_gbs, 3), "traffic": None, "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(ms, 4), "iterations": it,
             "bytes_per_cell_iteration": bytes_per_iteration,
-            "note": "the solver's working set is L2-resident at 128^3; DRAM traffic per launch is in profiles/"}
+            "note": "the solve's working set (~90 MB) is mostly L2-resident at 128^3; per-kernel times and DRAM traffic are in profiles/"}
 
 
 def cpu_baseline(sim, cfg, steps=2):
@@ -332,7 +363,7 @@ def bench_b200(args, rank, world, local):
     e2e_ms, _ = run_e2e(sim, driver, step0 + args.warmup, args.steps)
     barrier(world)
     e2e_ms = max_over_ranks(e2e_ms, world)
-    roof = solver_kernel_roofline(sim, n ** 3, *load_peaks(), bytes_per_iteration=MG_BYTES_PER_CELL_ITERATION, kernel="mgfcg_kernel (persistent multigrid-preconditioned FCG)")
+    roof = solver_kernel_roofline(sim, n ** 3, *load_peaks(), bytes_per_iteration=MG_BYTES_PER_CELL_ITERATION, kernel="multigrid-preconditioned FCG solve (one graph launch of the mg_* kernels)")
     cpu = cpu_baseline(sim, cfg) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     sim.close()
     if rank != 0:
@@ -352,7 +383,7 @@ def bench_b200(args, rank, world, local):
         "roofline": roof,
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": driver.h2d_bytes, "d2h_bytes_per_step": driver.d2h_bytes,
                 "includes": "per-step box inputs H2D, velocity/density/temperature views, source/force updates, step, total-density D2H, host sync"},
-        "gpu_launches": KERNELS_PER_STEP * args.steps,
+        "gpu_launches": round(args.steps * (STEP_KERNELS + solver_launches(n, its, FORMS[HEADLINE]["refinement"]))),
         "clocks": clocks.summary() if clocks is not None else None,
     }
     if cpu is not None:
@@ -387,7 +418,7 @@ def bench_reference(args, rank, world, local):
     return {
         "metric": METRIC, "impl": "reference", "value": round(ms, 4), "unit": "ms/step", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded plume scene)",
-        "config": {"workload": f"plume {n}^3 monotone-cubic, reference fixed CG x{REFERENCE_CG_ITERATIONS} (smallest count reaching rel-res 1e-5)", "grid": [n, n, n],
+        "config": {"workload": f"plume {n}^3 monotone-cubic, reference fixed CG x{REFERENCE_CG_ITERATIONS} (smallest count reaching its FP32 floor, rel-res ~2.5e-5)", "grid": [n, n, n],
                    "l2": "flushed between timed steps (256 MiB write)"},
         "pcg_iterations": REFERENCE_CG_ITERATIONS,
         "cpu_baseline": {"value": round(ms, 4), "unit": "ms/step", "cores": 1, "kind": "reference", "sample": sample,
@@ -395,6 +426,35 @@ def bench_reference(args, rank, world, local):
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": driver.h2d_bytes, "d2h_bytes_per_step": driver.d2h_bytes},
         "clocks": clocks.summary(),
     }
+
+
+def profile_workload(args):
+    """Profiling workloads (for ncu; prints one status line, no benchmark JSON): the 128^3 plume after the spin-up,
+    then --profile-count repetitions of: `solve` an eager multigrid solve (every kernel a plain launch), `solve-graph`
+    the multigrid solve graph, `step` an eager step (stage kernels launched one by one, the solve as its graph)."""
+    import torch
+
+    import plume_scene
+    import smoke_b200
+
+    n = args.n
+    lib = smoke_b200.SmokeLibrary()
+    stream = torch.cuda.Stream()
+    sim = smoke_b200.Simulation(lib, plume_scene.plume_config(n, abi.MONOTONIC_CUBIC), stream)
+    driver = plume_scene.PlumeDriver(sim, n, seed=1)
+    sim.set_solver(**FORMS[HEADLINE])
+    run_steps(sim, driver, 0, SPINUP_STEPS, None)
+    for k in range(args.profile_count):
+        if args.profile == "step":
+            driver.apply(SPINUP_STEPS + k)
+            sim.step_stages(abi.STAGE_SCALARS)
+        else:
+            sim.solve_pressure(eager=args.profile == "solve")
+    stream.synchronize()
+    st = sim.solver_status()
+    print(json.dumps({"profile": args.profile, "count": args.profile_count, "iterations": st.iterations, "passes": st.passes, "status": st.status,
+                      "true_rel_residual": st.true_relative_residual}), flush=True)
+    sim.close()
 
 
 def calibrate_reference(args):
@@ -435,11 +495,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--calibrate-reference", action="store_true")
     ap.add_argument("--calibrate-counts", type=int, nargs="*", default=[200, 300, 400, 500, 600, 800, 1000])
+    ap.add_argument("--profile", choices=["solve", "solve-graph", "step"], help="run a profiling workload instead of the benchmark")
+    ap.add_argument("--profile-count", type=int, default=1)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_setup(args.gpus)
     if args.calibrate_reference:
         calibrate_reference(args)
+        return
+    if args.profile:
+        profile_workload(args)
         return
     line = bench_reference(args, rank, world, local) if args.impl == "reference" else bench_b200(args, rank, world, local)
     barrier(world) if args.impl == "b200" else None

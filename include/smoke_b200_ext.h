@@ -91,9 +91,17 @@ typedef enum SmokeB200Stage {
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimulationContext context, uint32_t last_stage);
 
 /* Solves the pressure system of the context's current right-hand side (the FLOW_PRESSURE_RHS view) into the
- * pressure buffer with the selected solver: the step's pressure stage without the right-hand-side kernel. One
- * kernel launch on the context stream; the outcome is read with smoke_b200_get_solver_status_cuda. */
+ * pressure buffer with the selected solver: the step's pressure stage without the right-hand-side kernel. Enqueued
+ * on the context stream without a host wait (the multigrid solve is one CUDA-graph launch whose loop runs on the
+ * device; the Jacobi and fixed CG solves are one cooperative kernel); the outcome is read with
+ * smoke_b200_get_solver_status_cuda. */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext context);
+
+/* The same solve with every solver kernel launched directly on the context stream, no graph: the multigrid loop is
+ * driven from the host, which reads the loop condition after each iteration (one stream synchronisation per
+ * iteration, so slower). For profilers that do not follow graph loops, and for hosts that cannot use CUDA graphs.
+ * Results equal smoke_b200_solve_pressure_cuda's up to the summation order of the FP64 dot products. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_eager_cuda(SmokeSimulationContext context);
 
 /* Pressure solve that allocates nothing. No counterpart in the reference (which has no standalone solve and
  * allocates all its buffers with cudaMalloc when a context is created).

@@ -251,3 +251,22 @@ def test_fixed_cg_matches_reference_semantics(smoke_lib, cuda_stream):
         assert status.iterations == iters and status.status == abi.SOLVE_ITERATION_CAP
     report("fixed_cg", out)
     assert out[1] < 1e-5 and out[5] < 1e-4 and out[20] < 1e-3 and out[200] < 1e-4, out
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_multigrid_eager_matches_graph(smoke_lib, cuda_stream, name):
+    """The host-driven (eager) multigrid solve reproduces the graph solve: same kernels, same iteration count; the
+    FP64 dot products are summed by atomics, so the last bits may differ."""
+    cfg, inp = setup_case(smoke_lib, cuda_stream, name)
+    sim = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_PRESSURE, mode=abi.SOLVER_MG_FCG)
+    p_graph = cells(sim, abi.VIEW_FLOW_PRESSURE)
+    st_graph = sim.solver_status()
+    with torch.cuda.stream(cuda_stream):
+        sim.solve_pressure(eager=True)
+    p_eager = cells(sim, abi.VIEW_FLOW_PRESSURE)
+    st_eager = sim.solver_status()
+    sim.close()
+    assert st_graph.status == abi.SOLVE_CONVERGED and st_eager.status == abi.SOLVE_CONVERGED
+    assert abs(st_graph.iterations - st_eager.iterations) <= 1
+    assert st_eager.passes == st_graph.passes
+    assert scenes.rel_err(p_eager, p_graph) < 1e-6

@@ -247,6 +247,20 @@ struct SmokeSimulationContext_t {
             check(cudaGraphLaunch(solve_exec, s), "pressure solve (multigrid FCG graph)");
             return;
         }
+        check(enqueue_mg_solve(mg_args(S), S.fp64 != 0, &control->status, s, body_stream), "pressure solve (multigrid FCG)");
+    }
+
+    // The same solve with every kernel launched directly (the multigrid loop driven from the host).
+    void run_solve_eager(cudaStream_t s) {
+        const PcgSettings S = pcg_settings();
+        if (solver.mode != SMOKE_B200_SOLVER_MG_FCG) {
+            check(launch_pcg(P, S, pcg_shape, codes, rhs, pressure, pcg, control, s), "pressure solve");
+            return;
+        }
+        check(run_mg_solve_eager(mg_args(S), S.fp64 != 0, &control->status, s), "pressure solve (multigrid FCG, eager)");
+    }
+
+    MgSolveArgs mg_args(const PcgSettings& S) const {
         MgSolveArgs A{};
         A.H = mg;
         A.W = mg_work;
@@ -259,7 +273,7 @@ struct SmokeSimulationContext_t {
         A.max_iterations = S.max_iterations;
         A.refinement = S.refinement < mg_max_refinement() ? S.refinement : mg_max_refinement();
         A.tol = S.tolerance;
-        check(enqueue_mg_solve(A, S.fp64 != 0, &control->status, s, body_stream), "pressure solve (multigrid FCG)");
+        return A;
     }
 
     PcgSettings pcg_settings() const {
@@ -588,6 +602,15 @@ SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext c) {
     if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return guarded([&] {
         c->enqueue_solve(c->stream, false);
+        c->stepped = true;
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+SmokeSimulationResult smoke_b200_solve_pressure_eager_cuda(SmokeSimulationContext c) {
+    if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        c->run_solve_eager(c->stream);
         c->stepped = true;
         return SMOKE_SIMULATION_RESULT_OK;
     });

@@ -164,6 +164,7 @@ struct MgState {
     unsigned int done[5];  // last-block election counters
     int parity, first_iter, it, passes;
     uint32_t status, fail, halt, zero_solution;
+    uint32_t loop;         // the loop condition the last update set (read by the host in eager mode)
 };
 struct MgSolveArgs {
     MgHierarchy H;
@@ -184,6 +185,9 @@ cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uin
 // Records the multigrid-preconditioned FCG solve of A x = b into the graph being captured on `s` (kernels, and
 // one `while` node per pass whose body is captured on `body_stream`); the outcome lands in *status_out.
 cudaError_t enqueue_mg_solve(const MgSolveArgs& args, bool fp64, PcgStatusDevice* status_out, cudaStream_t s, cudaStream_t body_stream);
+// The same solve launched kernel by kernel on `s` (no graph): the host reads the loop condition after every update
+// (one stream synchronisation per iteration). For profilers that do not enter graph loops and hosts without graphs.
+cudaError_t run_mg_solve_eager(const MgSolveArgs& args, bool fp64, PcgStatusDevice* status_out, cudaStream_t s);
 
 // Picks the persistent grid (all blocks co-resident) for the current device.
 cudaError_t pcg_launch_shape(PcgLaunchShape* out);

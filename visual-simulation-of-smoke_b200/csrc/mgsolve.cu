@@ -310,7 +310,7 @@ __global__ void __launch_bounds__(kThreads) mg_setup_kernel(const __grid_constan
 // initial = 1: the pass's first round (alpha = 0, no iteration counted). The last block tests convergence, flips
 // the buffer parity and sets the loop condition `cond`.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_constant__ MgSolveArgs A, int initial, cudaGraphConditionalHandle cond) {
+__global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_constant__ MgSolveArgs A, int initial, cudaGraphConditionalHandle cond, int in_graph) {
     const MgLevel& L0 = A.H.L[0];
     MgState* st = A.st;
     const bool skip = st->halt || st->fail;  // uniform over the grid
@@ -349,7 +349,8 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
     }
     if (!last_block(&st->done[1])) return;
     if (st->halt) {
-        cudaGraphSetConditional(cond, 0);
+        st->loop = 0;
+        if (in_graph) cudaGraphSetConditional(cond, 0);
         return;
     }
     int stop = 0;
@@ -374,8 +375,9 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
     if (!initial) st->first_iter = 0;
     st->parity ^= 1;
     for (int k = kAccRR; k < kAccCount; ++k) zero_acc(st, k);
+    st->loop = stop ? 0u : 1u;
     __threadfence();
-    cudaGraphSetConditional(cond, stop ? 0u : 1u);
+    if (in_graph) cudaGraphSetConditional(cond, stop ? 0u : 1u);
 }
 
 // Level l >= 1: zp = w D^-1 r (pre-smoothing from zero), restriction of r - A zp into level l + 1.
@@ -763,19 +765,39 @@ cudaError_t add_while(cudaStream_t s, cudaStream_t body_stream, cudaGraphConditi
     return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
 }
 
+// One iteration's loop body (everything after the update that tests convergence, up to the next update).
 template <typename T>
-cudaError_t enqueue_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream_t s, cudaStream_t body_stream) {
+void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_graph, uint32_t block_bytes, cudaStream_t bs) {
     const MgHierarchy& H = A.H;
     const MgLevel& L0 = H.L[0];
     const int g = H.grid_levels;
+    for (int l = 1; l < g; ++l) mg_restrict_kernel<<<wave(mg_restrict_kernel, H.L[l]), kBlock, 0, bs>>>(H, l);
+    mg_block_kernel<<<1, kBlockLevelThreads, block_bytes, bs>>>(H);
+    for (int l = g - 1; l >= 1; --l) {
+        mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[l]), kBlock, 0, bs>>>(H, l);
+        mg_smooth_kernel<false, T><<<wave(mg_smooth_kernel<false, T>, H.L[l]), kBlock, 0, bs>>>(A, l);
+    }
+    mg_prolong_kernel<<<wave(mg_prolong_kernel, L0), kBlock, 0, bs>>>(H, 0);
+    mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0), kBlock, 0, bs>>>(A, 0);
+    mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0), kBlock, 0, bs>>>(A);
+    mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, bs>>>(A, 0, h, in_graph);
+}
+
+uint32_t block_level_bytes(const MgHierarchy& H) {
+    uint32_t bytes = 0;
+    for (int l = H.grid_levels; l < H.levels; ++l) bytes += 4u * mg_block_words(H.L[l].n);
+    return bytes;
+}
+
+template <typename T>
+cudaError_t enqueue_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream_t s, cudaStream_t body_stream) {
+    const MgLevel& L0 = A.H.L[0];
     cudaStreamCaptureStatus cs;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &graph, nullptr, nullptr);
     if (e != cudaSuccess) return e;
     if (cs != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureImplicit;
-    uint32_t block_bytes = 0;
-    for (int l = g; l < H.levels; ++l) block_bytes += 4u * mg_block_words(H.L[l].n);
-
+    const uint32_t block_bytes = block_level_bytes(A.H);
     e = cudaMemsetAsync(A.st, 0, sizeof(MgState), s);
     if (e != cudaSuccess) return e;
     mg_setup_kernel<T><<<wave(mg_setup_kernel<T>, L0), kBlock, 0, s>>>(A);
@@ -784,20 +806,39 @@ cudaError_t enqueue_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream
         cudaGraphConditionalHandle h;
         e = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
         if (e != cudaSuccess) return e;
-        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, s>>>(A, 1, h);
-        e = add_while(s, body_stream, h, [&](cudaStream_t bs) {
-            for (int l = 1; l < g; ++l) mg_restrict_kernel<<<wave(mg_restrict_kernel, H.L[l]), kBlock, 0, bs>>>(H, l);
-            mg_block_kernel<<<1, kBlockLevelThreads, block_bytes, bs>>>(H);
-            for (int l = g - 1; l >= 1; --l) {
-                mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[l]), kBlock, 0, bs>>>(H, l);
-                mg_smooth_kernel<false, T><<<wave(mg_smooth_kernel<false, T>, H.L[l]), kBlock, 0, bs>>>(A, l);
-            }
-            mg_prolong_kernel<<<wave(mg_prolong_kernel, L0), kBlock, 0, bs>>>(H, 0);
-            mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0), kBlock, 0, bs>>>(A, 0);
-            mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0), kBlock, 0, bs>>>(A);
-            mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, bs>>>(A, 0, h);
-        });
+        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, s>>>(A, 1, h, 1);
+        e = add_while(s, body_stream, h, [&](cudaStream_t bs) { launch_body<T>(A, h, 1, block_bytes, bs); });
         if (e != cudaSuccess) return e;
+        if (A.ir) {
+            mg_accumulate_kernel<<<wave(mg_accumulate_kernel, L0), kBlock, 0, s>>>(A);
+            mg_residual_kernel<<<wave(mg_residual_kernel, L0), kBlock, 0, s>>>(A);
+        }
+    }
+    mg_finalize_kernel<<<wave(mg_finalize_kernel, L0), kBlock, 0, s>>>(A, out);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t run_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream_t s) {
+    const MgLevel& L0 = A.H.L[0];
+    const uint32_t block_bytes = block_level_bytes(A.H);
+    cudaError_t e = cudaMemsetAsync(A.st, 0, sizeof(MgState), s);
+    if (e != cudaSuccess) return e;
+    mg_setup_kernel<T><<<wave(mg_setup_kernel<T>, L0), kBlock, 0, s>>>(A);
+    const int passes = A.ir ? A.refinement + 1 : 1;
+    auto loop_flag = [&](uint32_t& flag) {
+        const cudaError_t r = cudaMemcpyAsync(&flag, &A.st->loop, sizeof(flag), cudaMemcpyDeviceToHost, s);
+        return r == cudaSuccess ? cudaStreamSynchronize(s) : r;
+    };
+    for (int pass = 0; pass < passes; ++pass) {
+        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, s>>>(A, 1, 0, 0);
+        for (;;) {  // bounded: every update counts an iteration and stops at max_iterations
+            uint32_t flag = 0;
+            if ((e = loop_flag(flag)) != cudaSuccess) return e;
+            if (!flag) break;
+            launch_body<T>(A, 0, 0, block_bytes, s);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
         if (A.ir) {
             mg_accumulate_kernel<<<wave(mg_accumulate_kernel, L0), kBlock, 0, s>>>(A);
             mg_residual_kernel<<<wave(mg_residual_kernel, L0), kBlock, 0, s>>>(A);
@@ -899,6 +940,10 @@ cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uin
 
 cudaError_t enqueue_mg_solve(const MgSolveArgs& args, bool fp64, PcgStatusDevice* status_out, cudaStream_t s, cudaStream_t body_stream) {
     return fp64 ? enqueue_typed<double>(args, status_out, s, body_stream) : enqueue_typed<float>(args, status_out, s, body_stream);
+}
+
+cudaError_t run_mg_solve_eager(const MgSolveArgs& args, bool fp64, PcgStatusDevice* status_out, cudaStream_t s) {
+    return fp64 ? run_typed<double>(args, status_out, s) : run_typed<float>(args, status_out, s);
 }
 
 }  // namespace smoke_b200

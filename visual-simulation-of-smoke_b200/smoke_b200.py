@@ -51,6 +51,7 @@ class SmokeLibrary:
         ("smoke_b200_get_face_velocity_cuda", [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
         ("smoke_b200_step_stages_cuda", [C.c_void_p, C.c_uint32]),
         ("smoke_b200_solve_pressure_cuda", [C.c_void_p]),
+        ("smoke_b200_solve_pressure_eager_cuda", [C.c_void_p]),
     ]
 
     def __init__(self, path: str = DEFAULT_LIBRARY, extensions: bool = True):
@@ -212,5 +213,7 @@ class Simulation:
     def step_stages(self, last_stage: int):
         _check(self.lib.smoke_b200_step_stages_cuda(self.handle, last_stage), "step_stages")
 
-    def solve_pressure(self):
-        _check(self.lib.smoke_b200_solve_pressure_cuda(self.handle), "solve_pressure")
+    def solve_pressure(self, eager: bool = False):
+        """Pressure solve of the current right-hand side (eager: every kernel launched directly, host-driven loop)."""
+        fn = self.lib.smoke_b200_solve_pressure_eager_cuda if eager else self.lib.smoke_b200_solve_pressure_cuda
+        _check(fn(self.handle), "solve_pressure")
