@@ -141,12 +141,14 @@ def dist_setup(n_gpus):
 
 
 def max_over_ranks(value: float, world: int) -> float:
+    """The largest of the ranks' values (every rank takes part; NCCL on GPUs, gloo on host-only test ranks)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
