@@ -36,9 +36,9 @@ REF_LIBRARY = os.path.join(ROOT, "oracle", "_ref", "libvisual-simulation-of-smok
 # (measured on a B200 with `bench.py --calibrate-reference`).
 REFERENCE_CG_ITERATIONS = 900
 SPINUP_STEPS = 30
-# Kernels of one step outside the pressure solve: vorticity, cell force, face force, 3 velocity pads, advect velocity,
-# rhs, project, scalar prep, 5 pads (velocity + 2 scalars), advect scalars, density fill.
-STEP_KERNELS = 17
+# Kernels of one step outside the pressure solve: vorticity, cell force, face force, velocity pad, advect velocity,
+# rhs, project, scalar prep, velocity pad, scalar pad, advect scalars, density fill.
+STEP_KERNELS = 12
 
 
 def mg_grid_levels(n):

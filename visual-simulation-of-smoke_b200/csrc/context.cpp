@@ -289,6 +289,13 @@ struct SmokeSimulationContext_t {
         return S;
     }
 
+    cudaError_t pad_velocity(ConstFaces v, cudaStream_t s) {
+        const int kinds[3] = {0, 1, 2};
+        const float* fields[3] = {v.u, v.v, v.w};
+        float* pads[3] = {pad.u, pad.v, pad.w};
+        return launch_pads(P, 3, kinds, fields, pads, s);
+    }
+
     // Stages of one step, in the reference's order (backend-cuda.cu:2000-2057, views excluded).
     void enqueue_stages(cudaStream_t s, uint32_t last_stage, bool capturing) {
         const ConstFaces solid{solid_vx, solid_vy, solid_vz};
@@ -296,9 +303,7 @@ struct SmokeSimulationContext_t {
         check(launch_cell_force(P, wx, wy, wz, wmag, density, temperature, force_x, force_y, force_z, occupancy, fx, fy, fz, s), "cell force");
         check(launch_face_force(P, as_const(A), fx, fy, fz, occupancy, solid, B, s), "face force");
         if (last_stage < SMOKE_B200_STAGE_ADVECT_VELOCITY) return;
-        check(launch_pad(P, 0, B.u, pad.u, s), "pad u");
-        check(launch_pad(P, 1, B.v, pad.v, s), "pad v");
-        check(launch_pad(P, 2, B.w, pad.w, s), "pad w");
+        check(pad_velocity(as_const(B), s), "pad velocity");
         check(launch_advect_velocity(P, as_const(B), as_const(pad), occupancy, solid, C, s), "advect velocity");
         if (last_stage < SMOKE_B200_STAGE_PRESSURE) return;
         check(launch_rhs(P, as_const(C), occupancy, anchor, rhs, s), "pressure rhs");
@@ -309,11 +314,13 @@ struct SmokeSimulationContext_t {
         check(launch_project(P, as_const(C), pressure, p64, occupancy, solid, A, s), "project");
         if (last_stage < SMOKE_B200_STAGE_SCALARS) return;
         check(launch_scalar_prep(P, temperature, temperature_source, density, density_source, occupancy, solid_temperature, temperature_tmp, density_tmp, s), "scalar sources");
-        check(launch_pad(P, 0, A.u, pad.u, s), "pad u");
-        check(launch_pad(P, 1, A.v, pad.v, s), "pad v");
-        check(launch_pad(P, 2, A.w, pad.w, s), "pad w");
-        check(launch_pad(P, 4, temperature_tmp, pad_t, s), "pad temperature");
-        check(launch_pad(P, 3, density_tmp, pad_d, s), "pad density");
+        check(pad_velocity(as_const(A), s), "pad velocity");
+        {
+            const int kinds[2] = {4, 3};
+            const float* fields[2] = {temperature_tmp, density_tmp};
+            float* pads[2] = {pad_t, pad_d};
+            check(launch_pads(P, 2, kinds, fields, pads, s), "pad scalars");
+        }
         check(launch_advect_scalars(P, as_const(A), as_const(pad), occupancy, temperature_tmp, pad_t, density_tmp, pad_d, solid_temperature, temperature, density, s), "advect scalars");
         check(launch_density_fill(fill_list, fill_count, density, fill_blocks, s), "density fill");
     }

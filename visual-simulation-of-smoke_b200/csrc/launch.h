@@ -38,9 +38,10 @@ cudaError_t launch_cell_force(const StepParams& P, const float* wx, const float*
 // Forces: out = settled(in + dt * face-average of f) (domain, solid and periodic face rules applied).
 cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* fx, const float* fy, const float* fz, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
 // Padded copies (PadField): element count of the copy of field kind (0-2 face components, 3 density, 4
-// temperature), and the kernel that fills it from f.
+// temperature).
 size_t pad_count(const StepParams& P, int kind);
-cudaError_t launch_pad(const StepParams& P, int kind, const float* f, float* pad, cudaStream_t s);
+// Fills the padded copies of `count` (1..3) fields of the given kinds in one launch.
+cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const float* const* fields, float* const* pads, cudaStream_t s);
 // Velocity self-advection: out = settled(semi-Lagrangian sample of in along in); pad holds the padded copies of in.
 cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, ConstFaces pad, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
 // Pressure right-hand side from the advected velocity.

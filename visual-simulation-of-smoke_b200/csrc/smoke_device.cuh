@@ -56,6 +56,8 @@ struct StepParams {
     uint32_t n, nu, nv, nw; // cell and face counts
     FastDiv div_nx, div_ny, div_slab;            // cells: x fastest
     FastDiv div_fx[3], div_fy[3];                // faces of axis a: row length and rows per slab
+    float inv_h;                                 // 1 / h (grid coordinates of sample positions)
+    double dt_over_h64;                          // dt / h in FP64 (gradient of the refined FP64 pressure)
 };
 
 #if defined(__CUDACC__)
@@ -436,14 +438,26 @@ __device__ inline float centred_tap(const float* __restrict__ f, int x, int y, i
 }
 
 // Vorticity of the centred velocity at an in-range fluid cell: central differences / h (backend-cuda.cu:885-900).
+// A cell one cell or more inside every wall reads its 12 centred values directly; others go through the ghost rules.
 __device__ __forceinline__ float4 vorticity_at(const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, int x, int y, int z, const StepParams& P) {
-    const float h = P.h;
-    const float dvz_dy = 0.5f * (centred_tap<2>(w, x, y + 1, z, P) - centred_tap<2>(w, x, y - 1, z, P)) / h;
-    const float dvy_dz = 0.5f * (centred_tap<1>(v, x, y, z + 1, P) - centred_tap<1>(v, x, y, z - 1, P)) / h;
-    const float dvx_dz = 0.5f * (centred_tap<0>(u, x, y, z + 1, P) - centred_tap<0>(u, x, y, z - 1, P)) / h;
-    const float dvz_dx = 0.5f * (centred_tap<2>(w, x + 1, y, z, P) - centred_tap<2>(w, x - 1, y, z, P)) / h;
-    const float dvy_dx = 0.5f * (centred_tap<1>(v, x + 1, y, z, P) - centred_tap<1>(v, x - 1, y, z, P)) / h;
-    const float dvx_dy = 0.5f * (centred_tap<0>(u, x, y + 1, z, P) - centred_tap<0>(u, x, y - 1, z, P)) / h;
+    if (x > 0 && x < P.nx - 1 && y > 0 && y < P.ny - 1 && z > 0 && z < P.nz - 1) {
+        const float hh = 0.5f * P.inv_h;
+        const float dvz_dy = hh * (centred<2>(w, x, y + 1, z, P) - centred<2>(w, x, y - 1, z, P));
+        const float dvy_dz = hh * (centred<1>(v, x, y, z + 1, P) - centred<1>(v, x, y, z - 1, P));
+        const float dvx_dz = hh * (centred<0>(u, x, y, z + 1, P) - centred<0>(u, x, y, z - 1, P));
+        const float dvz_dx = hh * (centred<2>(w, x + 1, y, z, P) - centred<2>(w, x - 1, y, z, P));
+        const float dvy_dx = hh * (centred<1>(v, x + 1, y, z, P) - centred<1>(v, x - 1, y, z, P));
+        const float dvx_dy = hh * (centred<0>(u, x, y + 1, z, P) - centred<0>(u, x, y - 1, z, P));
+        const float wx = dvz_dy - dvy_dz, wy = dvx_dz - dvz_dx, wz = dvy_dx - dvx_dy;
+        return make_float4(wx, wy, wz, sqrtf(wx * wx + wy * wy + wz * wz));
+    }
+    const float hh = 0.5f * P.inv_h;
+    const float dvz_dy = hh * (centred_tap<2>(w, x, y + 1, z, P) - centred_tap<2>(w, x, y - 1, z, P));
+    const float dvy_dz = hh * (centred_tap<1>(v, x, y, z + 1, P) - centred_tap<1>(v, x, y, z - 1, P));
+    const float dvx_dz = hh * (centred_tap<0>(u, x, y, z + 1, P) - centred_tap<0>(u, x, y, z - 1, P));
+    const float dvz_dx = hh * (centred_tap<2>(w, x + 1, y, z, P) - centred_tap<2>(w, x - 1, y, z, P));
+    const float dvy_dx = hh * (centred_tap<1>(v, x + 1, y, z, P) - centred_tap<1>(v, x - 1, y, z, P));
+    const float dvx_dy = hh * (centred_tap<0>(u, x, y + 1, z, P) - centred_tap<0>(u, x, y - 1, z, P));
     const float wx = dvz_dy - dvy_dz;
     const float wy = dvx_dz - dvz_dx;
     const float wz = dvy_dx - dvx_dy;

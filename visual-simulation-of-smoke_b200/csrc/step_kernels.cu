@@ -130,10 +130,18 @@ __global__ void __launch_bounds__(kThreads) cell_force_kernel(const __grid_const
         int x, y, z;
         cell_xyz(P, q, x, y, z);
         ay += -P.alpha * density[q] + P.beta * (temperature[q] - P.ambient);
-        const float h = P.h;
-        const float gx = 0.5f * (flow_cell(wm, x + 1, y, z, P) - flow_cell(wm, x - 1, y, z, P)) / h;
-        const float gy = 0.5f * (flow_cell(wm, x, y + 1, z, P) - flow_cell(wm, x, y - 1, z, P)) / h;
-        const float gz = 0.5f * (flow_cell(wm, x, y, z + 1, P) - flow_cell(wm, x, y, z - 1, P)) / h;
+        const float h = P.h, hh = 0.5f * P.inv_h;
+        float gx, gy, gz;
+        if (x > 0 && x < P.nx - 1 && y > 0 && y < P.ny - 1 && z > 0 && z < P.nz - 1) {  // all six neighbours in range
+            const uint32_t sy = P.nx, sz = static_cast<uint32_t>(P.nx) * P.ny;
+            gx = hh * (__ldg(wm + q + 1) - __ldg(wm + q - 1));
+            gy = hh * (__ldg(wm + q + sy) - __ldg(wm + q - sy));
+            gz = hh * (__ldg(wm + q + sz) - __ldg(wm + q - sz));
+        } else {
+            gx = hh * (flow_cell(wm, x + 1, y, z, P) - flow_cell(wm, x - 1, y, z, P));
+            gy = hh * (flow_cell(wm, x, y + 1, z, P) - flow_cell(wm, x, y - 1, z, P));
+            gz = hh * (flow_cell(wm, x, y, z + 1, P) - flow_cell(wm, x, y, z - 1, P));
+        }
         const float gmag = sqrtf(gx * gx + gy * gy + gz * gz);
         if (!(gmag < 1.0e-6f)) {
             const float inv = 1.0f / gmag;
@@ -169,7 +177,7 @@ __device__ __forceinline__ void face_force_one(const StepParams& P, uint32_t q, 
             weight += 1.0f;
         }
         const float base = in[fidx<A>(P, a, b, c)];
-        return weight > 0.0f ? base + P.dt * (sum / weight) : base;
+        return weight > 0.0f ? base + P.dt * (weight > 1.0f ? 0.5f * sum : sum) : base;  // exact halving
     });
 }
 
@@ -222,17 +230,42 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
     }
 }
 
-// Padded copy of field KIND (see PadField): one thread per padded cell.
+// Padded copies (see PadField) of up to 3 fields in one launch: block z-range c * pz_max .. for field c, one thread
+// per padded cell, 32 x 8 cells per block.
+struct PadJob {
+    const float* f[3];
+    float* out[3];
+    int kind[3];
+    int count;
+    int pz_max;
+};
+
 template <int KIND>
-__global__ void __launch_bounds__(kThreads) pad_kernel(const __grid_constant__ StepParams P, const float* __restrict__ f, float* __restrict__ out) {
+__device__ __forceinline__ float pad_value(const StepParams& P, const float* __restrict__ f, int i, int j, int k) {
     const int fx = P.nx + (KIND == 0), fy = P.ny + (KIND == 1), fz = P.nz + (KIND == 2);
-    const uint32_t px = fx + 2 * kPad, py = fy + 2 * kPad, pz = fz + 2 * kPad;
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= px * py * pz) return;
-    const uint32_t row = t / px, slab = row / py;
-    const int i = static_cast<int>(t - row * px) - kPad, j = static_cast<int>(row - slab * py) - kPad, k = static_cast<int>(slab) - kPad;
-    const bool in = i >= 0 && i < fx && j >= 0 && j < fy && k >= 0 && k < fz;
-    out[t] = in ? f[(static_cast<uint32_t>(k) * fy + j) * fx + i] : boundary_tap<KIND>(f, i, j, k, P);
+    if (i >= 0 && i < fx && j >= 0 && j < fy && k >= 0 && k < fz) return __ldg(f + (static_cast<uint32_t>(k) * fy + j) * fx + i);
+    return boundary_tap<KIND>(f, i, j, k, P);
+}
+
+__global__ void __launch_bounds__(256) pad_kernel(const __grid_constant__ StepParams P, const __grid_constant__ PadJob J) {
+    const int c = blockIdx.z / J.pz_max, kp = blockIdx.z - c * J.pz_max;
+    if (c >= J.count) return;
+    const int kind = c == 0 ? J.kind[0] : (c == 1 ? J.kind[1] : J.kind[2]);
+    const int px = P.nx + (kind == 0) + 2 * kPad, py = P.ny + (kind == 1) + 2 * kPad, pz = P.nz + (kind == 2) + 2 * kPad;
+    const int ip = blockIdx.x * 32 + threadIdx.x, jp = blockIdx.y * 8 + threadIdx.y;
+    if (ip >= px || jp >= py || kp >= pz) return;
+    const int i = ip - kPad, j = jp - kPad, k = kp - kPad;
+    const float* f = c == 0 ? J.f[0] : (c == 1 ? J.f[1] : J.f[2]);
+    float* out = c == 0 ? J.out[0] : (c == 1 ? J.out[1] : J.out[2]);
+    float v;
+    switch (kind) {
+    case 0: v = pad_value<0>(P, f, i, j, k); break;
+    case 1: v = pad_value<1>(P, f, i, j, k); break;
+    case 2: v = pad_value<2>(P, f, i, j, k); break;
+    case 3: v = pad_value<3>(P, f, i, j, k); break;
+    default: v = pad_value<4>(P, f, i, j, k); break;
+    }
+    out[(static_cast<uint32_t>(kp) * py + jp) * px + ip] = v;
 }
 
 // ------------------------------------------------------------------------------------------ pressure rhs
@@ -247,7 +280,7 @@ __global__ void __launch_bounds__(kThreads) rhs_kernel(const __grid_constant__ S
     int x, y, z;
     cell_xyz(P, q, x, y, z);
     const float h = P.h;
-    const float div = (u[fidx<0>(P, x + 1, y, z)] - u[fidx<0>(P, x, y, z)] + v[fidx<1>(P, x, y + 1, z)] - v[fidx<1>(P, x, y, z)] + w[fidx<2>(P, x, y, z + 1)] - w[fidx<2>(P, x, y, z)]) / h;
+    const float div = (u[fidx<0>(P, x + 1, y, z)] - u[fidx<0>(P, x, y, z)] + v[fidx<1>(P, x, y + 1, z)] - v[fidx<1>(P, x, y, z)] + w[fidx<2>(P, x, y, z + 1)] - w[fidx<2>(P, x, y, z)]) * P.inv_h;
     float bsum = 0.0f;
     if (x == 0 && P.flow[0].type == kFlowOutflow) bsum += P.flow[0].pressure;
     if (x == P.nx - 1 && P.flow[1].type == kFlowOutflow) bsum += P.flow[1].pressure;
@@ -272,7 +305,7 @@ __device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, con
         const float base = in[fidx<A>(P, a, b, c)];
         if (!(hl && hr)) return base;
         if (p64 != nullptr) {  // FP64 solution of a refined solve: the gradient keeps its precision
-            const double g = static_cast<double>(P.dt) * (p64[cidx(P, r[0], r[1], r[2])] - p64[cidx(P, l[0], l[1], l[2])]) / static_cast<double>(P.h);
+            const double g = P.dt_over_h64 * (p64[cidx(P, r[0], r[1], r[2])] - p64[cidx(P, l[0], l[1], l[2])]);
             return base - static_cast<float>(g);
         }
         const float pr = p[cidx(P, r[0], r[1], r[2])];
@@ -359,7 +392,7 @@ __global__ void __launch_bounds__(kThreads) views_kernel(const __grid_constant__
     wy[q] = o.y;
     wz[q] = o.z;
     wm[q] = o.w;
-    div[q] = (u[fidx<0>(P, x + 1, y, z)] - u[fidx<0>(P, x, y, z)] + v[fidx<1>(P, x, y + 1, z)] - v[fidx<1>(P, x, y, z)] + w[fidx<2>(P, x, y, z + 1)] - w[fidx<2>(P, x, y, z)]) / P.h;
+    div[q] = (u[fidx<0>(P, x + 1, y, z)] - u[fidx<0>(P, x, y, z)] + v[fidx<1>(P, x, y + 1, z)] - v[fidx<1>(P, x, y, z)] + w[fidx<2>(P, x, y, z + 1)] - w[fidx<2>(P, x, y, z)]) * P.inv_h;
 }
 
 // ------------------------------------------------------------------------------------------ occupancy-derived
@@ -496,6 +529,8 @@ StepParams make_params(const SmokeSimulationConfig& cfg) {
     P.nu = (nx + 1) * ny * nz;
     P.nv = nx * (ny + 1) * nz;
     P.nw = nx * ny * (nz + 1);
+    P.inv_h = 1.0f / cfg.cell_size;
+    P.dt_over_h64 = static_cast<double>(cfg.dt) / static_cast<double>(cfg.cell_size);
     P.div_nx = FastDiv(nx);
     P.div_ny = FastDiv(ny);
     P.div_slab = FastDiv(nx * ny);
@@ -537,15 +572,18 @@ size_t pad_count(const StepParams& P, int kind) {
     return static_cast<size_t>(P.nx + (kind == 0) + 2 * kPad) * (P.ny + (kind == 1) + 2 * kPad) * (P.nz + (kind == 2) + 2 * kPad);
 }
 
-cudaError_t launch_pad(const StepParams& P, int kind, const float* f, float* pad, cudaStream_t s) {
-    const unsigned grid = static_cast<unsigned>((pad_count(P, kind) + kThreads - 1) / kThreads);
-    switch (kind) {
-    case 0: pad_kernel<0><<<grid, kThreads, 0, s>>>(P, f, pad); break;
-    case 1: pad_kernel<1><<<grid, kThreads, 0, s>>>(P, f, pad); break;
-    case 2: pad_kernel<2><<<grid, kThreads, 0, s>>>(P, f, pad); break;
-    case 3: pad_kernel<3><<<grid, kThreads, 0, s>>>(P, f, pad); break;
-    default: pad_kernel<4><<<grid, kThreads, 0, s>>>(P, f, pad); break;
+cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const float* const* fields, float* const* pads, cudaStream_t s) {
+    if (count < 1 || count > 3) return cudaErrorInvalidValue;
+    PadJob J{};
+    J.count = count;
+    J.pz_max = P.nz + 1 + 2 * kPad;
+    for (int c = 0; c < count; ++c) {
+        J.f[c] = fields[c];
+        J.out[c] = pads[c];
+        J.kind[c] = kinds[c];
     }
+    const dim3 grid((P.nx + 1 + 2 * kPad + 31) / 32, (P.ny + 1 + 2 * kPad + 7) / 8, J.pz_max * count);
+    pad_kernel<<<grid, dim3(32, 8), 0, s>>>(P, J);
     return cudaGetLastError();
 }
 
