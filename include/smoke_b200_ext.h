@@ -11,7 +11,9 @@
  *  - face-velocity access: the reference has no velocity setter (backend-cuda.cu:2085-2159), so a scene can
  *    only be seeded from rest; the setter lets a test or a checkpoint restore an arbitrary MAC state;
  *  - stage-wise stepping: runs the step's stages in order up to a given one, so each stage can be compared
- *    with a CPU restatement on its own.
+ *    with a CPU restatement on its own;
+ *  - batches: one call advances many independent scenes (the reference steps one context per call, each with its
+ *    own graph launch).
  */
 #ifndef SMOKE_B200_EXT_H
 #define SMOKE_B200_EXT_H
@@ -96,6 +98,20 @@ SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimu
  * device; the Jacobi and fixed CG solves are one cooperative kernel); the outcome is read with
  * smoke_b200_get_solver_status_cuda. */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext context);
+
+/* A batch: a fixed set of contexts advanced together, one step each, by one CUDA-graph launch in which every
+ * context's step is an independent branch, so scenes of any (different) sizes fill the GPU together. No reference
+ * counterpart (the reference launches one graph per context, backend-cuda.cu:2161-2172).
+ *  - create: the contexts must be distinct, on the current device, and idle (create waits for their streams). The
+ *    batch records each context's step as it is configured now; after smoke_b200_set_solver_cuda or
+ *    update_occupancy on a member, create the batch again. `stream` (NULL: a new stream) runs the batch graph;
+ *  - step: ordered after all work enqueued so far on every member's stream, and every member's later work is
+ *    ordered after it, so update_*, get_view and the status calls keep working per context;
+ *  - destroy: waits for the batch stream; the contexts stay alive and usable alone. */
+typedef struct SmokeB200Batch_t* SmokeB200Batch;
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_batch_create_cuda(const SmokeSimulationContext* contexts, uint32_t count, void* stream, SmokeB200Batch* out_batch);
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_batch_step_cuda(SmokeB200Batch batch);
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_batch_destroy_cuda(SmokeB200Batch batch);
 
 /* The same solve with every solver kernel launched directly on the context stream, no graph: the multigrid loop is
  * driven from the host, which reads the loop condition after each iteration (one stream synchronisation per

@@ -367,6 +367,64 @@ struct SmokeSimulationContext_t {
     }
 };
 
+// A batch of contexts advanced by one graph launch: the step of every context, recorded into one graph by stream
+// capture with one branch per context (each context's capture stream), branches independent of one another.
+struct SmokeB200Batch_t {
+    std::vector<SmokeSimulationContext_t*> contexts;
+    cudaStream_t stream = nullptr;
+    bool owns_stream = false;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaEvent_t> ready;  // one per context: the context's stream reached the batch step
+    cudaEvent_t done = nullptr;      // the batch step finished
+
+    ~SmokeB200Batch_t() {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (cudaEvent_t e : ready) cudaEventDestroy(e);
+        if (done) cudaEventDestroy(done);
+        if (owns_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    void build() {
+        const cudaStream_t root = contexts.front()->capture_stream;
+        cudaEvent_t fork = nullptr;
+        check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "batch fork event");
+        std::vector<cudaEvent_t> joins(contexts.size(), nullptr);
+        cudaGraph_t graph = nullptr;
+        cudaError_t err = cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal);
+        try {
+            check(err, "begin batch capture");
+            check(cudaEventRecord(fork, root), "batch fork");
+            for (size_t i = 0; i < contexts.size(); ++i) {
+                SmokeSimulationContext_t* c = contexts[i];
+                if (i > 0) check(cudaStreamWaitEvent(c->capture_stream, fork, 0), "batch branch");
+                c->enqueue_stages(c->capture_stream, SMOKE_B200_STAGE_SCALARS, true);
+                if (i > 0) {
+                    check(cudaEventCreateWithFlags(&joins[i], cudaEventDisableTiming), "batch join event");
+                    check(cudaEventRecord(joins[i], c->capture_stream), "batch join");
+                    check(cudaStreamWaitEvent(root, joins[i], 0), "batch join");
+                }
+            }
+            check(cudaStreamEndCapture(root, &graph), "end batch capture");
+        } catch (...) {
+            if (err == cudaSuccess) {
+                cudaGraph_t broken = nullptr;
+                cudaStreamEndCapture(root, &broken);
+                if (broken) cudaGraphDestroy(broken);
+            }
+            cudaEventDestroy(fork);
+            for (cudaEvent_t e : joins)
+                if (e) cudaEventDestroy(e);
+            throw;
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        cudaEventDestroy(fork);
+        for (cudaEvent_t e : joins)
+            if (e) cudaEventDestroy(e);
+        check(ie, "instantiate batch graph");
+    }
+};
+
 namespace {
 
 SmokeSimulationResult ok_or_fail(cudaError_t e) { return e == cudaSuccess ? SMOKE_SIMULATION_RESULT_OK : SMOKE_SIMULATION_RESULT_BACKEND_FAILURE; }
@@ -612,6 +670,61 @@ SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext c) {
         c->stepped = true;
         return SMOKE_SIMULATION_RESULT_OK;
     });
+}
+
+SmokeSimulationResult smoke_b200_batch_create_cuda(const SmokeSimulationContext* contexts, uint32_t count, void* stream, SmokeB200Batch* out_batch) {
+    if (contexts == nullptr || out_batch == nullptr || count == 0) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    *out_batch = nullptr;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (contexts[i] == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+        for (uint32_t j = 0; j < i; ++j)
+            if (contexts[j] == contexts[i]) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    }
+    std::unique_ptr<SmokeB200Batch_t> b(new (std::nothrow) SmokeB200Batch_t{});
+    if (!b) return SMOKE_SIMULATION_RESULT_OUT_OF_MEMORY;
+    const SmokeSimulationResult r = guarded([&] {
+        b->contexts.assign(contexts, contexts + count);
+        b->stream = static_cast<cudaStream_t>(stream);
+        if (b->stream == nullptr) {
+            check(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "batch stream");
+            b->owns_stream = true;
+        }
+        b->ready.assign(count, nullptr);
+        for (cudaEvent_t& e : b->ready) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "batch event");
+        check(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "batch event");
+        for (SmokeSimulationContext_t* c : b->contexts) check(cudaStreamSynchronize(c->stream), "batch: contexts idle");
+        b->build();
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+    if (r != SMOKE_SIMULATION_RESULT_OK) return r;
+    *out_batch = b.release();
+    return SMOKE_SIMULATION_RESULT_OK;
+}
+
+SmokeSimulationResult smoke_b200_batch_step_cuda(SmokeB200Batch batch) {
+    if (batch == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        for (size_t i = 0; i < batch->contexts.size(); ++i) {
+            SmokeSimulationContext_t* c = batch->contexts[i];
+            check(cudaEventRecord(batch->ready[i], c->stream), "batch step: context ready");
+            check(cudaStreamWaitEvent(batch->stream, batch->ready[i], 0), "batch step: wait");
+        }
+        check(cudaGraphLaunch(batch->exec, batch->stream), "batch step");
+        check(cudaEventRecord(batch->done, batch->stream), "batch step: done");
+        for (SmokeSimulationContext_t* c : batch->contexts) {
+            check(cudaStreamWaitEvent(c->stream, batch->done, 0), "batch step: order the context");
+            c->views_stale = true;
+            c->stepped = true;
+        }
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+SmokeSimulationResult smoke_b200_batch_destroy_cuda(SmokeB200Batch batch) {
+    if (batch == nullptr) return SMOKE_SIMULATION_RESULT_OK;
+    if (batch->stream) cudaStreamSynchronize(batch->stream);
+    delete batch;
+    return SMOKE_SIMULATION_RESULT_OK;
 }
 
 SmokeSimulationResult smoke_b200_solve_pressure_eager_cuda(SmokeSimulationContext c) {

@@ -474,6 +474,7 @@ __global__ void __launch_bounds__(kThreads) mg_pq_kernel(const __grid_constant__
             uint32_t nb[6];
             nbr_all(F, A.H.fper, c, nb);
             const uint16_t code = F.code[c.q];
+            const float rv = r[c.q];  // loaded with the rest, before this tile's stores
             const float pv = Z[c.q] + fb * po[c.q];
             float pnb[6];
 #pragma unroll
@@ -482,7 +483,7 @@ __global__ void __launch_bounds__(kThreads) mg_pq_kernel(const __grid_constant__
             pn[c.q] = pv;
             A.W.q[c.q] = qv;
             pq += static_cast<T>(pv) * static_cast<T>(qv);
-            pr += static_cast<T>(pv) * static_cast<T>(r[c.q]);
+            pr += static_cast<T>(pv) * static_cast<T>(rv);
         });
         block_accumulate<T>(st, kAccPQ, pq, kAccPR, pr);
     }

@@ -52,6 +52,9 @@ class SmokeLibrary:
         ("smoke_b200_step_stages_cuda", [C.c_void_p, C.c_uint32]),
         ("smoke_b200_solve_pressure_cuda", [C.c_void_p]),
         ("smoke_b200_solve_pressure_eager_cuda", [C.c_void_p]),
+        ("smoke_b200_batch_create_cuda", [C.POINTER(C.c_void_p), C.c_uint32, C.c_void_p, C.POINTER(C.c_void_p)]),
+        ("smoke_b200_batch_step_cuda", [C.c_void_p]),
+        ("smoke_b200_batch_destroy_cuda", [C.c_void_p]),
     ]
 
     def __init__(self, path: str = DEFAULT_LIBRARY, extensions: bool = True):
@@ -217,3 +220,30 @@ class Simulation:
         """Pressure solve of the current right-hand side (eager: every kernel launched directly, host-driven loop)."""
         fn = self.lib.smoke_b200_solve_pressure_eager_cuda if eager else self.lib.smoke_b200_solve_pressure_cuda
         _check(fn(self.handle), "solve_pressure")
+
+
+class Batch:
+    """Several Simulations advanced by one graph launch (smoke_b200_batch_*_cuda). Create it after the members are
+    configured (solver, occupancy); `stream` (a torch.cuda.Stream, optional) runs the batch graph."""
+
+    def __init__(self, sims, stream=None):
+        self.sims = list(sims)
+        self.lib = self.sims[0].lib
+        handles = (C.c_void_p * len(self.sims))(*[s.handle.value for s in self.sims])
+        out = C.c_void_p()
+        _check(self.lib.smoke_b200_batch_create_cuda(handles, len(self.sims), C.c_void_p(stream.cuda_stream if stream is not None else 0), C.byref(out)), "batch_create")
+        self.handle = out
+
+    def step(self):
+        _check(self.lib.smoke_b200_batch_step_cuda(self.handle), "batch_step")
+
+    def close(self):
+        if self.handle is not None and self.handle.value:
+            _check(self.lib.smoke_b200_batch_destroy_cuda(self.handle), "batch_destroy")
+        self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
