@@ -393,6 +393,161 @@ def bench_b200(args, rank, world, local):
     return line
 
 
+def _line(metric, ms, args, world, config, **extra):
+    line = {"metric": metric, "value": round(ms, 4), "unit": "ms/step", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (fp64 reductions)", "data": "synthetic (seeded plume scenes)", "config": config}
+    line.update(extra)
+    return line
+
+
+def bench_plume64(args, rank, world, local):
+    """Config 1: the plain method at 64^3 (trilinear advection, Jacobi-PCG to 1e-5, at most 500 iterations), with the
+    multigrid form on the same states beside it."""
+    import torch
+
+    import plume_scene
+    import smoke_b200
+
+    n = 64
+    lib = smoke_b200.SmokeLibrary()
+    stream = torch.cuda.Stream()
+    cfg = plume_scene.plume_config(n, abi.LINEAR)
+    sim = smoke_b200.Simulation(lib, cfg, stream)
+    driver = plume_scene.PlumeDriver(sim, n, seed=1 + rank)
+    forms = {"plain_fp32_jacobi": dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP32, max_iterations=500, tolerance=1e-5, refinement=0),
+             "multigrid_fp64": FORMS["multigrid_fp64"]}
+    sim.set_solver(**forms["plain_fp32_jacobi"])
+    run_steps(sim, driver, 0, SPINUP_STEPS, None)
+    state = save_state(sim)
+    flush = L2Flush()
+    results, clocks = {}, None
+    for name, form in forms.items():
+        restore_state(sim, state)
+        sim.set_solver(**form)
+        run_steps(sim, driver, SPINUP_STEPS, args.warmup, flush)
+        barrier(world)
+        with ClockSampler(local) as c:
+            t, its, res = run_steps(sim, driver, SPINUP_STEPS + args.warmup, args.steps, flush, status=True)
+        clocks = clocks or c
+        results[name] = (max_over_ranks(statistics.mean(t), world), statistics.mean(its), max(res))
+    sim.close()
+    if rank != 0:
+        return None
+    ms, its, res = results["plain_fp32_jacobi"]
+    return _line("ms/step and PCG iterations at 64^3 to rel-res 1e-5 (plain method)", ms, args, world,
+                 {"workload": "plume 64^3, trilinear, closed walls, source 8x4x8 at the bottom centre; Jacobi-PCG FP32 to 1e-5 (max 500)", "grid": [n, n, n],
+                  "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+                 dtype="f32", pcg_iterations=round(its, 1), rel_residual_max=res, cells_per_s=round(n ** 3 * world / (ms * 1e-3), 1),
+                 forms={k: {"ms_per_step": round(v[0], 4), "pcg_iterations": round(v[1], 1), "rel_residual_max": v[2]} for k, v in results.items()},
+                 clocks=clocks.summary() if clocks else None)
+
+
+def bench_large(args, rank, world, local):
+    """Config 3: 256 x 384 x 256 with a solid sphere and two plume sources, multigrid FCG to 1e-5."""
+    import torch
+
+    import plume_scene
+    import smoke_b200
+
+    cfg, occ, boxes = plume_scene.large_scene(seed=1 + rank)
+    lib = smoke_b200.SmokeLibrary()
+    stream = torch.cuda.Stream()
+    sim = smoke_b200.Simulation(lib, cfg, stream)
+    with torch.cuda.stream(stream):
+        occ_dev = torch.from_numpy(occ).cuda()
+        sim.update_occupancy(occ_dev)
+    stream.synchronize()
+    sim.set_solver(**FORMS[HEADLINE])
+    driver = plume_scene.SceneDriver(sim, boxes, seed=1 + rank)
+    flush = L2Flush()
+    spin = 10
+    run_steps(sim, driver, 0, spin + args.warmup, flush)
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        t, its, res = run_steps(sim, driver, spin + args.warmup, args.steps, flush, status=True)
+    cells = cfg.nx * cfg.ny * cfg.nz
+    roof = solver_kernel_roofline(sim, cells, *load_peaks(), repeats=3, bytes_per_iteration=MG_BYTES_PER_CELL_ITERATION, kernel="multigrid-preconditioned FCG solve (one graph launch of the mg_* kernels)")
+    sim.close()
+    ms = max_over_ranks(statistics.mean(t), world)
+    if rank != 0:
+        return None
+    return _line("ms/step and PCG iterations, 256x384x256 scene with a solid sphere, to rel-res 1e-5", ms, args, world,
+                 {"workload": "256x384x256, h=1/256, sphere r=40 cells at (128, 153.6, 128), two 32x8x32 floor sources, monotone cubic; multigrid FCG, FP64 dots + refinement",
+                  "grid": [cfg.nx, cfg.ny, cfg.nz], "spinup_steps": spin, "l2": "inputs (25.2 M cells) larger than L2; also flushed", "parallelism": f"replicas x{world}"},
+                 pcg_iterations=round(statistics.mean(its), 1), true_rel_residual_max=max(res), cells_per_s=round(cells * world / (ms * 1e-3), 1), roofline=roof,
+                 clocks=clocks.summary())
+
+
+def bench_batched(args, rank, world, local):
+    """Config 5: 48 independent plumes of uneven sizes and obstacles advanced together by one graph launch per
+    step (smoke_b200_batch_step_cuda); each scene also stepped alone for the per-scene latency distribution."""
+    import torch
+
+    import plume_scene
+    import smoke_b200
+
+    scenes_ = plume_scene.batched_scenes(48, seed=1 + rank)
+    lib = smoke_b200.SmokeLibrary()
+    sims, drivers, keep = [], [], []
+    for cfg, occ, boxes in scenes_:
+        stream = torch.cuda.Stream()
+        sim = smoke_b200.Simulation(lib, cfg, stream)
+        with torch.cuda.stream(stream):
+            o = torch.from_numpy(occ).cuda()
+            sim.update_occupancy(o)
+        keep.append(o)
+        sim.set_solver(**FORMS[HEADLINE])
+        sims.append(sim)
+        drivers.append(plume_scene.SceneDriver(sim, boxes, seed=1 + rank))
+    torch.cuda.synchronize()
+    cells = sum(s.config.nx * s.config.ny * s.config.nz for s in sims)
+    flush = L2Flush()
+    # solo: one step per scene alone (after a short spin-up), for the per-scene latency distribution
+    solo = []
+    for k, (sim, drv) in enumerate(zip(sims, drivers)):
+        run_steps(sim, drv, 0, 3, None)
+        t, _, _ = run_steps(sim, drv, 3, 2, flush)
+        solo.append(min(t))
+    batch_stream = torch.cuda.Stream()
+    batch = smoke_b200.Batch(sims, batch_stream)
+
+    def batch_steps(first, count, timed):
+        times = []
+        for k in range(count):
+            for sim, drv in zip(sims, drivers):
+                drv.apply(first + k)
+            with torch.cuda.stream(batch_stream):
+                flush()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(batch_stream)
+            batch.step()
+            e1.record(batch_stream)
+            batch_stream.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return times
+
+    batch_steps(5, args.warmup, False)
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        bt = batch_steps(5 + args.warmup, args.steps, True)
+    iters = [s.solver_status().iterations for s in sims]
+    batch.close()
+    for s in sims:
+        s.close()
+    ms = max_over_ranks(statistics.mean(bt), world)
+    if rank != 0:
+        return None
+    solo_sorted = sorted(solo)
+    return _line("ms per batched step of 48 uneven plumes (aggregate cells/s, per-scene latency)", ms, args, world,
+                 {"workload": "48 plumes, extents drawn in [32,128]x[32,192]x[32,128], one floor source and 0-3 spheres each, monotone cubic, multigrid FCG to 1e-5; one graph launch per batched step",
+                  "scenes": len(sims), "cells": cells, "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+                 cells_per_s=round(cells * world / (ms * 1e-3), 1),
+                 solo_step_ms={"p50": round(statistics.median(solo), 4), "p99": round(solo_sorted[min(len(solo) - 1, int(0.99 * len(solo)))], 4), "sum": round(sum(solo), 3)},
+                 batch_speedup_vs_sequential=round(sum(solo) / ms, 2), pcg_iterations={"min": min(iters), "max": max(iters), "mean": round(statistics.mean(iters), 1)},
+                 clocks=clocks.summary())
+
+
 def bench_reference(args, rank, world, local):
     import torch
 
@@ -498,6 +653,8 @@ def main():
     ap.add_argument("--calibrate-reference", action="store_true")
     ap.add_argument("--calibrate-counts", type=int, nargs="*", default=[200, 300, 400, 500, 600, 800, 1000])
     ap.add_argument("--profile", choices=["solve", "solve-graph", "step"], help="run a profiling workload instead of the benchmark")
+    ap.add_argument("--workload", default="plume128", choices=["plume128", "plume64", "large", "batched"],
+                    help="plume128: the headline (default); plume64, large, batched: the other benchmark configurations")
     ap.add_argument("--profile-count", type=int, default=1)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -508,7 +665,10 @@ def main():
     if args.profile:
         profile_workload(args)
         return
-    line = bench_reference(args, rank, world, local) if args.impl == "reference" else bench_b200(args, rank, world, local)
+    if args.impl == "reference":
+        line = bench_reference(args, rank, world, local)
+    else:
+        line = {"plume128": bench_b200, "plume64": bench_plume64, "large": bench_large, "batched": bench_batched}[args.workload](args, rank, world, local)
     barrier(world) if args.impl == "b200" else None
     if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)

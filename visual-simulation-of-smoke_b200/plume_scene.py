@@ -48,37 +48,41 @@ def source_box(n: int):
     return (slice(x0, x0 + bx), slice(0, by), slice(x0, x0 + bx))
 
 
-class PlumeDriver:
-    """Per-step inputs of the plume scene for one Simulation (any library). All work is enqueued on the
-    simulation's stream; `inputs_for(step)` is the host-side input of that step (pinned)."""
+class SceneDriver:
+    """Per-step inputs of a plume scene with any grid and any source boxes, for one Simulation (any library). Every
+    box holds density 1 and temperature 1 and drives an inflow v_y = 1 + xi (xi drawn per cell and step, the
+    boxes' cells in box order). All work is enqueued on the simulation's stream; `inputs_for(step)` is the host-side
+    input of that step (pinned)."""
 
-    def __init__(self, sim, n: int, seed: int = 1):
+    def __init__(self, sim, boxes, seed: int = 1):
         import torch
 
         self.sim = sim
-        self.n = n
         self.seed = seed
         self.dt = float(sim.config.dt)
-        zs, ys, xs = source_box(n)
-        self.box = (zs, ys, xs)
-        shape = (zs.stop - zs.start, ys.stop - ys.start, xs.stop - xs.start)
-        self.box_shape = shape
-        z, y, x = np.meshgrid(np.arange(zs.start, zs.stop), np.arange(ys.start, ys.stop), np.arange(xs.start, xs.stop), indexing="ij")
-        self.box_cells = (z * n * n + y * n + x).reshape(-1)
+        nx, ny, nz = sim.config.nx, sim.config.ny, sim.config.nz
+        self.shape = (nz, ny, nx)
+        self.boxes = list(boxes)
+        cells, self.sizes = [], []
+        for zs, ys, xs in self.boxes:
+            z, y, x = np.meshgrid(np.arange(zs.start, zs.stop), np.arange(ys.start, ys.stop), np.arange(xs.start, xs.stop), indexing="ij")
+            cells.append((z * ny * nx + y * nx + x).reshape(-1))
+            self.sizes.append((zs.stop - zs.start, ys.stop - ys.start, xs.stop - xs.start))
+        self.box_cells = np.concatenate(cells)
         dev = torch.device("cuda")
         with torch.cuda.stream(sim.stream):
-            self.force_y = torch.zeros((n, n, n), dtype=torch.float32, device=dev)
-            self.density_source = torch.zeros((n, n, n), dtype=torch.float32, device=dev)
-            self.temperature_source = torch.zeros((n, n, n), dtype=torch.float32, device=dev)
-            self.xi_dev = torch.zeros(shape, dtype=torch.float32, device=dev)
+            self.force_y = torch.zeros(self.shape, dtype=torch.float32, device=dev)
+            self.density_source = torch.zeros(self.shape, dtype=torch.float32, device=dev)
+            self.temperature_source = torch.zeros(self.shape, dtype=torch.float32, device=dev)
+            self.xi_dev = torch.zeros(self.box_cells.size, dtype=torch.float32, device=dev)
             self.total_dev = torch.zeros(1, dtype=torch.float32, device=dev)
-        self.xi_host = torch.zeros(shape, dtype=torch.float32).pin_memory()
+        self.xi_host = torch.zeros(self.box_cells.size, dtype=torch.float32).pin_memory()
         self.total_host = torch.zeros(1, dtype=torch.float32).pin_memory()
         self.h2d_bytes = self.xi_host.numel() * 4
         self.d2h_bytes = 4
 
     def inputs_for(self, step: int):
-        self.xi_host.copy_(__import__("torch").from_numpy(uniform(self.seed, step, self.box_cells, -0.1, 0.1).reshape(self.box_shape)))
+        self.xi_host.copy_(__import__("torch").from_numpy(uniform(self.seed, step, self.box_cells, -0.1, 0.1)))
         return self.xi_host
 
     def apply(self, step: int, host_inputs=None):
@@ -87,15 +91,19 @@ class PlumeDriver:
 
         sim = self.sim
         xi = host_inputs if host_inputs is not None else self.inputs_for(step)
-        zs, ys, xs = self.box
         with torch.cuda.stream(sim.stream):
             self.xi_dev.copy_(xi, non_blocking=True)
             _, vy, _ = sim.view(abi.VIEW_FLOW_VELOCITY)
-            self.force_y[zs, ys, xs] = (1.0 + self.xi_dev - vy[zs, ys, xs]) / self.dt
             rho = sim.view(abi.VIEW_DENSITY)
-            self.density_source[zs, ys, xs] = (1.0 - rho[zs, ys, xs]) / self.dt
             tem = sim.view(abi.VIEW_TEMPERATURE)
-            self.temperature_source[zs, ys, xs] = (1.0 - tem[zs, ys, xs]) / self.dt
+            start = 0
+            for (zs, ys, xs), size in zip(self.boxes, self.sizes):
+                count = size[0] * size[1] * size[2]
+                xi_box = self.xi_dev[start:start + count].reshape(size)
+                start += count
+                self.force_y[zs, ys, xs] = (1.0 + xi_box - vy[zs, ys, xs]) / self.dt
+                self.density_source[zs, ys, xs] = (1.0 - rho[zs, ys, xs]) / self.dt
+                self.temperature_source[zs, ys, xs] = (1.0 - tem[zs, ys, xs]) / self.dt
             sim.update_force(None, self.force_y, None)
             sim.update_density_source(self.density_source)
             sim.update_temperature_source(self.temperature_source)
@@ -108,6 +116,64 @@ class PlumeDriver:
             self.total_dev.copy_(torch.sum(self.sim.view(abi.VIEW_DENSITY)).reshape(1))
             self.total_host.copy_(self.total_dev, non_blocking=True)
         return self.total_host
+
+
+class PlumeDriver(SceneDriver):
+    """The n^3 plume: one source box at the bottom centre (source_box)."""
+
+    def __init__(self, sim, n: int, seed: int = 1):
+        self.n = n
+        super().__init__(sim, [source_box(n)], seed)
+        self.box = self.boxes[0]
+
+
+# --------------------------------------------------------------------------------------------- other scenes
+def scene_config(nx: int, ny: int, nz: int, mode: int = abi.MONOTONIC_CUBIC, pressure_iterations: int = 64) -> abi.Config:
+    """The plume scene's parameters on an nx x ny x nz grid, h = 1/nx."""
+    return abi.make_config(nx, ny, nz, cell_size=1.0 / nx, dt=0.01, pressure_iterations=pressure_iterations, ambient=0.0, alpha=0.08, beta=0.97, epsilon=0.35, mode=mode)
+
+
+def sphere_occupancy(shape_zyx, centre_xyz, radius: float) -> np.ndarray:
+    """uint8 occupancy (z, y, x): 1 where the cell centre lies within `radius` cells of `centre_xyz` (cell units)."""
+    nz, ny, nx = shape_zyx
+    z, y, x = np.meshgrid(np.arange(nz) + 0.5, np.arange(ny) + 0.5, np.arange(nx) + 0.5, indexing="ij")
+    cx, cy, cz = centre_xyz
+    return (((x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2) <= radius * radius).astype(np.uint8)
+
+
+def large_scene(seed: int = 1):
+    """256 x 384 x 256 with a solid sphere (radius 40 cells, centred at x = z = 128 and 40% of the height) and two
+    32 x 8 x 32 source boxes on the floor at seeded x, z positions. Returns (config, occupancy, boxes)."""
+    nx, ny, nz = 256, 384, 256
+    cfg = scene_config(nx, ny, nz)
+    occ = sphere_occupancy((nz, ny, nx), (128.0, 0.4 * ny, 128.0), 40.0)
+    pos = uniform(seed, 0, np.arange(4), 0.0, 1.0)
+    boxes = []
+    for k in range(2):
+        x0 = int(pos[2 * k] * (nx - 32))
+        z0 = int(pos[2 * k + 1] * (nz - 32))
+        boxes.append((slice(z0, z0 + 32), slice(0, 8), slice(x0, x0 + 32)))
+    return cfg, occ, boxes
+
+
+def batched_scenes(count: int = 48, seed: int = 1):
+    """`count` independent plume scenes of uneven sizes: per-axis extents drawn in [32, 128] x [32, 192] x
+    [32, 128], one source box (nx/8 x ny/16 x nz/8) at a random floor position and 0-3 solid spheres above it.
+    Returns a list of (config, occupancy, boxes)."""
+    out = []
+    for s in range(count):
+        u = uniform(seed, 1000 + s, np.arange(16), 0.0, 1.0)
+        nx, ny, nz = 32 + int(u[0] * 97), 32 + int(u[1] * 161), 32 + int(u[2] * 97)
+        cfg = scene_config(nx, ny, nz)
+        bx, by, bz = max(1, nx // 8), max(1, ny // 16), max(1, nz // 8)
+        x0, z0 = int(u[3] * (nx - bx)), int(u[4] * (nz - bz))
+        occ = np.zeros((nz, ny, nx), dtype=np.uint8)
+        for k in range(int(u[5] * 4)):  # 0-3 spheres in the upper part of the domain
+            r = 3.0 + u[6 + k] * 0.12 * min(nx, nz)
+            centre = (u[9 + k] * nx, (0.45 + 0.4 * u[12 + k]) * ny, (0.25 + 0.5 * u[6 + k]) * nz)
+            occ |= sphere_occupancy((nz, ny, nx), centre, r)
+        out.append((cfg, occ, [(slice(z0, z0 + bz), slice(0, by), slice(x0, x0 + bx))]))
+    return out
 
 
 def closed_box_residual(p, b):
