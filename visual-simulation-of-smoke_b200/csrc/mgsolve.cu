@@ -6,7 +6,7 @@
 //  - levels: level l+1 halves every extent of level l (rounding up) down to <= 4 cells per axis; a coarse cell is
 //    active (fluid) when any child is; each level's operator is the masked 7-point stencil of its active cells,
 //    built with the fine rules (periodic wrap, OUTFLOW faces on the diagonal) but without the anchor;
-//  - smoothing: damped Jacobi, weight kOmega; the pre-smoothing sweep starts from zero;
+//  - smoothing: damped Jacobi, weight kOmega = 6/7; the pre-smoothing sweep starts from zero;
 //  - restriction: r_{l+1}(C) = 1/2 * sum of the residuals of C's (up to 8) children after pre-smoothing; with the
 //    trilinear prolongation below this is the Petrov-Galerkin scaling of the 7-point operator (R A P ~ 2 A_coarse);
 //  - prolongation: cell-centred trilinear (weights 3/4 and 1/4 per axis); a corner outside the domain or on an
@@ -38,7 +38,7 @@ namespace {
 constexpr int TX = 32, TY = 4, TZ = 2;  // cells of one block; even extents, so blocks hold whole parents
 constexpr int kThreads = TX * TY * TZ;
 constexpr int kBlockLevelThreads = 512;
-constexpr float kOmega = 0.8f;
+constexpr float kOmega = 6.0f / 7.0f;  // damped Jacobi weight: the optimal smoothing factor of the 7-point Laplacian in 3D
 constexpr int kCoarsestSweeps = 16;
 constexpr uint32_t kTag = 0x7fc0feedu;  // t of an inactive coarse cell (a NaN payload arithmetic never produces)
 constexpr int kMaxPasses = 8;           // refinement passes in the graph (refinement is clamped to kMaxPasses - 1)
@@ -103,36 +103,21 @@ __device__ __forceinline__ bool wrap_c(int& v, int n, int per) {
     return true;
 }
 
-// Coarse index pair of one axis for fine coordinate v: the parent p = v >> 1 and its neighbour toward v's side
-// (wrapped across a periodic edge, clamped to p at a wall, where the corner takes the parent's value).
-__device__ __forceinline__ void corner_axis(int v, int n, int per, int& p, int& s) {
-    p = v >> 1;
-    s = (v & 1) ? p + 1 : p - 1;
-    if (s < 0) s = per ? s + n : p;
-    else if (s >= n) s = per ? s - n : p;
-}
 
-// Trilinear prolongation of C.t at fine cell (x, y, z); a corner on an inactive coarse cell (kTag) or beyond a
-// wall takes the parent's value.
-__device__ __forceinline__ float prolong_tagged(const MgLevel& C, const int* fper, int x, int y, int z) {
-    int x0, x1, y0, y1, z0, z1;
-    corner_axis(x, C.nx, fper[0], x0, x1);
-    corner_axis(y, C.ny, fper[1], y0, y1);
-    corner_axis(z, C.nz, fper[2], z0, z1);
-    const uint32_t nx = C.nx;
-    const uint32_t r00 = (static_cast<uint32_t>(z0) * C.ny + y0) * nx, r01 = (static_cast<uint32_t>(z0) * C.ny + y1) * nx;
-    const uint32_t r10 = (static_cast<uint32_t>(z1) * C.ny + y0) * nx, r11 = (static_cast<uint32_t>(z1) * C.ny + y1) * nx;
-    const bool wx = x1 == x0, wy = y1 == y0, wz = z1 == z0;  // clamped at a wall (or a 1-cell periodic axis)
-    const float* t = C.t;
-    const float c0 = t[r00 + x0], c1 = t[r00 + x1], c2 = t[r01 + x0], c3 = t[r01 + x1];
-    const float c4 = t[r10 + x0], c5 = t[r10 + x1], c6 = t[r11 + x0], c7 = t[r11 + x1];
+// Trilinear weights of the 8 corners of a fine cell; c(m) loads corner m (bit 0: the x neighbour, bit 1: y, bit 2: z
+// of the parent, corner 0). A corner clamped at a wall (w*), or on an inactive coarse cell (kTag), takes the
+// parent's value.
+template <class T>
+__device__ __forceinline__ float prolong_corners(bool wx, bool wy, bool wz, T&& c) {
+    const float c0 = c(0), c1 = c(1), c2 = c(2), c3 = c(3), c4 = c(4), c5 = c(5), c6 = c(6), c7 = c(7);
     const float parent = is_tag(c0) ? 0.0f : c0;
-    auto v = [&](float c, bool wall) { return (wall || is_tag(c)) ? parent : c; };
+    auto v = [&](float x, bool wall) { return (wall || is_tag(x)) ? parent : x; };
     // weights (3/4 or 1/4 per axis): 27/64 parent, 9/64 edge, 3/64 face-diagonal, 1/64 opposite corner
     const float near = 0.421875f * parent + 0.140625f * (v(c1, wx) + v(c2, wy) + v(c4, wz));
     const float far = 0.046875f * (v(c3, wx || wy) + v(c5, wx || wz) + v(c6, wy || wz)) + 0.015625f * v(c7, wx || wy || wz);
     return near + far;
 }
+
 
 // ---------------------------------------------------------------------------------------------- block helpers
 // Level kernels: one thread per cell of a TX x TY x TZ tile; block (bx, by, bz) walks the tiles (bx, by, k) for k in
@@ -404,16 +389,48 @@ __global__ void __launch_bounds__(kThreads) mg_restrict_kernel(const __grid_cons
     });
 }
 
-// Level l: zp += P(t_{l+1}) on active cells (in place; pointwise).
+// Level l: zp += P(t_{l+1}) on active cells (in place). One thread per coarse cell (X, Y, Z) of level l + 1: it
+// loads the 3 x 3 x 3 coarse neighbourhood once and writes its up to 8 children, each a trilinear blend of the
+// parent and the 7 corners toward the child (see prolong_corners).
 __global__ void __launch_bounds__(kThreads) mg_prolong_kernel(const __grid_constant__ MgHierarchy H, int l) {
     const MgLevel& F = H.L[l];
     const MgLevel& C = H.L[l + 1];
-    for_tiles(F, [&](const Cell& c) {
+    for_tiles(C, [&](const Cell& c) {
         if (!c.in) return;
-        const uint16_t code = F.code[c.q];
-        const float zp = F.zp[c.q];
-        const float p = prolong_tagged(C, H.fper, c.x, c.y, c.z);
-        if (active(code)) F.zp[c.q] = zp + p;
+        // per axis: index of the neighbour on each side (wrapped on a periodic axis, the cell itself at a wall)
+        auto side = [](int v, int n, int per, int d) {
+            int s = v + d;
+            if (s < 0) s = per ? s + n : v;
+            else if (s >= n) s = per ? s - n : v;
+            return s;
+        };
+        const int xs[3] = {side(c.x, C.nx, H.fper[0], -1), c.x, side(c.x, C.nx, H.fper[0], 1)};
+        const int ys[3] = {side(c.y, C.ny, H.fper[1], -1), c.y, side(c.y, C.ny, H.fper[1], 1)};
+        const int zs[3] = {side(c.z, C.nz, H.fper[2], -1), c.z, side(c.z, C.nz, H.fper[2], 1)};
+        float t[3][3][3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const uint32_t row = (static_cast<uint32_t>(zs[k]) * C.ny + ys[j]) * C.nx;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) t[k][j][i] = C.t[row + xs[i]];
+            }
+#pragma unroll
+        for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+            for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+                for (int dx = 0; dx < 2; ++dx) {
+                    const int x = 2 * c.x + dx, y = 2 * c.y + dy, z = 2 * c.z + dz;
+                    if (x >= F.nx || y >= F.ny || z >= F.nz) continue;
+                    const int ix = dx ? 2 : 0, iy = dy ? 2 : 0, iz = dz ? 2 : 0;  // the corner side of each axis
+                    const float p = prolong_corners(xs[ix] == c.x, ys[iy] == c.y, zs[iz] == c.z, [&](int m) {
+                        return t[(m & 4) ? iz : 1][(m & 2) ? iy : 1][(m & 1) ? ix : 1];
+                    });
+                    const uint32_t fq = lidx(F, x, y, z);
+                    if (active(F.code[fq])) F.zp[fq] += p;
+                }
     });
 }
 
@@ -775,10 +792,10 @@ void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_grap
     for (int l = 1; l < g; ++l) mg_restrict_kernel<<<wave(mg_restrict_kernel, H.L[l]), kBlock, 0, bs>>>(H, l);
     mg_block_kernel<<<1, kBlockLevelThreads, block_bytes, bs>>>(H);
     for (int l = g - 1; l >= 1; --l) {
-        mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[l]), kBlock, 0, bs>>>(H, l);
+        mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[l + 1]), kBlock, 0, bs>>>(H, l);
         mg_smooth_kernel<false, T><<<wave(mg_smooth_kernel<false, T>, H.L[l]), kBlock, 0, bs>>>(A, l);
     }
-    mg_prolong_kernel<<<wave(mg_prolong_kernel, L0), kBlock, 0, bs>>>(H, 0);
+    mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[1]), kBlock, 0, bs>>>(H, 0);
     mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0), kBlock, 0, bs>>>(A, 0);
     mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0), kBlock, 0, bs>>>(A);
     mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, bs>>>(A, 0, h, in_graph);

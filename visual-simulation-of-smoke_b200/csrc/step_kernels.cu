@@ -230,14 +230,15 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
     }
 }
 
-// Padded copies (see PadField) of up to 3 fields in one launch: block z-range c * pz_max .. for field c, one thread
-// per padded cell, 32 x 8 cells per block.
+// Padded copies (see PadField) of up to 3 fields in one launch: block z-range c * pz_blocks .. for field c; each
+// thread fills kPadPlanes cells of one column (loads first, then stores), 32 x 8 columns per block.
+constexpr int kPadPlanes = 4;
 struct PadJob {
     const float* f[3];
     float* out[3];
     int kind[3];
     int count;
-    int pz_max;
+    int pz_blocks;  // blocks per field along z (kPadPlanes planes each)
 };
 
 template <int KIND>
@@ -248,24 +249,30 @@ __device__ __forceinline__ float pad_value(const StepParams& P, const float* __r
 }
 
 __global__ void __launch_bounds__(256) pad_kernel(const __grid_constant__ StepParams P, const __grid_constant__ PadJob J) {
-    const int c = blockIdx.z / J.pz_max, kp = blockIdx.z - c * J.pz_max;
+    const int c = blockIdx.z / J.pz_blocks, kp0 = (blockIdx.z - c * J.pz_blocks) * kPadPlanes;
     if (c >= J.count) return;
     const int kind = c == 0 ? J.kind[0] : (c == 1 ? J.kind[1] : J.kind[2]);
     const int px = P.nx + (kind == 0) + 2 * kPad, py = P.ny + (kind == 1) + 2 * kPad, pz = P.nz + (kind == 2) + 2 * kPad;
     const int ip = blockIdx.x * 32 + threadIdx.x, jp = blockIdx.y * 8 + threadIdx.y;
-    if (ip >= px || jp >= py || kp >= pz) return;
-    const int i = ip - kPad, j = jp - kPad, k = kp - kPad;
+    if (ip >= px || jp >= py || kp0 >= pz) return;
+    const int i = ip - kPad, j = jp - kPad;
     const float* f = c == 0 ? J.f[0] : (c == 1 ? J.f[1] : J.f[2]);
     float* out = c == 0 ? J.out[0] : (c == 1 ? J.out[1] : J.out[2]);
-    float v;
-    switch (kind) {
-    case 0: v = pad_value<0>(P, f, i, j, k); break;
-    case 1: v = pad_value<1>(P, f, i, j, k); break;
-    case 2: v = pad_value<2>(P, f, i, j, k); break;
-    case 3: v = pad_value<3>(P, f, i, j, k); break;
-    default: v = pad_value<4>(P, f, i, j, k); break;
+    float v[kPadPlanes];
+#pragma unroll
+    for (int u = 0; u < kPadPlanes; ++u) {
+        const int k = kp0 + u - kPad;
+        switch (kind) {
+        case 0: v[u] = pad_value<0>(P, f, i, j, k); break;
+        case 1: v[u] = pad_value<1>(P, f, i, j, k); break;
+        case 2: v[u] = pad_value<2>(P, f, i, j, k); break;
+        case 3: v[u] = pad_value<3>(P, f, i, j, k); break;
+        default: v[u] = pad_value<4>(P, f, i, j, k); break;
+        }
     }
-    out[(static_cast<uint32_t>(kp) * py + jp) * px + ip] = v;
+#pragma unroll
+    for (int u = 0; u < kPadPlanes; ++u)
+        if (kp0 + u < pz) out[(static_cast<uint32_t>(kp0 + u) * py + jp) * px + ip] = v[u];
 }
 
 // ------------------------------------------------------------------------------------------ pressure rhs
@@ -576,13 +583,13 @@ cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const 
     if (count < 1 || count > 3) return cudaErrorInvalidValue;
     PadJob J{};
     J.count = count;
-    J.pz_max = P.nz + 1 + 2 * kPad;
+    J.pz_blocks = (P.nz + 1 + 2 * kPad + kPadPlanes - 1) / kPadPlanes;
     for (int c = 0; c < count; ++c) {
         J.f[c] = fields[c];
         J.out[c] = pads[c];
         J.kind[c] = kinds[c];
     }
-    const dim3 grid((P.nx + 1 + 2 * kPad + 31) / 32, (P.ny + 1 + 2 * kPad + 7) / 8, J.pz_max * count);
+    const dim3 grid((P.nx + 1 + 2 * kPad + 31) / 32, (P.ny + 1 + 2 * kPad + 7) / 8, J.pz_blocks * count);
     pad_kernel<<<grid, dim3(32, 8), 0, s>>>(P, J);
     return cudaGetLastError();
 }
