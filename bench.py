@@ -342,10 +342,13 @@ def bench_b200(args, rank, world, local):
     state = save_state(sim)
     step0 = SPINUP_STEPS
     results = {}
+    tunes = {}
     clocks = None
     for name, form in FORMS.items():
         restore_state(sim, state)
         sim.set_solver(**form)
+        if args.tune:  # launch shapes for this solver form (the tuner restores the state it timed on)
+            tunes[name] = sim.autotune()
         run_steps(sim, driver, step0, args.warmup, flush)
         barrier(world)
         torch.cuda.synchronize()
@@ -360,6 +363,8 @@ def bench_b200(args, rank, world, local):
     # e2e through the ABI (headline form), same state
     restore_state(sim, state)
     sim.set_solver(**FORMS[HEADLINE])
+    if args.tune:
+        sim.autotune()  # cached: the headline form's shapes
     run_e2e(sim, driver, step0, args.warmup)
     barrier(world)
     e2e_ms, _ = run_e2e(sim, driver, step0 + args.warmup, args.steps)
@@ -387,10 +392,20 @@ def bench_b200(args, rank, world, local):
                 "includes": "per-step box inputs H2D, velocity/density/temperature views, source/force updates, step, total-density D2H, host sync"},
         "gpu_launches": round(args.steps * (STEP_KERNELS + solver_launches(n, its, FORMS[HEADLINE]["refinement"]))),
         "clocks": clocks.summary() if clocks is not None else None,
+        "launch_tune": {k: tune_summary(v) for k, v in tunes.items()} if tunes else "defaults (--no-tune)",
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
     return line
+
+
+def tune_summary(rep):
+    """The autotuner's choice in words, with the step times it measured for the default and chosen shapes."""
+    c = rep["chosen"]
+    out = {"advect_tile": abi.ADVECT_TILE_NAMES[c["advect_tile"]], "mg_wave": abi.MG_WAVE_NAMES[c["mg_wave"]], "pcg_grid": abi.PCG_GRID_NAMES[c["pcg_grid"]]}
+    if not rep["from_cache"]:
+        out.update(default_ms=round(rep["default_ms"], 4), chosen_ms=round(rep["chosen_ms"], 4), candidates=len(rep["records"]))
+    return out
 
 
 def _line(metric, ms, args, world, config, **extra):
@@ -420,10 +435,12 @@ def bench_plume64(args, rank, world, local):
     run_steps(sim, driver, 0, SPINUP_STEPS, None)
     state = save_state(sim)
     flush = L2Flush()
-    results, clocks = {}, None
+    results, clocks, tunes = {}, None, {}
     for name, form in forms.items():
         restore_state(sim, state)
         sim.set_solver(**form)
+        if args.tune:
+            tunes[name] = tune_summary(sim.autotune())
         run_steps(sim, driver, SPINUP_STEPS, args.warmup, flush)
         barrier(world)
         with ClockSampler(local) as c:
@@ -439,7 +456,7 @@ def bench_plume64(args, rank, world, local):
                   "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
                  dtype="f32", pcg_iterations=round(its, 1), rel_residual_max=res, cells_per_s=round(n ** 3 * world / (ms * 1e-3), 1),
                  forms={k: {"ms_per_step": round(v[0], 4), "pcg_iterations": round(v[1], 1), "rel_residual_max": v[2]} for k, v in results.items()},
-                 clocks=clocks.summary() if clocks else None)
+                 clocks=clocks.summary() if clocks else None, launch_tune=tunes or "defaults (--no-tune)")
 
 
 def bench_large(args, rank, world, local):
@@ -461,7 +478,9 @@ def bench_large(args, rank, world, local):
     driver = plume_scene.SceneDriver(sim, boxes, seed=1 + rank)
     flush = L2Flush()
     spin = 10
-    run_steps(sim, driver, 0, spin + args.warmup, flush)
+    run_steps(sim, driver, 0, spin, flush)
+    tune = tune_summary(sim.autotune()) if args.tune else "defaults (--no-tune)"
+    run_steps(sim, driver, spin, args.warmup, flush)
     barrier(world)
     with ClockSampler(local) as clocks:
         t, its, res = run_steps(sim, driver, spin + args.warmup, args.steps, flush, status=True)
@@ -475,7 +494,7 @@ def bench_large(args, rank, world, local):
                  {"workload": "256x384x256, h=1/256, sphere r=40 cells at (128, 153.6, 128), two 32x8x32 floor sources, monotone cubic; multigrid FCG, FP64 dots + refinement",
                   "grid": [cfg.nx, cfg.ny, cfg.nz], "spinup_steps": spin, "l2": "inputs (25.2 M cells) larger than L2; also flushed", "parallelism": f"replicas x{world}"},
                  pcg_iterations=round(statistics.mean(its), 1), true_rel_residual_max=max(res), cells_per_s=round(cells * world / (ms * 1e-3), 1), roofline=roof,
-                 clocks=clocks.summary())
+                 clocks=clocks.summary(), launch_tune=tune)
 
 
 def bench_batched(args, rank, world, local):
@@ -504,8 +523,11 @@ def bench_batched(args, rank, world, local):
     flush = L2Flush()
     # solo: one step per scene alone (after a short spin-up), for the per-scene latency distribution
     solo = []
+    tuned = 0
     for k, (sim, drv) in enumerate(zip(sims, drivers)):
         run_steps(sim, drv, 0, 3, None)
+        if args.tune:
+            tuned += 0 if sim.autotune(steps=2)["from_cache"] else 1
         t, _, _ = run_steps(sim, drv, 3, 2, flush)
         solo.append(min(t))
     batch_stream = torch.cuda.Stream()
@@ -545,7 +567,7 @@ def bench_batched(args, rank, world, local):
                  cells_per_s=round(cells * world / (ms * 1e-3), 1),
                  solo_step_ms={"p50": round(statistics.median(solo), 4), "p99": round(solo_sorted[min(len(solo) - 1, int(0.99 * len(solo)))], 4), "sum": round(sum(solo), 3)},
                  batch_speedup_vs_sequential=round(sum(solo) / ms, 2), pcg_iterations={"min": min(iters), "max": max(iters), "mean": round(statistics.mean(iters), 1)},
-                 clocks=clocks.summary())
+                 clocks=clocks.summary(), launch_tune=f"each scene autotuned alone before the batch ({tuned} timed, {len(sims) - tuned} from the cache)" if args.tune else "defaults (--no-tune)")
 
 
 def bench_reference(args, rank, world, local):
@@ -600,6 +622,9 @@ def profile_workload(args):
     sim = smoke_b200.Simulation(lib, plume_scene.plume_config(n, abi.MONOTONIC_CUBIC), stream)
     driver = plume_scene.PlumeDriver(sim, n, seed=1)
     sim.set_solver(**FORMS[HEADLINE])
+    if args.shapes:  # explicit launch shapes (the autotuner's timing launches stay out of the profile)
+        a, w, g = (int(v) for v in args.shapes.split(","))
+        sim.set_launch_tune(advect_tile=a, mg_wave=w, pcg_grid=g)
     run_steps(sim, driver, 0, SPINUP_STEPS, None)
     for k in range(args.profile_count):
         if args.profile == "step":
@@ -656,6 +681,8 @@ def main():
     ap.add_argument("--workload", default="plume128", choices=["plume128", "plume64", "large", "batched"],
                     help="plume128: the headline (default); plume64, large, batched: the other benchmark configurations")
     ap.add_argument("--profile-count", type=int, default=1)
+    ap.add_argument("--no-tune", dest="tune", action="store_false", help="keep the default launch shapes (skip the autotuner)")
+    ap.add_argument("--shapes", default="", help="--profile only: launch shapes 'advect_tile,mg_wave,pcg_grid' (default: the defaults)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_setup(args.gpus)

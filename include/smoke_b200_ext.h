@@ -32,6 +32,10 @@ typedef enum SmokeB200SolverMode {
     SMOKE_B200_SOLVER_JACOBI_PCG = 1,
     /* Flexible CG preconditioned by one geometric multigrid V(1,1) cycle; same stopping rule as JACOBI_PCG. */
     SMOKE_B200_SOLVER_MG_FCG = 2,
+    /* Flexible CG preconditioned by the learned network set with smoke_b200_set_preconditioner_net_cuda (z = N(r));
+     * same stopping rule, so the network changes the iteration count, not the answer. With warm_start = 2 the
+     * network's estimate N(b) is also the initial guess (needs refinement >= 1). */
+    SMOKE_B200_SOLVER_LEARNED_FCG = 3,
 } SmokeB200SolverMode;
 
 typedef enum SmokeB200Reduction {
@@ -45,7 +49,8 @@ typedef struct SmokeB200SolverDesc {
     int32_t max_iterations;  /* JACOBI_PCG: iteration cap per refinement pass (FIXED_CG uses pressure_iterations) */
     float tolerance;         /* JACOBI_PCG: target ||b - A x||_2 / ||b||_2 */
     uint32_t refinement;     /* number of extra passes allowed when the FP64 true residual misses tolerance */
-    uint32_t warm_start;     /* 1: start from the previous step's pressure instead of 0 */
+    uint32_t warm_start;     /* 1: start from the previous step's pressure instead of 0 (with refinement >= 1);
+                                2 (LEARNED_FCG): start from the network's estimate of the pressure */
 } SmokeB200SolverDesc;
 
 typedef enum SmokeB200SolveStatus {
@@ -112,6 +117,98 @@ typedef struct SmokeB200Batch_t* SmokeB200Batch;
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_batch_create_cuda(const SmokeSimulationContext* contexts, uint32_t count, void* stream, SmokeB200Batch* out_batch);
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_batch_step_cuda(SmokeB200Batch batch);
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_batch_destroy_cuda(SmokeB200Batch batch);
+
+/* Launch shapes of a context's step (no reference counterpart; the reference fixes its launch shapes at compile
+ * time). Every shape computes the same values: the advection shape changes which faces or cells a block of 256
+ * threads covers, bit for bit the same results; the two solver grids change only the order in which the FP64 dot
+ * products are summed. */
+typedef struct SmokeB200LaunchTune {
+    uint32_t advect_tile;  /* advection blocks: 0 flat (256 consecutive faces or cells, the default); boxes of
+                              1: 32x8x1, 2: 32x4x2, 3: 16x4x4, 4: 8x8x4 faces or cells */
+    uint32_t mg_wave;      /* multigrid level kernels, grid depth: 0, 1 (default), 2, 3: 1/2, 1, 2, 4 waves of
+                              resident blocks; 4: one block per 32x4x2 tile */
+    uint32_t pcg_grid;     /* persistent CG kernel (FIXED_CG, JACOBI_PCG): 0 all resident blocks (default), 1 half,
+                              2 a quarter */
+    uint32_t reserved;     /* 0 */
+} SmokeB200LaunchTune;
+
+/* One timed candidate of smoke_b200_autotune_cuda. */
+typedef struct SmokeB200TuneRecord {
+    SmokeB200LaunchTune tune;
+    float ms_per_step;     /* best of the timed repeats, device time (CUDA events) */
+    uint32_t iterations;   /* pressure iterations of the last timed step */
+} SmokeB200TuneRecord;
+
+#define SMOKE_B200_TUNE_MAX_RECORDS 16
+#define SMOKE_B200_TUNE_FORCE 1u /* autotune flag: time the candidates even when the process has a result cached */
+
+typedef struct SmokeB200TuneReport {
+    SmokeB200LaunchTune chosen;
+    float default_ms;      /* ms per step of the default shapes (0 when the result came from the cache) */
+    float chosen_ms;       /* ms per step of the chosen shapes (0 when the result came from the cache) */
+    uint32_t from_cache;   /* 1: an earlier call in this process tuned the same grid, solver and device */
+    uint32_t record_count;
+    SmokeB200TuneRecord records[SMOKE_B200_TUNE_MAX_RECORDS];
+} SmokeB200TuneReport;
+
+/* Sets the launch shapes of the context's step and rebuilds its step graph (BACKEND_FAILURE for an unknown code).
+ * Like smoke_b200_set_solver_cuda, this is not ordered against work in flight on other streams. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_set_launch_tune_cuda(SmokeSimulationContext context, const SmokeB200LaunchTune* tune);
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_get_launch_tune_cuda(SmokeSimulationContext context, SmokeB200LaunchTune* out);
+
+/* Autotuner: times the context's own step under candidate launch shapes and keeps the fastest. Coordinate search
+ * from the current shapes: every advection shape, then every grid of the selected solver (multigrid depth, or the
+ * persistent CG grid), each candidate timed as `steps` (0: 4) graph steps from the same state, best of two
+ * repeats, after one untimed step. The context's device state is saved before and restored after (one temporary
+ * device allocation of the context's size), so tuning does not advance the simulation. The result is cached per
+ * process by device, grid extents, advection mode and solver settings: a later call for a context with the same
+ * key applies the cached shapes without timing unless `flags` has SMOKE_B200_TUNE_FORCE. Synchronises the context
+ * stream. `report` (optional) receives the candidates and their times. Tune before creating a batch that holds
+ * the context: a batch keeps the shapes its members had when it was created. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_autotune_cuda(SmokeSimulationContext context, uint32_t steps, uint32_t flags, SmokeB200TuneReport* report);
+
+/* Learned preconditioner (no reference counterpart): a 3-level 3-D U-Net on (r * s, fluid mask), s = sqrt(n) / ||r||,
+ * whose output y gives N(r) = y / s on fluid cells (0 on solids), so N(c r) = c N(r) for c > 0. Its 3x3x3
+ * convolutions run on the tensor cores (BF16 operands, FP32 accumulation), forward and backward; the parameters, their
+ * gradient and the Adam moments are FP32. Trained on (rhs, occupancy) -> pressure pairs with the relative loss
+ * ||N(b) - p||^2 / ||p||^2 over fluid cells.
+ *  - create: parameters drawn from `seed` (He-normal weights, zero biases);
+ *  - get/set_parameters: smoke_b200_net_parameter_count() FP32 values on the host, layer by layer, each layer its
+ *    weights [27][cin][cout] (tap = (dz+1)*9 + (dy+1)*3 + (dx+1)) then its cout biases; set resets the Adam state;
+ *  - apply: out = N(rhs) for one volume (device pointers, nx*ny*nz values each);
+ *  - gradient: the loss of one (rhs, occupancy, target) sample and its gradient (host, parameter layout);
+ *  - train: one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the mean gradient of `count` samples stored one after
+ *    another (count * nx*ny*nz values each); mean loss to *mean_loss_out.
+ * Every call synchronises `stream` and may grow the network's evaluation workspace (cudaMalloc). A network is used by
+ * one host thread at a time. */
+typedef struct SmokeB200Net_t* SmokeB200Net;
+SMOKE_SIMULATION_API uint32_t smoke_b200_net_parameter_count(void);
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_net_create_cuda(uint32_t seed, SmokeB200Net* out_net);
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_net_destroy_cuda(SmokeB200Net net);
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_net_get_parameters_cuda(SmokeB200Net net, float* out);
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_net_set_parameters_cuda(SmokeB200Net net, const float* values);
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_net_apply_cuda(SmokeB200Net net, int nx, int ny, int nz, const float* rhs, const uint8_t* occupancy, float* out, void* stream);
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_net_gradient_cuda(SmokeB200Net net, int nx, int ny, int nz, const float* rhs, const uint8_t* occupancy, const float* target, float* grad_out, double* loss_out, void* stream);
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_net_train_cuda(SmokeB200Net net, int nx, int ny, int nz, uint32_t count, const float* rhs, const uint8_t* occupancy, const float* target, float learning_rate, double* mean_loss_out, void* stream);
+
+/* out = A x, the matrix of the context's pressure system (the step's Poisson operator for the current occupancy:
+ * identity rows at solid cells and at the anchor cell), applied matrix-free; x and out: nx*ny*nz floats on the
+ * device, distinct. Enqueued on the context stream. For residual checks and for building training pairs
+ * (A e, e) of the learned preconditioner. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_apply_operator_cuda(SmokeSimulationContext context, const float* x, float* out);
+
+/* The context's copy of the network for SMOKE_B200_SOLVER_LEARNED_FCG (the parameters as they are now; later training
+ * of `net` does not change the context until this is called again). Allocates the context's evaluation workspace and
+ * rebuilds the step graph. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_set_preconditioner_net_cuda(SmokeSimulationContext context, SmokeB200Net net);
+
+/* 3x3x3 convolution (zero padding) of a channels-last BF16 volume on the tensor cores, the layer of the learned
+ * preconditioner's network. `in`: nx*ny*nz cells x S(cin) BF16 values, S(c) = 8 for c <= 8 and 16 for c <= 16
+ * (channels past cin must be 0); `weights`: FP32 [27][cin][cout] on the device, tap = (dz+1)*9 + (dy+1)*3 + (dx+1);
+ * `bias`: cout FP32 on the device or NULL. out = act(conv + bias), act = ReLU when `relu`: `out` (optional) gets
+ * nx*ny*nz x S(cout) BF16 values, `out_f32` (optional) channel 0 as FP32. Allocates a small scratch buffer and
+ * synchronises `stream`. 1 <= cin, cout <= 16. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_conv3d_cuda(int nx, int ny, int nz, int cin, int cout, const void* in, const float* weights, const float* bias, int relu, void* out, float* out_f32, void* stream);
 
 /* The same solve with every solver kernel launched directly on the context stream, no graph: the multigrid loop is
  * driven from the host, which reads the loop condition after each iteration (one stream synchronisation per

@@ -32,6 +32,9 @@ STRUCTS = [
     ("SmokeSimulationView", abi.View, ["layout", "nx", "row_stride_bytes", "slice_stride_bytes", "data0", "data2"]),
     ("SmokeB200SolverDesc", abi.SolverDesc, ["mode", "reduction", "max_iterations", "tolerance", "refinement", "warm_start"]),
     ("SmokeB200SolverStatus", abi.SolverStatus, ["iterations", "status", "rhs_norm", "true_relative_residual"]),
+    ("SmokeB200LaunchTune", abi.LaunchTune, ["advect_tile", "mg_wave", "pcg_grid", "reserved"]),
+    ("SmokeB200TuneRecord", abi.TuneRecord, ["tune", "ms_per_step", "iterations"]),
+    ("SmokeB200TuneReport", abi.TuneReport, ["chosen", "default_ms", "chosen_ms", "from_cache", "record_count", "records"]),
 ]
 
 
@@ -154,6 +157,12 @@ def test_null_arguments(library):
         fn = getattr(library, name)
         fn.argtypes = [C.c_void_p, C.c_void_p]
         assert fn(None, None) == abi.RESULT_BACKEND_FAILURE
+    for name in ("smoke_b200_set_launch_tune_cuda", "smoke_b200_get_launch_tune_cuda"):
+        fn = getattr(library, name)
+        fn.argtypes = [C.c_void_p, C.c_void_p]
+        assert fn(None, None) == abi.RESULT_BACKEND_FAILURE
+    library.smoke_b200_autotune_cuda.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
+    assert library.smoke_b200_autotune_cuda(None, 0, 0, None) == abi.RESULT_BACKEND_FAILURE
     for name in ("smoke_b200_solve_pressure_cuda", "smoke_b200_solve_pressure_eager_cuda", "smoke_b200_step_stages_cuda"):
         fn = getattr(library, name)
         assert fn(None, 0) if name.endswith("stages_cuda") else fn(None)  # nonzero: BACKEND_FAILURE

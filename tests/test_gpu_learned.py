@@ -1,0 +1,148 @@
+"""The learned preconditioner on the GPU: the tensor-core network against its float64 oracle (forward and gradient,
+with the oracle rounding to BF16 where the GPU stores BF16), training, and the learned FCG solve, which must reach the
+same tolerance and the same answer as the plain solver (the network changes the iteration count, not the answer)."""
+import numpy as np
+import pytest
+import torch
+
+import smoke_abi as abi
+import smoke_b200
+import train_preconditioner as T
+import unet_oracle as U
+
+pytestmark = pytest.mark.gpu
+
+OFFSETS = np.cumsum([0] + [27 * ci * co + co for ci, co, _ in U.LAYERS])
+SHAPE = (32, 48, 32)  # nx, ny, nz of the solve tests
+
+
+def sample(shape_zyx, seed):
+    rng = np.random.default_rng(seed)
+    r = rng.standard_normal(shape_zyx).astype(np.float32)
+    occ = (rng.random(shape_zyx) < 0.15).astype(np.uint8)
+    t = rng.standard_normal(shape_zyx).astype(np.float32)
+    return r, occ, t
+
+
+@pytest.fixture(scope="module")
+def net(smoke_lib):
+    n = smoke_b200.Net(smoke_lib, seed=3)
+    yield n
+    n.close()
+
+
+@pytest.mark.parametrize("shape", [(9, 11, 13), (16, 5, 33), (1, 7, 4)])
+def test_apply_matches_oracle(net, shape):
+    r, occ, _ = sample(shape, 1)
+    p = U.initial_like(2)
+    net.set_parameters(p)
+    got = net.apply(torch.from_numpy(r).cuda(), torch.from_numpy(occ).cuda()).cpu().numpy()
+    want = U.apply(p, r, occ, emulate=True)
+    assert np.abs(got - want).max() <= 1e-4 * np.abs(want).max()
+    assert not got[occ != 0].any()
+
+
+@pytest.mark.parametrize("shape", [(9, 11, 13), (6, 17, 10)])
+def test_gradient_matches_oracle(net, shape):
+    """The backward-data and weight-gradient tensor-core kernels, layer by layer."""
+    r, occ, t = sample(shape, 4)
+    p = U.initial_like(5)
+    net.set_parameters(p)
+    loss, g = net.gradient(*(torch.from_numpy(a).cuda() for a in (r, occ, t)))
+    want_loss, want = U.loss_and_gradient(p, r, occ, t, emulate=True)
+    assert abs(loss - want_loss) <= 1e-5 * want_loss
+    for L in range(len(U.LAYERS)):
+        a, b = g[OFFSETS[L]:OFFSETS[L + 1]], want[OFFSETS[L]:OFFSETS[L + 1]]
+        assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(b), L
+
+
+def test_parameters_round_trip(smoke_lib):
+    with smoke_b200.Net(smoke_lib, seed=11) as a, smoke_b200.Net(smoke_lib, seed=11) as b, smoke_b200.Net(smoke_lib, seed=12) as c:
+        pa, pb, pc = a.parameters(), b.parameters(), c.parameters()
+        assert pa.size == U.param_count() and np.array_equal(pa, pb) and not np.array_equal(pa, pc)
+        c.set_parameters(pa)
+        assert np.array_equal(c.parameters(), pa)
+
+
+@pytest.fixture(scope="module")
+def trained(smoke_lib):
+    """A network trained briefly on plume systems and synthetic pairs of the solve tests' grid, and the losses."""
+    data = T.generate(smoke_lib, SHAPE, 6, 4, seed=0, synthetic=12)
+    n = smoke_b200.Net(smoke_lib, seed=0)
+    losses = T.train(n, data, 1200, 8, 2e-3, seed=0)
+    yield n, losses
+    n.close()
+
+
+def test_training_reduces_the_loss(trained):
+    _, losses = trained
+    assert np.mean(losses[-50:]) < 0.5 * np.mean(losses[:5])
+
+
+def held_out_system(lib):
+    cfg, occ, boxes = T.scene(SHAPE, 999)
+    s = torch.cuda.Stream()
+    sim = smoke_b200.Simulation(lib, cfg, s)
+    with torch.cuda.stream(s):
+        o = torch.from_numpy(occ).cuda()
+        sim.update_occupancy(o)
+    sim.set_solver(**T.DATA_SOLVER)
+    drv = __import__("plume_scene").SceneDriver(sim, boxes, seed=5)
+    for k in range(12):
+        drv.apply(k)
+        sim.step()
+    return sim, o
+
+
+def solve(sim, form, net=None):
+    if net is not None:
+        sim.set_preconditioner_net(net)
+    sim.set_solver(**form)
+    sim.solve_pressure()
+    st = sim.solver_status()
+    return st, sim.snapshot([abi.VIEW_FLOW_PRESSURE])["pressure"]
+
+
+LEARNED = dict(mode=abi.SOLVER_LEARNED_FCG, reduction=abi.REDUCTION_FP64, max_iterations=3000, tolerance=1e-5, refinement=3)
+JACOBI = dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP64, max_iterations=4000, tolerance=1e-5, refinement=3)
+
+
+def test_learned_solve_same_answer_and_gain(smoke_lib, trained):
+    """Ablation: the same learned FCG with the untrained network stalls where the trained one converges; the
+    converged answer is the Jacobi-PCG answer within the tolerance's reach."""
+    net, _ = trained
+    sim, keep = held_out_system(smoke_lib)
+    st_j, p_j = solve(sim, JACOBI)
+    assert st_j.status == abi.SOLVE_CONVERGED
+    st_t, p_t = solve(sim, LEARNED, net)
+    assert st_t.status == abi.SOLVE_CONVERGED and st_t.true_relative_residual <= 1e-5
+    assert np.abs(p_t - p_j).max() <= 5e-3 * np.abs(p_j).max()
+    with smoke_b200.Net(smoke_lib, seed=0) as untrained:
+        st_u, _ = solve(sim, LEARNED, untrained)
+    assert st_u.status != abi.SOLVE_CONVERGED or st_u.iterations > 1.5 * st_t.iterations
+    # the network's estimate as the initial guess as well
+    st_w, p_w = solve(sim, dict(LEARNED, warm_start=2), net)
+    assert st_w.status == abi.SOLVE_CONVERGED and np.abs(p_w - p_j).max() <= 5e-3 * np.abs(p_j).max()
+    sim.close()
+
+
+def test_learned_mode_needs_a_network(smoke_lib):
+    cfg, occ, boxes = T.scene((16, 16, 16), 3)
+    sim = smoke_b200.Simulation(smoke_lib, cfg, torch.cuda.Stream())
+    with pytest.raises(smoke_b200.SmokeError):
+        sim.set_solver(**LEARNED)
+    with pytest.raises(smoke_b200.SmokeError):  # the network warm start exists only in the learned mode
+        sim.set_solver(**dict(JACOBI, warm_start=2))
+    sim.close()
+
+
+def test_operator_apply_matches_solution(smoke_lib):
+    """A p = b for the converged pressure of a step (the operator the learned trainer builds its pairs with)."""
+    sim, keep = held_out_system(smoke_lib)
+    st, p = solve(sim, dict(JACOBI, tolerance=1e-7, max_iterations=8000))
+    b = sim.snapshot([abi.VIEW_FLOW_PRESSURE_RHS])["pressure_rhs"]
+    with torch.cuda.stream(sim.stream):
+        ap = sim.apply_operator(sim.view(abi.VIEW_FLOW_PRESSURE).clone())
+    sim.stream.synchronize()
+    assert np.linalg.norm(ap.cpu().numpy() - b) <= 1e-5 * np.linalg.norm(b)
+    sim.close()

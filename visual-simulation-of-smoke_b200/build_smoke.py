@@ -16,9 +16,9 @@ LIB = os.path.join(HERE, "libsmoke_b200.so")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
-CU_SOURCES = ["step_kernels.cu", "pcg.cu", "mgsolve.cu", "noalloc.cu"]
-CPP_SOURCES = ["context.cpp"]
-HEADERS = ["smoke_device.cuh", "launch.h", "grid_sync.cuh", "march.cuh"]
+CU_SOURCES = ["step_kernels.cu", "pcg.cu", "mgsolve.cu", "noalloc.cu", "unet.cu"]
+CPP_SOURCES = ["context.cpp", "learned.cpp"]
+HEADERS = ["smoke_device.cuh", "launch.h", "grid_sync.cuh", "march.cuh", "unet.h", "tcgen05.cuh"]
 INCLUDES = [os.path.join(ROOT, "include"), CSRC]
 
 NVCC_FLAGS = [

@@ -10,18 +10,24 @@
 //    materialised before an occupancy or velocity change so they always reflect the state right after the step;
 //  - occupancy-derived data (pressure anchor, operator row codes, density fill list) is rebuilt only when
 //    occupancy changes.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include <nvtx3/nvtx3.hpp>
 
 #include "launch.h"
 #include "smoke_b200_ext.h"
+#include "unet.h"
 #include "visual-simulation-of-smoke-3d.h"
 
 static_assert(sizeof(SmokeSimulationFlowBoundaryFaceDesc) == 20);
@@ -120,7 +126,12 @@ struct SmokeSimulationContext_t {
     MgState* mg_state = nullptr;
 
     SmokeB200SolverDesc solver{SMOKE_B200_SOLVER_FIXED_CG, SMOKE_B200_REDUCTION_FP32, 500, 1.0e-5f, 0, 0};
+    SmokeB200LaunchTune tune{0, kMgWaveDefault, 0, 0};
     PcgLaunchShape pcg_shape{};
+    void* learned_mem = nullptr;  // the preconditioner network's images and workspace (LEARNED_FCG)
+    size_t learned_bytes = 0;
+    LearnedSolve learned{};
+    bool has_net = false;
     bool views_stale = false;
     bool stepped = false;
 
@@ -135,6 +146,8 @@ struct SmokeSimulationContext_t {
         solve_exec = nullptr;
         if (arena) cudaFree(arena);
         arena = nullptr;
+        if (learned_mem) cudaFree(learned_mem);
+        learned_mem = nullptr;
         if (capture_stream) cudaStreamDestroy(capture_stream);
         capture_stream = nullptr;
         if (body_stream) cudaStreamDestroy(body_stream);
@@ -239,7 +252,7 @@ struct SmokeSimulationContext_t {
     // recorded into the capture when `s` is capturing, else launched as the prebuilt solve graph.
     void enqueue_solve(cudaStream_t s, bool capturing) {
         const PcgSettings S = pcg_settings();
-        if (solver.mode != SMOKE_B200_SOLVER_MG_FCG) {
+        if (!uses_mg()) {
             check(launch_pcg(P, S, pcg_shape, codes, rhs, pressure, pcg, control, s), "pressure solve");
             return;
         }
@@ -253,7 +266,7 @@ struct SmokeSimulationContext_t {
     // The same solve with every kernel launched directly (the multigrid loop driven from the host).
     void run_solve_eager(cudaStream_t s) {
         const PcgSettings S = pcg_settings();
-        if (solver.mode != SMOKE_B200_SOLVER_MG_FCG) {
+        if (!uses_mg()) {
             check(launch_pcg(P, S, pcg_shape, codes, rhs, pressure, pcg, control, s), "pressure solve");
             return;
         }
@@ -273,7 +286,47 @@ struct SmokeSimulationContext_t {
         A.max_iterations = S.max_iterations;
         A.refinement = S.refinement < mg_max_refinement() ? S.refinement : mg_max_refinement();
         A.tol = S.tolerance;
+        A.wave = static_cast<int>(tune.mg_wave);
+        A.learned = solver.mode == SMOKE_B200_SOLVER_LEARNED_FCG ? 1 : 0;
+        A.net = A.learned ? &learned : nullptr;
+        A.net_warm = A.learned && A.warm && solver.warm_start == 2 ? 1 : 0;
         return A;
+    }
+
+    // The multigrid FCG machinery runs the multigrid and the learned solves.
+    bool uses_mg() const { return solver.mode == SMOKE_B200_SOLVER_MG_FCG || solver.mode == SMOKE_B200_SOLVER_LEARNED_FCG; }
+
+    // The context's copy of a network: its packed images and an activation workspace on this grid.
+    void set_net(const SmokeB200Net_t* net) {
+        const VolumeDims d = volume_dims(P.nx, P.ny, P.nz);
+        const size_t ib = (net_images_bytes() + 255) & ~size_t(255);
+        const size_t need = ib + net_acts_bytes(d);
+        check(cudaStreamSynchronize(stream), "preconditioner network: idle");
+        if (need > learned_bytes) {
+            if (learned_mem) check(cudaFree(learned_mem), "preconditioner network");
+            learned_mem = nullptr;
+            learned_bytes = 0;
+            check(cudaMalloc(&learned_mem, need), "preconditioner network");
+            learned_bytes = need;
+        }
+        check(cudaMemcpy(learned_mem, smoke_b200_net_images_block(net), net_images_bytes(), cudaMemcpyDeviceToDevice), "preconditioner network");
+        net_images_bind(learned.images, learned_mem);
+        net_acts_bind(learned.acts, static_cast<char*>(learned_mem) + ib, d);
+        learned.occupancy = occupancy;
+        check(cudaMemset(learned.acts.error, 0, sizeof(unsigned)), "preconditioner network");
+        has_net = true;
+    }
+
+    // Launch shapes: takes effect in the step graph, which is recaptured.
+    void apply_tune(const SmokeB200LaunchTune& t) {
+        if (!valid_tune(t)) throw std::invalid_argument("launch tune");
+        tune = t;
+        set_advect_tile(P, static_cast<int>(t.advect_tile));
+        pcg_shape.grid = static_cast<int>(t.pcg_grid);
+        capture_step_graph();
+    }
+    static bool valid_tune(const SmokeB200LaunchTune& t) {
+        return t.advect_tile < static_cast<uint32_t>(kAdvectTileCount) && t.mg_wave < static_cast<uint32_t>(kMgWaveCount) && t.pcg_grid < static_cast<uint32_t>(kPcgGridCount) && t.reserved == 0;
     }
 
     PcgSettings pcg_settings() const {
@@ -343,7 +396,7 @@ struct SmokeSimulationContext_t {
         check(cudaGraphInstantiate(&exec, graph, 0), "instantiate step graph");
         if (solve_exec) cudaGraphExecDestroy(solve_exec);
         solve_exec = nullptr;
-        if (solver.mode != SMOKE_B200_SOLVER_MG_FCG) return;
+        if (!uses_mg()) return;
         cudaGraph_t solve_graph = nullptr;
         check(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal), "begin solve capture");
         try {
@@ -443,6 +496,64 @@ SmokeSimulationResult guarded(F&& f) {
 cudaError_t copy_or_zero(float* dst, const float* src, size_t count, cudaStream_t s) {
     if (src == nullptr) return cudaMemsetAsync(dst, 0, count * sizeof(float), s);
     return cudaMemcpyAsync(dst, src, count * sizeof(float), cudaMemcpyDeviceToDevice, s);
+}
+
+// ---------------------------------------------------------------------------------------------- autotuner
+// Tuned shapes, per process: (device, nx, ny, nz, cubic, solver mode, reduction, refinement, max iterations,
+// tolerance bits).
+using TuneKey = std::tuple<int, int, int, int, int, uint32_t, uint32_t, uint32_t, int32_t, uint32_t>;
+std::mutex tune_lock;
+std::map<TuneKey, SmokeB200LaunchTune> tune_cache;
+
+TuneKey tune_key(const SmokeSimulationContext_t& c) {
+    int dev = 0;
+    check(cudaGetDevice(&dev), "device");
+    uint32_t tol_bits = 0;
+    std::memcpy(&tol_bits, &c.solver.tolerance, sizeof(tol_bits));
+    const bool fixed = c.solver.mode == SMOKE_B200_SOLVER_FIXED_CG;
+    return TuneKey{dev, c.P.nx, c.P.ny, c.P.nz, c.P.cubic, c.solver.mode, c.solver.reduction, fixed ? 0u : c.solver.refinement, fixed ? c.config.pressure_iterations : c.solver.max_iterations, fixed ? 0u : tol_bits};
+}
+
+// Device buffer freed on scope exit.
+struct DeviceBuffer {
+    void* p = nullptr;
+    ~DeviceBuffer() {
+        if (p) cudaFree(p);
+    }
+};
+struct Events {
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~Events() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+// Times `steps` graph steps of `c` under shapes `t`, each repeat from the state saved in `snapshot`.
+SmokeB200TuneRecord time_candidate(SmokeSimulationContext_t& c, const SmokeB200LaunchTune& t, uint32_t steps, const void* snapshot, Events& ev) {
+    const cudaStream_t s = c.stream;
+    check(cudaStreamSynchronize(s), "tune: idle");
+    c.apply_tune(t);
+    auto restore = [&] { check(cudaMemcpyAsync(c.arena, snapshot, c.arena_bytes, cudaMemcpyDeviceToDevice, s), "tune: restore state"); };
+    restore();
+    check(cudaGraphLaunch(c.exec, s), "tune: untimed step");
+    SmokeB200TuneRecord r{};
+    r.tune = t;
+    r.ms_per_step = std::numeric_limits<float>::infinity();
+    for (int rep = 0; rep < 2; ++rep) {
+        restore();
+        check(cudaEventRecord(ev.a, s), "tune: event");
+        for (uint32_t i = 0; i < steps; ++i) check(cudaGraphLaunch(c.exec, s), "tune: timed step");
+        check(cudaEventRecord(ev.b, s), "tune: event");
+        check(cudaEventSynchronize(ev.b), "tune: timed steps");
+        float ms = 0.0f;
+        check(cudaEventElapsedTime(&ms, ev.a, ev.b), "tune: elapsed");
+        r.ms_per_step = std::min(r.ms_per_step, ms / static_cast<float>(steps));
+    }
+    PcgStatusDevice st{};
+    check(cudaMemcpy(&st, &c.control->status, sizeof(st), cudaMemcpyDeviceToHost), "tune: status");
+    r.iterations = st.iterations;
+    return r;
 }
 
 }  // namespace
@@ -609,7 +720,9 @@ SmokeSimulationResult smoke_simulation_get_view_cuda(SmokeSimulationContext c, c
 // ---------------------------------------------------------------------------------------------- extensions
 SmokeSimulationResult smoke_b200_set_solver_cuda(SmokeSimulationContext c, const SmokeB200SolverDesc* desc) {
     if (c == nullptr || desc == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-    if (desc->mode > SMOKE_B200_SOLVER_MG_FCG || desc->reduction > SMOKE_B200_REDUCTION_FP64) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (desc->mode > SMOKE_B200_SOLVER_LEARNED_FCG || desc->reduction > SMOKE_B200_REDUCTION_FP64) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (desc->mode == SMOKE_B200_SOLVER_LEARNED_FCG && !c->has_net) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (desc->warm_start > (desc->mode == SMOKE_B200_SOLVER_LEARNED_FCG ? 2u : 1u)) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     if (desc->mode != SMOKE_B200_SOLVER_FIXED_CG && (desc->max_iterations <= 0 || !(desc->tolerance > 0.0f))) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return guarded([&] {
         c->solver = *desc;
@@ -725,6 +838,126 @@ SmokeSimulationResult smoke_b200_batch_destroy_cuda(SmokeB200Batch batch) {
     if (batch->stream) cudaStreamSynchronize(batch->stream);
     delete batch;
     return SMOKE_SIMULATION_RESULT_OK;
+}
+
+SmokeSimulationResult smoke_b200_apply_operator_cuda(SmokeSimulationContext c, const float* x, float* out) {
+    if (c == nullptr || x == nullptr || out == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return ok_or_fail(launch_mg_apply(c->mg, x, out, c->stream));
+}
+
+SmokeSimulationResult smoke_b200_set_preconditioner_net_cuda(SmokeSimulationContext c, SmokeB200Net net) {
+    if (c == nullptr || net == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        c->set_net(net);
+        c->capture_step_graph();
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+SmokeSimulationResult smoke_b200_set_launch_tune_cuda(SmokeSimulationContext c, const SmokeB200LaunchTune* tune) {
+    if (c == nullptr || tune == nullptr || !SmokeSimulationContext_t::valid_tune(*tune)) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        c->apply_tune(*tune);
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+SmokeSimulationResult smoke_b200_get_launch_tune_cuda(SmokeSimulationContext c, SmokeB200LaunchTune* out) {
+    if (c == nullptr || out == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    *out = c->tune;
+    return SMOKE_SIMULATION_RESULT_OK;
+}
+
+SmokeSimulationResult smoke_b200_autotune_cuda(SmokeSimulationContext c, uint32_t steps, uint32_t flags, SmokeB200TuneReport* report) {
+    nvtx3::scoped_range range("smoke_b200.autotune");
+    if (c == nullptr || steps > 64 || (flags & ~SMOKE_B200_TUNE_FORCE) != 0) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (steps == 0) steps = 4;
+    return guarded([&] {
+        SmokeB200TuneReport rep{};
+        const TuneKey key = tune_key(*c);
+        if (!(flags & SMOKE_B200_TUNE_FORCE)) {
+            std::lock_guard<std::mutex> guard(tune_lock);
+            auto it = tune_cache.find(key);
+            if (it != tune_cache.end()) {
+                c->apply_tune(it->second);
+                rep.chosen = it->second;
+                rep.from_cache = 1;
+                if (report) *report = rep;
+                return SMOKE_SIMULATION_RESULT_OK;
+            }
+        }
+        const cudaStream_t s = c->stream;
+        check(cudaStreamSynchronize(s), "tune: idle");
+        const bool views_stale = c->views_stale, stepped = c->stepped;
+        const SmokeB200LaunchTune start = c->tune;
+        DeviceBuffer snap;
+        check(cudaMalloc(&snap.p, c->arena_bytes), "tune: state copy");
+        check(cudaMemcpyAsync(snap.p, c->arena, c->arena_bytes, cudaMemcpyDeviceToDevice, s), "tune: save state");
+        Events ev;
+        check(cudaEventCreate(&ev.a), "tune: event");
+        check(cudaEventCreate(&ev.b), "tune: event");
+        auto record = [&](const SmokeB200TuneRecord& r) {
+            if (rep.record_count < SMOKE_B200_TUNE_MAX_RECORDS) rep.records[rep.record_count++] = r;
+        };
+        try {
+            SmokeB200TuneRecord best = time_candidate(*c, start, steps, snap.p, ev);
+            record(best);
+            rep.default_ms = best.ms_per_step;
+            // a candidate replaces the best only when it is at least 1% faster (timing noise)
+            auto consider = [&](SmokeB200LaunchTune t) {
+                const SmokeB200TuneRecord r = time_candidate(*c, t, steps, snap.p, ev);
+                record(r);
+                if (r.ms_per_step < 0.99f * best.ms_per_step) best = r;
+            };
+            const SmokeB200LaunchTune base_tiles = best.tune;
+            for (uint32_t v = 0; v < static_cast<uint32_t>(kAdvectTileCount); ++v)
+                if (v != base_tiles.advect_tile) {
+                    SmokeB200LaunchTune t = best.tune;
+                    t.advect_tile = v;
+                    consider(t);
+                }
+            const SmokeB200LaunchTune base_grid = best.tune;
+            if (c->uses_mg()) {
+                for (uint32_t v = 0; v < static_cast<uint32_t>(kMgWaveCount); ++v)
+                    if (v != base_grid.mg_wave) {
+                        SmokeB200LaunchTune t = best.tune;
+                        t.mg_wave = v;
+                        consider(t);
+                    }
+            } else {
+                for (uint32_t v = 0; v < static_cast<uint32_t>(kPcgGridCount); ++v)
+                    if (v != base_grid.pcg_grid) {
+                        SmokeB200LaunchTune t = best.tune;
+                        t.pcg_grid = v;
+                        consider(t);
+                    }
+            }
+            check(cudaStreamSynchronize(s), "tune: idle");
+            c->apply_tune(best.tune);
+            rep.chosen = best.tune;
+            rep.chosen_ms = best.ms_per_step;
+        } catch (...) {
+            // leave the context as it was: its shapes and its state
+            cudaStreamSynchronize(s);
+            try {
+                c->apply_tune(start);
+            } catch (...) {
+            }
+            cudaMemcpyAsync(c->arena, snap.p, c->arena_bytes, cudaMemcpyDeviceToDevice, s);
+            cudaStreamSynchronize(s);
+            throw;
+        }
+        check(cudaMemcpyAsync(c->arena, snap.p, c->arena_bytes, cudaMemcpyDeviceToDevice, s), "tune: restore state");
+        check(cudaStreamSynchronize(s), "tune: restore state");
+        c->views_stale = views_stale;
+        c->stepped = stepped;
+        {
+            std::lock_guard<std::mutex> guard(tune_lock);
+            tune_cache[key] = rep.chosen;
+        }
+        if (report) *report = rep;
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
 }
 
 SmokeSimulationResult smoke_b200_solve_pressure_eager_cuda(SmokeSimulationContext c) {

@@ -31,6 +31,19 @@ struct FillEntry {
 
 StepParams make_params(const SmokeSimulationConfig& cfg);
 
+// Launch shapes the autotuner chooses between (every choice computes the same values).
+// Advection blocks of 256 threads: flat (256 consecutive faces or cells), or a box of 2^x x 2^y x 2^z of them.
+constexpr int kAdvectTileCount = 5;
+constexpr int kAdvectTiles[kAdvectTileCount][3] = {{-1, 0, 0}, {5, 3, 0}, {5, 2, 1}, {4, 2, 2}, {3, 3, 2}};
+// Sets P.tile to the advection shape `code` (index into kAdvectTiles); false for an unknown code.
+bool set_advect_tile(StepParams& P, int code);
+// Multigrid level kernels: grid depth along z as a multiple of one wave of resident blocks (x 1/2, 1, 2, 4), or
+// one z tile per block.
+constexpr int kMgWaveCount = 5;
+constexpr int kMgWaveDefault = 1;
+// Persistent CG kernel: all resident blocks, half of them, a quarter.
+constexpr int kPcgGridCount = 3;
+
 // Forces: vorticity of the cell-centred velocity (writes the four vorticity buffers).
 cudaError_t launch_vorticity(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* wx, float* wy, float* wz, float* wmag, cudaStream_t s);
 // Forces: f = user force + buoyancy + vorticity confinement per cell.
@@ -117,6 +130,7 @@ struct PcgWork {
 struct PcgLaunchShape {
     int blocks;
     int threads;
+    int grid;  // kPcgGridCount code: the persistent grid is the resident blocks divided by 1 << grid
 };
 
 // ------------------------------------------------------------------------------------------ multigrid hierarchy
@@ -176,11 +190,17 @@ struct MgSolveArgs {
     MgState* st;
     int ir, warm, max_iterations, refinement;
     float tol;
+    int wave;                        // grid depth of the level kernels (kMgWaveCount codes)
+    int learned;                     // 1: the preconditioner is the network of `net`, not the V-cycle
+    int net_warm;                    // 1 (learned): the initial guess is the network's estimate N(b)
+    const struct LearnedSolve* net;  // host-side: the network's images, workspace and mask (learned only)
 };
 // Level extents and the number of grid-wide levels for a fine grid.
 int mg_level_count(int nx, int ny, int nz);
 // Largest refinement count the multigrid solve honours (the graph unrolls refinement + 1 passes).
 int mg_max_refinement();
+// out = A x with the fine operator (the pressure system's matrix, matrix-free from the level-0 codes).
+cudaError_t launch_mg_apply(const MgHierarchy& H, const float* x, float* out, cudaStream_t s);
 // Builds level fluid masks and codes from the occupancy (after the fine codes and anchor exist).
 cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uint8_t* occ, cudaStream_t s);
 // Records the multigrid-preconditioned FCG solve of A x = b into the graph being captured on `s` (kernels, and

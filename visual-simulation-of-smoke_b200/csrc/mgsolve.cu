@@ -24,11 +24,13 @@
 // kernel tests convergence and sets the loop condition (cudaGraphSetConditional), so the host never waits.
 // Dot products: block sums, then FP64 atomic adds spread over kMgSlots addresses, summed in slot order.
 // Each restriction block covers whole 2x2x2 parents and writes the coarse right-hand side directly.
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <utility>
 
 #include "launch.h"
+#include "unet.h"
 #include "smoke_b200_ext.h"
 
 namespace smoke_b200 {
@@ -314,21 +316,23 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
                 const uint16_t code = L0.code[c.q];
                 const float rq = r[c.q], qq = A.W.q[c.q];
                 const float pq = initial ? 0.0f : pn[c.q], eq = initial ? 0.0f : A.e[c.q];
-                float un[6];
-#pragma unroll
-                for (int k = 0; k < 6; ++k) un[k] = wdiag(L0.code[nb[k]]) * (r[nb[k]] - a * A.W.q[nb[k]]);
                 const float rn = rq - a * qq;
-                float zp = 0.0f;
-                if (active(code)) {
-                    zp = wdiag(code) * rn;
-                    res = 0.5f * (rn - masked_stencil(code, zp, un));
+                if (!A.learned) {  // pre-smoothing and the residual restricted to level 1
+                    float un[6];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) un[k] = wdiag(L0.code[nb[k]]) * (r[nb[k]] - a * A.W.q[nb[k]]);
+                    float zp = 0.0f;
+                    if (active(code)) {
+                        zp = wdiag(code) * rn;
+                        res = 0.5f * (rn - masked_stencil(code, zp, un));
+                    }
+                    L0.zp[c.q] = zp;
                 }
                 rn_out[c.q] = rn;
-                L0.zp[c.q] = zp;
                 if (!initial) A.e[c.q] = eq + a * pq;
                 rr += static_cast<T>(rn) * static_cast<T>(rn);
             }
-            restrict_tile(res, A.H.L[1], c);
+            if (!A.learned) restrict_tile(res, A.H.L[1], c);
         });
         block_accumulate<T>(st, kAccRR, rr, -1, T(0));
     }
@@ -470,6 +474,26 @@ __global__ void __launch_bounds__(kThreads) mg_smooth_kernel(const __grid_consta
     const double beta = st->first_iter ? 0.0 : -total(st, kAccZQ) / st->pq_prev;
     if (!isfinite(beta) || !isfinite(total(st, kAccZR))) st->fail = SMOKE_B200_SOLVE_NOT_FINITE;
     st->beta = static_cast<float>(beta);
+}
+
+// Learned preconditioner, first half: zp = N(r) = y / s on active cells (y the network's output for the current
+// residual, s = sqrt(n / ||r||^2) its input scale), 0 elsewhere. mg_smooth_kernel<true> then post-smooths it,
+// z = zp + w D^-1 (r - A zp): the network supplies the smooth part of the correction, the Jacobi step the rough part.
+__global__ void __launch_bounds__(kThreads) mg_net_zp_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
+    const MgLevel& F = A.H.L[0];
+    const double rn2 = A.st->rnorm2;
+    const float inv_s = rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n))) : 0.0f;
+    for_tiles(F, [&](const Cell& c) {
+        if (c.in) F.zp[c.q] = active(F.code[c.q]) ? y[c.q] * inv_s : 0.0f;
+    });
+}
+
+// Initial guess of a learned solve: x64 = the network's estimate on active cells, 0 elsewhere.
+__global__ void __launch_bounds__(kThreads) mg_net_guess_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ guess) {
+    const MgLevel& F = A.H.L[0];
+    for_tiles(F, [&](const Cell& c) {
+        if (c.in) A.W.x64[c.q] = active(F.code[c.q]) ? static_cast<double>(guess[c.q]) : 0.0;
+    });
 }
 
 // p' = z + beta p, q = A p'; (p', q) and (p', r). The last block computes alpha = (p', r) / (p', q).
@@ -722,13 +746,28 @@ __global__ void __launch_bounds__(kThreads) mg_finalize_kernel(const __grid_cons
     *out = s;
 }
 
+// out = A x with the level-0 operator (identity rows at solid cells and the anchor).
+__global__ void __launch_bounds__(kThreads) mg_apply_kernel(const __grid_constant__ MgHierarchy H, const float* __restrict__ x, float* __restrict__ out) {
+    const MgLevel& L = H.L[0];
+    for_tiles(L, [&](const Cell& c) {
+        if (!c.in) return;
+        uint32_t nb[6];
+        nbr_all(L, H.fper, c, nb);
+        float v[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[k] = x[nb[k]];
+        out[c.q] = masked_stencil(L.code[c.q], x[c.q], v);
+    });
+}
+
 // ---------------------------------------------------------------------------------------------- host side
 const dim3 kBlock(TX, TY, TZ);
 
-// Grid of one wave for `kernel` on level L: the level's tile columns (x, y), and as many z shares as the resident
-// blocks (per SM x SMs, cached per kernel and device) allow.
+// Grid for `kernel` on level L: the level's tile columns (x, y), and as many z shares as `depth` waves of resident
+// blocks (per SM x SMs, cached per kernel and device) allow: depth code 0..3 = 1/2, 1, 2, 4 waves, 4 = one z tile
+// per block.
 template <class K>
-dim3 wave(K kernel, const MgLevel& L) {
+dim3 wave(K kernel, const MgLevel& L, int depth) {
     static std::mutex lock;
     static std::map<std::pair<const void*, int>, int> cache;
     int dev = 0;
@@ -747,7 +786,9 @@ dim3 wave(K kernel, const MgLevel& L) {
         resident = it->second;
     }
     const int tx = (L.nx + TX - 1) / TX, ty = (L.ny + TY - 1) / TY, tz = (L.nz + TZ - 1) / TZ;
-    int gz = resident / (tx * ty);
+    if (depth >= kMgWaveCount - 1) return dim3(tx, ty, tz);
+    const long long blocks = depth <= 0 ? resident / 2 : static_cast<long long>(resident) << (depth - 1);
+    int gz = static_cast<int>(std::min<long long>(blocks / (tx * ty), tz));
     if (gz < 1) gz = 1;
     if (gz > tz) gz = tz;
     gz = (tz + ((tz + gz - 1) / gz) - 1) / ((tz + gz - 1) / gz);  // no empty z shares
@@ -788,17 +829,38 @@ template <typename T>
 void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_graph, uint32_t block_bytes, cudaStream_t bs) {
     const MgHierarchy& H = A.H;
     const MgLevel& L0 = H.L[0];
+    if (A.learned) {  // z = N(r): the network on the current residual (its parity and norm read on the device)
+        const LearnedSolve& N = *A.net;
+        if (net_forward(N.images, N.acts, A.W.r[0], A.W.r[1], &A.st->parity, &A.st->rnorm2, N.occupancy, bs) != cudaSuccess) return;
+        mg_net_zp_kernel<<<wave(mg_net_zp_kernel, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
+        mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
+        mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
+        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
+        return;
+    }
     const int g = H.grid_levels;
-    for (int l = 1; l < g; ++l) mg_restrict_kernel<<<wave(mg_restrict_kernel, H.L[l]), kBlock, 0, bs>>>(H, l);
+    for (int l = 1; l < g; ++l) mg_restrict_kernel<<<wave(mg_restrict_kernel, H.L[l], A.wave), kBlock, 0, bs>>>(H, l);
     mg_block_kernel<<<1, kBlockLevelThreads, block_bytes, bs>>>(H);
     for (int l = g - 1; l >= 1; --l) {
-        mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[l + 1]), kBlock, 0, bs>>>(H, l);
-        mg_smooth_kernel<false, T><<<wave(mg_smooth_kernel<false, T>, H.L[l]), kBlock, 0, bs>>>(A, l);
+        mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[l + 1], A.wave), kBlock, 0, bs>>>(H, l);
+        mg_smooth_kernel<false, T><<<wave(mg_smooth_kernel<false, T>, H.L[l], A.wave), kBlock, 0, bs>>>(A, l);
     }
-    mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[1]), kBlock, 0, bs>>>(H, 0);
-    mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0), kBlock, 0, bs>>>(A, 0);
-    mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0), kBlock, 0, bs>>>(A);
-    mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, bs>>>(A, 0, h, in_graph);
+    mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[1], A.wave), kBlock, 0, bs>>>(H, 0);
+    mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
+    mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
+    mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
+}
+
+// Learned solve with the network's warm start: x64 = N(b) (through the q array, which the set-up clears), so the
+// set-up's warm path starts from r = b - A x64.
+cudaError_t learned_guess(const MgSolveArgs& A, cudaStream_t s) {
+    if (!A.learned || !A.net_warm) return cudaSuccess;
+    const LearnedSolve& N = *A.net;
+    cudaError_t e = net_forward(N.images, N.acts, A.b, nullptr, nullptr, nullptr, N.occupancy, s);
+    if (e == cudaSuccess) e = net_output(N.acts, nullptr, N.occupancy, A.W.q, s);
+    if (e != cudaSuccess) return e;
+    mg_net_guess_kernel<<<wave(mg_net_guess_kernel, A.H.L[0], A.wave), kBlock, 0, s>>>(A, A.W.q);
+    return cudaGetLastError();
 }
 
 uint32_t block_level_bytes(const MgHierarchy& H) {
@@ -818,21 +880,22 @@ cudaError_t enqueue_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream
     const uint32_t block_bytes = block_level_bytes(A.H);
     e = cudaMemsetAsync(A.st, 0, sizeof(MgState), s);
     if (e != cudaSuccess) return e;
-    mg_setup_kernel<T><<<wave(mg_setup_kernel<T>, L0), kBlock, 0, s>>>(A);
+    if ((e = learned_guess(A, s)) != cudaSuccess) return e;
+    mg_setup_kernel<T><<<wave(mg_setup_kernel<T>, L0, A.wave), kBlock, 0, s>>>(A);
     const int passes = A.ir ? A.refinement + 1 : 1;
     for (int pass = 0; pass < passes; ++pass) {
         cudaGraphConditionalHandle h;
         e = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
         if (e != cudaSuccess) return e;
-        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, s>>>(A, 1, h, 1);
+        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0, A.wave), kBlock, 0, s>>>(A, 1, h, 1);
         e = add_while(s, body_stream, h, [&](cudaStream_t bs) { launch_body<T>(A, h, 1, block_bytes, bs); });
         if (e != cudaSuccess) return e;
         if (A.ir) {
-            mg_accumulate_kernel<<<wave(mg_accumulate_kernel, L0), kBlock, 0, s>>>(A);
-            mg_residual_kernel<<<wave(mg_residual_kernel, L0), kBlock, 0, s>>>(A);
+            mg_accumulate_kernel<<<wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s>>>(A);
+            mg_residual_kernel<<<wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s>>>(A);
         }
     }
-    mg_finalize_kernel<<<wave(mg_finalize_kernel, L0), kBlock, 0, s>>>(A, out);
+    mg_finalize_kernel<<<wave(mg_finalize_kernel, L0, A.wave), kBlock, 0, s>>>(A, out);
     return cudaGetLastError();
 }
 
@@ -842,14 +905,15 @@ cudaError_t run_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream_t s
     const uint32_t block_bytes = block_level_bytes(A.H);
     cudaError_t e = cudaMemsetAsync(A.st, 0, sizeof(MgState), s);
     if (e != cudaSuccess) return e;
-    mg_setup_kernel<T><<<wave(mg_setup_kernel<T>, L0), kBlock, 0, s>>>(A);
+    if ((e = learned_guess(A, s)) != cudaSuccess) return e;
+    mg_setup_kernel<T><<<wave(mg_setup_kernel<T>, L0, A.wave), kBlock, 0, s>>>(A);
     const int passes = A.ir ? A.refinement + 1 : 1;
     auto loop_flag = [&](uint32_t& flag) {
         const cudaError_t r = cudaMemcpyAsync(&flag, &A.st->loop, sizeof(flag), cudaMemcpyDeviceToHost, s);
         return r == cudaSuccess ? cudaStreamSynchronize(s) : r;
     };
     for (int pass = 0; pass < passes; ++pass) {
-        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0), kBlock, 0, s>>>(A, 1, 0, 0);
+        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0, A.wave), kBlock, 0, s>>>(A, 1, 0, 0);
         for (;;) {  // bounded: every update counts an iteration and stops at max_iterations
             uint32_t flag = 0;
             if ((e = loop_flag(flag)) != cudaSuccess) return e;
@@ -858,11 +922,11 @@ cudaError_t run_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream_t s
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (A.ir) {
-            mg_accumulate_kernel<<<wave(mg_accumulate_kernel, L0), kBlock, 0, s>>>(A);
-            mg_residual_kernel<<<wave(mg_residual_kernel, L0), kBlock, 0, s>>>(A);
+            mg_accumulate_kernel<<<wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s>>>(A);
+            mg_residual_kernel<<<wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s>>>(A);
         }
     }
-    mg_finalize_kernel<<<wave(mg_finalize_kernel, L0), kBlock, 0, s>>>(A, out);
+    mg_finalize_kernel<<<wave(mg_finalize_kernel, L0, A.wave), kBlock, 0, s>>>(A, out);
     return cudaGetLastError();
 }
 
@@ -953,6 +1017,11 @@ cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uin
         mg_coarsen_kernel<<<(H.L[l].n + 255) / 256, 256, 0, s>>>(H.L[l - 1], H.L[l]);
         mg_code_kernel<<<(H.L[l].n + 2 + 255) / 256, 256, 0, s>>>(H.L[l], P);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mg_apply(const MgHierarchy& H, const float* x, float* out, cudaStream_t s) {
+    mg_apply_kernel<<<wave(mg_apply_kernel, H.L[0], kMgWaveDefault), kBlock, 0, s>>>(H, x, out);
     return cudaGetLastError();
 }
 

@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ S
 }
 
 template <bool J, typename T>
-cudaError_t launch_one(const StepParams& P, const PcgSettings& S, const uint16_t* codes, const float* b, float* x, PcgWork work, PcgControl* ctl, cudaStream_t s) {
+cudaError_t launch_one(const StepParams& P, const PcgSettings& S, int grid, const uint16_t* codes, const float* b, float* x, PcgWork work, PcgControl* ctl, cudaStream_t s) {
     static int max_blocks = 0;
     if (max_blocks == 0) {
         int dev = 0, sms = 0, per_sm = 0;
@@ -373,7 +373,9 @@ cudaError_t launch_one(const StepParams& P, const PcgSettings& S, const uint16_t
     // at least ~8 planes per block, so the two-plane prologue of a segment stays a small share of its work
     uint32_t want = C.total / 8u;
     if (want < 1u) want = 1u;
-    const int blocks = static_cast<int>(want < static_cast<uint32_t>(max_blocks) ? want : static_cast<uint32_t>(max_blocks));
+    const int shift = grid < 0 ? 0 : (grid >= kPcgGridCount ? kPcgGridCount - 1 : grid);
+    const uint32_t cap = static_cast<uint32_t>(max_blocks >> shift) > 0u ? static_cast<uint32_t>(max_blocks >> shift) : 1u;
+    const int blocks = static_cast<int>(want < cap ? want : cap);
     cudaError_t e = cudaMemsetAsync(ctl, 0, kPcgControlResetBytes, s);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg{};
@@ -398,12 +400,14 @@ cudaError_t pcg_launch_shape(PcgLaunchShape* out) {
     if (e != cudaSuccess) return e;
     out->blocks = sms;
     out->threads = kThreads;
+    out->grid = 0;
     return cudaSuccess;
 }
 
-cudaError_t launch_pcg(const StepParams& P, const PcgSettings& S, const PcgLaunchShape&, const uint16_t* codes, const float* b, float* x, PcgWork work, PcgControl* ctl, cudaStream_t s) {
-    if (S.jacobi) return S.fp64 ? launch_one<true, double>(P, S, codes, b, x, work, ctl, s) : launch_one<true, float>(P, S, codes, b, x, work, ctl, s);
-    return S.fp64 ? launch_one<false, double>(P, S, codes, b, x, work, ctl, s) : launch_one<false, float>(P, S, codes, b, x, work, ctl, s);
+cudaError_t launch_pcg(const StepParams& P, const PcgSettings& S, const PcgLaunchShape& shape, const uint16_t* codes, const float* b, float* x, PcgWork work, PcgControl* ctl, cudaStream_t s) {
+    const int g = shape.grid;
+    if (S.jacobi) return S.fp64 ? launch_one<true, double>(P, S, g, codes, b, x, work, ctl, s) : launch_one<true, float>(P, S, g, codes, b, x, work, ctl, s);
+    return S.fp64 ? launch_one<false, double>(P, S, g, codes, b, x, work, ctl, s) : launch_one<false, float>(P, S, g, codes, b, x, work, ctl, s);
 }
 
 }  // namespace smoke_b200

@@ -58,6 +58,8 @@ struct StepParams {
     FastDiv div_fx[3], div_fy[3];                // faces of axis a: row length and rows per slab
     float inv_h;                                 // 1 / h (grid coordinates of sample positions)
     double dt_over_h64;                          // dt / h in FP64 (gradient of the refined FP64 pressure)
+    int tile[3];                                 // advection blocks: log2 extents (x, y, z) of the box of faces or
+                                                 // cells one block covers (sum 8); tile[0] < 0: 256 consecutive ones
 };
 
 #if defined(__CUDACC__)

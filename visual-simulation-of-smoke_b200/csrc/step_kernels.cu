@@ -198,10 +198,37 @@ __global__ void __launch_bounds__(kThreads) face_force_kernel(const __grid_const
 }
 
 // ------------------------------------------------------------------------------------------ velocity advection
-template <int A, bool CUBIC>
-__device__ __forceinline__ void advect_face_one(const StepParams& P, uint32_t q, const PadField& u, const PadField& v, const PadField& w, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
+// Point (i, j, k) of this thread in block b of an nx x ny x nz grid of points covered by boxes of P.tile; false
+// outside the grid. Boxes run x fastest, then y, then z.
+__device__ __forceinline__ bool tile_point(const StepParams& P, unsigned b, int nx, int ny, int nz, int& i, int& j, int& k) {
+    const int lx = P.tile[0], ly = P.tile[1], lz = P.tile[2];
+    const unsigned ntx = (nx + (1 << lx) - 1) >> lx, nty = (ny + (1 << ly) - 1) >> ly;
+    const unsigned r = b / ntx, bx = b - r * ntx, bz = r / nty, by = r - bz * nty;
+    const unsigned t = threadIdx.x;
+    i = static_cast<int>((bx << lx) + (t & ((1u << lx) - 1u)));
+    j = static_cast<int>((by << ly) + ((t >> lx) & ((1u << ly) - 1u)));
+    k = static_cast<int>((bz << lz) + (t >> (lx + ly)));
+    return i < nx && j < ny && k < nz;
+}
+// Blocks of kThreads that cover an nx x ny x nz grid of points in the advection shape of P.
+unsigned advect_blocks(const StepParams& P, int nx, int ny, int nz) {
+    if (P.tile[0] < 0) return blocks_for(static_cast<uint64_t>(nx) * ny * nz);
+    const uint64_t tx = 1u << P.tile[0], ty = 1u << P.tile[1], tz = 1u << P.tile[2];
+    return static_cast<unsigned>(((nx + tx - 1) / tx) * ((ny + ty - 1) / ty) * ((nz + tz - 1) / tz));
+}
+
+template <int A, bool CUBIC, bool TILED>
+__device__ __forceinline__ void advect_face_one(const StepParams& P, unsigned blk, const PadField& u, const PadField& v, const PadField& w, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
     int i, j, k;
-    face_ijk<A>(P, q, i, j, k);
+    uint32_t q;
+    if (TILED) {
+        if (!tile_point(P, blk, fsx<A>(P), fsy<A>(P), fsz<A>(P), i, j, k)) return;
+        q = fidx<A>(P, i, j, k);
+    } else {
+        q = blk * kThreads + threadIdx.x;
+        if (q >= (A == 0 ? P.nu : (A == 1 ? P.nv : P.nw))) return;
+        face_ijk<A>(P, q, i, j, k);
+    }
     const PadField& src = A == 0 ? u : (A == 1 ? v : w);
     out[q] = settle<A, false>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
         const float h = P.h;
@@ -213,21 +240,15 @@ __device__ __forceinline__ void advect_face_one(const StepParams& P, uint32_t q,
     });
 }
 
-// Samples and traces read the padded copies of the velocity (ghost cells hold the boundary taps).
-template <bool CUBIC>
+// Samples and traces read the padded copies of the velocity (ghost cells hold the boundary taps). Blocks
+// [0, bu) advect u faces, [bu, bu + bv) v faces, the rest w faces, each in the shape P.tile selects.
+template <bool CUBIC, bool TILED>
 __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ StepParams P, const PadField u, const PadField v, const PadField w, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou, float* __restrict__ ov,
                                                                     float* __restrict__ ow, unsigned bu, unsigned bv) {
     const unsigned b = blockIdx.x;
-    if (b < bu) {
-        const uint32_t q = b * kThreads + threadIdx.x;
-        if (q < P.nu) advect_face_one<0, CUBIC>(P, q, u, v, w, occ, su, ou);
-    } else if (b < bu + bv) {
-        const uint32_t q = (b - bu) * kThreads + threadIdx.x;
-        if (q < P.nv) advect_face_one<1, CUBIC>(P, q, u, v, w, occ, sv, ov);
-    } else {
-        const uint32_t q = (b - bu - bv) * kThreads + threadIdx.x;
-        if (q < P.nw) advect_face_one<2, CUBIC>(P, q, u, v, w, occ, sw, ow);
-    }
+    if (b < bu) advect_face_one<0, CUBIC, TILED>(P, b, u, v, w, occ, su, ou);
+    else if (b < bu + bv) advect_face_one<1, CUBIC, TILED>(P, b - bu, u, v, w, occ, sv, ov);
+    else advect_face_one<2, CUBIC, TILED>(P, b - bu - bv, u, v, w, occ, sw, ow);
 }
 
 // Padded copies (see PadField) of up to 3 fields in one launch: block z-range c * pz_blocks .. for field c; each
@@ -350,17 +371,23 @@ __global__ void __launch_bounds__(kThreads) scalar_prep_kernel(const __grid_cons
 
 // Fluid cells: one back-trace, then both scalars sampled with their own boundary rules (:1221-1233).
 // Solid cells: temperature = solid temperature (:1235-1241), density = 0 until the fill pass.
-template <bool CUBIC>
+template <bool CUBIC, bool TILED>
 __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ StepParams P, const PadField u, const PadField v, const PadField w, const uint8_t* __restrict__ occ, const PadField t_tmp, const PadField d_tmp, const float* __restrict__ solid_t, float* __restrict__ t, float* __restrict__ d) {
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= P.n) return;
+    int x, y, z;
+    uint32_t q;
+    if (TILED) {
+        if (!tile_point(P, blockIdx.x, P.nx, P.ny, P.nz, x, y, z)) return;
+        q = cidx(P, x, y, z);
+    } else {
+        q = blockIdx.x * blockDim.x + threadIdx.x;
+        if (q >= P.n) return;
+        cell_xyz(P, q, x, y, z);
+    }
     if (occ[q] != 0) {
         t[q] = solid_t[q];
         d[q] = 0.0f;
         return;
     }
-    int x, y, z;
-    cell_xyz(P, q, x, y, z);
     const float h = P.h;
     const float3 p = trace_rk2((static_cast<float>(x) + 0.5f) * h, (static_cast<float>(y) + 0.5f) * h, (static_cast<float>(z) + 0.5f) * h, u, v, w, occ, P);
     t[q] = sample_pad<4, CUBIC>(t_tmp, p.x, p.y, p.z, P);
@@ -545,7 +572,14 @@ StepParams make_params(const SmokeSimulationConfig& cfg) {
         P.div_fx[a] = FastDiv(nx + (a == 0));
         P.div_fy[a] = FastDiv(ny + (a == 1));
     }
+    set_advect_tile(P, 0);
     return P;
+}
+
+bool set_advect_tile(StepParams& P, int code) {
+    if (code < 0 || code >= kAdvectTileCount) return false;
+    for (int a = 0; a < 3; ++a) P.tile[a] = kAdvectTiles[code][a];
+    return true;
 }
 
 cudaError_t launch_vorticity(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* wx, float* wy, float* wz, float* wmag, cudaStream_t s) {
@@ -595,10 +629,10 @@ cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const 
 }
 
 cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, ConstFaces pad, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
-    const unsigned bu = blocks_for(P.nu), bv = blocks_for(P.nv), bw = blocks_for(P.nw);
+    const unsigned bu = advect_blocks(P, P.nx + 1, P.ny, P.nz), bv = advect_blocks(P, P.nx, P.ny + 1, P.nz), bw = advect_blocks(P, P.nx, P.ny, P.nz + 1);
     const PadField u = pad_field(P, 0, in.u, pad.u), v = pad_field(P, 1, in.v, pad.v), w = pad_field(P, 2, in.w, pad.w);
-    if (P.cubic) advect_velocity_kernel<true><<<bu + bv + bw, kThreads, 0, s>>>(P, u, v, w, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
-    else advect_velocity_kernel<false><<<bu + bv + bw, kThreads, 0, s>>>(P, u, v, w, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
+    auto kernel = P.tile[0] < 0 ? (P.cubic ? advect_velocity_kernel<true, false> : advect_velocity_kernel<false, false>) : (P.cubic ? advect_velocity_kernel<true, true> : advect_velocity_kernel<false, true>);
+    kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, u, v, w, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
     return cudaGetLastError();
 }
 
@@ -621,8 +655,8 @@ cudaError_t launch_scalar_prep(const StepParams& P, const float* temperature, co
 cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, ConstFaces vel_pad, const uint8_t* occ, const float* t_tmp, const float* t_pad, const float* d_tmp, const float* d_pad, const float* solid_temperature, float* temperature, float* density, cudaStream_t s) {
     const PadField u = pad_field(P, 0, vel.u, vel_pad.u), v = pad_field(P, 1, vel.v, vel_pad.v), w = pad_field(P, 2, vel.w, vel_pad.w);
     const PadField t = pad_field(P, 4, t_tmp, t_pad), d = pad_field(P, 3, d_tmp, d_pad);
-    if (P.cubic) advect_scalars_kernel<true><<<blocks_for(P.n), kThreads, 0, s>>>(P, u, v, w, occ, t, d, solid_temperature, temperature, density);
-    else advect_scalars_kernel<false><<<blocks_for(P.n), kThreads, 0, s>>>(P, u, v, w, occ, t, d, solid_temperature, temperature, density);
+    auto kernel = P.tile[0] < 0 ? (P.cubic ? advect_scalars_kernel<true, false> : advect_scalars_kernel<false, false>) : (P.cubic ? advect_scalars_kernel<true, true> : advect_scalars_kernel<false, true>);
+    kernel<<<advect_blocks(P, P.nx, P.ny, P.nz), kThreads, 0, s>>>(P, u, v, w, occ, t, d, solid_temperature, temperature, density);
     return cudaGetLastError();
 }
 

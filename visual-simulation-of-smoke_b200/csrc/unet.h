@@ -1,0 +1,122 @@
+// Learned preconditioner: a small 3-D U-Net on channels-last BF16 volumes, its 3x3x3 convolutions as implicit GEMMs
+// on the tcgen05 tensor cores (forward, backward-data, backward-weight), and the glue kernels between them. Host
+// launchers only; the kernels are in unet.cu.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace smoke_b200 {
+
+// ------------------------------------------------------------------------------------------ network shape
+// Three levels (level l halves the extents of level l - 1, rounding up). Layers, in execution order:
+//   a: level 0, [input r * s, fluid] (2) -> e0 (8), ReLU        b: level 1, pool(e0) (8) -> e1 (16), ReLU
+//   c: level 2, pool(e1) (16) -> e2 (16), ReLU                  d: level 1, up(e2) + e1 (16) -> d1 (8), ReLU
+//   e: level 0, up(d1) + e0 (8) -> d0 (8), ReLU                 f: level 0, d0 (8) -> y (1)
+// Every convolution is 3x3x3 with zero padding; pool = mean of the existing children of a coarse cell; up = copy
+// of the parent. The input scale s = sqrt(n) / ||r|| makes the network positively homogeneous: the output is y / s.
+constexpr int kNetLayers = 6;
+struct NetLayer {
+    int cin, cout;  // real channel counts
+    int level;
+};
+constexpr NetLayer kNet[kNetLayers] = {{2, 8, 0}, {8, 16, 1}, {16, 16, 2}, {16, 8, 1}, {8, 8, 0}, {8, 1, 0}};
+// Stored channels of a volume with c real channels (8 or 16; extra channels are 0).
+__host__ __device__ constexpr int net_store(int c) { return c <= 8 ? 8 : 16; }
+// FP32 parameters of layer L: weights [27][cin][cout] (tap = (dz+1)*9 + (dy+1)*3 + (dx+1)), then bias [cout].
+constexpr int net_weight_count(int L) { return 27 * kNet[L].cin * kNet[L].cout; }
+constexpr int net_param_count(int L) { return net_weight_count(L) + kNet[L].cout; }
+constexpr int net_param_offset(int L) { return L == 0 ? 0 : net_param_offset(L - 1) + net_param_count(L - 1); }
+constexpr int kNetParams = net_param_offset(kNetLayers);
+
+// Packed BF16 operand image of one convolution (K-major B operand of the implicit GEMM, N = 16 output channels):
+// bytes for an input of `cin_store` stored channels.
+__host__ __device__ constexpr int conv_taps(int cin_store) { return cin_store == 8 ? 28 : 27; }
+__host__ __device__ constexpr uint32_t conv_pack_bytes(int cin_store) { return static_cast<uint32_t>(conv_taps(cin_store) * cin_store / 8) * 2u * 128u; }
+
+// ------------------------------------------------------------------------------------------ launchers
+struct VolumeDims {
+    int nx, ny, nz;
+    uint32_t n;
+};
+inline VolumeDims volume_dims(int nx, int ny, int nz) { return {nx, ny, nz, static_cast<uint32_t>(nx) * ny * nz}; }
+inline VolumeDims coarse_dims(const VolumeDims& d) { return volume_dims((d.nx + 1) / 2, (d.ny + 1) / 2, (d.nz + 1) / 2); }
+
+// 3x3x3 convolution of `in` ([n][cin_store] BF16) with the packed weights `wpack`: out = act(conv + bias) where act
+// is ReLU when `relu`, then zeroed where `gate` ([n][cout_store] BF16, optional) is not positive. Writes `out`
+// ([n][cout_store] BF16, optional) and/or `out_f32` (channel 0, [n] FP32, optional). bias: 16 floats or null.
+// `error` (device word) gets bit 0 when a tensor-core completion wait ran out.
+cudaError_t launch_conv3(const VolumeDims& d, int cin_store, const __nv_bfloat16* in, const uint8_t* wpack, const float* bias, int relu, const __nv_bfloat16* gate, __nv_bfloat16* out, int cout_store, float* out_f32, unsigned* error, cudaStream_t s);
+
+// Packs layer weights W [27][cin][cout] (FP32) into the operand image of the forward convolution (input stored
+// channels net_store(cin)), or with `transpose` of the backward-data convolution (input = the output gradient,
+// net_store(cout) channels; output = cin channels; taps mirrored).
+cudaError_t launch_pack_conv(const float* w, int cin, int cout, int transpose, uint8_t* pack, cudaStream_t s);
+
+// ------------------------------------------------------------------------------------------ whole network
+// Device images of the network's parameters the kernels read: FP32 master copy, packed BF16 operand images of every
+// forward convolution and of the backward-data convolutions of layers 1..5, and the biases padded to 16.
+struct NetImages {
+    uint8_t* fwd[kNetLayers];
+    uint8_t* bwd[kNetLayers];  // bwd[0] unused
+    float* bias16[kNetLayers];
+};
+// Bytes of NetImages storage and the binding of its pointers inside one buffer.
+size_t net_images_bytes();
+void net_images_bind(NetImages& I, void* base);
+// Rebuilds the packed images and padded biases from the FP32 parameters w (kNetParams floats).
+cudaError_t net_pack(const float* w, const NetImages& I, cudaStream_t s);
+
+// Activations of one evaluation on a level-0 volume d0 (levels 1 and 2 are coarse_dims of the one before).
+struct NetActs {
+    VolumeDims d[3];
+    __nv_bfloat16 *x0, *e0, *s0, *d0;  // level 0, 8 channels
+    __nv_bfloat16 *p1, *d1;            // level 1, 8 channels
+    __nv_bfloat16 *e1, *s1;            // level 1, 16 channels
+    __nv_bfloat16 *p2, *e2;            // level 2, 16 channels
+    float* y;                          // level 0, network output (before the 1 / s scale)
+    double* norm2;                     // ||input||^2 when the caller does not supply it
+    unsigned* error;                   // tensor-core wait timeouts (bit 0)
+};
+size_t net_acts_bytes(const VolumeDims& d0);
+void net_acts_bind(NetActs& A, void* base, const VolumeDims& d0);
+
+// Gradient scratch of one evaluation (same volume as the NetActs it belongs to).
+struct NetGrads {
+    __nv_bfloat16 *gy, *ge, *gs0, *ga;  // level 0, 8 channels
+    __nv_bfloat16 *gd, *gp1;            // level 1, 8 channels
+    __nv_bfloat16 *gs1, *gb;            // level 1, 16 channels
+    __nv_bfloat16 *gc, *gp2;            // level 2, 16 channels
+    float* partial;                     // weight-gradient partials: [blocks][512][16]
+    float* tmask;                       // masked target
+    double* sums;                       // [0] target norm^2, [1] loss
+};
+size_t net_grads_bytes(const VolumeDims& d0);
+void net_grads_bind(NetGrads& G, void* base, const VolumeDims& d0);
+
+// Forward pass on the input r (r1 and *parity pick the buffer on the device when parity is given); norm2 is ||r||^2
+// on the device, or null to compute it into A.norm2. Leaves the network output in A.y.
+cudaError_t net_forward(const NetImages& I, const NetActs& A, const float* r0, const float* r1, const int* parity, const double* norm2, const uint8_t* occ, cudaStream_t s);
+// out = fluid ? A.y / s : 0 (the preconditioned vector with the input's scale restored).
+cudaError_t net_output(const NetActs& A, const double* norm2, const uint8_t* occ, float* out, cudaStream_t s);
+// Loss of the last forward pass against `target` and the parameter gradient: grad (kNetParams floats) is
+// overwritten, or accumulated into when `accumulate`; the loss is added into G.sums[1].
+cudaError_t net_backward(const NetImages& I, const NetActs& A, const NetGrads& G, const double* norm2, const float* target, const uint8_t* occ, float* grad, int accumulate, cudaStream_t s);
+// One Adam step on w with moments m, v (step >= 1), gradient scaled by gscale; then the images are repacked.
+cudaError_t net_adam(float* w, const float* grad, float* m, float* v, float lr, int step, float gscale, const NetImages& I, cudaStream_t s);
+
+// What a solve with the learned preconditioner needs: the network's images, an activation workspace on the solve's
+// volume and the occupancy (the fluid-mask input channel).
+struct LearnedSolve {
+    NetImages images;
+    NetActs acts;
+    const uint8_t* occupancy;
+};
+
+}  // namespace smoke_b200
+
+// The device block of a network's packed images (net_images_bytes() long), for copies into a context.
+struct SmokeB200Net_t;
+const void* smoke_b200_net_images_block(const SmokeB200Net_t* net);

@@ -58,6 +58,7 @@ LAYOUT_F32_3D_SOA3 = 1
 SOLVER_FIXED_CG = 0
 SOLVER_JACOBI_PCG = 1
 SOLVER_MG_FCG = 2
+SOLVER_LEARNED_FCG = 3
 REDUCTION_FP32 = 0
 REDUCTION_FP64 = 1
 SOLVE_CONVERGED = 0
@@ -121,6 +122,28 @@ class SolverStatus(C.Structure):
     _fields_ = [
         ("iterations", C.c_int32), ("passes", C.c_int32), ("status", C.c_uint32), ("reserved", C.c_uint32), ("rhs_norm", C.c_double),
         ("relative_residual", C.c_double), ("true_relative_residual", C.c_double),
+    ]
+
+
+class LaunchTune(C.Structure):
+    _fields_ = [("advect_tile", C.c_uint32), ("mg_wave", C.c_uint32), ("pcg_grid", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class TuneRecord(C.Structure):
+    _fields_ = [("tune", LaunchTune), ("ms_per_step", C.c_float), ("iterations", C.c_uint32)]
+
+
+TUNE_MAX_RECORDS = 16
+TUNE_FORCE = 1
+ADVECT_TILE_NAMES = ("flat", "32x8x1", "32x4x2", "16x4x4", "8x8x4")
+MG_WAVE_NAMES = ("0.5 wave", "1 wave", "2 waves", "4 waves", "tile per block")
+PCG_GRID_NAMES = ("all resident", "half", "quarter")
+
+
+class TuneReport(C.Structure):
+    _fields_ = [
+        ("chosen", LaunchTune), ("default_ms", C.c_float), ("chosen_ms", C.c_float), ("from_cache", C.c_uint32), ("record_count", C.c_uint32),
+        ("records", TuneRecord * TUNE_MAX_RECORDS),
     ]
 
 

@@ -55,6 +55,19 @@ class SmokeLibrary:
         ("smoke_b200_batch_create_cuda", [C.POINTER(C.c_void_p), C.c_uint32, C.c_void_p, C.POINTER(C.c_void_p)]),
         ("smoke_b200_batch_step_cuda", [C.c_void_p]),
         ("smoke_b200_batch_destroy_cuda", [C.c_void_p]),
+        ("smoke_b200_set_launch_tune_cuda", [C.c_void_p, C.POINTER(abi.LaunchTune)]),
+        ("smoke_b200_get_launch_tune_cuda", [C.c_void_p, C.POINTER(abi.LaunchTune)]),
+        ("smoke_b200_autotune_cuda", [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(abi.TuneReport)]),
+        ("smoke_b200_net_create_cuda", [C.c_uint32, C.POINTER(C.c_void_p)]),
+        ("smoke_b200_net_destroy_cuda", [C.c_void_p]),
+        ("smoke_b200_net_get_parameters_cuda", [C.c_void_p, C.c_void_p]),
+        ("smoke_b200_net_set_parameters_cuda", [C.c_void_p, C.c_void_p]),
+        ("smoke_b200_net_apply_cuda", [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        ("smoke_b200_net_gradient_cuda", [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
+        ("smoke_b200_net_train_cuda", [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_double), C.c_void_p]),
+        ("smoke_b200_set_preconditioner_net_cuda", [C.c_void_p, C.c_void_p]),
+        ("smoke_b200_apply_operator_cuda", [C.c_void_p, C.c_void_p, C.c_void_p]),
+        ("smoke_b200_conv3d_cuda", [C.c_int] * 5 + [C.c_void_p] * 3 + [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     ]
 
     def __init__(self, path: str = DEFAULT_LIBRARY, extensions: bool = True):
@@ -67,6 +80,9 @@ class SmokeLibrary:
             fn = getattr(self.lib, name)
             fn.argtypes = args
             fn.restype = C.c_int
+        if extensions:
+            self.lib.smoke_b200_net_parameter_count.argtypes = []
+            self.lib.smoke_b200_net_parameter_count.restype = C.c_uint32
 
     def symbols(self):
         return [n for n, _ in self.ABI + (self.EXTENSIONS if self.extensions else [])]
@@ -187,7 +203,7 @@ class Simulation:
 
     # ------------------------------------------------------------------ extensions (libsmoke_b200.so only)
     def set_solver(self, mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP64, max_iterations=500, tolerance=1e-5, refinement=0, warm_start=False):
-        d = abi.SolverDesc(mode, reduction, max_iterations, tolerance, refinement, 1 if warm_start else 0)
+        d = abi.SolverDesc(mode, reduction, max_iterations, tolerance, refinement, int(warm_start))
         _check(self.lib.smoke_b200_set_solver_cuda(self.handle, C.byref(d)), "set_solver")
 
     def solver_status(self) -> abi.SolverStatus:
@@ -216,10 +232,124 @@ class Simulation:
     def step_stages(self, last_stage: int):
         _check(self.lib.smoke_b200_step_stages_cuda(self.handle, last_stage), "step_stages")
 
+    def set_launch_tune(self, advect_tile: int = 0, mg_wave: int = 1, pcg_grid: int = 0):
+        t = _tune_struct({"advect_tile": advect_tile, "mg_wave": mg_wave, "pcg_grid": pcg_grid})
+        _check(self.lib.smoke_b200_set_launch_tune_cuda(self.handle, C.byref(t)), "set_launch_tune")
+
+    def launch_tune(self) -> dict:
+        t = abi.LaunchTune()
+        _check(self.lib.smoke_b200_get_launch_tune_cuda(self.handle, C.byref(t)), "get_launch_tune")
+        return _tune_dict(t)
+
+    def autotune(self, steps: int = 4, force: bool = False) -> dict:
+        """Times the step under candidate launch shapes, keeps the fastest (state restored afterwards)."""
+        rep = abi.TuneReport()
+        flags = abi.TUNE_FORCE if force else 0
+        _check(self.lib.smoke_b200_autotune_cuda(self.handle, steps, flags, C.byref(rep)), "autotune")
+        records = [dict(_tune_dict(r.tune), ms_per_step=r.ms_per_step, iterations=r.iterations) for r in rep.records[: rep.record_count]]
+        return {"chosen": _tune_dict(rep.chosen), "default_ms": rep.default_ms, "chosen_ms": rep.chosen_ms, "from_cache": bool(rep.from_cache), "records": records}
+
+    def apply_operator(self, x):
+        """A x with the context's pressure matrix (x: float32 CUDA tensor of nz x ny x nx values)."""
+        import torch
+
+        out = torch.empty_like(x)
+        with torch.cuda.stream(self.stream):
+            _check(self.lib.smoke_b200_apply_operator_cuda(self.handle, _ptr(x), _ptr(out)), "apply_operator")
+        return out
+
+    def set_preconditioner_net(self, net: "Net"):
+        _check(self.lib.smoke_b200_set_preconditioner_net_cuda(self.handle, net.handle), "set_preconditioner_net")
+
     def solve_pressure(self, eager: bool = False):
         """Pressure solve of the current right-hand side (eager: every kernel launched directly, host-driven loop)."""
         fn = self.lib.smoke_b200_solve_pressure_eager_cuda if eager else self.lib.smoke_b200_solve_pressure_cuda
         _check(fn(self.handle), "solve_pressure")
+
+
+class Net:
+    """The learned preconditioner's network (smoke_b200_net_*_cuda). Device inputs are contiguous torch CUDA tensors;
+    every call synchronises the current torch stream."""
+
+    def __init__(self, library: SmokeLibrary, seed: int = 0):
+        self.L = library
+        self.lib = library.lib
+        self.handle = C.c_void_p()
+        _check(self.lib.smoke_b200_net_create_cuda(seed, C.byref(self.handle)), "net_create")
+
+    @property
+    def parameter_count(self) -> int:
+        return int(self.lib.smoke_b200_net_parameter_count())
+
+    def close(self):
+        if self.handle:
+            self.lib.smoke_b200_net_destroy_cuda(self.handle)
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def _stream():
+        import torch
+
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def parameters(self):
+        import numpy as np
+
+        out = np.zeros(self.parameter_count, np.float32)
+        _check(self.lib.smoke_b200_net_get_parameters_cuda(self.handle, out.ctypes.data_as(C.c_void_p)), "net_get_parameters")
+        return out
+
+    def set_parameters(self, values):
+        import numpy as np
+
+        v = np.ascontiguousarray(values, np.float32)
+        if v.size != self.parameter_count:
+            raise SmokeError(f"expected {self.parameter_count} parameters, got {v.size}")
+        _check(self.lib.smoke_b200_net_set_parameters_cuda(self.handle, v.ctypes.data_as(C.c_void_p)), "net_set_parameters")
+
+    def apply(self, rhs, occupancy):
+        """N(rhs) for one volume: rhs float32 [nz, ny, nx], occupancy uint8 [nz, ny, nx] (CUDA tensors)."""
+        import torch
+
+        nz, ny, nx = rhs.shape
+        out = torch.empty_like(rhs)
+        _check(self.lib.smoke_b200_net_apply_cuda(self.handle, nx, ny, nz, _ptr(rhs), _ptr(occupancy), _ptr(out), self._stream()), "net_apply")
+        return out
+
+    def gradient(self, rhs, occupancy, target):
+        """(loss, gradient) of one sample; the gradient in parameter layout (numpy float32)."""
+        import numpy as np
+
+        nz, ny, nx = rhs.shape
+        g = np.zeros(self.parameter_count, np.float32)
+        loss = C.c_double()
+        _check(self.lib.smoke_b200_net_gradient_cuda(self.handle, nx, ny, nz, _ptr(rhs), _ptr(occupancy), _ptr(target), g.ctypes.data_as(C.c_void_p), C.byref(loss), self._stream()), "net_gradient")
+        return loss.value, g
+
+    def train_step(self, rhs, occupancy, target, learning_rate: float) -> float:
+        """One Adam step on a batch: rhs / target float32 [count, nz, ny, nx], occupancy uint8 of the same shape."""
+        count, nz, ny, nx = rhs.shape
+        loss = C.c_double()
+        _check(self.lib.smoke_b200_net_train_cuda(self.handle, nx, ny, nz, count, _ptr(rhs), _ptr(occupancy), _ptr(target), float(learning_rate), C.byref(loss), self._stream()), "net_train")
+        return loss.value
+
+
+def _tune_dict(t: abi.LaunchTune) -> dict:
+    return {"advect_tile": t.advect_tile, "mg_wave": t.mg_wave, "pcg_grid": t.pcg_grid}
+
+
+def _tune_struct(d: dict) -> abi.LaunchTune:
+    t = abi.LaunchTune()
+    t.advect_tile = d.get("advect_tile", 0)
+    t.mg_wave = d.get("mg_wave", 1)
+    t.pcg_grid = d.get("pcg_grid", 0)
+    return t
 
 
 class Batch:
