@@ -76,6 +76,15 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def peak_tflops():
+    """Measured dense BF16 tensor throughput (burst) of this pool's B200s, else the fallback figure."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except Exception:
+        return 1590.0
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
 
@@ -360,6 +369,7 @@ def bench_b200(args, rank, world, local):
         torch.cuda.synchronize()
         barrier(world)
         results[name] = (max_over_ranks(statistics.mean(t), world), statistics.mean(its), max(res))
+    learned = bench_learned(sim, driver, state, step0, flush, n, args, world)
     # e2e through the ABI (headline form), same state
     restore_state(sim, state)
     sim.set_solver(**FORMS[HEADLINE])
@@ -393,10 +403,68 @@ def bench_b200(args, rank, world, local):
         "gpu_launches": round(args.steps * (STEP_KERNELS + solver_launches(n, its, FORMS[HEADLINE]["refinement"]))),
         "clocks": clocks.summary() if clocks is not None else None,
         "launch_tune": {k: tune_summary(v) for k, v in tunes.items()} if tunes else "defaults (--no-tune)",
+        "learned": learned,
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
     return line
+
+
+LEARNED_FORM = dict(mode=abi.SOLVER_LEARNED_FCG, reduction=abi.REDUCTION_FP64, max_iterations=3000, tolerance=1e-5, refinement=3)
+
+
+def net_flops(nx, ny, nz):
+    """Dense FLOPs of one network evaluation: 2 * 27 * cin * cout per cell of each layer's level (real channels)."""
+    dims = [(nx, ny, nz)]
+    for _ in range(2):
+        dims.append(tuple((v + 1) // 2 for v in dims[-1]))
+    layers = [(2, 8, 0), (8, 16, 1), (16, 16, 2), (16, 8, 1), (8, 8, 0), (8, 1, 0)]
+    return sum(2 * 27 * ci * co * dims[l][0] * dims[l][1] * dims[l][2] for ci, co, l in layers)
+
+
+def bench_learned(sim, driver, state, step0, flush, n, args, world, timed_steps=2):
+    """The learned-preconditioner form on the same states (trained weights of the package), timed over a few steps
+    (its solves take seconds), and the network evaluation alone: ms per apply and dense tensor FLOP rate."""
+    import torch
+
+    import smoke_b200
+    import train_preconditioner
+
+    if not os.path.exists(train_preconditioner.DEFAULT_WEIGHTS):
+        return {"unavailable": "no trained weights"}
+    net = smoke_b200.Net(sim.L, seed=0)
+    train_preconditioner.load(net)
+    restore_state(sim, state)
+    sim.set_preconditioner_net(net)
+    sim.set_solver(**LEARNED_FORM)
+    run_steps(sim, driver, step0, 1, flush)
+    barrier(world)
+    t, its, res = run_steps(sim, driver, step0 + 1, timed_steps, flush, status=True)
+    flags = sim.solver_status().flags
+    with torch.cuda.stream(sim.stream):
+        rhs = sim.view(abi.VIEW_FLOW_PRESSURE_RHS).clone()
+        occ = torch.zeros(rhs.shape, dtype=torch.uint8, device="cuda")
+    sim.stream.synchronize()
+    net.apply(rhs, occ)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 10
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        net.apply(rhs, occ)
+    e1.record()
+    torch.cuda.synchronize()
+    apply_ms = e0.elapsed_time(e1) / reps
+    net.close()
+    flops = net_flops(n, n, n)
+    tflops = flops / (apply_ms * 1e-3) / 1e12
+    bf16_peak = peak_tflops()
+    return {"form": "FCG, z = N(r) + one Jacobi step (tcgen05 BF16 U-Net, 3 levels, 16257 parameters), FP64 dots + refinement, to 1e-5",
+            "ms_per_step": round(max_over_ranks(statistics.mean(t), world), 2), "pcg_iterations": round(statistics.mean(its), 1), "true_rel_residual_max": max(res),
+            "fell_back_to_jacobi": bool(flags & 1), "timed_steps": timed_steps,
+            "net_apply_ms_128": round(apply_ms, 4), "net_dense_gflop_per_apply": round(flops / 1e9, 2),
+            "tensor_roofline": {"bound": "tensor", "achieved": round(tflops, 2), "peak": bf16_peak, "unit": "TFLOP/s", "frac": round(tflops / bf16_peak, 5),
+                                "note": "dense FLOPs of real channels over the whole apply (11 kernels); the convolutions are bound by their neighbour gathers, not the tensor pipe"}}
 
 
 def tune_summary(rep):
@@ -610,7 +678,8 @@ def bench_reference(args, rank, world, local):
 def profile_workload(args):
     """Profiling workloads (for ncu; prints one status line, no benchmark JSON): the 128^3 plume after the spin-up,
     then --profile-count repetitions of: `solve` an eager multigrid solve (every kernel a plain launch), `solve-graph`
-    the multigrid solve graph, `step` an eager step (stage kernels launched one by one, the solve as its graph)."""
+    the multigrid solve graph, `step` an eager step (stage kernels launched one by one, the solve as its graph), `net`
+    the learned preconditioner's network on the step's right-hand side (packaged weights)."""
     import torch
 
     import plume_scene
@@ -626,6 +695,22 @@ def profile_workload(args):
         a, w, g = (int(v) for v in args.shapes.split(","))
         sim.set_launch_tune(advect_tile=a, mg_wave=w, pcg_grid=g)
     run_steps(sim, driver, 0, SPINUP_STEPS, None)
+    if args.profile == "net":  # the learned preconditioner's network on the step's right-hand side
+        import train_preconditioner
+
+        net = smoke_b200.Net(lib, seed=0)
+        train_preconditioner.load(net)
+        with torch.cuda.stream(stream):
+            rhs = sim.view(abi.VIEW_FLOW_PRESSURE_RHS).clone()
+            occ = torch.zeros(rhs.shape, dtype=torch.uint8, device="cuda")
+        stream.synchronize()
+        for k in range(args.profile_count):
+            out = net.apply(rhs, occ)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": "net", "count": args.profile_count, "out_norm": float(out.norm())}), flush=True)
+        net.close()
+        sim.close()
+        return
     for k in range(args.profile_count):
         if args.profile == "step":
             driver.apply(SPINUP_STEPS + k)
@@ -677,7 +762,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--calibrate-reference", action="store_true")
     ap.add_argument("--calibrate-counts", type=int, nargs="*", default=[200, 300, 400, 500, 600, 800, 1000])
-    ap.add_argument("--profile", choices=["solve", "solve-graph", "step"], help="run a profiling workload instead of the benchmark")
+    ap.add_argument("--profile", choices=["solve", "solve-graph", "step", "net"], help="run a profiling workload instead of the benchmark")
     ap.add_argument("--workload", default="plume128", choices=["plume128", "plume64", "large", "batched"],
                     help="plume128: the headline (default); plume64, large, batched: the other benchmark configurations")
     ap.add_argument("--profile-count", type=int, default=1)

@@ -96,7 +96,7 @@ struct PcgStatusDevice {
     int32_t iterations;
     int32_t passes;
     uint32_t status;
-    uint32_t reserved;
+    uint32_t flags;     // bit 0: the learned solve fell back to the plain preconditioner
     double rhs_norm;
     double relative_residual;
     double true_relative_residual;
@@ -180,7 +180,13 @@ struct MgState {
     int parity, first_iter, it, passes;
     uint32_t status, fail, halt, zero_solution;
     uint32_t loop;         // the loop condition the last update set (read by the host in eager mode)
+    uint32_t fallback;     // learned solve: 1 once the network is dropped for the plain (Jacobi) preconditioner
+    int stall_it;          // learned solve: iteration of the last stagnation checkpoint
+    double stall_ref;      // learned solve: ||r||^2 at that checkpoint
 };
+// Learned solve: the network is dropped for the plain preconditioner when ||r|| shrank less than 1.2x over this many
+// iterations (stagnation).
+constexpr int kLearnedStallWindow = 100;
 struct MgSolveArgs {
     MgHierarchy H;
     MgWork W;

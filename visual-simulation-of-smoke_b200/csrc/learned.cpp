@@ -248,7 +248,7 @@ SmokeSimulationResult smoke_b200_conv3d_cuda(int nx, int ny, int nz, int cin, in
     if (bias && cudaMemcpyAsync(b16, bias, cout * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     if (launch_pack_conv(weights, cin, cout, 0, pack, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     const VolumeDims d = volume_dims(nx, ny, nz);
-    if (launch_conv3(d, cin_store, static_cast<const __nv_bfloat16*>(in), pack, b16, relu, nullptr, static_cast<__nv_bfloat16*>(out), cout_store, out_f32, error, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (launch_conv3(d, cin_store, static_cast<const __nv_bfloat16*>(in), pack, b16, relu, nullptr, static_cast<__nv_bfloat16*>(out), cout_store, out_f32, error, s, nullptr) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     unsigned err = 0;
     if (cudaMemcpyAsync(&err, error, sizeof(err), cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return err ? SMOKE_SIMULATION_RESULT_BACKEND_FAILURE : SMOKE_SIMULATION_RESULT_OK;

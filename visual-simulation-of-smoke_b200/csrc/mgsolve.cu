@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(kThreads) mg_setup_kernel(const __grid_constan
 // Level-0 update: r' = r - alpha q, e += alpha p, zp = w D^-1 r', restriction of r' - A zp into level 1, ||r'||^2.
 // initial = 1: the pass's first round (alpha = 0, no iteration counted). The last block tests convergence, flips
 // the buffer parity and sets the loop condition `cond`.
-template <typename T>
+template <typename T, bool LEARNED>
 __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_constant__ MgSolveArgs A, int initial, cudaGraphConditionalHandle cond, int in_graph) {
     const MgLevel& L0 = A.H.L[0];
     MgState* st = A.st;
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
                 const float rq = r[c.q], qq = A.W.q[c.q];
                 const float pq = initial ? 0.0f : pn[c.q], eq = initial ? 0.0f : A.e[c.q];
                 const float rn = rq - a * qq;
-                if (!A.learned) {  // pre-smoothing and the residual restricted to level 1
+                if constexpr (!LEARNED) {  // pre-smoothing and the residual restricted to level 1
                     float un[6];
 #pragma unroll
                     for (int k = 0; k < 6; ++k) un[k] = wdiag(L0.code[nb[k]]) * (r[nb[k]] - a * A.W.q[nb[k]]);
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
                 if (!initial) A.e[c.q] = eq + a * pq;
                 rr += static_cast<T>(rn) * static_cast<T>(rn);
             }
-            if (!A.learned) restrict_tile(res, A.H.L[1], c);
+            if constexpr (!LEARNED) restrict_tile(res, A.H.L[1], c);
         });
         block_accumulate<T>(st, kAccRR, rr, -1, T(0));
     }
@@ -362,6 +362,16 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
         }
     }
     if (!initial) st->first_iter = 0;
+    if (LEARNED && !stop && !st->fallback) {  // plain-preconditioner fallback of a stalled learned solve
+        if (initial) {
+            st->stall_it = st->it;
+            st->stall_ref = st->rnorm2;
+        } else if (st->it - st->stall_it >= kLearnedStallWindow) {
+            if (st->rnorm2 > st->stall_ref * (1.0 / 1.44)) st->fallback = 1;
+            st->stall_it = st->it;
+            st->stall_ref = st->rnorm2;
+        }
+    }
     st->parity ^= 1;
     for (int k = kAccRR; k < kAccCount; ++k) zero_acc(st, k);
     st->loop = stop ? 0u : 1u;
@@ -477,14 +487,16 @@ __global__ void __launch_bounds__(kThreads) mg_smooth_kernel(const __grid_consta
 }
 
 // Learned preconditioner, first half: zp = N(r) = y / s on active cells (y the network's output for the current
-// residual, s = sqrt(n / ||r||^2) its input scale), 0 elsewhere. mg_smooth_kernel<true> then post-smooths it,
-// z = zp + w D^-1 (r - A zp): the network supplies the smooth part of the correction, the Jacobi step the rough part.
+// residual, s = sqrt(n / ||r||^2) its input scale), 0 elsewhere; 0 everywhere once the solve fell back to the plain
+// preconditioner. mg_smooth_kernel<true> then post-smooths it, z = zp + w D^-1 (r - A zp): the network supplies the
+// smooth part of the correction, the Jacobi step the rough part (and all of it after the fallback).
 __global__ void __launch_bounds__(kThreads) mg_net_zp_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
     const MgLevel& F = A.H.L[0];
     const double rn2 = A.st->rnorm2;
+    const bool fallback = A.st->fallback != 0;  // then z is the Jacobi step alone: the plain preconditioner
     const float inv_s = rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n))) : 0.0f;
     for_tiles(F, [&](const Cell& c) {
-        if (c.in) F.zp[c.q] = active(F.code[c.q]) ? y[c.q] * inv_s : 0.0f;
+        if (c.in) F.zp[c.q] = active(F.code[c.q]) && !fallback ? y[c.q] * inv_s : 0.0f;
     });
 }
 
@@ -738,6 +750,7 @@ __global__ void __launch_bounds__(kThreads) mg_finalize_kernel(const __grid_cons
     if (block_linear() != 0 || tid() != 0) return;
     PcgStatusDevice s{};
     s.iterations = st->it;
+    s.flags = st->fallback ? 1u : 0u;
     s.passes = st->passes;
     s.status = st->status;
     s.rhs_norm = sqrt(st->bb);
@@ -824,6 +837,13 @@ cudaError_t add_while(cudaStream_t s, cudaStream_t body_stream, cudaGraphConditi
     return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
 }
 
+// The level-0 update of the solve's preconditioner kind.
+template <typename T>
+void launch_update(const MgSolveArgs& A, int initial, cudaGraphConditionalHandle h, int in_graph, cudaStream_t s) {
+    if (A.learned) mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, A.H.L[0], A.wave), kBlock, 0, s>>>(A, initial, h, in_graph);
+    else mg_update_kernel<T, false><<<wave(mg_update_kernel<T, false>, A.H.L[0], A.wave), kBlock, 0, s>>>(A, initial, h, in_graph);
+}
+
 // One iteration's loop body (everything after the update that tests convergence, up to the next update).
 template <typename T>
 void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_graph, uint32_t block_bytes, cudaStream_t bs) {
@@ -831,11 +851,11 @@ void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_grap
     const MgLevel& L0 = H.L[0];
     if (A.learned) {  // z = N(r): the network on the current residual (its parity and norm read on the device)
         const LearnedSolve& N = *A.net;
-        if (net_forward(N.images, N.acts, A.W.r[0], A.W.r[1], &A.st->parity, &A.st->rnorm2, N.occupancy, bs) != cudaSuccess) return;
+        if (net_forward(N.images, N.acts, A.W.r[0], A.W.r[1], &A.st->parity, &A.st->rnorm2, N.occupancy, bs, &A.st->fallback) != cudaSuccess) return;
         mg_net_zp_kernel<<<wave(mg_net_zp_kernel, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
         mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
         mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
-        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
+        mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
         return;
     }
     const int g = H.grid_levels;
@@ -848,7 +868,7 @@ void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_grap
     mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[1], A.wave), kBlock, 0, bs>>>(H, 0);
     mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
     mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
-    mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
+    mg_update_kernel<T, false><<<wave(mg_update_kernel<T, false>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
 }
 
 // Learned solve with the network's warm start: x64 = N(b) (through the q array, which the set-up clears), so the
@@ -887,7 +907,7 @@ cudaError_t enqueue_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream
         cudaGraphConditionalHandle h;
         e = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
         if (e != cudaSuccess) return e;
-        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0, A.wave), kBlock, 0, s>>>(A, 1, h, 1);
+        launch_update<T>(A, 1, h, 1, s);
         e = add_while(s, body_stream, h, [&](cudaStream_t bs) { launch_body<T>(A, h, 1, block_bytes, bs); });
         if (e != cudaSuccess) return e;
         if (A.ir) {
@@ -913,7 +933,7 @@ cudaError_t run_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream_t s
         return r == cudaSuccess ? cudaStreamSynchronize(s) : r;
     };
     for (int pass = 0; pass < passes; ++pass) {
-        mg_update_kernel<T><<<wave(mg_update_kernel<T>, L0, A.wave), kBlock, 0, s>>>(A, 1, 0, 0);
+        launch_update<T>(A, 1, 0, 0, s);
         for (;;) {  // bounded: every update counts an iteration and stops at max_iterations
             uint32_t flag = 0;
             if ((e = loop_flag(flag)) != cudaSuccess) return e;

@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ S
         st.rhs_norm = sqrt(static_cast<double>(bb));
         st.relative_residual = bb > T(0) ? sqrt(static_cast<double>(rnorm2) / static_cast<double>(bb)) : 0.0;
         st.true_relative_residual = true_rel;
-        st.reserved = 0;
+        st.flags = 0;
         ctl->status = st;
     }
 }

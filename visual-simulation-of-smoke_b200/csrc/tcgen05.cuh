@@ -95,6 +95,20 @@ __device__ __forceinline__ void tmem_load16(uint32_t addr, float v[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// One arrival on the mbarrier that also expects `bytes` of asynchronous (TMA) transfer before its phase completes.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// TMA: the box of the 4-D tensor map at coordinates (c0, c1, c2, c3) into shared memory at `dst`, completing
+// `bytes` on the mbarrier. Out-of-range elements (negative coordinates included) read as zero. No multicast.
+__device__ __forceinline__ void tma_load_4d(void* dst, const void* map, int c0, int c1, int c2, int c3, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+        : "memory");
+}
+
 #endif  // __CUDACC__
 
 }  // namespace tc

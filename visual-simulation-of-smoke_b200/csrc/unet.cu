@@ -11,6 +11,9 @@
 #include <map>
 #include <mutex>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "tcgen05.cuh"
 #include "unet.h"
 
@@ -20,18 +23,32 @@ namespace {
 constexpr int kConvThreads = 128;
 constexpr long long kSpinCycles = 4000000000ll;  // ~2 s: bound of every tensor-core completion wait
 
+// Tiles of 8 x 16 x 1 cells (M = 128 rows, row m = cell (m % 8, m / 8) of the tile). A tile's input is its halo box
+// of 10 x 18 x 3 cells, brought into shared memory by one TMA load per 8-channel plane (zeros outside the volume):
+// cell (x, y, z) of the box at byte ((z * 18 + y) * 10 + x) * 16 of its plane. The A operand of tap (dx, dy, dz) is
+// that box read from offset ((1 + dz) * 18 + 1 + dy) * 160 + (1 + dx) * 16: every 8 cells of a tile row are 8
+// consecutive 16-byte rows of the box, i.e. one core matrix, and the next tile row starts one box row (160 bytes) on
+// (SBO). So no im2col copy exists: each MMA reads its two K columns (two taps of an 8-channel input, or the two
+// planes of one tap of a 16-channel input; LBO = their distance) straight from the box.
 template <int CIN>
 struct ConvShape {
-    static constexpr int kTaps = conv_taps(CIN);        // 28 for 8 channels: a zero tap pads K to a multiple of 16
-    static constexpr int kK = kTaps * CIN;              // 224 or 432
-    static constexpr int kKSteps = kK / 16;             // MMAs per tile (K = 16 each)
-    static constexpr int kKGroups = kK / 8;             // core-matrix columns (8 BF16 each)
-    static constexpr uint32_t kABytes = kKGroups * 16u * 128u;  // 16 row groups of 8 cells
+    static constexpr int kTX = 8, kTY = 16;
+    static constexpr int kHX = kTX + 2, kHY = kTY + 2, kHZ = 3;
+    static constexpr uint32_t kRow = kHX * 16;                               // bytes of one box row (SBO)
+    static constexpr uint32_t kBox = kHX * kHY * kHZ * 16;                   // 8640 bytes per plane
+    static constexpr uint32_t kPlane = 8704;                                 // plane pitch: box + zero slack, 128-aligned
+    static constexpr int kPlanes = CIN / 8;
+    static constexpr uint32_t kStage = (kPlanes * kPlane + 1023u) & ~1023u;  // one pipeline stage
+    static constexpr int kKSteps = conv_taps(CIN) * CIN / 16;                // MMAs per tile (K = 16 each)
     static constexpr uint32_t kBBytes = conv_pack_bytes(CIN);
-    static constexpr uint32_t kARegion = kABytes;
-    static constexpr uint32_t kBRegion = kBBytes;
-    static constexpr uint32_t kSmem = kARegion + kBRegion;
+    static constexpr uint32_t kSmem = 2 * kStage + kBBytes;
 };
+__host__ __device__ constexpr uint32_t tap_offset(int tap) {
+    return ((tap / 9) * 18 + (tap / 3) % 3) * 160u + (tap % 3) * 16u;  // (dz + 1, dy + 1, dx + 1) of the tap
+}
+// the padding tap's K column (tap 26's rows, 16 bytes on) stays inside the plane's zero slack
+static_assert(tap_offset(26) + 16 + 15 * ConvShape<8>::kRow + 128 <= ConvShape<8>::kPlane, "zero slack");
+static_assert(tap_offset(26) + 15 * ConvShape<8>::kRow + 128 <= ConvShape<8>::kBox, "box");
 
 struct ConvArgs {
     const __nv_bfloat16* in;
@@ -41,6 +58,7 @@ struct ConvArgs {
     __nv_bfloat16* out;
     float* out_f32;
     unsigned* error;
+    const uint32_t* skip;  // optional: the launch does nothing when *skip is nonzero
     int relu, cout_store;
     int nx, ny, nz;
     uint32_t n;
@@ -51,81 +69,89 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
+// Persistent over tiles with two pipeline stages: while the tensor core works on tile j (stage j % 2, accumulator
+// j % 2 in tensor memory), the TMA load of tile j + 1 fills the other stage. Thread 0 issues the loads and the MMAs;
+// all 128 threads run the epilogue (tensor memory -> bias, ReLU, gate -> BF16/FP32 stores).
 template <int CIN>
-__global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_constant__ ConvArgs a) {
+__global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_constant__ ConvArgs a, const __grid_constant__ CUtensorMap map) {
     using S = ConvShape<CIN>;
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* As = smem;
-    uint8_t* Bs = smem + S::kARegion;
-    __shared__ uint64_t bar;
+    uint8_t* Bs = smem + 2 * S::kStage;
+    __shared__ uint64_t full[2], done[2];
     __shared__ uint32_t tmem_slot;
+    if (a.skip && *a.skip) return;  // uniform: every block reads the same word
     const int t = threadIdx.x, warp = t >> 5;
     const uint4* wsrc = reinterpret_cast<const uint4*>(a.wpack);
     for (uint32_t i = t; i < S::kBBytes / 16u; i += kConvThreads) reinterpret_cast<uint4*>(Bs)[i] = wsrc[i];
-    if constexpr (S::kTaps > 27) {  // the padding tap's core matrices stay zero
-        for (int i = t; i < (S::kTaps - 27) * (CIN / 8) * 16 * 8; i += kConvThreads) reinterpret_cast<uint4*>(As + 27u * (CIN / 8) * 16u * 128u)[i] = make_uint4(0, 0, 0, 0);
+    for (int st = 0; st < 2; ++st)  // the slack after each box stays zero (read by the padding tap, times zero weights)
+        for (int p = 0; p < S::kPlanes; ++p)
+            for (uint32_t i = t; i < (S::kPlane - S::kBox) / 16u; i += kConvThreads) reinterpret_cast<uint4*>(smem + st * S::kStage + p * S::kPlane + S::kBox)[i] = make_uint4(0, 0, 0, 0);
+    if (t == 0) {
+        for (int st = 0; st < 2; ++st) {
+            tc::mbar_init(&full[st], 1);
+            tc::mbar_init(&done[st], 1);
+        }
     }
-    if (t == 0) tc::mbar_init(&bar, 1);
     if (warp == 0) tc::tmem_alloc(&tmem_slot, 32);
+    tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
     constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 16, false, false);
-    const uint32_t a_base = tc::smem_addr(As), b_base = tc::smem_addr(Bs);
-    const uint32_t tiles = (a.n + 127u) / 128u;
-    const int rg = t >> 3, rr = t & 7;
+    const uint32_t b_base = tc::smem_addr(Bs);
+    const int ntx = (a.nx + S::kTX - 1) / S::kTX, nty = (a.ny + S::kTY - 1) / S::kTY;
+    const uint32_t tiles = static_cast<uint32_t>(ntx) * nty * a.nz;
+    auto load = [&](uint32_t tile, int st) {
+        const int tx = static_cast<int>(tile % ntx), rest = static_cast<int>(tile / ntx);
+        const int ty = rest % nty, tz = rest / nty;
+        tc::mbar_arrive_expect_tx(&full[st], S::kPlanes * S::kBox);
+        for (int p = 0; p < S::kPlanes; ++p) tc::tma_load_4d(smem + st * S::kStage + p * S::kPlane, &map, 8 * p, tx * S::kTX - 1, ty * S::kTY - 1, tz - 1, &full[st]);
+    };
     float bias[16];
 #pragma unroll
     for (int c = 0; c < 16; ++c) bias[c] = a.bias ? __ldg(a.bias + c) : 0.0f;
-    uint32_t phase = 0;
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const uint32_t q = tile * 128u + t;
-        const bool in = q < a.n;
-        int x = 0, y = 0, z = 0;
-        if (in) {
-            const uint32_t row = q / a.nx;
-            x = q - row * a.nx;
-            z = row / a.ny;
-            y = row - z * a.ny;
-        }
-#pragma unroll 3
-        for (int tap = 0; tap < 27; ++tap) {
-            const int xx = x + tap % 3 - 1, yy = y + (tap / 3) % 3 - 1, zz = z + tap / 9 - 1;
-            const bool inside = in && xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny && zz >= 0 && zz < a.nz;
-            const uint4* src = reinterpret_cast<const uint4*>(a.in) + static_cast<size_t>(inside ? (static_cast<uint32_t>(zz) * a.ny + yy) * a.nx + xx : 0u) * (CIN / 8);
-#pragma unroll
-            for (int cg = 0; cg < CIN / 8; ++cg) {
-                const uint4 v = inside ? __ldg(src + cg) : make_uint4(0, 0, 0, 0);
-                const int kg = tap * (CIN / 8) + cg;
-                *reinterpret_cast<uint4*>(As + (kg * 16 + rg) * 128 + rr * 16) = v;
-            }
-        }
-        tc::fence_async_smem();
-        tc::fence_before_sync();
-        __syncthreads();
-        tc::fence_after_sync();
+    if (t == 0 && blockIdx.x < tiles) load(blockIdx.x, 0);
+    uint32_t j = 0;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++j) {
+        const int st = static_cast<int>(j & 1u);
+        const uint32_t parity = (j >> 1) & 1u;
         if (t == 0) {
+            // the other stage was last read by the MMAs of tile j - 1, which completed before that tile's epilogue
+            if (tile + gridDim.x < tiles) load(tile + gridDim.x, st ^ 1);
+            if (tc::mbar_wait(&full[st], parity, kSpinCycles)) {
+                tc::fence_after_sync();
+                const uint32_t a_base = tc::smem_addr(smem + st * S::kStage);
 #pragma unroll 1
-            for (int k = 0; k < S::kKSteps; ++k) {
-                // K step k: core-matrix columns 2k, 2k + 1 (LBO: next column, 16 row groups on); SBO: next row group
-                const uint64_t ad = tc::smem_desc(a_base + k * 4096u, 2048u, 128u);
-                const uint64_t bd = tc::smem_desc(b_base + k * 512u, 256u, 128u);
-                tc::mma_bf16(tmem, ad, bd, idesc, k > 0 ? 1u : 0u);
+                for (int k = 0; k < S::kKSteps; ++k) {
+                    uint32_t start, lbo;
+                    if constexpr (CIN == 8) {  // taps 2k and 2k + 1 (tap 27: zero weights, any finite A)
+                        start = a_base + tap_offset(2 * k);
+                        lbo = 2 * k + 1 < 27 ? tap_offset(2 * k + 1) - tap_offset(2 * k) : 16u;
+                    } else {  // tap k, channel planes 0 and 1
+                        start = a_base + tap_offset(k);
+                        lbo = S::kPlane;
+                    }
+                    tc::mma_bf16(tmem + st * 16, tc::smem_desc(start, lbo, S::kRow), tc::smem_desc(b_base + k * 512u, 256u, 128u), idesc, k > 0 ? 1u : 0u);
+                }
+                tc::commit(&done[st]);
+            } else {
+                atomicOr(a.error, 1u);
             }
-            tc::commit(&bar);
         }
         __syncwarp();
-        const bool done = __syncthreads_and(tc::mbar_wait(&bar, phase, kSpinCycles) ? 1 : 0) != 0;
-        phase ^= 1u;
-        if (!done) {
+        const bool ok = __syncthreads_and(tc::mbar_wait(&done[st], parity, kSpinCycles) ? 1 : 0) != 0;
+        if (!ok) {
             if (t == 0) atomicOr(a.error, 1u);
             break;
         }
         tc::fence_after_sync();
         float acc[16];
-        tc::tmem_load16(tmem + (static_cast<uint32_t>(warp * 32) << 16), acc);
-        if (in) {
+        tc::tmem_load16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + st * 16, acc);
+        const int tx = static_cast<int>(tile % ntx), rest = static_cast<int>(tile / ntx);
+        const int x = tx * S::kTX + (t & 7), y = (rest % nty) * S::kTY + (t >> 3), z = rest / nty;
+        if (x < a.nx && y < a.ny) {
+            const uint32_t q = (static_cast<uint32_t>(z) * a.ny + y) * a.nx + x;
             float v[16];
 #pragma unroll
             for (int c = 0; c < 16; ++c) {
@@ -152,7 +178,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
             }
         }
         tc::fence_before_sync();
-        __syncthreads();  // the accumulator is read out before the next tile's MMAs overwrite it
+        __syncthreads();  // this accumulator is read out before tile j + 2's MMAs overwrite it
         tc::fence_after_sync();
     }
     tc::fence_before_sync();
@@ -181,8 +207,11 @@ __global__ void pack_conv_kernel(const float* __restrict__ w, int cin, int cout,
     }
 }
 
-// Resident blocks of a kernel (per SM x SMs), cached per kernel and device.
-int resident_blocks(const void* kernel, int threads, size_t smem) {
+// Resident blocks of a kernel that uses `smem` bytes of dynamic shared memory (per SM x SMs): the shared memory of
+// an SM over what one block takes (its dynamic bytes, 1 KB of static data and the 1 KB the system reserves per
+// block), at most 6 (tensor memory: 6 x 64 columns at most of 512). These kernels' 128 threads and < 64 registers
+// never bind first. Cached per kernel and device.
+int resident_blocks(const void* kernel, size_t smem) {
     static std::mutex lock;
     static std::map<std::pair<const void*, int>, int> cache;
     int dev = 0;
@@ -190,26 +219,60 @@ int resident_blocks(const void* kernel, int threads, size_t smem) {
     std::lock_guard<std::mutex> guard(lock);
     auto it = cache.find({kernel, dev});
     if (it != cache.end()) return it->second;
-    int sms = 1, per_sm = 1;
+    int sms = 1, smem_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1) per_sm = 1;
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    const int per_sm = std::min(6, std::max(1, smem_sm / static_cast<int>(smem + 2048)));
     const int r = std::max(1, sms * per_sm);
     cache.emplace(std::make_pair(kernel, dev), r);
     return r;
+}
+
+// cuTensorMapEncodeTiled from the driver, found once through the runtime (no link against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess) fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// Tensor map of a channels-last BF16 volume with `cin` stored channels: dimensions (channel, x, y, z), boxes of
+// 8 channels x the halo of one tile, zeros outside.
+template <int CIN>
+cudaError_t halo_map(CUtensorMap* map, const ConvArgs& a) {
+    using S = ConvShape<CIN>;
+    const auto encode = tensor_map_encoder();
+    if (encode == nullptr) return cudaErrorNotSupported;
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(CIN), static_cast<cuuint64_t>(a.nx), static_cast<cuuint64_t>(a.ny), static_cast<cuuint64_t>(a.nz)};
+    const cuuint64_t strides[3] = {static_cast<cuuint64_t>(CIN) * 2, static_cast<cuuint64_t>(a.nx) * CIN * 2, static_cast<cuuint64_t>(a.nx) * a.ny * CIN * 2};
+    const cuuint32_t box[4] = {8, S::kHX, S::kHY, S::kHZ};
+    const cuuint32_t step[4] = {1, 1, 1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(a.in), dims, strides, box, step, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 template <int CIN>
 cudaError_t conv_typed(const VolumeDims& d, const ConvArgs& a, cudaStream_t s) {
     using S = ConvShape<CIN>;
     static bool configured = false;
-    if (!configured) {
-        const cudaError_t e = cudaFuncSetAttribute(conv3_kernel<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::kSmem));
+    if (!configured) {  // all of the unified L1 as shared memory, so that several blocks fit on an SM
+        cudaError_t e = cudaFuncSetAttribute(conv3_kernel<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::kSmem));
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(conv3_kernel<CIN>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    const uint32_t tiles = (d.n + 127u) / 128u;
-    const int grid = static_cast<int>(std::min<uint32_t>(tiles, static_cast<uint32_t>(resident_blocks(reinterpret_cast<const void*>(conv3_kernel<CIN>), kConvThreads, S::kSmem))));
-    conv3_kernel<CIN><<<grid, kConvThreads, S::kSmem, s>>>(a);
+    if ((reinterpret_cast<uintptr_t>(a.in) & 15u) != 0) return cudaErrorMisalignedAddress;
+    CUtensorMap map;
+    const cudaError_t e = halo_map<CIN>(&map, a);
+    if (e != cudaSuccess) return e;
+    const uint64_t tiles = static_cast<uint64_t>((d.nx + S::kTX - 1) / S::kTX) * ((d.ny + S::kTY - 1) / S::kTY) * d.nz;
+    const int grid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(resident_blocks(reinterpret_cast<const void*>(conv3_kernel<CIN>), S::kSmem))));
+    conv3_kernel<CIN><<<grid, kConvThreads, S::kSmem, s>>>(a, map);
     return cudaGetLastError();
 }
 
@@ -227,11 +290,9 @@ struct WgradShape {
     static constexpr int kMTiles = kMPad / 128;            // 2 or 4
     static constexpr int kMGroups = kMPad / 8;             // core matrices along M
     static constexpr uint32_t kABytes = (kWgradCells / 8) * kMGroups * 128u;
-    // A region with room past the operand for any descriptor of the tile, whichever of its two strides the MMA
-    // applies along M (kept until this MN-major layout is checked against the float64 gradient)
-    static constexpr uint32_t kARegion = kABytes + (kMTiles == 2 ? 57344u : 122880u);
+    static constexpr uint32_t kARegion = kABytes;
     static constexpr uint32_t kBBytes = (kWgradCells / 8) * 2u * 128u;
-    static constexpr uint32_t kBRegion = kBBytes + 2048u;
+    static constexpr uint32_t kBRegion = kBBytes;
     static constexpr uint32_t kSmem = kARegion + kBRegion;
     static constexpr uint32_t kTmemCols = kMTiles * 16 <= 32 ? 32u : 64u;
 };
@@ -393,7 +454,8 @@ __global__ void sumsq_kernel(const float* __restrict__ v, uint32_t n, double* __
 }
 
 // X0[q] = (r[q] * s, fluid, 0, ...), s = sqrt(n / ||r||^2) (0 when r = 0); r = r_sel[*parity] when parity is given.
-__global__ void net_input_kernel(VolumeDims d, const float* __restrict__ r0, const float* __restrict__ r1, const int* __restrict__ parity, const double* __restrict__ norm2, const uint8_t* __restrict__ occ, __nv_bfloat16* __restrict__ x0) {
+__global__ void net_input_kernel(VolumeDims d, const float* __restrict__ r0, const float* __restrict__ r1, const int* __restrict__ parity, const double* __restrict__ norm2, const uint8_t* __restrict__ occ, __nv_bfloat16* __restrict__ x0, const uint32_t* __restrict__ skip) {
+    if (skip && *skip) return;
     const float* r = (parity && *parity) ? r1 : r0;
     const double nn = *norm2;
     const float s = nn > 0.0 ? static_cast<float>(sqrt(static_cast<double>(d.n) / nn)) : 0.0f;
@@ -405,7 +467,8 @@ __global__ void net_input_kernel(VolumeDims d, const float* __restrict__ r0, con
 
 // coarse[Q][c] = mean of the existing children fine[q][c]
 template <int C>
-__global__ void pool_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __restrict__ fine, __nv_bfloat16* __restrict__ coarse) {
+__global__ void pool_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __restrict__ fine, __nv_bfloat16* __restrict__ coarse, const uint32_t* __restrict__ skip) {
+    if (skip && *skip) return;
     for (uint32_t Q = blockIdx.x * blockDim.x + threadIdx.x; Q < c.n; Q += gridDim.x * blockDim.x) {
         int X, Y, Z;
         cell_of(c, Q, X, Y, Z);
@@ -439,7 +502,8 @@ __global__ void pool_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __r
 
 // out[q][c] = coarse[parent(q)][c] + skip[q][c]
 template <int C>
-__global__ void up_add_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip, __nv_bfloat16* __restrict__ out) {
+__global__ void up_add_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip, __nv_bfloat16* __restrict__ out, const uint32_t* __restrict__ off) {
+    if (off && *off) return;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < f.n; q += gridDim.x * blockDim.x) {
         int x, y, z;
         cell_of(f, q, x, y, z);
@@ -564,7 +628,7 @@ __global__ void bias16_kernel(const float* __restrict__ bias, int cout, float* _
 
 }  // namespace
 
-cudaError_t launch_conv3(const VolumeDims& d, int cin_store, const __nv_bfloat16* in, const uint8_t* wpack, const float* bias, int relu, const __nv_bfloat16* gate, __nv_bfloat16* out, int cout_store, float* out_f32, unsigned* error, cudaStream_t s) {
+cudaError_t launch_conv3(const VolumeDims& d, int cin_store, const __nv_bfloat16* in, const uint8_t* wpack, const float* bias, int relu, const __nv_bfloat16* gate, __nv_bfloat16* out, int cout_store, float* out_f32, unsigned* error, cudaStream_t s, const uint32_t* skip) {
     if (d.n == 0) return cudaSuccess;
     if ((cin_store != 8 && cin_store != 16) || (cout_store != 8 && cout_store != 16) || error == nullptr) return cudaErrorInvalidValue;
     ConvArgs a{};
@@ -575,6 +639,7 @@ cudaError_t launch_conv3(const VolumeDims& d, int cin_store, const __nv_bfloat16
     a.out = out;
     a.out_f32 = out_f32;
     a.error = error;
+    a.skip = skip;
     a.relu = relu;
     a.cout_store = cout_store;
     a.nx = d.nx;
@@ -601,7 +666,8 @@ cudaError_t wgrad_typed(const VolumeDims& d, const WgradArgs& a, int blocks, cud
     using S = WgradShape<CIN>;
     static bool configured = false;
     if (!configured) {
-        const cudaError_t e = cudaFuncSetAttribute(wgrad_kernel<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::kSmem));
+        cudaError_t e = cudaFuncSetAttribute(wgrad_kernel<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::kSmem));
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(wgrad_kernel<CIN>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess) return e;
         configured = true;
     }
@@ -640,14 +706,14 @@ cudaError_t layer_wgrad(int L, const VolumeDims& d, const __nv_bfloat16* in, con
     return cudaGetLastError();
 }
 
-cudaError_t conv_layer(int L, const VolumeDims& d, const NetImages& I, const __nv_bfloat16* in, __nv_bfloat16* out, float* out_f32, unsigned* error, cudaStream_t s) {
+cudaError_t conv_layer(int L, const VolumeDims& d, const NetImages& I, const __nv_bfloat16* in, __nv_bfloat16* out, float* out_f32, unsigned* error, cudaStream_t s, const uint32_t* skip = nullptr) {
     const int relu = L < kNetLayers - 1;
-    return launch_conv3(d, net_store(kNet[L].cin), in, I.fwd[L], I.bias16[L], relu, nullptr, out, net_store(kNet[L].cout), out_f32, error, s);
+    return launch_conv3(d, net_store(kNet[L].cin), in, I.fwd[L], I.bias16[L], relu, nullptr, out, net_store(kNet[L].cout), out_f32, error, s, skip);
 }
 // Gradient through layer L's convolution: gin = conv^T(g), gated by `gate` (the layer's input activation when it is
 // a ReLU output consumed only by this layer).
 cudaError_t conv_layer_bwd(int L, const VolumeDims& d, const NetImages& I, const __nv_bfloat16* g, const __nv_bfloat16* gate, __nv_bfloat16* gin, unsigned* error, cudaStream_t s) {
-    return launch_conv3(d, net_store(kNet[L].cout), g, I.bwd[L], nullptr, 0, gate, gin, net_store(kNet[L].cin), nullptr, error, s);
+    return launch_conv3(d, net_store(kNet[L].cout), g, I.bwd[L], nullptr, 0, gate, gin, net_store(kNet[L].cin), nullptr, error, s, nullptr);
 }
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
@@ -752,7 +818,7 @@ void net_grads_bind(NetGrads& G, void* base, const VolumeDims& d0) {
     G.sums = reinterpret_cast<double*>(p);
 }
 
-cudaError_t net_forward(const NetImages& I, const NetActs& A, const float* r0, const float* r1, const int* parity, const double* norm2, const uint8_t* occ, cudaStream_t s) {
+cudaError_t net_forward(const NetImages& I, const NetActs& A, const float* r0, const float* r1, const int* parity, const double* norm2, const uint8_t* occ, cudaStream_t s, const uint32_t* skip) {
     const VolumeDims *d = A.d;
     cudaError_t e;
     if (norm2 == nullptr) {
@@ -760,18 +826,18 @@ cudaError_t net_forward(const NetImages& I, const NetActs& A, const float* r0, c
         sumsq_kernel<<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(r0, d[0].n, A.norm2);
         norm2 = A.norm2;
     }
-    net_input_kernel<<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], r0, r1, parity, norm2, occ, A.x0);
+    net_input_kernel<<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], r0, r1, parity, norm2, occ, A.x0, skip);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = conv_layer(0, d[0], I, A.x0, A.e0, nullptr, A.error, s)) != cudaSuccess) return e;
-    pool_kernel<8><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[0], d[1], A.e0, A.p1);
-    if ((e = conv_layer(1, d[1], I, A.p1, A.e1, nullptr, A.error, s)) != cudaSuccess) return e;
-    pool_kernel<16><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[1], d[2], A.e1, A.p2);
-    if ((e = conv_layer(2, d[2], I, A.p2, A.e2, nullptr, A.error, s)) != cudaSuccess) return e;
-    up_add_kernel<16><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[1], d[2], A.e2, A.e1, A.s1);
-    if ((e = conv_layer(3, d[1], I, A.s1, A.d1, nullptr, A.error, s)) != cudaSuccess) return e;
-    up_add_kernel<8><<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], d[1], A.d1, A.e0, A.s0);
-    if ((e = conv_layer(4, d[0], I, A.s0, A.d0, nullptr, A.error, s)) != cudaSuccess) return e;
-    return conv_layer(5, d[0], I, A.d0, nullptr, A.y, A.error, s);
+    if ((e = conv_layer(0, d[0], I, A.x0, A.e0, nullptr, A.error, s, skip)) != cudaSuccess) return e;
+    pool_kernel<8><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[0], d[1], A.e0, A.p1, skip);
+    if ((e = conv_layer(1, d[1], I, A.p1, A.e1, nullptr, A.error, s, skip)) != cudaSuccess) return e;
+    pool_kernel<16><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[1], d[2], A.e1, A.p2, skip);
+    if ((e = conv_layer(2, d[2], I, A.p2, A.e2, nullptr, A.error, s, skip)) != cudaSuccess) return e;
+    up_add_kernel<16><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[1], d[2], A.e2, A.e1, A.s1, skip);
+    if ((e = conv_layer(3, d[1], I, A.s1, A.d1, nullptr, A.error, s, skip)) != cudaSuccess) return e;
+    up_add_kernel<8><<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], d[1], A.d1, A.e0, A.s0, skip);
+    if ((e = conv_layer(4, d[0], I, A.s0, A.d0, nullptr, A.error, s, skip)) != cudaSuccess) return e;
+    return conv_layer(5, d[0], I, A.d0, nullptr, A.y, A.error, s, skip);
 }
 
 cudaError_t net_output(const NetActs& A, const double* norm2, const uint8_t* occ, float* out, cudaStream_t s) {

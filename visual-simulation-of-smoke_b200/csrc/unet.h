@@ -47,8 +47,9 @@ inline VolumeDims coarse_dims(const VolumeDims& d) { return volume_dims((d.nx + 
 // 3x3x3 convolution of `in` ([n][cin_store] BF16) with the packed weights `wpack`: out = act(conv + bias) where act
 // is ReLU when `relu`, then zeroed where `gate` ([n][cout_store] BF16, optional) is not positive. Writes `out`
 // ([n][cout_store] BF16, optional) and/or `out_f32` (channel 0, [n] FP32, optional). bias: 16 floats or null.
-// `error` (device word) gets bit 0 when a tensor-core completion wait ran out.
-cudaError_t launch_conv3(const VolumeDims& d, int cin_store, const __nv_bfloat16* in, const uint8_t* wpack, const float* bias, int relu, const __nv_bfloat16* gate, __nv_bfloat16* out, int cout_store, float* out_f32, unsigned* error, cudaStream_t s);
+// `error` (device word) gets bit 0 when a tensor-core completion wait ran out. With `skip` (device word, optional)
+// nonzero when the kernel starts, it does nothing.
+cudaError_t launch_conv3(const VolumeDims& d, int cin_store, const __nv_bfloat16* in, const uint8_t* wpack, const float* bias, int relu, const __nv_bfloat16* gate, __nv_bfloat16* out, int cout_store, float* out_f32, unsigned* error, cudaStream_t s, const uint32_t* skip = nullptr);
 
 // Packs layer weights W [27][cin][cout] (FP32) into the operand image of the forward convolution (input stored
 // channels net_store(cin)), or with `transpose` of the backward-data convolution (input = the output gradient,
@@ -97,8 +98,9 @@ size_t net_grads_bytes(const VolumeDims& d0);
 void net_grads_bind(NetGrads& G, void* base, const VolumeDims& d0);
 
 // Forward pass on the input r (r1 and *parity pick the buffer on the device when parity is given); norm2 is ||r||^2
-// on the device, or null to compute it into A.norm2. Leaves the network output in A.y.
-cudaError_t net_forward(const NetImages& I, const NetActs& A, const float* r0, const float* r1, const int* parity, const double* norm2, const uint8_t* occ, cudaStream_t s);
+// on the device, or null to compute it into A.norm2. Leaves the network output in A.y. Every kernel of the pass does
+// nothing when `skip` (device word, optional) is nonzero.
+cudaError_t net_forward(const NetImages& I, const NetActs& A, const float* r0, const float* r1, const int* parity, const double* norm2, const uint8_t* occ, cudaStream_t s, const uint32_t* skip = nullptr);
 // out = fluid ? A.y / s : 0 (the preconditioned vector with the input's scale restored).
 cudaError_t net_output(const NetActs& A, const double* norm2, const uint8_t* occ, float* out, cudaStream_t s);
 // Loss of the last forward pass against `target` and the parameter gradient: grad (kNetParams floats) is

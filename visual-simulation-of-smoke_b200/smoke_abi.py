@@ -120,7 +120,7 @@ class SolverDesc(C.Structure):
 
 class SolverStatus(C.Structure):
     _fields_ = [
-        ("iterations", C.c_int32), ("passes", C.c_int32), ("status", C.c_uint32), ("reserved", C.c_uint32), ("rhs_norm", C.c_double),
+        ("iterations", C.c_int32), ("passes", C.c_int32), ("status", C.c_uint32), ("flags", C.c_uint32), ("rhs_norm", C.c_double),
         ("relative_residual", C.c_double), ("true_relative_residual", C.c_double),
     ]
 
