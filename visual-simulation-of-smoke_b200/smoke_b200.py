@@ -80,7 +80,7 @@ class SmokeLibrary:
             fn = getattr(self.lib, name)
             fn.argtypes = args
             fn.restype = C.c_int
-        if extensions:
+        if extensions and hasattr(self.lib, "smoke_b200_net_parameter_count"):
             self.lib.smoke_b200_net_parameter_count.argtypes = []
             self.lib.smoke_b200_net_parameter_count.restype = C.c_uint32
 
