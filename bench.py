@@ -470,7 +470,8 @@ def bench_learned(sim, driver, state, step0, flush, n, args, world, timed_steps=
 def tune_summary(rep):
     """The autotuner's choice in words, with the step times it measured for the default and chosen shapes."""
     c = rep["chosen"]
-    out = {"advect_tile": abi.ADVECT_TILE_NAMES[c["advect_tile"]], "mg_wave": abi.MG_WAVE_NAMES[c["mg_wave"]], "pcg_grid": abi.PCG_GRID_NAMES[c["pcg_grid"]]}
+    out = {"advect_tile": abi.ADVECT_TILE_NAMES[c["advect_tile"]], "mg_wave": abi.MG_WAVE_NAMES[c["mg_wave"]], "pcg_grid": abi.PCG_GRID_NAMES[c["pcg_grid"]],
+           "pcg_regs": abi.PCG_REGS_NAMES[c["pcg_regs"]]}
     if not rep["from_cache"]:
         out.update(default_ms=round(rep["default_ms"], 4), chosen_ms=round(rep["chosen_ms"], 4), candidates=len(rep["records"]))
     return out

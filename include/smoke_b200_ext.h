@@ -131,7 +131,8 @@ typedef struct SmokeB200LaunchTune {
                               resident blocks; 4: one block per 32x4x2 tile */
     uint32_t pcg_grid;     /* persistent CG kernel (FIXED_CG, JACOBI_PCG): 0 all resident blocks (default), 1 half,
                               2 a quarter */
-    uint32_t reserved;     /* 0 */
+    uint32_t pcg_regs;     /* persistent CG kernel: 0 compiled without a register cap (default, 2 blocks per SM),
+                              1 capped at 64 registers (4 blocks per SM, more loads in flight, a few spills) */
 } SmokeB200LaunchTune;
 
 /* One timed candidate of smoke_b200_autotune_cuda. */
@@ -160,7 +161,7 @@ SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_get_launch_tune_cuda(Smoke
 
 /* Autotuner: times the context's own step under candidate launch shapes and keeps the fastest. Coordinate search
  * from the current shapes: every advection shape, then every grid of the selected solver (multigrid depth, or the
- * persistent CG grid), each candidate timed as `steps` (0: 4) graph steps from the same state, best of two
+ * persistent CG grid and register variant), each candidate timed as `steps` (0: 4) graph steps from the same state, best of two
  * repeats, after one untimed step. The context's device state is saved before and restored after (one temporary
  * device allocation of the context's size), so tuning does not advance the simulation. The result is cached per
  * process by device, grid extents, advection mode and solver settings: a later call for a context with the same

@@ -32,7 +32,7 @@ STRUCTS = [
     ("SmokeSimulationView", abi.View, ["layout", "nx", "row_stride_bytes", "slice_stride_bytes", "data0", "data2"]),
     ("SmokeB200SolverDesc", abi.SolverDesc, ["mode", "reduction", "max_iterations", "tolerance", "refinement", "warm_start"]),
     ("SmokeB200SolverStatus", abi.SolverStatus, ["iterations", "status", "rhs_norm", "true_relative_residual"]),
-    ("SmokeB200LaunchTune", abi.LaunchTune, ["advect_tile", "mg_wave", "pcg_grid", "reserved"]),
+    ("SmokeB200LaunchTune", abi.LaunchTune, ["advect_tile", "mg_wave", "pcg_grid", "pcg_regs"]),
     ("SmokeB200TuneRecord", abi.TuneRecord, ["tune", "ms_per_step", "iterations"]),
     ("SmokeB200TuneReport", abi.TuneReport, ["chosen", "default_ms", "chosen_ms", "from_cache", "record_count", "records"]),
 ]

@@ -18,6 +18,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 CU_SOURCES = ["step_kernels.cu", "pcg.cu", "mgsolve.cu", "noalloc.cu", "unet.cu"]
 CPP_SOURCES = ["context.cpp", "learned.cpp"]
+CLI = os.path.join(os.path.dirname(os.path.abspath(__file__)), "smoke_b200_benchmark")
 HEADERS = ["smoke_device.cuh", "launch.h", "grid_sync.cuh", "march.cuh", "unet.h", "tcgen05.cuh"]
 INCLUDES = [os.path.join(ROOT, "include"), CSRC]
 
@@ -63,6 +64,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
             _run(["g++", *CXX_FLAGS, *inc, f"-I{CUDA_HOME}/include", "-c", s, "-o", o])
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest(objects):
         _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB, *objects, "-cudart", "static", "-Xlinker", "--no-undefined"])
+    # the benchmark CLI (loads the library, or any library exporting the ABI, at run time)
+    cli_src = os.path.join(CSRC, "benchmark_cli.cpp")
+    if force or not os.path.exists(CLI) or os.path.getmtime(CLI) < max(dep_time, os.path.getmtime(cli_src)):
+        _run(["g++", "-std=c++23", "-O2", "-Wall", "-Wextra", *inc, f"-I{CUDA_HOME}/include", cli_src, "-o", CLI, f"-L{CUDA_HOME}/lib64", "-lcudart_static", "-ldl", "-lpthread", "-lrt"])
     return LIB
 
 

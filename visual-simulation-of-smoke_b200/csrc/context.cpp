@@ -323,10 +323,11 @@ struct SmokeSimulationContext_t {
         tune = t;
         set_advect_tile(P, static_cast<int>(t.advect_tile));
         pcg_shape.grid = static_cast<int>(t.pcg_grid);
+        pcg_shape.regs = static_cast<int>(t.pcg_regs);
         capture_step_graph();
     }
     static bool valid_tune(const SmokeB200LaunchTune& t) {
-        return t.advect_tile < static_cast<uint32_t>(kAdvectTileCount) && t.mg_wave < static_cast<uint32_t>(kMgWaveCount) && t.pcg_grid < static_cast<uint32_t>(kPcgGridCount) && t.reserved == 0;
+        return t.advect_tile < static_cast<uint32_t>(kAdvectTileCount) && t.mg_wave < static_cast<uint32_t>(kMgWaveCount) && t.pcg_grid < static_cast<uint32_t>(kPcgGridCount) && t.pcg_regs < static_cast<uint32_t>(kPcgRegsCount);
     }
 
     PcgSettings pcg_settings() const {
@@ -929,6 +930,13 @@ SmokeSimulationResult smoke_b200_autotune_cuda(SmokeSimulationContext c, uint32_
                     if (v != base_grid.pcg_grid) {
                         SmokeB200LaunchTune t = best.tune;
                         t.pcg_grid = v;
+                        consider(t);
+                    }
+                const SmokeB200LaunchTune base_regs = best.tune;
+                for (uint32_t v = 0; v < static_cast<uint32_t>(kPcgRegsCount); ++v)
+                    if (v != base_regs.pcg_regs) {
+                        SmokeB200LaunchTune t = best.tune;
+                        t.pcg_regs = v;
                         consider(t);
                     }
             }

@@ -41,8 +41,9 @@ bool set_advect_tile(StepParams& P, int code);
 // one z tile per block.
 constexpr int kMgWaveCount = 5;
 constexpr int kMgWaveDefault = 1;
-// Persistent CG kernel: all resident blocks, half of them, a quarter.
+// Persistent CG kernel: all resident blocks, half of them, a quarter; and its register-capped variant or not.
 constexpr int kPcgGridCount = 3;
+constexpr int kPcgRegsCount = 2;
 
 // Forces: vorticity of the cell-centred velocity (writes the four vorticity buffers).
 cudaError_t launch_vorticity(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* wx, float* wy, float* wz, float* wmag, cudaStream_t s);
@@ -131,6 +132,7 @@ struct PcgLaunchShape {
     int blocks;
     int threads;
     int grid;  // kPcgGridCount code: the persistent grid is the resident blocks divided by 1 << grid
+    int regs;  // 0: kernel compiled without a register cap (2 blocks per SM); 1: capped to 64 (4 blocks per SM)
 };
 
 // ------------------------------------------------------------------------------------------ multigrid hierarchy

@@ -81,8 +81,10 @@ struct X64Data {
 template <typename T>
 __device__ __forceinline__ bool finite_all(T a, T b, T c) { return isfinite(a) && isfinite(b) && isfinite(c); }
 
-template <bool JACOBI, typename T>
-__global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ StepParams P, const PcgSettings S, const Columns C, const uint16_t* __restrict__ codes, const float* __restrict__ b, float* x, PcgWork W, PcgControl* ctl) {
+// MINB: blocks per SM the register allocation must allow (1: unconstrained, about 125 registers and 2 blocks per SM;
+// 4: at most 64 registers, a few spills, twice the loads in flight; the autotuner picks per grid).
+template <bool JACOBI, typename T, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) pcg_kernel(const __grid_constant__ StepParams P, const PcgSettings S, const Columns C, const uint16_t* __restrict__ codes, const float* __restrict__ b, float* x, PcgWork W, PcgControl* ctl) {
     __shared__ __align__(16) double ring_raw[3][kPlane];
     const MarchGeom G = zmarch::geom_of(P.nx, P.ny, P.nz, P.fper);
     float(*ring_f)[kPlane] = reinterpret_cast<float(*)[kPlane]>(ring_raw);
@@ -353,14 +355,14 @@ __global__ void __launch_bounds__(kThreads) pcg_kernel(const __grid_constant__ S
     }
 }
 
-template <bool J, typename T>
+template <bool J, typename T, int MINB>
 cudaError_t launch_one(const StepParams& P, const PcgSettings& S, int grid, const uint16_t* codes, const float* b, float* x, PcgWork work, PcgControl* ctl, cudaStream_t s) {
     static int max_blocks = 0;
     if (max_blocks == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaError_t e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<J, T>, kThreads, 0);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<J, T, MINB>, kThreads, 0);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) return cudaErrorLaunchOutOfResources;
         max_blocks = sms * per_sm;
@@ -388,7 +390,7 @@ cudaError_t launch_one(const StepParams& P, const PcgSettings& S, int grid, cons
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, pcg_kernel<J, T>, P, S, C, codes, b, x, work, ctl);
+    return cudaLaunchKernelEx(&cfg, pcg_kernel<J, T, MINB>, P, S, C, codes, b, x, work, ctl);
 }
 
 }  // namespace
@@ -401,13 +403,18 @@ cudaError_t pcg_launch_shape(PcgLaunchShape* out) {
     out->blocks = sms;
     out->threads = kThreads;
     out->grid = 0;
+    out->regs = 0;
     return cudaSuccess;
 }
 
+template <int MINB>
+cudaError_t launch_variant(const StepParams& P, const PcgSettings& S, int g, const uint16_t* codes, const float* b, float* x, PcgWork work, PcgControl* ctl, cudaStream_t s) {
+    if (S.jacobi) return S.fp64 ? launch_one<true, double, MINB>(P, S, g, codes, b, x, work, ctl, s) : launch_one<true, float, MINB>(P, S, g, codes, b, x, work, ctl, s);
+    return S.fp64 ? launch_one<false, double, MINB>(P, S, g, codes, b, x, work, ctl, s) : launch_one<false, float, MINB>(P, S, g, codes, b, x, work, ctl, s);
+}
+
 cudaError_t launch_pcg(const StepParams& P, const PcgSettings& S, const PcgLaunchShape& shape, const uint16_t* codes, const float* b, float* x, PcgWork work, PcgControl* ctl, cudaStream_t s) {
-    const int g = shape.grid;
-    if (S.jacobi) return S.fp64 ? launch_one<true, double>(P, S, g, codes, b, x, work, ctl, s) : launch_one<true, float>(P, S, g, codes, b, x, work, ctl, s);
-    return S.fp64 ? launch_one<false, double>(P, S, g, codes, b, x, work, ctl, s) : launch_one<false, float>(P, S, g, codes, b, x, work, ctl, s);
+    return shape.regs ? launch_variant<4>(P, S, shape.grid, codes, b, x, work, ctl, s) : launch_variant<1>(P, S, shape.grid, codes, b, x, work, ctl, s);
 }
 
 }  // namespace smoke_b200

@@ -126,7 +126,7 @@ class SolverStatus(C.Structure):
 
 
 class LaunchTune(C.Structure):
-    _fields_ = [("advect_tile", C.c_uint32), ("mg_wave", C.c_uint32), ("pcg_grid", C.c_uint32), ("reserved", C.c_uint32)]
+    _fields_ = [("advect_tile", C.c_uint32), ("mg_wave", C.c_uint32), ("pcg_grid", C.c_uint32), ("pcg_regs", C.c_uint32)]
 
 
 class TuneRecord(C.Structure):
@@ -138,6 +138,7 @@ TUNE_FORCE = 1
 ADVECT_TILE_NAMES = ("flat", "32x8x1", "32x4x2", "16x4x4", "8x8x4")
 MG_WAVE_NAMES = ("0.5 wave", "1 wave", "2 waves", "4 waves", "tile per block")
 PCG_GRID_NAMES = ("all resident", "half", "quarter")
+PCG_REGS_NAMES = ("uncapped", "64 registers")
 
 
 class TuneReport(C.Structure):

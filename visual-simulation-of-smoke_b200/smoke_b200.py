@@ -232,8 +232,8 @@ class Simulation:
     def step_stages(self, last_stage: int):
         _check(self.lib.smoke_b200_step_stages_cuda(self.handle, last_stage), "step_stages")
 
-    def set_launch_tune(self, advect_tile: int = 0, mg_wave: int = 1, pcg_grid: int = 0):
-        t = _tune_struct({"advect_tile": advect_tile, "mg_wave": mg_wave, "pcg_grid": pcg_grid})
+    def set_launch_tune(self, advect_tile: int = 0, mg_wave: int = 1, pcg_grid: int = 0, pcg_regs: int = 0):
+        t = _tune_struct({"advect_tile": advect_tile, "mg_wave": mg_wave, "pcg_grid": pcg_grid, "pcg_regs": pcg_regs})
         _check(self.lib.smoke_b200_set_launch_tune_cuda(self.handle, C.byref(t)), "set_launch_tune")
 
     def launch_tune(self) -> dict:
@@ -341,7 +341,7 @@ class Net:
 
 
 def _tune_dict(t: abi.LaunchTune) -> dict:
-    return {"advect_tile": t.advect_tile, "mg_wave": t.mg_wave, "pcg_grid": t.pcg_grid}
+    return {"advect_tile": t.advect_tile, "mg_wave": t.mg_wave, "pcg_grid": t.pcg_grid, "pcg_regs": t.pcg_regs}
 
 
 def _tune_struct(d: dict) -> abi.LaunchTune:
@@ -349,6 +349,7 @@ def _tune_struct(d: dict) -> abi.LaunchTune:
     t.advect_tile = d.get("advect_tile", 0)
     t.mg_wave = d.get("mg_wave", 1)
     t.pcg_grid = d.get("pcg_grid", 0)
+    t.pcg_regs = d.get("pcg_regs", 0)
     return t
 
 
