@@ -101,15 +101,12 @@ __global__ void __launch_bounds__(kThreads) vorticity_kernel(const __grid_consta
     if (q >= P.n) return;
     int x, y, z;
     cell_xyz(P, q, x, y, z);
-    if (occ[q] != 0) {
-        wx[q] = wy[q] = wz[q] = wm[q] = 0.0f;
-        return;
-    }
-    const float4 o = vorticity_at(u, v, w, x, y, z, P);
-    wx[q] = o.x;
-    wy[q] = o.y;
-    wz[q] = o.z;
-    wm[q] = o.w;
+    const bool solid = occ[q] != 0;
+    const float4 o = vorticity_at(u, v, w, x, y, z, P);  // also for solid cells: no load waits on occupancy
+    wx[q] = solid ? 0.0f : o.x;
+    wy[q] = solid ? 0.0f : o.y;
+    wz[q] = solid ? 0.0f : o.z;
+    wm[q] = solid ? 0.0f : o.w;
 }
 
 // |w| lookup with clamp (or wrap on periodic axes), no occupancy test (load_flow_cell, :202-226).
@@ -162,6 +159,28 @@ __device__ __forceinline__ void face_force_one(const StepParams& P, uint32_t q, 
     int i, j, k;
     face_ijk<A>(P, q, i, j, k);
     const int n = axis_n(P, A);
+    const int s = A == 0 ? i : (A == 1 ? j : k);
+    if (s > 0 && s < n) {
+        // interior face: all loads first, then the rules (same values as the general path below)
+        const uint32_t ri = cidx(P, i, j, k), li = ri - (A == 0 ? 1u : (A == 1 ? static_cast<uint32_t>(P.nx) : static_cast<uint32_t>(P.nx) * P.ny));
+        const uint8_t ol = occ[li], orr = occ[ri];
+        const float base = in[q], fl = f[li], fr = f[ri];
+        if (ol != 0 || orr != 0) {
+            float value = 0.0f, weight = 0.0f;
+            if (ol != 0) {
+                value += solid[li];
+                weight += 1.0f;
+            }
+            if (orr != 0) {
+                value += solid[ri];
+                weight += 1.0f;
+            }
+            out[q] = value / weight;
+        } else {
+            out[q] = base + P.dt * (0.5f * (0.0f + fl + fr));
+        }
+        return;
+    }
     out[q] = settle<A, false>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
         const int s = A == 0 ? a : (A == 1 ? b : c);
         float sum = 0.0f, weight = 0.0f;
@@ -324,6 +343,32 @@ template <int A>
 __device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, const float* __restrict__ in, const float* __restrict__ p, const double* __restrict__ p64, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
     int i, j, k;
     face_ijk<A>(P, q, i, j, k);
+    const int s = A == 0 ? i : (A == 1 ? j : k);
+    if (s > 0 && s < axis_n(P, A)) {
+        // interior face: both cells exist unwrapped, so every load is issued before any rule is decided; the
+        // values are those of the general path below (solid rule, else the gradient step)
+        const uint32_t ri = cidx(P, i, j, k), li = ri - (A == 0 ? 1u : (A == 1 ? static_cast<uint32_t>(P.nx) : static_cast<uint32_t>(P.nx) * P.ny));
+        const uint8_t ol = occ[li], orr = occ[ri];
+        const float base = in[q];
+        float g;
+        if (p64 != nullptr) g = static_cast<float>(P.dt_over_h64 * (p64[ri] - p64[li]));
+        else g = P.dt * (p[ri] - p[li]) / P.h;
+        if (ol != 0 || orr != 0) {
+            float value = 0.0f, weight = 0.0f;
+            if (ol != 0) {
+                value += solid[li];
+                weight += 1.0f;
+            }
+            if (orr != 0) {
+                value += solid[ri];
+                weight += 1.0f;
+            }
+            out[q] = value / weight;
+        } else {
+            out[q] = base - g;
+        }
+        return;
+    }
     out[q] = settle<A, true>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
         int l[3] = {a, b, c};
         int r[3] = {a, b, c};
