@@ -320,14 +320,16 @@ __global__ void __launch_bounds__(256) pad_kernel(const __grid_constant__ StepPa
 __global__ void __launch_bounds__(kThreads) rhs_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const int32_t* __restrict__ anchor, float* __restrict__ rhs) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.n) return;
-    if (static_cast<int32_t>(q) == *anchor || occ[q] != 0) {
-        rhs[q] = 0.0f;
-        return;
-    }
+    // every load is issued before the anchor/solid test (the six faces of a cell always exist)
+    const bool zero = static_cast<int32_t>(q) == __ldg(anchor) || occ[q] != 0;
     int x, y, z;
     cell_xyz(P, q, x, y, z);
     const float h = P.h;
     const float div = (u[fidx<0>(P, x + 1, y, z)] - u[fidx<0>(P, x, y, z)] + v[fidx<1>(P, x, y + 1, z)] - v[fidx<1>(P, x, y, z)] + w[fidx<2>(P, x, y, z + 1)] - w[fidx<2>(P, x, y, z)]) * P.inv_h;
+    if (zero) {
+        rhs[q] = 0.0f;
+        return;
+    }
     float bsum = 0.0f;
     if (x == 0 && P.flow[0].type == kFlowOutflow) bsum += P.flow[0].pressure;
     if (x == P.nx - 1 && P.flow[1].type == kFlowOutflow) bsum += P.flow[1].pressure;
