@@ -2,7 +2,9 @@
 
 Each stage is checked in isolation: the GPU state right before the stage is loaded into the oracle, the oracle
 runs that one stage, and the result must match the GPU's within FP32 rounding. Full steps are then checked end
-to end. Tolerances are normwise: max|gpu - oracle| / max|oracle| per field.
+to end. Tolerances are normwise: max|gpu - oracle| / max|oracle| per field. The two advection stages compare each
+element with the FP32 oracle or, where a back-trace ends within rounding of a domain or solid edge and the two FP32
+executions bisect it apart, with the FP64 oracle; such elements are counted, reported and bounded.
 """
 import json
 import os
@@ -24,6 +26,9 @@ CASES = {
     "plume_cubic_solids": dict(boundary="plume", shape=(16, 12, 8), mode=abi.MONOTONIC_CUBIC, solids=True),
     "mixed_linear_solids": dict(boundary="mixed", shape=(9, 11, 7), mode=abi.LINEAR, solids=True),
     "slip_cubic_solids": dict(boundary="slip", shape=(10, 8, 12), mode=abi.MONOTONIC_CUBIC, solids=True),
+    # low-side outflow faces, a periodic y axis, and a grid only 2 cells thick in z
+    "zout_cubic_solids": dict(boundary="zout", shape=(37, 11, 13), mode=abi.MONOTONIC_CUBIC, solids=True),
+    "thin_linear": dict(boundary="mixed", shape=(9, 10, 2), mode=abi.LINEAR, solids=False),
 }
 
 # FP32 rounding: the GPU contracts a*b+c into FMAs, the oracle does not.
@@ -100,14 +105,20 @@ def test_stage_advect_velocity(smoke_lib, cuda_stream, name, cfl):
     sim = gpu_after(smoke_lib, cuda_stream, cfg, inp, abi.STAGE_ADVECT_VELOCITY)
     cu, cv, cw = faces(sim, 1)
     sim.close()
-    st = oracle_from(cfg, inp)
-    st.set("u", bu)
-    st.set("v", bv)
-    st.set("w", bw)
-    st.step(1, 1)
-    errs = [scenes.rel_err(g, st[k]) for g, k in zip((cu, cv, cw), ("temp_u", "temp_v", "temp_w"))]
-    report(f"advect/{name}/cfl{cfl}", errs)
+    out = {}
+    for bits in (32, 64):  # the FP32 mirror, and the FP64 truth for back-traces that end within rounding of an edge
+        st = O.OracleState(cfg, bits)
+        scenes.load_oracle(st, inp)
+        st.set("u", bu)
+        st.set("v", bv)
+        st.set("w", bw)
+        st.step(1, 1)
+        out[bits] = [st[k] for k in ("temp_u", "temp_v", "temp_w")]
+    res = [scenes.rel_err_either(g, o32, o64, STAGE_TOL) for g, o32, o64 in zip((cu, cv, cw), out[32], out[64])]
+    errs, flips = [e for e, _ in res], [f for _, f in res]
+    report(f"advect/{name}/cfl{cfl}", {"err": errs, "faces_matching_only_fp64": flips})
     assert max(errs) < STAGE_TOL, errs
+    assert sum(flips) <= max(2, (cu.size + cv.size + cw.size) // 1000), flips
 
 
 @pytest.mark.parametrize("mode", [abi.SOLVER_JACOBI_PCG, abi.SOLVER_MG_FCG], ids=["jacobi", "multigrid"])
@@ -170,16 +181,23 @@ def test_stage_scalars(smoke_lib, cuda_stream, name, cfl):
     d = cells(sim, abi.VIEW_DENSITY)
     t = cells(sim, abi.VIEW_TEMPERATURE)
     sim.close()
-    st = oracle_from(cfg, inp)
-    st.set("u", au)
-    st.set("v", av)
-    st.set("w", aw)
+    out = {}
     occ = inp["occupancy"] != 0
-    st.set("temperature", np.where(occ, inp["solid_temperature"], inp["temperature"]))  # step-start solid rule
-    st.step(4, 4)
-    errs = {"density": scenes.rel_err(d, st["density"]), "temperature": scenes.rel_err(t, st["temperature"])}
-    report(f"scalars/{name}/cfl{cfl}", errs)
+    for bits in (32, 64):  # the FP32 mirror, and the FP64 truth for back-traces that end within rounding of an edge
+        st = O.OracleState(cfg, bits)
+        scenes.load_oracle(st, inp)
+        st.set("u", au)
+        st.set("v", av)
+        st.set("w", aw)
+        st.set("temperature", np.where(occ, inp["solid_temperature"], inp["temperature"]))  # step-start solid rule
+        st.step(4, 4)
+        out[bits] = (st["density"], st["temperature"])
+    res = {"density": scenes.rel_err_either(d, out[32][0], out[64][0], STAGE_TOL), "temperature": scenes.rel_err_either(t, out[32][1], out[64][1], STAGE_TOL)}
+    errs = {k: v[0] for k, v in res.items()}
+    flips = {k: v[1] for k, v in res.items()}
+    report(f"scalars/{name}/cfl{cfl}", {"err": errs, "cells_matching_only_fp64": flips})
     assert max(errs.values()) < STAGE_TOL, errs
+    assert sum(flips.values()) <= max(2, 2 * d.size // 1000), flips
 
 
 @pytest.mark.parametrize("name", list(CASES))

@@ -27,6 +27,7 @@ CASES = {
     "plume_cubic_solids": ((24, 20, 16), "plume", abi.MONOTONIC_CUBIC, True),
     "mixed_linear_solids": ((17, 13, 11), "mixed", abi.LINEAR, True),
     "slip_cubic_solids": ((12, 16, 20), "slip", abi.MONOTONIC_CUBIC, True),
+    "zout_cubic_solids": ((37, 11, 13), "zout", abi.MONOTONIC_CUBIC, True),
 }
 STEPS = 4
 # normwise max|b200 - reference| / max|reference| per field

@@ -132,7 +132,7 @@ struct SmokeSimulationContext_t {
     size_t learned_bytes = 0;
     LearnedSolve learned{};
     bool has_net = false;
-    bool views_stale = false;
+    uint32_t views_stale = 0;  // view groups (kViews*) not yet computed for the current state
     bool stepped = false;
 
     ~SmokeSimulationContext_t() { release(); }
@@ -414,10 +414,11 @@ struct SmokeSimulationContext_t {
         check(e, "instantiate solve graph");
     }
 
-    void materialise_views() {
-        if (!views_stale) return;
-        check(launch_views(P, as_const(A), occupancy, cx, cy, cz, vmag, wx, wy, wz, wmag, divergence, stream), "views");
-        views_stale = false;
+    void materialise_views(uint32_t groups = kViewsAll) {
+        const uint32_t todo = views_stale & groups;
+        if (!todo) return;
+        check(launch_views(P, as_const(A), occupancy, cx, cy, cz, vmag, wx, wy, wz, wmag, divergence, todo, stream), "views");
+        views_stale &= ~todo;
     }
 };
 
@@ -663,7 +664,7 @@ SmokeSimulationResult smoke_simulation_step_cuda(SmokeSimulationContext c) {
     nvtx3::scoped_range range("smoke_b200.step");
     if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     if (cudaGraphLaunch(c->exec, c->stream) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-    c->views_stale = true;
+    c->views_stale = kViewsAll;
     c->stepped = true;
     return SMOKE_SIMULATION_RESULT_OK;
 }
@@ -694,13 +695,13 @@ SmokeSimulationResult smoke_simulation_get_view_cuda(SmokeSimulationContext c, c
         case SMOKE_SIMULATION_VIEW_FORCE: three(c->force_x, c->force_y, c->force_z); break;
         case SMOKE_SIMULATION_VIEW_SOLID_VELOCITY: three(c->solid_vx, c->solid_vy, c->solid_vz); break;
         case SMOKE_SIMULATION_VIEW_SOLID_TEMPERATURE: one(c->solid_temperature); break;
-        case SMOKE_SIMULATION_VIEW_FLOW_VELOCITY: c->materialise_views(); three(c->cx, c->cy, c->cz); break;
-        case SMOKE_SIMULATION_VIEW_FLOW_VELOCITY_MAGNITUDE: c->materialise_views(); one(c->vmag); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_VELOCITY: c->materialise_views(kViewsVelocity); three(c->cx, c->cy, c->cz); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_VELOCITY_MAGNITUDE: c->materialise_views(kViewsVelocity); one(c->vmag); break;
         case SMOKE_SIMULATION_VIEW_FLOW_PRESSURE: one(c->pressure); break;
         case SMOKE_SIMULATION_VIEW_FLOW_PRESSURE_RHS: one(c->rhs); break;
-        case SMOKE_SIMULATION_VIEW_FLOW_DIVERGENCE: c->materialise_views(); one(c->divergence); break;
-        case SMOKE_SIMULATION_VIEW_FLOW_VORTICITY: c->materialise_views(); three(c->wx, c->wy, c->wz); break;
-        case SMOKE_SIMULATION_VIEW_FLOW_VORTICITY_MAGNITUDE: c->materialise_views(); one(c->wmag); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_DIVERGENCE: c->materialise_views(kViewsVorticity); one(c->divergence); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_VORTICITY: c->materialise_views(kViewsVorticity); three(c->wx, c->wy, c->wz); break;
+        case SMOKE_SIMULATION_VIEW_FLOW_VORTICITY_MAGNITUDE: c->materialise_views(kViewsVorticity); one(c->wmag); break;
         case SMOKE_SIMULATION_VIEW_OCCUPANCY: one(c->occupancy_float); break;
         default: return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
         }
@@ -771,7 +772,7 @@ SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimulationContext c, uint
     if (c == nullptr || last_stage > SMOKE_B200_STAGE_SCALARS) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return guarded([&] {
         c->enqueue_stages(c->stream, last_stage, false);
-        c->views_stale = true;
+        c->views_stale = kViewsAll;
         c->stepped = true;
         return SMOKE_SIMULATION_RESULT_OK;
     });
@@ -827,7 +828,7 @@ SmokeSimulationResult smoke_b200_batch_step_cuda(SmokeB200Batch batch) {
         check(cudaEventRecord(batch->done, batch->stream), "batch step: done");
         for (SmokeSimulationContext_t* c : batch->contexts) {
             check(cudaStreamWaitEvent(c->stream, batch->done, 0), "batch step: order the context");
-            c->views_stale = true;
+            c->views_stale = kViewsAll;
             c->stepped = true;
         }
         return SMOKE_SIMULATION_RESULT_OK;
@@ -889,7 +890,8 @@ SmokeSimulationResult smoke_b200_autotune_cuda(SmokeSimulationContext c, uint32_
         }
         const cudaStream_t s = c->stream;
         check(cudaStreamSynchronize(s), "tune: idle");
-        const bool views_stale = c->views_stale, stepped = c->stepped;
+        const uint32_t views_stale = c->views_stale;
+        const bool stepped = c->stepped;
         const SmokeB200LaunchTune start = c->tune;
         DeviceBuffer snap;
         check(cudaMalloc(&snap.p, c->arena_bytes), "tune: state copy");

@@ -69,7 +69,9 @@ cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, ConstFace
 // Scalars: solid cells copy their nearest fluid cell's density.
 cudaError_t launch_density_fill(const FillEntry* list, const uint32_t* count, float* density, int max_blocks, cudaStream_t s);
 // Derived views: centred velocity, |u|, vorticity, |w|, divergence of the step's final velocity.
-cudaError_t launch_views(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* cx, float* cy, float* cz, float* vmag, float* wx, float* wy, float* wz, float* wmag, float* div, cudaStream_t s);
+// View groups the views kernel computes: centred velocity and its magnitude; vorticity, its magnitude and divergence.
+constexpr uint32_t kViewsVelocity = 1, kViewsVorticity = 2, kViewsAll = 3;
+cudaError_t launch_views(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* cx, float* cy, float* cz, float* vmag, float* wx, float* wy, float* wz, float* wmag, float* div, uint32_t groups, cudaStream_t s);
 
 // Occupancy-derived data (run when occupancy changes).
 cudaError_t launch_occupancy_float(const StepParams& P, const uint8_t* occ, float* out, cudaStream_t s);

@@ -60,6 +60,7 @@ struct StepParams {
     double dt_over_h64;                          // dt / h in FP64 (gradient of the refined FP64 pressure)
     int tile[3];                                 // advection blocks: log2 extents (x, y, z) of the box of faces or
                                                  // cells one block covers (sum 8); tile[0] < 0: 256 consecutive ones
+    int h_pow2;                                  // h and 1 / h are normal powers of two (see over_h)
 };
 
 #if defined(__CUDACC__)
@@ -164,6 +165,15 @@ __device__ __forceinline__ float wrap_pos(float p, int n, float h) {
     p = fmodf(p, extent);
     if (p < 0.0f) p += extent;
     return p;
+}
+
+// x / h exactly as the IEEE division computes it. For a power-of-two h (P.h_pow2, with 1 / h exact and normal) the
+// product x * (1 / h) rounds the same real number x * 2^-k once, so it is the identical float; __fmul_rn keeps the
+// product out of FMA contraction with a following add, which would skip that rounding.
+template <bool POW2>
+__device__ __forceinline__ float over_h(float x, const StepParams& P) {
+    if constexpr (POW2) return __fmul_rn(x, P.inv_h);
+    else return x / P.h;
 }
 
 // Field kinds: 0,1,2 = MAC face component of that axis; 3 = density; 4 = temperature.
@@ -299,14 +309,14 @@ struct PadField {
     uint32_t px, pxy;  // padded row and slab pitch
 };
 
-template <int KIND, bool CUBIC>
+template <int KIND, bool CUBIC, bool POW2>
 __device__ __forceinline__ float sample_pad(const PadField& F, float x, float y, float z, const StepParams& P) {
     if (periodic_axis<KIND>(P, 0)) x = wrap_pos(x, P.nx, P.h);
     if (periodic_axis<KIND>(P, 1)) y = wrap_pos(y, P.ny, P.h);
     if (periodic_axis<KIND>(P, 2)) z = wrap_pos(z, P.nz, P.h);
-    const float gx = KIND == 0 ? x / P.h : x / P.h - 0.5f;
-    const float gy = KIND == 1 ? y / P.h : y / P.h - 0.5f;
-    const float gz = KIND == 2 ? z / P.h : z / P.h - 0.5f;
+    const float gx = KIND == 0 ? over_h<POW2>(x, P) : over_h<POW2>(x, P) - 0.5f;
+    const float gy = KIND == 1 ? over_h<POW2>(y, P) : over_h<POW2>(y, P) - 0.5f;
+    const float gz = KIND == 2 ? over_h<POW2>(z, P) : over_h<POW2>(z, P) - 0.5f;
     const int x0 = static_cast<int>(floorf(gx));
     const int y0 = static_cast<int>(floorf(gy));
     const int z0 = static_cast<int>(floorf(gz));
@@ -362,14 +372,15 @@ __device__ __forceinline__ float boundary_tap(const float* __restrict__ f, int i
 // ---------------------------------------------------------------------------------------------- trace
 // End-point / probe test of the back-trace (backend-cuda.cu:781-812): outside [0, n*h] on a non-periodic
 // axis, or inside a solid cell.
+template <bool POW2>
 __device__ __forceinline__ bool blocked(float x, float y, float z, const uint8_t* __restrict__ occ, const StepParams& P) {
     if (P.fper[0]) x = wrap_pos(x, P.nx, P.h);
     if (P.fper[1]) y = wrap_pos(y, P.ny, P.h);
     if (P.fper[2]) z = wrap_pos(z, P.nz, P.h);
     if (x < 0.0f || x > static_cast<float>(P.nx) * P.h || y < 0.0f || y > static_cast<float>(P.ny) * P.h || z < 0.0f || z > static_cast<float>(P.nz) * P.h) return true;
-    int cx = static_cast<int>(floorf(x / P.h));
-    int cy = static_cast<int>(floorf(y / P.h));
-    int cz = static_cast<int>(floorf(z / P.h));
+    int cx = static_cast<int>(floorf(over_h<POW2>(x, P)));
+    int cy = static_cast<int>(floorf(over_h<POW2>(y, P)));
+    int cz = static_cast<int>(floorf(over_h<POW2>(z, P)));
     if (cx == P.nx) cx = P.nx - 1;
     if (cy == P.ny) cy = P.ny - 1;
     if (cz == P.nz) cz = P.nz - 1;
@@ -378,11 +389,12 @@ __device__ __forceinline__ bool blocked(float x, float y, float z, const uint8_t
 }
 
 // Bisection of a blocked back-trace end point towards the start, 10 steps (backend-cuda.cu:760-838).
-__device__ __noinline__ inline float3 bisect_blocked(float sx, float sy, float sz, float tx, float ty, float tz, const uint8_t* __restrict__ occ, const StepParams& P) {
+template <bool POW2>
+__device__ __noinline__ float3 bisect_blocked(float sx, float sy, float sz, float tx, float ty, float tz, const uint8_t* __restrict__ occ, const StepParams& P) {
     float lo = 0.0f, hi = 1.0f;
     for (int it = 0; it < 10; ++it) {
         const float mid = 0.5f * (lo + hi);
-        if (blocked(sx + (tx - sx) * mid, sy + (ty - sy) * mid, sz + (tz - sz) * mid, occ, P)) hi = mid;
+        if (blocked<POW2>(sx + (tx - sx) * mid, sy + (ty - sy) * mid, sz + (tz - sz) * mid, occ, P)) hi = mid;
         else lo = mid;
     }
     return make_float3(sx + (tx - sx) * lo, sy + (ty - sy) * lo, sz + (tz - sz) * lo);
@@ -390,18 +402,19 @@ __device__ __noinline__ inline float3 bisect_blocked(float sx, float sy, float s
 
 // Midpoint RK2 back-trace through the face velocities (padded copies of u, v, w), trilinear samples; a blocked end
 // point is pulled back towards the start by bisection (backend-cuda.cu:760-838).
+template <bool POW2>
 __device__ __forceinline__ float3 trace_rk2(float sx, float sy, float sz, const PadField& u, const PadField& v, const PadField& w, const uint8_t* __restrict__ occ, const StepParams& P) {
     const float dt = P.dt;
-    const float a0 = sample_pad<0, false>(u, sx, sy, sz, P);
-    const float b0 = sample_pad<1, false>(v, sx, sy, sz, P);
-    const float c0 = sample_pad<2, false>(w, sx, sy, sz, P);
+    const float a0 = sample_pad<0, false, POW2>(u, sx, sy, sz, P);
+    const float b0 = sample_pad<1, false, POW2>(v, sx, sy, sz, P);
+    const float c0 = sample_pad<2, false, POW2>(w, sx, sy, sz, P);
     const float mx = sx - 0.5f * dt * a0, my = sy - 0.5f * dt * b0, mz = sz - 0.5f * dt * c0;
-    const float a1 = sample_pad<0, false>(u, mx, my, mz, P);
-    const float b1 = sample_pad<1, false>(v, mx, my, mz, P);
-    const float c1 = sample_pad<2, false>(w, mx, my, mz, P);
+    const float a1 = sample_pad<0, false, POW2>(u, mx, my, mz, P);
+    const float b1 = sample_pad<1, false, POW2>(v, mx, my, mz, P);
+    const float c1 = sample_pad<2, false, POW2>(w, mx, my, mz, P);
     const float tx = sx - dt * a1, ty = sy - dt * b1, tz = sz - dt * c1;
-    if (!blocked(tx, ty, tz, occ, P)) return make_float3(tx, ty, tz);
-    return bisect_blocked(sx, sy, sz, tx, ty, tz, occ, P);
+    if (!blocked<POW2>(tx, ty, tz, occ, P)) return make_float3(tx, ty, tz);
+    return bisect_blocked<POW2>(sx, sy, sz, tx, ty, tz, occ, P);
 }
 
 // ---------------------------------------------------------------------------------------------- centred velocity

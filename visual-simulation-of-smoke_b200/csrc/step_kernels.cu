@@ -10,6 +10,8 @@
 //  - temperature and density share one back-trace per cell;
 //  - the density fill of solid cells is a precomputed (cell, nearest fluid cell) list built when occupancy
 //    changes, instead of a per-step Chebyshev-shell search (:1243-1290).
+#include <cmath>
+
 #include "launch.h"
 
 namespace smoke_b200 {
@@ -236,7 +238,7 @@ unsigned advect_blocks(const StepParams& P, int nx, int ny, int nz) {
     return static_cast<unsigned>(((nx + tx - 1) / tx) * ((ny + ty - 1) / ty) * ((nz + tz - 1) / tz));
 }
 
-template <int A, bool CUBIC, bool TILED>
+template <int A, bool CUBIC, bool TILED, bool POW2>
 __device__ __forceinline__ void advect_face_one(const StepParams& P, unsigned blk, const PadField& u, const PadField& v, const PadField& w, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
     int i, j, k;
     uint32_t q;
@@ -254,20 +256,21 @@ __device__ __forceinline__ void advect_face_one(const StepParams& P, unsigned bl
         const float px = A == 0 ? static_cast<float>(a) * h : (static_cast<float>(a) + 0.5f) * h;
         const float py = A == 1 ? static_cast<float>(b) * h : (static_cast<float>(b) + 0.5f) * h;
         const float pz = A == 2 ? static_cast<float>(c) * h : (static_cast<float>(c) + 0.5f) * h;
-        const float3 p = trace_rk2(px, py, pz, u, v, w, occ, P);
-        return sample_pad<A, CUBIC>(src, p.x, p.y, p.z, P);
+        const float3 p = trace_rk2<POW2>(px, py, pz, u, v, w, occ, P);
+        return sample_pad<A, CUBIC, POW2>(src, p.x, p.y, p.z, P);
     });
 }
 
 // Samples and traces read the padded copies of the velocity (ghost cells hold the boundary taps). Blocks
-// [0, bu) advect u faces, [bu, bu + bv) v faces, the rest w faces, each in the shape P.tile selects.
-template <bool CUBIC, bool TILED>
+// [0, bu) advect u faces, [bu, bu + bv) v faces, the rest w faces, each in the shape P.tile selects. POW2: the cell
+// size is a power of two, so grid coordinates are products instead of divisions (over_h, the same floats).
+template <bool CUBIC, bool TILED, bool POW2>
 __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ StepParams P, const PadField u, const PadField v, const PadField w, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou, float* __restrict__ ov,
                                                                     float* __restrict__ ow, unsigned bu, unsigned bv) {
     const unsigned b = blockIdx.x;
-    if (b < bu) advect_face_one<0, CUBIC, TILED>(P, b, u, v, w, occ, su, ou);
-    else if (b < bu + bv) advect_face_one<1, CUBIC, TILED>(P, b - bu, u, v, w, occ, sv, ov);
-    else advect_face_one<2, CUBIC, TILED>(P, b - bu - bv, u, v, w, occ, sw, ow);
+    if (b < bu) advect_face_one<0, CUBIC, TILED, POW2>(P, b, u, v, w, occ, su, ou);
+    else if (b < bu + bv) advect_face_one<1, CUBIC, TILED, POW2>(P, b - bu, u, v, w, occ, sv, ov);
+    else advect_face_one<2, CUBIC, TILED, POW2>(P, b - bu - bv, u, v, w, occ, sw, ow);
 }
 
 // Padded copies (see PadField) of up to 3 fields in one launch: block z-range c * pz_blocks .. for field c; each
@@ -418,7 +421,7 @@ __global__ void __launch_bounds__(kThreads) scalar_prep_kernel(const __grid_cons
 
 // Fluid cells: one back-trace, then both scalars sampled with their own boundary rules (:1221-1233).
 // Solid cells: temperature = solid temperature (:1235-1241), density = 0 until the fill pass.
-template <bool CUBIC, bool TILED>
+template <bool CUBIC, bool TILED, bool POW2>
 __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ StepParams P, const PadField u, const PadField v, const PadField w, const uint8_t* __restrict__ occ, const PadField t_tmp, const PadField d_tmp, const float* __restrict__ solid_t, float* __restrict__ t, float* __restrict__ d) {
     int x, y, z;
     uint32_t q;
@@ -436,9 +439,9 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_c
         return;
     }
     const float h = P.h;
-    const float3 p = trace_rk2((static_cast<float>(x) + 0.5f) * h, (static_cast<float>(y) + 0.5f) * h, (static_cast<float>(z) + 0.5f) * h, u, v, w, occ, P);
-    t[q] = sample_pad<4, CUBIC>(t_tmp, p.x, p.y, p.z, P);
-    d[q] = sample_pad<3, CUBIC>(d_tmp, p.x, p.y, p.z, P);
+    const float3 p = trace_rk2<POW2>((static_cast<float>(x) + 0.5f) * h, (static_cast<float>(y) + 0.5f) * h, (static_cast<float>(z) + 0.5f) * h, u, v, w, occ, P);
+    t[q] = sample_pad<4, CUBIC, POW2>(t_tmp, p.x, p.y, p.z, P);
+    d[q] = sample_pad<3, CUBIC, POW2>(d_tmp, p.x, p.y, p.z, P);
 }
 
 __global__ void density_fill_kernel(const FillEntry* __restrict__ list, const uint32_t* __restrict__ count, float* __restrict__ d) {
@@ -451,18 +454,21 @@ __global__ void density_fill_kernel(const FillEntry* __restrict__ list, const ui
 
 // ------------------------------------------------------------------------------------------ views
 __global__ void __launch_bounds__(kThreads) views_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, float* __restrict__ cx, float* __restrict__ cy, float* __restrict__ cz, float* __restrict__ vm, float* __restrict__ wx, float* __restrict__ wy,
-                                                          float* __restrict__ wz, float* __restrict__ wm, float* __restrict__ div) {
+                                                          float* __restrict__ wz, float* __restrict__ wm, float* __restrict__ div, uint32_t groups) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.n) return;
     int x, y, z;
     cell_xyz(P, q, x, y, z);
-    const float a = centred<0>(u, x, y, z, P);
-    const float b = centred<1>(v, x, y, z, P);
-    const float c = centred<2>(w, x, y, z, P);
-    cx[q] = a;
-    cy[q] = b;
-    cz[q] = c;
-    vm[q] = sqrtf(a * a + b * b + c * c);
+    if (groups & kViewsVelocity) {
+        const float a = centred<0>(u, x, y, z, P);
+        const float b = centred<1>(v, x, y, z, P);
+        const float c = centred<2>(w, x, y, z, P);
+        cx[q] = a;
+        cy[q] = b;
+        cz[q] = c;
+        vm[q] = sqrtf(a * a + b * b + c * c);
+    }
+    if (!(groups & kViewsVorticity)) return;
     if (occ[q] != 0) {
         wx[q] = wy[q] = wz[q] = wm[q] = 0.0f;
         div[q] = 0.0f;
@@ -611,6 +617,10 @@ StepParams make_params(const SmokeSimulationConfig& cfg) {
     P.nv = nx * (ny + 1) * nz;
     P.nw = nx * ny * (nz + 1);
     P.inv_h = 1.0f / cfg.cell_size;
+    {  // a normal power of two with a normal reciprocal: x * inv_h == x / h for every float x
+        int e = 0;
+        P.h_pow2 = std::isnormal(cfg.cell_size) && std::isnormal(P.inv_h) && std::frexp(cfg.cell_size, &e) == 0.5f && P.inv_h * cfg.cell_size == 1.0f;
+    }
     P.dt_over_h64 = static_cast<double>(cfg.dt) / static_cast<double>(cfg.cell_size);
     P.div_nx = FastDiv(nx);
     P.div_ny = FastDiv(ny);
@@ -675,10 +685,18 @@ cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const 
     return cudaGetLastError();
 }
 
+// The advection kernel instance <CUBIC, TILED, POW2> of P, from the 8 given in that binary order.
+template <class K>
+K pick_advect(const StepParams& P, K k000, K k001, K k010, K k011, K k100, K k101, K k110, K k111) {
+    const K all[8] = {k000, k001, k010, k011, k100, k101, k110, k111};
+    return all[(P.cubic ? 4 : 0) + (P.tile[0] >= 0 ? 2 : 0) + (P.h_pow2 ? 1 : 0)];
+}
+
 cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, ConstFaces pad, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
     const unsigned bu = advect_blocks(P, P.nx + 1, P.ny, P.nz), bv = advect_blocks(P, P.nx, P.ny + 1, P.nz), bw = advect_blocks(P, P.nx, P.ny, P.nz + 1);
     const PadField u = pad_field(P, 0, in.u, pad.u), v = pad_field(P, 1, in.v, pad.v), w = pad_field(P, 2, in.w, pad.w);
-    auto kernel = P.tile[0] < 0 ? (P.cubic ? advect_velocity_kernel<true, false> : advect_velocity_kernel<false, false>) : (P.cubic ? advect_velocity_kernel<true, true> : advect_velocity_kernel<false, true>);
+    auto kernel = pick_advect(P, advect_velocity_kernel<false, false, false>, advect_velocity_kernel<false, false, true>, advect_velocity_kernel<false, true, false>, advect_velocity_kernel<false, true, true>, advect_velocity_kernel<true, false, false>,
+                              advect_velocity_kernel<true, false, true>, advect_velocity_kernel<true, true, false>, advect_velocity_kernel<true, true, true>);
     kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, u, v, w, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
     return cudaGetLastError();
 }
@@ -702,7 +720,8 @@ cudaError_t launch_scalar_prep(const StepParams& P, const float* temperature, co
 cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, ConstFaces vel_pad, const uint8_t* occ, const float* t_tmp, const float* t_pad, const float* d_tmp, const float* d_pad, const float* solid_temperature, float* temperature, float* density, cudaStream_t s) {
     const PadField u = pad_field(P, 0, vel.u, vel_pad.u), v = pad_field(P, 1, vel.v, vel_pad.v), w = pad_field(P, 2, vel.w, vel_pad.w);
     const PadField t = pad_field(P, 4, t_tmp, t_pad), d = pad_field(P, 3, d_tmp, d_pad);
-    auto kernel = P.tile[0] < 0 ? (P.cubic ? advect_scalars_kernel<true, false> : advect_scalars_kernel<false, false>) : (P.cubic ? advect_scalars_kernel<true, true> : advect_scalars_kernel<false, true>);
+    auto kernel = pick_advect(P, advect_scalars_kernel<false, false, false>, advect_scalars_kernel<false, false, true>, advect_scalars_kernel<false, true, false>, advect_scalars_kernel<false, true, true>, advect_scalars_kernel<true, false, false>,
+                              advect_scalars_kernel<true, false, true>, advect_scalars_kernel<true, true, false>, advect_scalars_kernel<true, true, true>);
     kernel<<<advect_blocks(P, P.nx, P.ny, P.nz), kThreads, 0, s>>>(P, u, v, w, occ, t, d, solid_temperature, temperature, density);
     return cudaGetLastError();
 }
@@ -712,8 +731,8 @@ cudaError_t launch_density_fill(const FillEntry* list, const uint32_t* count, fl
     return cudaGetLastError();
 }
 
-cudaError_t launch_views(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* cx, float* cy, float* cz, float* vmag, float* wx, float* wy, float* wz, float* wmag, float* div, cudaStream_t s) {
-    views_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, vel.u, vel.v, vel.w, occ, cx, cy, cz, vmag, wx, wy, wz, wmag, div);
+cudaError_t launch_views(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* cx, float* cy, float* cz, float* vmag, float* wx, float* wy, float* wz, float* wmag, float* div, uint32_t groups, cudaStream_t s) {
+    views_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, vel.u, vel.v, vel.w, occ, cx, cy, cz, vmag, wx, wy, wz, wmag, div, groups);
     return cudaGetLastError();
 }
 
