@@ -45,7 +45,7 @@ def mg_grid_levels(n):
     """Levels of the multigrid hierarchy of an n^3 grid and how many run grid-wide (mirrors context.cpp)."""
     dims, (x, y, z) = [], (n, n, n)
     dims.append((x, y, z))
-    while (x > 4 or y > 4 or z > 4) and len(dims) < 12:
+    while (x > 1 or y > 1 or z > 1) and len(dims) < 12:
         x, y, z = (x + 1) // 2, (y + 1) // 2, (z + 1) // 2
         dims.append((x, y, z))
     cells = [a * b * c for a, b, c in dims]

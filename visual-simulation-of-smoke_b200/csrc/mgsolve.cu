@@ -3,7 +3,7 @@
 // No reference counterpart: the reference solves with unpreconditioned CG (backend-cuda.cu:1788-1824), which at
 // 128^3 needs ~900 iterations and stalls near relative residual 2.5e-5 in FP32. Here the preconditioner is one
 // geometric multigrid V(1,1) cycle:
-//  - levels: level l+1 halves every extent of level l (rounding up) down to <= 4 cells per axis; a coarse cell is
+//  - levels: level l+1 halves every extent of level l (rounding up) down to a single cell; a coarse cell is
 //    active (fluid) when any child is; each level's operator is the masked 7-point stencil of its active cells,
 //    built with the fine rules (periodic wrap, OUTFLOW faces on the diagonal) but without the anchor;
 //  - smoothing: damped Jacobi, weight kOmega = 6/7; the pre-smoothing sweep starts from zero;
@@ -12,7 +12,10 @@
 //  - prolongation: cell-centred trilinear (weights 3/4 and 1/4 per axis); a corner outside the domain or on an
 //    inactive coarse cell takes the parent's value (inactive coarse cells carry the bit pattern kTag in t);
 //  - the coarsest levels (at most kMgBlockLevelCells cells, kMgBlockBytes in all) run in one block from shared
-//    memory; every other level pass is one kernel with one thread per cell at full occupancy.
+//    memory, the coarsest one with kCoarsestSweeps Jacobi sweeps in a single warp; every other level pass is one
+//    kernel with one thread per cell at full occupancy. Going down to one cell (instead of stopping at 4^3) brings
+//    the coarse-grid correction of the smoothest modes close to exact: 14 -> 12 iterations at 128^3 and 16 -> 12 at
+//    256^3 on the plume.
 // The outer iteration is flexible CG (Notay 2000: beta_k = -(z_k, q_{k-1}) / (p_{k-1}, q_{k-1})), which stays
 // valid when the preconditioner is not exactly symmetric. Refinement passes accumulate the solution in FP64 and
 // restart from the FP64 residual b - A x64, as in pcg.cu.
@@ -42,10 +45,11 @@ constexpr int kThreads = TX * TY * TZ;
 constexpr int kBlockLevelThreads = 512;
 constexpr float kOmega = 6.0f / 7.0f;  // damped Jacobi weight: the optimal smoothing factor of the 7-point Laplacian in 3D
 constexpr int kCoarsestSweeps = 16;
+constexpr uint32_t kWarpCoarsestCells = 128;  // coarsest levels this small sweep in one warp
 constexpr uint32_t kTag = 0x7fc0feedu;  // t of an inactive coarse cell (a NaN payload arithmetic never produces)
 constexpr int kMaxPasses = 8;           // refinement passes in the graph (refinement is clamped to kMaxPasses - 1)
 // Refined solves: one FP32 pass may reduce ||r|| by at most 1e5 (||r||^2 by 1e10) of its starting residual before
-// the FP64 true residual is recomputed. The multigrid FCG takes ~14 iterations, so its FP32 recurrence residual stays
+// the FP64 true residual is recomputed. The multigrid FCG takes ~12 iterations, so its FP32 recurrence residual stays
 // close to the true one over that range and one pass usually meets 1e-5; a limit of 3.3e3 per pass forced a second
 // pass, with its restart, on every solve at 128^3. The FP64 check still adds passes when needed.
 constexpr double kPassReduction2 = 1e-10;
@@ -639,22 +643,28 @@ __global__ void __launch_bounds__(kBlockLevelThreads) mg_block_kernel(const __gr
     }
     {  // coarsest level: Jacobi sweeps from zero, ping-pong between t and zp, result in t
         const MgLevel L = smem_level<NT>(H, area, lc);
-        for (uint32_t q = t; q < L.n; q += NT) {
-            const uint16_t code = L.code[q];
-            L.t[q] = active(code) ? wdiag(code) * L.r[q] : 0.0f;
-        }
-        for (int sweep = 0; sweep < kCoarsestSweeps; ++sweep) {
-            __syncthreads();
-            float* src = (sweep & 1) ? L.zp : L.t;
-            float* dst = (sweep & 1) ? L.t : L.zp;
-            for (uint32_t q = t; q < L.n; q += NT) {
+        // a coarsest level of at most kWarpCoarsestCells cells sweeps in warp 0 alone, __syncwarp between sweeps
+        const bool by_warp = L.n <= kWarpCoarsestCells;
+        const int lanes = by_warp ? 32 : NT;
+        if (t < lanes) {
+            for (uint32_t q = t; q < L.n; q += lanes) {
                 const uint16_t code = L.code[q];
-                float v = 0.0f;
-                if (active(code)) {
-                    const float s0 = src[q];
-                    v = s0 + wdiag(code) * (L.r[q] - stencil_q<float>(L, q, code, s0, [&](uint32_t nb) { return src[nb]; }));
+                L.t[q] = active(code) ? wdiag(code) * L.r[q] : 0.0f;
+            }
+            for (int sweep = 0; sweep < kCoarsestSweeps; ++sweep) {
+                if (by_warp) __syncwarp();
+                else __syncthreads();
+                float* src = (sweep & 1) ? L.zp : L.t;
+                float* dst = (sweep & 1) ? L.t : L.zp;
+                for (uint32_t q = t; q < L.n; q += lanes) {
+                    const uint16_t code = L.code[q];
+                    float v = 0.0f;
+                    if (active(code)) {
+                        const float s0 = src[q];
+                        v = s0 + wdiag(code) * (L.r[q] - stencil_q<float>(L, q, code, s0, [&](uint32_t nb) { return src[nb]; }));
+                    }
+                    dst[q] = v;
                 }
-                dst[q] = v;
             }
         }
         __syncthreads();
@@ -1024,7 +1034,7 @@ __global__ void mg_code_tail_kernel(uint16_t* code, uint32_t n) {
 
 int mg_level_count(int nx, int ny, int nz) {
     int levels = 1;
-    while ((nx > 4 || ny > 4 || nz > 4) && levels < kMgMaxLevels) {
+    while ((nx > 1 || ny > 1 || nz > 1) && levels < kMgMaxLevels) {  // down to a single cell
         nx = (nx + 1) / 2;
         ny = (ny + 1) / 2;
         nz = (nz + 1) / 2;
