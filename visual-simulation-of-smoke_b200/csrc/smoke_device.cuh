@@ -361,6 +361,41 @@ __device__ __forceinline__ float sample_pad(const PadField& F, float x, float y,
     }
 }
 
+// Trilinear sample of field KIND at the start of a back-trace: the centre of face (i, j, k) of axis START (0-2) or of
+// cell (i, j, k) (START = 3), for a power-of-two cell size. Its grid coordinate is then exact on every axis, with
+// fraction 1/2 where exactly one of "START is this axis" and "KIND is this axis" holds and 0 otherwise, so only the
+// taps of nonzero weight are read (1, 2 or 4 of 8) and every tap lies inside the padded copy. The blends are those of
+// sample_pad; a tap of weight 0 enters there as c + (d - c) * 0, which is c for finite values (a zero may change sign,
+// which the position arithmetic p - dt * v it feeds cannot see), so the sample is sample_pad's.
+template <int KIND, int START>
+__device__ __forceinline__ float start_sample(const PadField& F, int i, int j, int k) {
+    constexpr bool hx = (START == 0) != (KIND == 0), hy = (START == 1) != (KIND == 1), hz = (START == 2) != (KIND == 2);
+    const int x0 = (START == 0 && KIND != 0) ? i - 1 : i;
+    const int y0 = (START == 1 && KIND != 1) ? j - 1 : j;
+    const int z0 = (START == 2 && KIND != 2) ? k - 1 : k;
+    const uint32_t sy = F.px, sz = F.pxy;
+    const float* f = F.p + static_cast<uint32_t>(z0 + kPad) * sz + static_cast<uint32_t>(y0 + kPad) * sy + static_cast<uint32_t>(x0 + kPad);
+    const float c000 = __ldg(f);
+    float c00 = c000, c10 = 0.0f, c01 = 0.0f, c11 = 0.0f;
+    if constexpr (hx) c00 = c000 + (__ldg(f + 1) - c000) * 0.5f;
+    if constexpr (hy) {
+        const float c010 = __ldg(f + sy);
+        c10 = hx ? c010 + (__ldg(f + sy + 1) - c010) * 0.5f : c010;
+    }
+    if constexpr (hz) {
+        const float c001 = __ldg(f + sz);
+        c01 = hx ? c001 + (__ldg(f + sz + 1) - c001) * 0.5f : c001;
+        if constexpr (hy) {
+            const float c011 = __ldg(f + sz + sy);
+            c11 = hx ? c011 + (__ldg(f + sz + sy + 1) - c011) * 0.5f : c011;
+        }
+    }
+    const float c0 = hy ? c00 + (c10 - c00) * 0.5f : c00;
+    if constexpr (!hz) return c0;
+    const float c1 = hy ? c01 + (c11 - c01) * 0.5f : c01;
+    return c0 + (c1 - c0) * 0.5f;
+}
+
 // The boundary tap of field KIND at any integer index (the value a ghost cell of the padded copy holds).
 template <int KIND>
 __device__ __forceinline__ float boundary_tap(const float* __restrict__ f, int i, int j, int k, const StepParams& P) {
@@ -401,13 +436,15 @@ __device__ __noinline__ float3 bisect_blocked(float sx, float sy, float sz, floa
 }
 
 // Midpoint RK2 back-trace through the face velocities (padded copies of u, v, w), trilinear samples; a blocked end
-// point is pulled back towards the start by bisection (backend-cuda.cu:760-838).
-template <bool POW2>
-__device__ __forceinline__ float3 trace_rk2(float sx, float sy, float sz, const PadField& u, const PadField& v, const PadField& w, const uint8_t* __restrict__ occ, const StepParams& P) {
+// point is pulled back towards the start by bisection (backend-cuda.cu:760-838). (sx, sy, sz) is the centre of face
+// (i, j, k) of axis START, or of cell (i, j, k) for START = 3; with a power-of-two cell size the start samples use
+// start_sample.
+template <bool POW2, int START>
+__device__ __forceinline__ float3 trace_rk2(float sx, float sy, float sz, int i, int j, int k, const PadField& u, const PadField& v, const PadField& w, const uint8_t* __restrict__ occ, const StepParams& P) {
     const float dt = P.dt;
-    const float a0 = sample_pad<0, false, POW2>(u, sx, sy, sz, P);
-    const float b0 = sample_pad<1, false, POW2>(v, sx, sy, sz, P);
-    const float c0 = sample_pad<2, false, POW2>(w, sx, sy, sz, P);
+    const float a0 = POW2 ? start_sample<0, START>(u, i, j, k) : sample_pad<0, false, POW2>(u, sx, sy, sz, P);
+    const float b0 = POW2 ? start_sample<1, START>(v, i, j, k) : sample_pad<1, false, POW2>(v, sx, sy, sz, P);
+    const float c0 = POW2 ? start_sample<2, START>(w, i, j, k) : sample_pad<2, false, POW2>(w, sx, sy, sz, P);
     const float mx = sx - 0.5f * dt * a0, my = sy - 0.5f * dt * b0, mz = sz - 0.5f * dt * c0;
     const float a1 = sample_pad<0, false, POW2>(u, mx, my, mz, P);
     const float b1 = sample_pad<1, false, POW2>(v, mx, my, mz, P);

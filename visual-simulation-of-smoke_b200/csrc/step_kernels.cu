@@ -256,7 +256,7 @@ __device__ __forceinline__ void advect_face_one(const StepParams& P, unsigned bl
         const float px = A == 0 ? static_cast<float>(a) * h : (static_cast<float>(a) + 0.5f) * h;
         const float py = A == 1 ? static_cast<float>(b) * h : (static_cast<float>(b) + 0.5f) * h;
         const float pz = A == 2 ? static_cast<float>(c) * h : (static_cast<float>(c) + 0.5f) * h;
-        const float3 p = trace_rk2<POW2>(px, py, pz, u, v, w, occ, P);
+        const float3 p = trace_rk2<POW2, A>(px, py, pz, a, b, c, u, v, w, occ, P);
         return sample_pad<A, CUBIC, POW2>(src, p.x, p.y, p.z, P);
     });
 }
@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_c
         return;
     }
     const float h = P.h;
-    const float3 p = trace_rk2<POW2>((static_cast<float>(x) + 0.5f) * h, (static_cast<float>(y) + 0.5f) * h, (static_cast<float>(z) + 0.5f) * h, u, v, w, occ, P);
+    const float3 p = trace_rk2<POW2, 3>((static_cast<float>(x) + 0.5f) * h, (static_cast<float>(y) + 0.5f) * h, (static_cast<float>(z) + 0.5f) * h, x, y, z, u, v, w, occ, P);
     t[q] = sample_pad<4, CUBIC, POW2>(t_tmp, p.x, p.y, p.z, P);
     d[q] = sample_pad<3, CUBIC, POW2>(d_tmp, p.x, p.y, p.z, P);
 }
