@@ -60,10 +60,11 @@ def mg_grid_levels(n):
 
 def solver_launches(n, iterations, refinement):
     """Kernels the multigrid solve graph launches: set-up and write-back, per refinement pass the first update, the
-    accumulation and the FP64 residual, and per iteration the loop body (restriction, prolongation and smoothing of
-    every grid level below 0, the block-level cycle, level-0 prolongation, smoothing, p/q and update)."""
+    accumulation and the FP64 residual, and per iteration the loop body (restriction and the fused prolongation +
+    smoothing of every grid level below 0, the block-level cycle, level-0 prolongation, smoothing, p/q and update)."""
     _, g = mg_grid_levels(n)
-    per_iteration = 3 * (g - 1) + 5
+    # coarse grid levels of at most 64^3 cells fuse prolongation and smoothing (mg_up_kernel)
+    per_iteration = sum(2 if -(-n // (1 << l)) ** 3 <= 64 ** 3 else 3 for l in range(1, g)) + 5
     return 2 + 3 * (refinement + 1) + per_iteration * iterations
 
 

@@ -56,5 +56,5 @@ def test_solver_launch_count_formula():
 
     assert bench.mg_grid_levels(128) == (8, 4)   # 128 64 32 16 on the grid, 8 4 2 1 in one block
     assert bench.mg_grid_levels(12) == (5, 1)    # 12 on the grid, 6 3 2 1 in one block
-    # per iteration: 3 coarse grid levels x (restrict, prolong, smooth) + block + prolong0 + smooth0 + p/q + update
-    assert bench.solver_launches(128, 15, 3) == 2 + 3 * 4 + 14 * 15
+    # per iteration: 3 coarse grid levels x (restrict, prolong + smooth) + block + prolong0 + smooth0 + p/q + update
+    assert bench.solver_launches(128, 15, 3) == 2 + 3 * 4 + 11 * 15
