@@ -56,6 +56,16 @@ constexpr int kMaxPasses = 8;           // refinement passes in the graph (refin
 // close to the true one over that range and one pass usually meets 1e-5; a limit of 3.3e3 per pass forced a second
 // pass, with its restart, on every solve at 128^3. The FP64 check still adds passes when needed.
 constexpr double kPassReduction2 = 1e-10;
+// An FP32 pass stops when its recurrence residual reaches a fraction of the tolerance, because the recurrence drifts
+// below the true residual as the pass goes on: a pass from ||r0|| = ||b|| (a cold start) ends about 3x below its true
+// residual at 1e-5, so it aims at 0.3 tol (squared: 0.09). A pass that starts within 0.5 ||b|| (a warm start from the
+// previous step's pressure, about 0.37 ||b|| on the 128^3 plume, or a later refinement pass) drifts at most about
+// 1.4x, so 0.7 tol (0.49) still ends below tol: one iteration fewer per warm solve at 128^3. The FP64 check decides
+// either way.
+__device__ __forceinline__ double pass_target2(double tol2, double rtot, double btot) {
+    const double margin2 = rtot <= 0.25 * btot ? 0.49 : 0.09;
+    return fmax(margin2 * tol2, kPassReduction2 * rtot);
+}
 
 __device__ __forceinline__ bool active(uint16_t code) { return (code & kCodeActive) != 0; }
 __device__ __forceinline__ float diagf(uint16_t code) { return static_cast<float>((code >> 8) & 7u); }
@@ -295,7 +305,7 @@ __global__ void __launch_bounds__(kThreads) mg_setup_kernel(const __grid_constan
     st->beta = 0.0f;
     st->status = SMOKE_B200_SOLVE_ITERATION_CAP;
     const double tol2 = static_cast<double>(A.tol) * A.tol * btot;
-    st->target2 = A.ir ? fmax(0.09 * tol2, kPassReduction2 * rtot) : tol2;
+    st->target2 = A.ir ? pass_target2(tol2, rtot, btot) : tol2;
     if (!(btot > 0.0)) {  // b = 0 (solution 0) or not finite
         st->status = isfinite(btot) ? SMOKE_B200_SOLVE_CONVERGED : SMOKE_B200_SOLVE_NOT_FINITE;
         st->halt = 1;
@@ -792,7 +802,7 @@ __global__ void __launch_bounds__(kThreads) mg_residual_kernel(const __grid_cons
         st->rnorm2 = rtot;
         st->pass_rr0 = rtot;
         const double tol2 = static_cast<double>(A.tol) * A.tol * st->bb;
-        st->target2 = fmax(0.09 * tol2, kPassReduction2 * rtot);
+        st->target2 = pass_target2(tol2, rtot, st->bb);
         st->first_iter = 1;
         st->status = SMOKE_B200_SOLVE_ITERATION_CAP;
     }
