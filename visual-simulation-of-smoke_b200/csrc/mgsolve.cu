@@ -284,6 +284,7 @@ __global__ void __launch_bounds__(kThreads) mg_setup_kernel(const __grid_constan
             const uint16_t code = L0.code[c.q];
             double rv = 0.0;
             if (active(code)) rv = static_cast<double>(bv) - stencil_xyz<double>(L0, c.q, c.x, c.y, c.z, code, A.W.x64[c.q], [&](uint32_t nb) { return A.W.x64[nb]; });
+            else A.W.x64[c.q] = 0.0;  // solid or anchor now (occupancy may have changed): its pressure is 0, as from zero
             A.W.r[0][c.q] = static_cast<float>(rv);
             rr += static_cast<T>(rv * rv);
         } else {
