@@ -7,8 +7,8 @@
 //  - the density view is read back for its total and peak (benchmark.cu:204-212);
 //  - the same two output lines (benchmark.cu:214-236); `--json` adds one JSON line with the solver's outcome.
 // Beyond the reference's flags: --library PATH drives any library exporting the ABI (the reference's build too);
-// --solver/--tolerance/--refinement/--max-iters select this library's solvers; --autotune runs its tuner first;
-// --weights loads the learned preconditioner.
+// --solver/--tolerance/--refinement/--max-iters/--warm-start select this library's solvers; --autotune runs its tuner
+// first; --weights loads the learned preconditioner.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 
@@ -36,7 +36,7 @@ struct Options {
     std::string library, solver = "fixed", weights;
     float tolerance = 1e-5f;
     int refinement = 3, max_iters = 500;
-    bool autotune = false, json = false;
+    bool autotune = false, json = false, warm_start = false;
 };
 
 // The ABI entry points, looked up in the library at run time; the extension ones may be missing.
@@ -92,7 +92,7 @@ void usage() {
         "                     [--buoyancy-density A] [--buoyancy-temperature B]\n"
         "                     [--vorticity-confinement E] [--linear-advection]\n"
         "                     [--library PATH] [--solver fixed|jacobi|multigrid|learned] [--tolerance R]\n"
-        "                     [--refinement N] [--max-iters N] [--weights PATH] [--autotune] [--json]\n");
+        "                     [--refinement N] [--max-iters N] [--weights PATH] [--warm-start] [--autotune] [--json]\n");
 }
 
 // Parses argv into `o`; returns -1 to go on, else the exit code.
@@ -146,6 +146,7 @@ int parse(int argc, char** argv, Options& o) {
         if (matched) continue;
         if (a == "--linear-advection") o.cubic = false;
         else if (a == "--autotune") o.autotune = true;
+        else if (a == "--warm-start") o.warm_start = true;
         else if (a == "--json") o.json = true;
         else if (a == "--help") {
             usage();
@@ -264,6 +265,7 @@ int run(const Options& o, Api& api) {
         sd.max_iterations = o.max_iters;
         sd.tolerance = o.tolerance;
         sd.refinement = static_cast<uint32_t>(o.refinement);
+        sd.warm_start = o.warm_start ? 1u : 0u;  // each solve from the previous step's pressure (refinement >= 1)
         if (o.solver == "jacobi") sd.mode = SMOKE_B200_SOLVER_JACOBI_PCG;
         else if (o.solver == "multigrid") sd.mode = SMOKE_B200_SOLVER_MG_FCG;
         else if (o.solver == "learned") {
