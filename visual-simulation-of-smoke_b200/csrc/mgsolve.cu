@@ -1053,8 +1053,8 @@ __global__ void mg_coarsen_kernel(const MgLevel F, const MgLevel C) {
     C.fluid[cq] = any;
 }
 
-// Operator codes of a coarse level: the fine rules (stencil_code_kernel) without the anchor. The two spare
-// entries past the end are zero (inactive).
+// Operator codes of a coarse level: the fine rules (stencil_code_kernel) without the anchor, except on periodic axes
+// of one or two cells (below). The two spare entries past the end are zero (inactive).
 __global__ void mg_code_kernel(const MgLevel L, const __grid_constant__ StepParams P) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= L.n + 2) return;
@@ -1083,9 +1083,12 @@ __global__ void mg_code_kernel(const MgLevel L, const __grid_constant__ StepPara
         }
         const uint32_t nb = lidx(L, d[0], d[1], d[2]);
         if (!L.fluid[nb]) continue;
-        ++diag;
+        // A periodic axis that coarsened to one cell couples a cell to itself (no term: p - 2p + p = 0); one of two
+        // cells couples the pair once (p - p_other). Counting those on the diagonal, as the fine level's rules do,
+        // would add a mass term to the coarse operator and damp its correction of the smoothest modes.
         if (nb == q) continue;
         if ((e & 1) && nn[a] == 2 && P.fper[a]) continue;
+        ++diag;
         mask |= 1u << e;
     }
     if (diag == 0) diag = 1;
