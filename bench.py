@@ -326,10 +326,11 @@ def build_sim(lib, cfg, stream):
 
 # Solver forms measured on the same plume states. The headline ("value") is the first one: multigrid FCG that starts
 # each step's solve from the previous step's FP64 pressure (warm start) and stops on the same test as a cold start,
-# ||b - A x|| <= 1e-5 ||b||; the cold form is measured beside it.
+# ||b - A x|| <= 1e-5 ||b||; the cold form is measured beside it. One FP32 pass reaches 1e-5 on these scenes; a
+# second (refinement = 1) is the margin, and the graph carries no further unrolled passes that would launch as no-ops.
 FORMS = {
-    "multigrid_fp64": dict(mode=abi.SOLVER_MG_FCG, reduction=abi.REDUCTION_FP64, max_iterations=500, tolerance=1e-5, refinement=3, warm_start=True),
-    "multigrid_fp64_cold": dict(mode=abi.SOLVER_MG_FCG, reduction=abi.REDUCTION_FP64, max_iterations=500, tolerance=1e-5, refinement=3),
+    "multigrid_fp64": dict(mode=abi.SOLVER_MG_FCG, reduction=abi.REDUCTION_FP64, max_iterations=500, tolerance=1e-5, refinement=1, warm_start=True),
+    "multigrid_fp64_cold": dict(mode=abi.SOLVER_MG_FCG, reduction=abi.REDUCTION_FP64, max_iterations=500, tolerance=1e-5, refinement=1),
     "jacobi_fp64": dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP64, max_iterations=3000, tolerance=1e-5, refinement=3),
     "plain_fp32": dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP32, max_iterations=1500, tolerance=1e-5, refinement=0),
 }
