@@ -178,28 +178,10 @@ __device__ __forceinline__ float over_h(float x, const StepParams& P) {
 
 // Field kinds: 0,1,2 = MAC face component of that axis; 3 = density; 4 = temperature.
 template <int KIND>
-struct FieldTraits {
-    static constexpr bool kFace = KIND < 3;
-};
-
-template <int KIND>
-__device__ __forceinline__ float tap(const float* __restrict__ f, int i, int j, int k, const StepParams& P) {
-    if constexpr (KIND < 3) return face_tap_slow<KIND>(f, i, j, k, P);
-    else if constexpr (KIND == 3) return scalar_tap_slow(f, i, j, k, P, P.den, P.dper);
-    else return scalar_tap_slow(f, i, j, k, P, P.tem, P.tper);
-}
-
-template <int KIND>
 __device__ __forceinline__ bool periodic_axis(const StepParams& P, int a) {
     if constexpr (KIND < 3) return P.fper[a] != 0;
     else if constexpr (KIND == 3) return P.dper[a] != 0;
     else return P.tper[a] != 0;
-}
-
-template <int KIND>
-__device__ __forceinline__ uint32_t lin(const StepParams& P, int i, int j, int k) {
-    if constexpr (KIND < 3) return fidx<KIND>(P, i, j, k);
-    else return cidx(P, i, j, k);
 }
 
 // Boundary-aware taps and interpolation with a runtime field kind. Only reached when some tap of a sample lies
@@ -243,60 +225,6 @@ __device__ __noinline__ inline float sample_edge(const float* __restrict__ f, in
     return mono_cubic(zs[0], zs[1], zs[2], zs[3], tz);
 }
 
-// Samples field KIND at world position (x,y,z): periodic wrap of the position, conversion to grid coordinates
-// (cell-centred axes offset by -0.5, backend-cuda.cu:413-415, 505-507), then trilinear (8 taps) or tensor
-// monotone cubic (64 taps). When the tap box is inside the array the taps are plain loads (inline); otherwise
-// sample_edge applies the boundary rules.
-template <int KIND, bool CUBIC>
-__device__ __forceinline__ float sample(const float* __restrict__ f, float x, float y, float z, const StepParams& P) {
-    if (periodic_axis<KIND>(P, 0)) x = wrap_pos(x, P.nx, P.h);
-    if (periodic_axis<KIND>(P, 1)) y = wrap_pos(y, P.ny, P.h);
-    if (periodic_axis<KIND>(P, 2)) z = wrap_pos(z, P.nz, P.h);
-    const float gx = KIND == 0 ? x / P.h : x / P.h - 0.5f;
-    const float gy = KIND == 1 ? y / P.h : y / P.h - 0.5f;
-    const float gz = KIND == 2 ? z / P.h : z / P.h - 0.5f;
-    const int x0 = static_cast<int>(floorf(gx));
-    const int y0 = static_cast<int>(floorf(gy));
-    const int z0 = static_cast<int>(floorf(gz));
-    const float tx = gx - static_cast<float>(x0);
-    const float ty = gy - static_cast<float>(y0);
-    const float tz = gz - static_cast<float>(z0);
-    const int ex = P.nx + (KIND == 0) - 1, ey = P.ny + (KIND == 1) - 1, ez = P.nz + (KIND == 2) - 1;
-    const uint32_t sy = static_cast<uint32_t>(ex + 1);
-    const uint32_t sz = sy * static_cast<uint32_t>(ey + 1);
-    if constexpr (!CUBIC) {
-        // written so that saturated conversions (huge or infinite positions) cannot overflow the test
-        if (!(x0 >= 0 && x0 < ex && y0 >= 0 && y0 < ey && z0 >= 0 && z0 < ez)) return sample_edge(f, KIND, 0, x0, y0, z0, tx, ty, tz, P);
-        const uint32_t b = lin<KIND>(P, x0, y0, z0);
-        const float c000 = __ldg(f + b), c100 = __ldg(f + b + 1);
-        const float c010 = __ldg(f + b + sy), c110 = __ldg(f + b + sy + 1);
-        const float c001 = __ldg(f + b + sz), c101 = __ldg(f + b + sz + 1);
-        const float c011 = __ldg(f + b + sz + sy), c111 = __ldg(f + b + sz + sy + 1);
-        const float c00 = c000 + (c100 - c000) * tx;
-        const float c10 = c010 + (c110 - c010) * tx;
-        const float c01 = c001 + (c101 - c001) * tx;
-        const float c11 = c011 + (c111 - c011) * tx;
-        const float c0 = c00 + (c10 - c00) * ty;
-        const float c1 = c01 + (c11 - c01) * ty;
-        return c0 + (c1 - c0) * tz;
-    } else {
-        if (!(x0 >= 1 && x0 <= ex - 2 && y0 >= 1 && y0 <= ey - 2 && z0 >= 1 && z0 <= ez - 2)) return sample_edge(f, KIND, 1, x0, y0, z0, tx, ty, tz, P);
-        const uint32_t base = lin<KIND>(P, x0 - 1, y0 - 1, z0 - 1);
-        float zs[4];
-#pragma unroll
-        for (int dz = 0; dz < 4; ++dz) {
-            float ys[4];
-#pragma unroll
-            for (int dy = 0; dy < 4; ++dy) {
-                const uint32_t b = base + dz * sz + dy * sy;
-                ys[dy] = mono_cubic(__ldg(f + b), __ldg(f + b + 1), __ldg(f + b + 2), __ldg(f + b + 3), tx);
-            }
-            zs[dz] = mono_cubic(ys[0], ys[1], ys[2], ys[3], ty);
-        }
-        return mono_cubic(zs[0], zs[1], zs[2], zs[3], tz);
-    }
-}
-
 // ---------------------------------------------------------------------------------------------- padded fields
 // A sampled field copied with kPad ghost cells on every side, each ghost cell holding exactly the boundary tap of
 // its index (face_tap_slow / scalar_tap_slow), so that a sample whose taps all lie within kPad cells of the array
@@ -309,6 +237,9 @@ struct PadField {
     uint32_t px, pxy;  // padded row and slab pitch
 };
 
+// Samples field KIND at world position (x,y,z): periodic wrap of the position, conversion to grid coordinates
+// (cell-centred axes offset by -0.5, backend-cuda.cu:413-415, 505-507), then trilinear (8 taps) or tensor monotone
+// cubic (64 taps) from the padded copy; a tap box reaching beyond the padding goes through sample_edge.
 template <int KIND, bool CUBIC, bool POW2>
 __device__ __forceinline__ float sample_pad(const PadField& F, float x, float y, float z, const StepParams& P) {
     if (periodic_axis<KIND>(P, 0)) x = wrap_pos(x, P.nx, P.h);
