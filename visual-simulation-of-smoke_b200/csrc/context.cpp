@@ -189,6 +189,7 @@ struct SmokeSimulationContext_t {
         // multigrid levels: level 0 shares the Jacobi solver's vectors; coarser levels get their own arrays
         mg.levels = mg_level_count(P.nx, P.ny, P.nz);
         for (int a = 0; a < 3; ++a) mg.fper[a] = P.fper[a];
+        for (int e = 0; e < 6; ++e) mg.fout[e] = !P.fper[e >> 1] && P.flow[e].type == kFlowOutflow ? 1 : 0;
         int lx = P.nx, ly = P.ny, lz = P.nz;
         for (int l = 0; l < mg.levels; ++l) {
             MgLevel& L = mg.L[l];

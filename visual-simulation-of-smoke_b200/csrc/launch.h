@@ -162,6 +162,7 @@ struct MgHierarchy {
     int levels;       // >= 2
     int grid_levels;  // levels [0, grid_levels) run on the whole grid; coarser ones inside block 0's shared memory
     int fper[3];
+    int fout[6];      // non-periodic OUTFLOW faces (x-, x+, y-, y+, z-, z+): prolongation extrapolates to -parent there
     MgLevel L[kMgMaxLevels];
 };
 // Level-0 vectors of the multigrid FCG solve (the residual and search direction are double-buffered: a pass reads
