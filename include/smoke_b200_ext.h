@@ -232,6 +232,13 @@ SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_eager_cuda(
  * nx*ny*nz floats), on `stream`, with `solver` (NULL = the reference's fixed-count CG; warm_start is ignored).
  * The result equals smoke_b200_solve_pressure_cuda on a context holding the same occupancy and right-hand side.
  *
+ * `config` is checked as smoke_simulation_create_context_cuda checks it (extents, cell size, dt and
+ * pressure_iterations positive; boundary types in range; a periodic face only opposite a periodic face).
+ * `solver` may select SMOKE_B200_SOLVER_FIXED_CG or SMOKE_B200_SOLVER_JACOBI_PCG (the persistent CG kernel), with
+ * FP32 or FP64 reductions and refinement <= 64; the multigrid and learned modes need a context's hierarchy and are
+ * refused. Every refusal returns BACKEND_FAILURE with its reason in smoke_b200_last_error() ("invalid
+ * configuration ...", "invalid solver description ...", "... exceeds the no-allocation limit ...").
+ *
  * Limits and rules:
  *  - at most smoke_b200_noalloc_max_cells() = 64^3 = 262,144 cells; a larger grid returns BACKEND_FAILURE and
  *    smoke_b200_last_error() says why. The scratch array (about 11 MB) is held on every GPU that loads the library
@@ -241,7 +248,9 @@ SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_eager_cuda(
  *  - every call shares the one array: calls that overlap on the GPU (different streams, or several host threads)
  *    race and corrupt each other. Serialise them on one stream. The array keeps the last call's contents; the
  *    call itself clears whatever must start at zero;
- *  - out_status (optional) synchronises `stream` and reports like smoke_b200_get_solver_status_cuda. */
+ *  - out_status (optional) synchronises `stream` and reports like smoke_b200_get_solver_status_cuda. Without it
+ *    the call returns as soon as the work is enqueued; a failure of a CUDA call is also reported with its name and
+ *    CUDA's error text in smoke_b200_last_error(). */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_noalloc_cuda(const SmokeSimulationConfig* config, const uint8_t* occupancy, const float* rhs, float* pressure,
                                                                                  const SmokeB200SolverDesc* solver, void* stream, SmokeB200SolverStatus* out_status);
 

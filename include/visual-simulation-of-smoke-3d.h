@@ -4,7 +4,7 @@
  * Every enum value, struct layout and function signature here is the one the reference library
  * exports, so a program built against the reference header links and runs against this library
  * unchanged (reference: visual-simulation-of-smoke-3d.h:1-162). The layouts are pinned by
- * static_asserts in visual-simulation-of-smoke_b200/csrc/context.cpp and by tests/test_abi_layout.py.
+ * static_asserts in visual-simulation-of-smoke_b200/csrc/context.cpp and by tests/test_abi_host.py.
  *
  * Semantics shared with the reference (backend-cuda.cu:1833-2282):
  *   - every call enqueues work on the context stream and returns without synchronising,

@@ -171,3 +171,55 @@ def test_null_arguments(library):
 def test_noalloc_limit_is_reported(library):
     library.smoke_b200_noalloc_max_cells.restype = C.c_ulonglong
     assert library.smoke_b200_noalloc_max_cells() == 64 ** 3
+
+
+def _bind_noalloc(library):
+    fn = library.smoke_b200_solve_pressure_noalloc_cuda
+    fn.argtypes = [C.POINTER(abi.Config), C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(abi.SolverDesc), C.c_void_p, C.POINTER(abi.SolverStatus)]
+    fn.restype = C.c_int
+    library.smoke_b200_last_error.restype = C.c_char_p
+    return fn
+
+
+@pytest.mark.parametrize("bad", ["periodic_one_side", "dt0", "cell0", "bad_flow_type", "bad_scalar_type"])
+def test_noalloc_refuses_the_configs_context_creation_refuses(library, bad):
+    """The allocation-free solve validates its configuration as context creation does (backend-cuda.cu:1835-1863),
+    before any device work, so these refusals need no GPU. Dummy non-NULL pointers are never dereferenced."""
+    solve = _bind_noalloc(library)
+    cfg = abi.make_config(8, 8, 8)
+    if bad == "periodic_one_side":
+        cfg.flow_boundary.z_plus.type = abi.PERIODIC
+    elif bad == "dt0":
+        cfg.dt = 0.0
+    elif bad == "cell0":
+        cfg.cell_size = -1.0
+    elif bad == "bad_flow_type":
+        cfg.flow_boundary.x_plus.type = 9
+    elif bad == "bad_scalar_type":
+        cfg.density_boundary.y_minus.type = 9
+    assert _create(library, cfg)[0] == abi.RESULT_BACKEND_FAILURE
+    fake = C.c_void_p(0x1000)
+    rc = solve(C.byref(cfg), None, fake, fake, None, None, None)
+    assert rc == abi.RESULT_BACKEND_FAILURE
+    assert library.smoke_b200_last_error().startswith(b"invalid configuration")
+
+
+@pytest.mark.parametrize("mode", ["multigrid", "learned", "refinement", "jacobi_no_tolerance"])
+def test_noalloc_refuses_solver_modes_it_cannot_run(library, mode):
+    """Only the fixed-count CG and Jacobi-PCG run without a context; the multigrid and learned modes are refused
+    with the reason, as is an out-of-range refinement count."""
+    solve = _bind_noalloc(library)
+    cfg = abi.make_config(8, 8, 8)
+    desc = abi.SolverDesc(abi.SOLVER_JACOBI_PCG, abi.REDUCTION_FP64, 100, 1e-5, 1, 0)
+    if mode == "multigrid":
+        desc.mode = abi.SOLVER_MG_FCG
+    elif mode == "learned":
+        desc.mode = abi.SOLVER_LEARNED_FCG
+    elif mode == "refinement":
+        desc.refinement = 65
+    elif mode == "jacobi_no_tolerance":
+        desc.tolerance = 0.0
+    fake = C.c_void_p(0x1000)
+    rc = solve(C.byref(cfg), None, fake, fake, C.byref(desc), None, None)
+    assert rc == abi.RESULT_BACKEND_FAILURE
+    assert library.smoke_b200_last_error().startswith(b"invalid solver description")

@@ -25,6 +25,7 @@
 
 #include <nvtx3/nvtx3.hpp>
 
+#include "config_check.h"
 #include "launch.h"
 #include "smoke_b200_ext.h"
 #include "unet.h"
@@ -55,32 +56,6 @@ struct CudaError : std::runtime_error {
 
 void check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-bool valid_flow_axis(const SmokeSimulationFlowBoundaryFaceDesc& a, const SmokeSimulationFlowBoundaryFaceDesc& b) {
-    auto ok = [](uint32_t t) { return t <= SMOKE_SIMULATION_FLOW_BOUNDARY_PERIODIC; };
-    if (!ok(a.type) || !ok(b.type)) return false;
-    return (a.type == SMOKE_SIMULATION_FLOW_BOUNDARY_PERIODIC) == (b.type == SMOKE_SIMULATION_FLOW_BOUNDARY_PERIODIC);
-}
-bool valid_scalar_axis(const SmokeSimulationScalarBoundaryFaceDesc& a, const SmokeSimulationScalarBoundaryFaceDesc& b) {
-    auto ok = [](uint32_t t) { return t <= SMOKE_SIMULATION_SCALAR_BOUNDARY_PERIODIC; };
-    if (!ok(a.type) || !ok(b.type)) return false;
-    return (a.type == SMOKE_SIMULATION_SCALAR_BOUNDARY_PERIODIC) == (b.type == SMOKE_SIMULATION_SCALAR_BOUNDARY_PERIODIC);
-}
-
-// The reference's create-time validation (backend-cuda.cu:1835-1863), plus the 32-bit index range this
-// library's kernels use.
-bool valid_config(const SmokeSimulationConfig& c) {
-    if (c.nx <= 0 || c.ny <= 0 || c.nz <= 0 || !(c.cell_size > 0.0f) || !(c.dt > 0.0f) || c.pressure_iterations <= 0) return false;
-    const auto& f = c.flow_boundary;
-    const auto& d = c.density_boundary;
-    const auto& t = c.temperature_boundary;
-    if (!valid_flow_axis(f.x_minus, f.x_plus) || !valid_flow_axis(f.y_minus, f.y_plus) || !valid_flow_axis(f.z_minus, f.z_plus)) return false;
-    if (!valid_scalar_axis(d.x_minus, d.x_plus) || !valid_scalar_axis(d.y_minus, d.y_plus) || !valid_scalar_axis(d.z_minus, d.z_plus)) return false;
-    if (!valid_scalar_axis(t.x_minus, t.x_plus) || !valid_scalar_axis(t.y_minus, t.y_plus) || !valid_scalar_axis(t.z_minus, t.z_plus)) return false;
-    const uint64_t nx = c.nx, ny = c.ny, nz = c.nz;
-    const uint64_t biggest = (nx + 1) * (ny + 1) * (nz + 1);
-    return biggest < (1ull << 31);
 }
 
 }  // namespace

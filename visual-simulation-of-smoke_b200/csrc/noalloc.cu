@@ -12,6 +12,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "config_check.h"
 #include "launch.h"
 #include "smoke_b200_ext.h"
 
@@ -19,6 +20,7 @@ namespace smoke_b200 {
 namespace {
 
 constexpr uint64_t kNoAllocMaxCells = 64ull * 64ull * 64ull;
+constexpr uint32_t kNoAllocMaxRefinement = 64;  // refinement passes accepted (each is one FP64 residual restart)
 constexpr uint64_t align256(uint64_t v) { return (v + 255) & ~uint64_t(255); }
 
 // Scratch layout: operator codes, anchor, occupancy (used when the caller passes none), 8 FP32 CG vectors,
@@ -44,16 +46,30 @@ void set_error(const char* msg) {
     std::snprintf(g_last_error, sizeof(g_last_error), "%s", msg);
 }
 
+// Records `step` and the CUDA error text as the reason of this call's failure.
+SmokeSimulationResult cuda_failure(const char* step, cudaError_t e) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s", step, cudaGetErrorString(e));
+    return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+}
+
 // Device address of the scratch array on the current device, looked up once per device.
 unsigned char* scratch_for_current_device() {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    const cudaError_t ed = cudaGetDevice(&dev);
+    if (ed != cudaSuccess) {
+        cuda_failure("cudaGetDevice", ed);
+        return nullptr;
+    }
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("device ordinal beyond the 64 devices the scratch table covers");
+        return nullptr;
+    }
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (g_scratch_ptr[dev] == nullptr) {
         void* ptr = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
         if (e != cudaSuccess || ptr == nullptr) {
-            set_error("cudaGetSymbolAddress of the scratch array failed");
+            cuda_failure("cudaGetSymbolAddress of the scratch array", e);
             return nullptr;
         }
         g_scratch_ptr[dev] = static_cast<unsigned char*>(ptr);
@@ -75,8 +91,8 @@ SmokeSimulationResult smoke_b200_solve_pressure_noalloc_cuda(const SmokeSimulati
         set_error("config, rhs and pressure must not be NULL");
         return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     }
-    if (config->nx <= 0 || config->ny <= 0 || config->nz <= 0 || config->pressure_iterations <= 0) {
-        set_error("grid extents and pressure_iterations must be positive");
+    if (!valid_config(*config)) {  // the same configurations smoke_simulation_create_context_cuda refuses
+        set_error("invalid configuration (extents, cell size, dt and pressure_iterations must be positive; boundary types in range; a periodic face only opposite a periodic face)");
         return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     }
     const uint64_t cells = static_cast<uint64_t>(config->nx) * config->ny * config->nz;
@@ -87,8 +103,9 @@ SmokeSimulationResult smoke_b200_solve_pressure_noalloc_cuda(const SmokeSimulati
     }
     SmokeB200SolverDesc d{SMOKE_B200_SOLVER_FIXED_CG, SMOKE_B200_REDUCTION_FP32, 500, 1.0e-5f, 0, 0};
     if (solver != nullptr) d = *solver;
-    if (d.mode > SMOKE_B200_SOLVER_JACOBI_PCG || d.reduction > SMOKE_B200_REDUCTION_FP64 || (d.mode == SMOKE_B200_SOLVER_JACOBI_PCG && (d.max_iterations <= 0 || !(d.tolerance > 0.0f)))) {
-        set_error("invalid solver description");
+    if (d.mode > SMOKE_B200_SOLVER_JACOBI_PCG || d.reduction > SMOKE_B200_REDUCTION_FP64 || d.refinement > kNoAllocMaxRefinement ||
+        (d.mode == SMOKE_B200_SOLVER_JACOBI_PCG && (d.max_iterations <= 0 || !(d.tolerance > 0.0f)))) {
+        set_error("invalid solver description (mode FIXED_CG or JACOBI_PCG only, reduction FP32 or FP64, refinement <= 64; JACOBI_PCG needs max_iterations > 0 and tolerance > 0)");
         return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     }
     unsigned char* base = scratch_for_current_device();
@@ -100,7 +117,8 @@ SmokeSimulationResult smoke_b200_solve_pressure_noalloc_cuda(const SmokeSimulati
     int32_t* anchor = reinterpret_cast<int32_t*>(base + kOffAnchor);
     const uint8_t* occ = occupancy;
     if (occ == nullptr) {  // no solids: an all-fluid occupancy in scratch
-        if (cudaMemsetAsync(base + kOffOcc, 0, cells, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+        const cudaError_t e = cudaMemsetAsync(base + kOffOcc, 0, cells, s);
+        if (e != cudaSuccess) return cuda_failure("clearing the scratch occupancy", e);
         occ = base + kOffOcc;
     }
     PcgWork work{};
@@ -128,16 +146,14 @@ SmokeSimulationResult smoke_b200_solve_pressure_noalloc_cuda(const SmokeSimulati
     S.warm_start = 0;  // the scratch holds the previous call's solution, which need not belong to this problem
 
     PcgLaunchShape shape{};
-    if (launch_anchor(P, occ, anchor, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-    if (launch_stencil_codes(P, occ, anchor, codes, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-    if (launch_pcg(P, S, shape, codes, rhs, pressure, work, control, s) != cudaSuccess) {
-        set_error("solver launch failed");
-        return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-    }
+    cudaError_t e = launch_anchor(P, occ, anchor, s);
+    if (e != cudaSuccess) return cuda_failure("pressure anchor launch", e);
+    if ((e = launch_stencil_codes(P, occ, anchor, codes, s)) != cudaSuccess) return cuda_failure("operator code launch", e);
+    if ((e = launch_pcg(P, S, shape, codes, rhs, pressure, work, control, s)) != cudaSuccess) return cuda_failure("solver launch", e);
     if (out_status != nullptr) {
         PcgStatusDevice st{};
-        if (cudaMemcpyAsync(&st, &control->status, sizeof(st), cudaMemcpyDeviceToHost, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-        if (cudaStreamSynchronize(s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+        if ((e = cudaMemcpyAsync(&st, &control->status, sizeof(st), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_failure("status read-back", e);
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_failure("stream synchronisation", e);
         std::memcpy(out_status, &st, sizeof(st));
     }
     return SMOKE_SIMULATION_RESULT_OK;

@@ -20,6 +20,9 @@
 //    residual can go below the FP32 floor of the pressure itself;
 //  - every grid barrier waits at most kBarrierTimeoutNs, then raises an abort flag that makes all blocks leave; the
 //    host reads the outcome from the status block.
+#include <map>
+#include <mutex>
+
 #include "grid_sync.cuh"
 #include "march.cuh"
 #include "launch.h"
@@ -357,16 +360,28 @@ __global__ void __launch_bounds__(kThreads, MINB) pcg_kernel(const __grid_consta
 
 template <bool J, typename T, int MINB>
 cudaError_t launch_one(const StepParams& P, const PcgSettings& S, int grid, const uint16_t* codes, const float* b, float* x, PcgWork work, PcgControl* ctl, cudaStream_t s) {
-    static int max_blocks = 0;
+    // co-resident blocks of this kernel instance, per device (devices may differ in SM count)
+    static std::mutex cache_mutex;
+    static std::map<int, int> cache;
+    int dev = 0;
+    cudaError_t ed = cudaGetDevice(&dev);
+    if (ed != cudaSuccess) return ed;
+    int max_blocks = 0;
+    {
+        std::lock_guard<std::mutex> lock(cache_mutex);
+        auto it = cache.find(dev);
+        if (it != cache.end()) max_blocks = it->second;
+    }
     if (max_blocks == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int sms = 0, per_sm = 0;
+        cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<J, T, MINB>, kThreads, 0);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) return cudaErrorLaunchOutOfResources;
         max_blocks = sms * per_sm;
         if (max_blocks > kPcgMaxBlocks) max_blocks = kPcgMaxBlocks;
+        std::lock_guard<std::mutex> lock(cache_mutex);
+        cache[dev] = max_blocks;
     }
     Columns C{};
     C.ncx = (P.nx + CX - 1) / CX;
