@@ -219,6 +219,15 @@ SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_conv3d_cuda(int nx, int ny
  * Results equal smoke_b200_solve_pressure_cuda's up to the summation order of the FP64 dot products. */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_solve_pressure_eager_cuda(SmokeSimulationContext context);
 
+/* Test hook of the solver's bounded waits (no counterpart in the reference, whose waits are library calls that
+ * return error codes, backend-cuda.cu:1611-1614, 2063-2071). Runs the context's persistent CG solve (solver mode
+ * FIXED_CG or JACOBI_PCG; the multigrid modes have no grid barrier and are refused) on its current right-hand side
+ * with block `block` (>= 1) of the cooperative grid leaving before its first grid barrier, and every barrier wait
+ * bounded by `timeout_ms` (1..10000). The other blocks' waits run out, the solve aborts and the status (synchronised,
+ * written to out_status) reads SMOKE_B200_SOLVE_BARRIER_TIMEOUT; the context stays usable. A block index beyond the
+ * grid withholds nothing, and the solve runs normally. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_test_barrier_timeout_cuda(SmokeSimulationContext context, uint32_t block, uint32_t timeout_ms, SmokeB200SolverStatus* out_status);
+
 /* Pressure solve that allocates nothing. No counterpart in the reference (which has no standalone solve and
  * allocates all its buffers with cudaMalloc when a context is created).
  *

@@ -754,6 +754,22 @@ SmokeSimulationResult smoke_b200_step_stages_cuda(SmokeSimulationContext c, uint
     });
 }
 
+SmokeSimulationResult smoke_b200_test_barrier_timeout_cuda(SmokeSimulationContext c, uint32_t block, uint32_t timeout_ms, SmokeB200SolverStatus* out_status) {
+    if (c == nullptr || out_status == nullptr || block == 0 || timeout_ms == 0 || timeout_ms > 10000 || c->uses_mg()) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        PcgSettings S = c->pcg_settings();
+        S.withhold_block = static_cast<int32_t>(block) + 1;
+        S.barrier_timeout_ms = timeout_ms;
+        check(launch_pcg(c->P, S, c->pcg_shape, c->codes, c->rhs, c->pressure, c->pcg, c->control, c->stream), "pressure solve with a withheld block");
+        c->stepped = true;
+        PcgStatusDevice st{};
+        check(cudaMemcpyAsync(&st, &c->control->status, sizeof(st), cudaMemcpyDeviceToHost, c->stream), "status read-back");
+        check(cudaStreamSynchronize(c->stream), "status read-back");
+        std::memcpy(out_status, &st, sizeof(st));
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
 SmokeSimulationResult smoke_b200_solve_pressure_cuda(SmokeSimulationContext c) {
     if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return guarded([&] {

@@ -7,7 +7,7 @@
 namespace smoke_b200 {
 namespace gsync {
 
-constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s: the default bound of a barrier wait
 constexpr unsigned kBarrierMaxSpins = 1u << 26;
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -46,9 +46,10 @@ __device__ void block_sum4(T v[4], T (*scratch)[THREADS / 32]) {
 //  - sums: block b adds its partials (FP64 atomics) into copy b % kPcgSumCopies of ring slot phase % 3; after the
 //    barrier every block adds the copies in copy order. Once past barrier k, block 0 clears slot (k + 2) % 3, which
 //    no block reads again and none writes before barrier k + 2.
-// Every wait is bounded; returns false if the solve was aborted.
+// Every wait is bounded (timeout_ns of globaltimer, or kBarrierMaxSpins polls); returns false if the solve was
+// aborted.
 template <int THREADS, typename T>
-__device__ bool barrier_allreduce(PcgControl* ctl, unsigned& phase, T local[4], T out[4], bool reduce = true) {
+__device__ bool barrier_allreduce(PcgControl* ctl, unsigned& phase, T local[4], T out[4], bool reduce = true, unsigned long long timeout_ns = kBarrierTimeoutNs) {
     __shared__ T scratch[4][THREADS / 32];
     __shared__ int s_ok;
     if (reduce) block_sum4<THREADS>(local, scratch);  // its __syncthreads orders the block's earlier writes
@@ -74,7 +75,7 @@ __device__ bool barrier_allreduce(PcgControl* ctl, unsigned& phase, T local[4], 
                 break;
             }
             ++spins;
-            if (spins >= kBarrierMaxSpins || ((spins & 63u) == 0 && global_ns() - t0 > kBarrierTimeoutNs)) {
+            if (spins >= kBarrierMaxSpins || ((spins & 63u) == 0 && global_ns() - t0 > timeout_ns)) {
                 atomicExch(&ctl->abort, 1);
                 ok = 0;
                 break;

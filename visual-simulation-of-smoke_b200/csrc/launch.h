@@ -92,7 +92,9 @@ struct PcgSettings {
     float tolerance;
     int32_t refinement;      // extra passes on the FP64 true residual
     int32_t warm_start;      // start from x instead of 0
-    int32_t reserved;
+    int32_t withhold_block;  // test only: > 0 makes block withhold_block - 1 leave before its first grid barrier
+    uint32_t barrier_timeout_ms;  // bound of every grid-barrier wait (0: the default, 2000 ms)
+    uint32_t pad;
 };
 
 struct PcgStatusDevice {

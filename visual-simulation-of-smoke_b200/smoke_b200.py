@@ -68,6 +68,7 @@ class SmokeLibrary:
         ("smoke_b200_set_preconditioner_net_cuda", [C.c_void_p, C.c_void_p]),
         ("smoke_b200_apply_operator_cuda", [C.c_void_p, C.c_void_p, C.c_void_p]),
         ("smoke_b200_conv3d_cuda", [C.c_int] * 5 + [C.c_void_p] * 3 + [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+        ("smoke_b200_test_barrier_timeout_cuda", [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(abi.SolverStatus)]),
     ]
 
     def __init__(self, path: str = DEFAULT_LIBRARY, extensions: bool = True):
