@@ -200,18 +200,31 @@ SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_net_train_cuda(SmokeB200Ne
  * (A e, e) of the learned preconditioner. */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_apply_operator_cuda(SmokeSimulationContext context, const float* x, float* out);
 
+/* z = V(r): one V(1,1) cycle of the multigrid preconditioner of SMOKE_B200_SOLVER_MG_FCG on the residual r, over the
+ * context's hierarchy (current occupancy). r and z: nx*ny*nz floats on the device, distinct; z is 0 at solid cells and
+ * the anchor. Enqueued on the context stream; uses the hierarchy's scratch, so it must not overlap a solve of this
+ * context. For building the learned preconditioner's training pairs (what the V-cycle leaves of an error). */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_apply_multigrid_cuda(SmokeSimulationContext context, const float* r, float* z);
+
 /* The context's copy of the network for SMOKE_B200_SOLVER_LEARNED_FCG (the parameters as they are now; later training
  * of `net` does not change the context until this is called again). Allocates the context's evaluation workspace and
  * rebuilds the step graph. */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_set_preconditioner_net_cuda(SmokeSimulationContext context, SmokeB200Net net);
 
 /* 3x3x3 convolution (zero padding) of a channels-last BF16 volume on the tensor cores, the layer of the learned
- * preconditioner's network. `in`: nx*ny*nz cells x S(cin) BF16 values, S(c) = 8 for c <= 8 and 16 for c <= 16
- * (channels past cin must be 0); `weights`: FP32 [27][cin][cout] on the device, tap = (dz+1)*9 + (dy+1)*3 + (dx+1);
- * `bias`: cout FP32 on the device or NULL. out = act(conv + bias), act = ReLU when `relu`: `out` (optional) gets
- * nx*ny*nz x S(cout) BF16 values, `out_f32` (optional) channel 0 as FP32. Allocates a small scratch buffer and
- * synchronises `stream`. 1 <= cin, cout <= 16. */
+ * preconditioner's network. `in`: nx*ny*nz cells x S(cin) BF16 values, S(c) = 8 for c <= 8, else c rounded up to a
+ * multiple of 16 (channels past cin must be 0); `weights`: FP32 [27][cin][cout] on the device, tap = (dz+1)*9 +
+ * (dy+1)*3 + (dx+1); `bias`: cout FP32 on the device or NULL. out = act(conv + bias), act = ReLU when `relu`: `out`
+ * (optional) gets nx*ny*nz x S(cout) BF16 values, `out_f32` (optional) channel 0 as FP32. Allocates a small scratch
+ * buffer and synchronises `stream`. S(cin) in {8, 16, 32, 64, 128} and 1 <= cout <= 128. */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_conv3d_cuda(int nx, int ny, int nz, int cin, int cout, const void* in, const float* weights, const float* bias, int relu, void* out, float* out_f32, void* stream);
+
+/* Test hook of the convolution kernels' bounded waits (no counterpart in the reference, which has no tensor-core
+ * code). Runs the 16-channel convolution over an nx*ny*nz zero volume with every TMA load expected but never
+ * issued, and every wait bounded by `wait_cycles` clock cycles (1..4e9): each block's first wait runs out, the block
+ * frees its tensor memory and leaves, and the error word (bit 0 set) is written to *error_out. Synchronises `stream`;
+ * allocates a scratch buffer. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_test_conv_wait_timeout_cuda(int nx, int ny, int nz, unsigned long long wait_cycles, unsigned* error_out, void* stream);
 
 /* The same solve with every solver kernel launched directly on the context stream, no graph: the multigrid loop is
  * driven from the host, which reads the loop condition after each iteration (one stream synchronisation per

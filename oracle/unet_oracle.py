@@ -6,16 +6,17 @@ network (unet.h, unet.cu) in numpy float64, forward and backward (hand-written, 
 of the tensor-core kernels. With `emulate=True` the values the GPU stores in BF16 (weights, activations, activation
 gradients) are rounded to BF16 at the same points, which leaves only FP32-versus-FP64 summation differences.
 
-Network: level 0 is the volume, level l + 1 halves each extent of level l (rounding up).
-    e0 = relu(conv_a([r s, fluid]))      p1 = pool(e0)     e1 = relu(conv_b(p1))     p2 = pool(e1)
-    e2 = relu(conv_c(p2))                s1 = up(e2) + e1  d1 = relu(conv_d(s1))     s0 = up(d1) + e0
-    d0 = relu(conv_e(s0))                y = conv_f(d0)    N(r) = fluid * y / s,     s = sqrt(n) / ||r||
-Loss of one sample: L = sum_fluid (y - s t)^2 / (s^2 sum_fluid t^2).
+Network: level 0 is the volume, level l + 1 halves each extent of level l (rounding up); channels 16, 32, 64, 128.
+    e0 = relu(conv_a([r s, fluid]))      p1 = pool(e0)      e1 = relu(conv_b(p1))      p2 = pool(e1)
+    e2 = relu(conv_c(p2))                p3 = pool(e2)      e3 = relu(conv_d(p3))      m3 = relu(conv_m(e3))
+    s2 = up(m3) + e2                     u2 = relu(conv_e(s2))                         s1 = up(u2) + e1
+    u1 = relu(conv_f(s1))                s0 = up(u1) + e0   y = conv_g(s0)             N(r) = fluid * y / s,
+with s = sqrt(n) / ||r||. Loss of one sample: L = sum_fluid (y - s t)^2 / (s^2 sum_fluid t^2).
 """
 import numpy as np
 
-# (cin, cout, level) per layer, in execution order
-LAYERS = [(2, 8, 0), (8, 16, 1), (16, 16, 2), (16, 8, 1), (8, 8, 0), (8, 1, 0)]
+# (cin, cout, level) per layer, in execution order: a, b, c, d, m, e, f, g
+LAYERS = [(2, 16, 0), (16, 32, 1), (32, 64, 2), (64, 128, 3), (128, 64, 3), (64, 32, 2), (32, 16, 1), (16, 1, 0)]
 
 
 def param_count():
@@ -142,11 +143,15 @@ def forward(params, r, occ, emulate=False):
     A["e1"] = rnd(relu(conv(A["p1"], *layers[1])))
     A["p2"] = rnd(pool(A["e1"]))
     A["e2"] = rnd(relu(conv(A["p2"], *layers[2])))
-    A["s1"] = rnd(up(A["e2"], A["e1"].shape[:3]) + A["e1"])
-    A["d1"] = rnd(relu(conv(A["s1"], *layers[3])))
-    A["s0"] = rnd(up(A["d1"], A["e0"].shape[:3]) + A["e0"])
-    A["d0"] = rnd(relu(conv(A["s0"], *layers[4])))
-    A["y"] = conv(A["d0"], *layers[5])[..., 0]
+    A["p3"] = rnd(pool(A["e2"]))
+    A["e3"] = rnd(relu(conv(A["p3"], *layers[3])))
+    A["m3"] = rnd(relu(conv(A["e3"], *layers[4])))
+    A["s2"] = rnd(up(A["m3"], A["e2"].shape[:3]) + A["e2"])
+    A["u2"] = rnd(relu(conv(A["s2"], *layers[5])))
+    A["s1"] = rnd(up(A["u2"], A["e1"].shape[:3]) + A["e1"])
+    A["u1"] = rnd(relu(conv(A["s1"], *layers[6])))
+    A["s0"] = rnd(up(A["u1"], A["e0"].shape[:3]) + A["e0"])
+    A["y"] = conv(A["s0"], *layers[7])[..., 0]
     return A
 
 
@@ -165,22 +170,36 @@ def loss_and_gradient(params, r, occ, target, emulate=False):
     e = fluid * (A["y"] - s * t)
     loss = float(np.sum(e * e) / denom)
     gy = rnd(2.0 * e / denom)[..., None]
-    grads = [None] * 6
-    grads[5] = conv_weight(A["d0"], gy)
-    ge = rnd(conv_data(gy, L[5][0]) * (A["d0"] > 0))
-    grads[4] = conv_weight(A["s0"], ge)
-    gs0 = rnd(conv_data(ge, L[4][0]))
-    gd = rnd(up_adjoint(gs0, A["d1"].shape[:3]) * (A["d1"] > 0))
-    grads[3] = conv_weight(A["s1"], gd)
-    gs1 = rnd(conv_data(gd, L[3][0]))
-    gc = rnd(up_adjoint(gs1, A["e2"].shape[:3]) * (A["e2"] > 0))
-    grads[2] = conv_weight(A["p2"], gc)
-    gp2 = rnd(conv_data(gc, L[2][0]))
-    gb = rnd((gs1 + pool_adjoint(gp2, A["e1"].shape[:3])) * (A["e1"] > 0))
-    grads[1] = conv_weight(A["p1"], gb)
-    gp1 = rnd(conv_data(gb, L[1][0]))
-    ga = rnd((gs0 + pool_adjoint(gp1, A["e0"].shape[:3])) * (A["e0"] > 0))
-    grads[0] = conv_weight(A["x0"], ga)
+    grads = [None] * len(LAYERS)
+    # g: y = conv_g(s0), s0 = up(u1) + e0
+    grads[7] = conv_weight(A["s0"], gy)
+    gs0 = rnd(conv_data(gy, L[7][0]))
+    # f: u1 = relu(conv_f(s1)), s1 = up(u2) + e1
+    gu1 = rnd(up_adjoint(gs0, A["u1"].shape[:3]) * (A["u1"] > 0))
+    grads[6] = conv_weight(A["s1"], gu1)
+    gs1 = rnd(conv_data(gu1, L[6][0]))
+    # e: u2 = relu(conv_e(s2)), s2 = up(m3) + e2
+    gu2 = rnd(up_adjoint(gs1, A["u2"].shape[:3]) * (A["u2"] > 0))
+    grads[5] = conv_weight(A["s2"], gu2)
+    gs2 = rnd(conv_data(gu2, L[5][0]))
+    # m: m3 = relu(conv_m(e3)); e3 feeds m only
+    gm3 = rnd(up_adjoint(gs2, A["m3"].shape[:3]) * (A["m3"] > 0))
+    grads[4] = conv_weight(A["e3"], gm3)
+    ge3 = rnd(conv_data(gm3, L[4][0]) * (A["e3"] > 0))
+    # d: e3 = relu(conv_d(p3)), p3 = pool(e2)
+    grads[3] = conv_weight(A["p3"], ge3)
+    gp3 = rnd(conv_data(ge3, L[3][0]))
+    # c: e2 feeds p3 and s2
+    ge2 = rnd((gs2 + pool_adjoint(gp3, A["e2"].shape[:3])) * (A["e2"] > 0))
+    grads[2] = conv_weight(A["p2"], ge2)
+    gp2 = rnd(conv_data(ge2, L[2][0]))
+    # b: e1 feeds p2 and s1
+    ge1 = rnd((gs1 + pool_adjoint(gp2, A["e1"].shape[:3])) * (A["e1"] > 0))
+    grads[1] = conv_weight(A["p1"], ge1)
+    gp1 = rnd(conv_data(ge1, L[1][0]))
+    # a: e0 feeds p1 and s0
+    ge0 = rnd((gs0 + pool_adjoint(gp1, A["e0"].shape[:3])) * (A["e0"] > 0))
+    grads[0] = conv_weight(A["x0"], ge0)
     return loss, pack(grads)
 
 

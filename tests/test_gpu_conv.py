@@ -11,11 +11,13 @@ import smoke_abi as abi
 
 pytestmark = pytest.mark.gpu
 
-LAYERS = [(2, 8), (8, 16), (16, 16), (16, 8), (8, 8), (8, 1)]
+# the network's forward layers (2->16 ... 16->1) and a few other shapes (output channels that need several
+# chunks of 16 or 32, odd channel counts); the backward-data convolutions are covered by the gradient tests
+LAYERS = [(2, 16), (16, 32), (32, 64), (64, 128), (128, 64), (64, 32), (32, 16), (16, 1), (8, 1), (5, 3), (20, 40), (64, 16)]
 
 
 def store(c):
-    return 8 if c <= 8 else 16
+    return 8 if c <= 8 else ((c + 15) // 16) * 16
 
 
 def reference(x, w, b, relu):

@@ -1,6 +1,11 @@
 """The learned preconditioner on the GPU: the tensor-core network against its float64 oracle (forward and gradient,
-with the oracle rounding to BF16 where the GPU stores BF16), training, and the learned FCG solve, which must reach the
-same tolerance and the same answer as the plain solver (the network changes the iteration count, not the answer)."""
+with the oracle rounding to BF16 where the GPU stores BF16), training, and the learned FCG solve (z = V(r) +
+N(r - A V(r)): the network corrects what the multigrid V-cycle leaves), which must reach the same tolerance and the
+same answer as the plain solvers (the network changes the iteration count, not the answer), compared with the same
+FCG without the network (multigrid alone), with Jacobi-preconditioned CG, and with the untrained network."""
+import json
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -13,7 +18,14 @@ import unet_oracle as U
 pytestmark = pytest.mark.gpu
 
 OFFSETS = np.cumsum([0] + [27 * ci * co + co for ci, co, _ in U.LAYERS])
-SHAPE = (32, 48, 32)  # nx, ny, nz of the solve tests
+SHAPE = (48, 64, 48)  # nx, ny, nz of the solve tests
+REPORT = os.environ.get("SMOKE_PARITY_REPORT")
+
+
+def report(name, value):
+    if REPORT:
+        with open(REPORT, "a") as f:
+            f.write(json.dumps({"check": name, "value": value}) + "\n")
 
 
 def sample(shape_zyx, seed):
@@ -66,28 +78,29 @@ def test_parameters_round_trip(smoke_lib):
 
 @pytest.fixture(scope="module")
 def trained(smoke_lib):
-    """A network trained briefly on plume systems and synthetic pairs of the solve tests' grid, and the losses."""
-    data = T.generate(smoke_lib, SHAPE, 6, 4, seed=0, synthetic=12)
+    """A network trained briefly on the V-cycle's leftover errors of plume systems of the solve tests' grid, and
+    the losses."""
+    data = T.generate(smoke_lib, SHAPE, 6, 3, seed=0, synthetic=6)
     n = smoke_b200.Net(smoke_lib, seed=0)
-    losses = T.train(n, data, 1200, 8, 2e-3, seed=0)
+    losses = T.train(n, data, 800, 8, 1e-3, seed=0)
     yield n, losses
     n.close()
 
 
 def test_training_reduces_the_loss(trained):
     _, losses = trained
-    assert np.mean(losses[-50:]) < 0.5 * np.mean(losses[:5])
+    assert np.mean(losses[-50:]) < 0.7 * np.mean(losses[:5])
 
 
 def held_out_system(lib):
-    cfg, occ, boxes = T.scene(SHAPE, 999)
+    cfg, occ, boxes, strength = T.scene(SHAPE, 999)
     s = torch.cuda.Stream()
     sim = smoke_b200.Simulation(lib, cfg, s)
     with torch.cuda.stream(s):
         o = torch.from_numpy(occ).cuda()
         sim.update_occupancy(o)
-    sim.set_solver(**T.DATA_SOLVER)
-    drv = __import__("plume_scene").SceneDriver(sim, boxes, seed=5)
+    sim.set_solver(**T.STEP_SOLVER)
+    drv = __import__("plume_scene").SceneDriver(sim, boxes, seed=5, strength=strength)
     for k in range(12):
         drv.apply(k)
         sim.step()
@@ -103,32 +116,40 @@ def solve(sim, form, net=None):
     return st, sim.snapshot([abi.VIEW_FLOW_PRESSURE])["pressure"]
 
 
-LEARNED = dict(mode=abi.SOLVER_LEARNED_FCG, reduction=abi.REDUCTION_FP64, max_iterations=3000, tolerance=1e-5, refinement=3)
+LEARNED = dict(mode=abi.SOLVER_LEARNED_FCG, reduction=abi.REDUCTION_FP64, max_iterations=300, tolerance=1e-5, refinement=3)
+MULTIGRID = dict(LEARNED, mode=abi.SOLVER_MG_FCG)
 JACOBI = dict(mode=abi.SOLVER_JACOBI_PCG, reduction=abi.REDUCTION_FP64, max_iterations=4000, tolerance=1e-5, refinement=3)
 
 
 def test_learned_solve_same_answer_and_gain(smoke_lib, trained):
-    """Ablation: the same learned FCG with the untrained network needs clearly more iterations than with the
-    trained one (both reach the tolerance, the untrained one usually by falling back to the plain preconditioner);
-    the converged answer is the Jacobi-PCG answer within the tolerance's reach."""
+    """The trained learned FCG against the same FCG without the network (multigrid alone), Jacobi-PCG and the
+    untrained network: all reach the tolerance with the same answer (within its reach); the trained network needs no
+    more iterations than the multigrid alone, nor than with the untrained network, and an order of magnitude fewer
+    than Jacobi-PCG."""
     net, _ = trained
     sim, keep = held_out_system(smoke_lib)
     st_j, p_j = solve(sim, JACOBI)
-    assert st_j.status == abi.SOLVE_CONVERGED
+    st_m, p_m = solve(sim, MULTIGRID)
     st_t, p_t = solve(sim, LEARNED, net)
-    assert st_t.status == abi.SOLVE_CONVERGED and st_t.true_relative_residual <= 1e-5
-    assert np.abs(p_t - p_j).max() <= 5e-3 * np.abs(p_j).max()
     with smoke_b200.Net(smoke_lib, seed=0) as untrained:
-        st_u, _ = solve(sim, LEARNED, untrained)
-    assert st_u.status != abi.SOLVE_CONVERGED or st_t.iterations < 0.85 * st_u.iterations
+        st_u, p_u = solve(sim, LEARNED, untrained)
     # the network's estimate as the initial guess as well
     st_w, p_w = solve(sim, dict(LEARNED, warm_start=2), net)
-    assert st_w.status == abi.SOLVE_CONVERGED and np.abs(p_w - p_j).max() <= 5e-3 * np.abs(p_j).max()
     sim.close()
+    report("learned/held_out", {"jacobi": st_j.iterations, "multigrid": st_m.iterations, "learned_trained": st_t.iterations, "learned_untrained": st_u.iterations,
+                                "learned_trained_net_warm_start": st_w.iterations, "dropped_trained": int(st_t.flags & 1), "dropped_untrained": int(st_u.flags & 1)})
+    scale = np.abs(p_j).max()
+    for st, p in ((st_j, p_j), (st_m, p_m), (st_t, p_t), (st_u, p_u), (st_w, p_w)):
+        assert st.status == abi.SOLVE_CONVERGED and st.true_relative_residual <= 1e-5
+        assert np.abs(p - p_j).max() <= 5e-3 * scale
+    assert not (st_t.flags & 1)  # the trained network was kept
+    assert st_t.iterations <= st_m.iterations
+    assert st_t.iterations <= st_u.iterations or (st_u.flags & 1)
+    assert st_t.iterations < 0.1 * st_j.iterations
 
 
 def test_learned_mode_needs_a_network(smoke_lib):
-    cfg, occ, boxes = T.scene((16, 16, 16), 3)
+    cfg, occ, boxes, _ = T.scene((16, 16, 16), 3)
     sim = smoke_b200.Simulation(smoke_lib, cfg, torch.cuda.Stream())
     with pytest.raises(smoke_b200.SmokeError):
         sim.set_solver(**LEARNED)
@@ -149,13 +170,43 @@ def test_operator_apply_matches_solution(smoke_lib):
     sim.close()
 
 
-def test_stalled_network_falls_back_to_the_plain_preconditioner(smoke_lib):
-    """A network of huge random weights is a useless preconditioner: the solve detects the stall, drops it (flags
-    bit 0) and still reaches the tolerance with the Jacobi preconditioner."""
+def test_multigrid_apply_is_the_solvers_preconditioner(smoke_lib):
+    """The standalone V-cycle (smoke_b200_apply_multigrid_cuda, the trainer's) is the solve's preconditioner: flexible
+    CG iterations with it, run in torch around the library's operator and V-cycle, reach the same relative residual
+    in the same number of iterations as the library's multigrid FCG (up to one)."""
+    sim, keep = held_out_system(smoke_lib)
+    st_m, _ = solve(sim, dict(MULTIGRID, refinement=0, tolerance=1e-5))
+    with torch.cuda.stream(sim.stream):
+        b = sim.view(abi.VIEW_FLOW_PRESSURE_RHS).clone()
+        r = b.clone()
+        p_prev = q_prev = None
+        its = 0
+        bb = float(torch.sum(b.double() ** 2))
+        while float(torch.sum(r.double() ** 2)) > 1e-10 * bb and its < 60:
+            z = sim.apply_multigrid(r)
+            if p_prev is None:
+                p = z
+            else:
+                beta = -float(torch.sum(z.double() * q_prev.double())) / float(torch.sum(p_prev.double() * q_prev.double()))
+                p = z + beta * p_prev
+            q = sim.apply_operator(p)
+            alpha = float(torch.sum(p.double() * r.double())) / float(torch.sum(p.double() * q.double()))
+            r = r - alpha * q
+            p_prev, q_prev = p, q
+            its += 1
+    sim.stream.synchronize()
+    sim.close()
+    assert st_m.status == abi.SOLVE_CONVERGED
+    assert abs(its - st_m.iterations) <= 1, (its, st_m.iterations)
+
+
+def test_stalled_network_falls_back_to_the_multigrid_preconditioner(smoke_lib):
+    """A network of huge random weights is a useless correction: the solve detects the stall, drops it (flags
+    bit 0) and still reaches the tolerance with the V-cycle alone."""
     sim, keep = held_out_system(smoke_lib)
     with smoke_b200.Net(smoke_lib, seed=0) as bad:
         bad.set_parameters(U.initial_like(7, scale=30.0))
-        st, p = solve(sim, dict(LEARNED, max_iterations=6000), bad)
+        st, p = solve(sim, dict(LEARNED, max_iterations=600), bad)
     st_j, p_j = solve(sim, JACOBI)
     assert st.status == abi.SOLVE_CONVERGED and (st.flags & 1)
     assert np.abs(p - p_j).max() <= 5e-3 * np.abs(p_j).max()

@@ -15,7 +15,7 @@ def sample(shape, seed):
 
 
 def test_parameter_count_matches_library():
-    assert U.param_count() == 16257
+    assert U.param_count() == 582257
 
 
 @pytest.mark.parametrize("shape", [(5, 4, 3), (4, 6, 7)])
@@ -26,7 +26,7 @@ def test_backward_matches_finite_differences(shape):
     rng = np.random.default_rng(5)
     offsets = np.cumsum([0] + [27 * ci * co + co for ci, co, _ in U.LAYERS])
     picks = []
-    for L in range(6):  # weights and the bias of every layer
+    for L in range(len(U.LAYERS)):  # weights and the bias of every layer
         picks += list(rng.integers(offsets[L], offsets[L + 1] - U.LAYERS[L][1], 4)) + [offsets[L + 1] - 1]
     h = 1e-6
     for i in picks:
@@ -63,5 +63,5 @@ def test_network_is_positively_homogeneous():
     p = U.initial_like(4)
     a = U.apply(p, r, occ)
     b = U.apply(p, 3.5 * r, occ)
-    assert np.allclose(b, 3.5 * a, rtol=1e-5, atol=1e-9 * np.abs(a).max())  # the input scale s is FP32, as on the GPU
+    assert np.allclose(b, 3.5 * a, rtol=1e-5, atol=1e-6 * np.abs(a).max())  # the input scale s is FP32, as on the GPU
     assert not np.any(a[occ != 0])

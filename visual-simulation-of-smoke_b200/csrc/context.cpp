@@ -839,6 +839,11 @@ SmokeSimulationResult smoke_b200_apply_operator_cuda(SmokeSimulationContext c, c
     return ok_or_fail(launch_mg_apply(c->mg, x, out, c->stream));
 }
 
+SmokeSimulationResult smoke_b200_apply_multigrid_cuda(SmokeSimulationContext c, const float* r, float* z) {
+    if (c == nullptr || r == nullptr || z == nullptr || r == z) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return ok_or_fail(launch_mg_vcycle(c->mg, static_cast<int>(c->tune.mg_wave), r, z, c->stream));
+}
+
 SmokeSimulationResult smoke_b200_set_preconditioner_net_cuda(SmokeSimulationContext c, SmokeB200Net net) {
     if (c == nullptr || net == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return guarded([&] {

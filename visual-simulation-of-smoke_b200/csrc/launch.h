@@ -178,22 +178,25 @@ struct MgWork {
 };
 // Device-side scalars of one multigrid solve (reset at the start of every solve).
 constexpr int kMgSlots = 32;  // addresses each FP64 dot-product accumulator is spread over
-enum MgAccumulator { kAccBB = 0, kAccRR, kAccZR, kAccZQ, kAccPQ, kAccPR, kAccCount };
+enum MgAccumulator { kAccBB = 0, kAccRR, kAccZR, kAccZQ, kAccPQ, kAccPR, kAccNet, kAccCount };
 struct MgState {
     double acc[kAccCount][kMgSlots];
     double bb, rnorm2, pq_prev, target2, pass_rr0, true_rel;
+    double net_rr;         // learned solve: ||r - A z_V||^2, the squared norm of the network's input
     float alpha, beta;     // step sizes, computed by the last block of the kernel that completes their sums
-    unsigned int done[5];  // last-block election counters
+    unsigned int done[6];  // last-block election counters
     int parity, first_iter, it, passes;
     uint32_t status, fail, halt, zero_solution;
     uint32_t loop;         // the loop condition the last update set (read by the host in eager mode)
-    uint32_t fallback;     // learned solve: 1 once the network is dropped for the plain (Jacobi) preconditioner
+    uint32_t fallback;     // learned solve: 1 once the network is dropped (the V-cycle alone preconditions)
     int stall_it;          // learned solve: iteration of the last stagnation checkpoint
     double stall_ref;      // learned solve: ||r||^2 at that checkpoint
 };
-// Learned solve: the network is dropped for the plain preconditioner when ||r|| shrank less than 1.2x over this many
-// iterations (stagnation).
-constexpr int kLearnedStallWindow = 100;
+// Learned solve: the network is dropped, leaving the V-cycle alone, when ||r|| shrank less than 10x
+// (||r||^2 less than kLearnedStallReduction2) over kLearnedStallWindow iterations; the V-cycle alone gains about
+// 3x per iteration.
+constexpr int kLearnedStallWindow = 6;
+constexpr double kLearnedStallReduction2 = 1e-2;
 struct MgSolveArgs {
     MgHierarchy H;
     MgWork W;
@@ -204,7 +207,7 @@ struct MgSolveArgs {
     int ir, warm, max_iterations, refinement;
     float tol;
     int wave;                        // grid depth of the level kernels (kMgWaveCount codes)
-    int learned;                     // 1: the preconditioner is the network of `net`, not the V-cycle
+    int learned;                     // 1: the V-cycle's result is corrected by the network of `net`
     int net_warm;                    // 1 (learned): the initial guess is the network's estimate N(b)
     const struct LearnedSolve* net;  // host-side: the network's images, workspace and mask (learned only)
 };
@@ -212,6 +215,8 @@ struct MgSolveArgs {
 int mg_level_count(int nx, int ny, int nz);
 // Largest refinement count the multigrid solve honours (the graph unrolls refinement + 1 passes).
 int mg_max_refinement();
+// z = V(r): one V-cycle of the multigrid preconditioner on the residual r (the solve's preconditioner, standalone).
+cudaError_t launch_mg_vcycle(const MgHierarchy& H, int wave_depth, const float* r, float* z, cudaStream_t s);
 // out = A x with the fine operator (the pressure system's matrix, matrix-free from the level-0 codes).
 cudaError_t launch_mg_apply(const MgHierarchy& H, const float* x, float* out, cudaStream_t s);
 // Builds level fluid masks and codes from the occupancy (after the fine codes and anchor exist).

@@ -234,24 +234,48 @@ SmokeSimulationResult smoke_b200_net_train_cuda(SmokeB200Net net, int nx, int ny
 }
 
 SmokeSimulationResult smoke_b200_conv3d_cuda(int nx, int ny, int nz, int cin, int cout, const void* in, const float* weights, const float* bias, int relu, void* out, float* out_f32, void* stream) {
-    if (!valid_volume(nx, ny, nz) || cin < 1 || cin > 16 || cout < 1 || cout > 16 || in == nullptr || weights == nullptr || (out == nullptr && out_f32 == nullptr)) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    const int cin_store = cin >= 1 ? net_store(cin) : 0;
+    const bool cin_ok = cin_store == 8 || cin_store == 16 || cin_store == 32 || cin_store == 64 || cin_store == 128;
+    if (!valid_volume(nx, ny, nz) || !cin_ok || cout < 1 || cout > 128 || in == nullptr || weights == nullptr || (out == nullptr && out_f32 == nullptr)) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int cin_store = net_store(cin), cout_store = net_store(cout);
-    const size_t pack_bytes = conv_pack_bytes(cin_store);
+    const int cout_store = net_store(cout), cpad = net_cout_pad(cout);
+    const size_t pack_bytes = (conv_pack_bytes(cin_store, cout) + 255) & ~size_t(255);
     DeviceScratch scratch;
-    // [pack | 16 bias floats | error word]
-    if (cudaMalloc(&scratch.p, pack_bytes + 16 * sizeof(float) + 16) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    // [pack | cpad bias floats | error word]
+    if (cudaMalloc(&scratch.p, pack_bytes + cpad * sizeof(float) + 16) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     uint8_t* pack = static_cast<uint8_t*>(scratch.p);
-    float* b16 = reinterpret_cast<float*>(pack + pack_bytes);
-    unsigned* error = reinterpret_cast<unsigned*>(b16 + 16);
-    if (cudaMemsetAsync(b16, 0, 16 * sizeof(float) + 16, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-    if (bias && cudaMemcpyAsync(b16, bias, cout * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
-    if (launch_pack_conv(weights, cin, cout, 0, pack, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    float* bpad = reinterpret_cast<float*>(pack + pack_bytes);
+    unsigned* error = reinterpret_cast<unsigned*>(bpad + cpad);
+    if (cudaMemsetAsync(bpad, 0, cpad * sizeof(float) + 16, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (bias && cudaMemcpyAsync(bpad, bias, cout * sizeof(float), cudaMemcpyDeviceToDevice, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (launch_pack_conv(weights, cin, cout, 0, cin_store, pack, s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     const VolumeDims d = volume_dims(nx, ny, nz);
-    if (launch_conv3(d, cin_store, static_cast<const __nv_bfloat16*>(in), pack, b16, relu, nullptr, static_cast<__nv_bfloat16*>(out), cout_store, out_f32, error, s, nullptr) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    if (launch_conv3(d, cin_store, cout, static_cast<const __nv_bfloat16*>(in), pack, bpad, relu, nullptr, static_cast<__nv_bfloat16*>(out), cout_store, out_f32, error, s, nullptr) != cudaSuccess)
+        return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     unsigned err = 0;
     if (cudaMemcpyAsync(&err, error, sizeof(err), cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return err ? SMOKE_SIMULATION_RESULT_BACKEND_FAILURE : SMOKE_SIMULATION_RESULT_OK;
+}
+
+SmokeSimulationResult smoke_b200_test_conv_wait_timeout_cuda(int nx, int ny, int nz, unsigned long long wait_cycles, unsigned* error_out, void* stream) {
+    if (!valid_volume(nx, ny, nz) || error_out == nullptr || wait_cycles == 0 || wait_cycles > 4000000000ull) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    return guarded([&] {
+        const VolumeDims d = volume_dims(nx, ny, nz);
+        const size_t in_bytes = (static_cast<size_t>(d.n) * 16 * 2 + 255) & ~size_t(255);
+        const size_t pack_bytes = (conv_pack_bytes(16, 16) + 255) & ~size_t(255);
+        DeviceScratch scratch;
+        check(cudaMalloc(&scratch.p, in_bytes + pack_bytes + 256), "scratch");
+        auto* in = static_cast<__nv_bfloat16*>(scratch.p);
+        auto* pack = static_cast<uint8_t*>(scratch.p) + in_bytes;
+        auto* error = reinterpret_cast<unsigned*>(pack + pack_bytes);
+        check(cudaMemsetAsync(scratch.p, 0, in_bytes + pack_bytes + 256, s), "scratch");
+        // the loads of every tile are expected but never issued: each block's first wait must run out
+        check(launch_conv3(d, 16, 16, in, pack, nullptr, 0, nullptr, nullptr, 16, nullptr, error, s, nullptr, static_cast<long long>(wait_cycles), 1), "convolution");
+        check(cudaMemcpyAsync(error_out, error, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "error word");
+        check(cudaStreamSynchronize(s), "error word");
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
 }
 
 }  // extern "C"

@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
                 const float rq = r[c.q], qq = A.W.q[c.q];
                 const float pq = initial ? 0.0f : pn[c.q], eq = initial ? 0.0f : A.e[c.q];
                 const float rn = rq - a * qq;
-                if constexpr (!LEARNED) {  // pre-smoothing and the residual restricted to level 1
+                {  // pre-smoothing and the residual restricted to level 1
                     float un[6];
 #pragma unroll
                     for (int k = 0; k < 6; ++k) un[k] = wdiag(L0.code[nb[k]]) * (r[nb[k]] - a * A.W.q[nb[k]]);
@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
                 if (!initial) A.e[c.q] = eq + a * pq;
                 rr += static_cast<T>(rn) * static_cast<T>(rn);
             }
-            if constexpr (!LEARNED) restrict_tile(res, A.H.L[1], c);
+            restrict_tile(res, A.H.L[1], c);
         });
         block_accumulate<T>(st, kAccRR, rr, -1, T(0));
     }
@@ -388,12 +388,12 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
         }
     }
     if (!initial) st->first_iter = 0;
-    if (LEARNED && !stop && !st->fallback) {  // plain-preconditioner fallback of a stalled learned solve
+    if (LEARNED && !stop && !st->fallback) {  // the V-cycle alone, once the learned solve stagnates
         if (initial) {
             st->stall_it = st->it;
             st->stall_ref = st->rnorm2;
         } else if (st->it - st->stall_it >= kLearnedStallWindow) {
-            if (st->rnorm2 > st->stall_ref * (1.0 / 1.44)) st->fallback = 1;
+            if (st->rnorm2 > st->stall_ref * kLearnedStallReduction2) st->fallback = 1;
             st->stall_it = st->it;
             st->stall_ref = st->rnorm2;
         }
@@ -478,7 +478,8 @@ __global__ void __launch_bounds__(kThreads) mg_prolong_kernel(const __grid_const
 // Level l post-smoothing: t = zp + w D^-1 (r - A zp) on active cells; inactive cells get kTag (coarse levels) or 0
 // (level 0, whose t is the preconditioned residual z). Level 0 also accumulates (z, r) and (z, q), and its last
 // block computes beta (0 on a pass's first iteration).
-template <bool LEVEL0, typename T>
+// DOTS = false (level 0 of a learned solve): z only; the network's correction and the dot products follow.
+template <bool LEVEL0, typename T, bool DOTS = true>
 __global__ void __launch_bounds__(kThreads) mg_smooth_kernel(const __grid_constant__ MgSolveArgs A, int l) {
     const MgLevel& F = A.H.L[LEVEL0 ? 0 : l];
     MgState* st = A.st;
@@ -498,14 +499,14 @@ __global__ void __launch_bounds__(kThreads) mg_smooth_kernel(const __grid_consta
         float z = inactive_value;
         if (active(code)) {
             z = s0 + wdiag(code) * (rv - masked_stencil(code, s0, sn));
-            if (LEVEL0) {
+            if (LEVEL0 && DOTS) {
                 zr += static_cast<T>(z) * static_cast<T>(rv);
                 zq += static_cast<T>(z) * static_cast<T>(qv);
             }
         }
         F.t[c.q] = z;
     });
-    if (!LEVEL0) return;
+    if (!LEVEL0 || !DOTS) return;
     block_accumulate<T>(st, kAccZR, zr, kAccZQ, zq);
     if (!last_block(&st->done[3])) return;
     const double beta = st->first_iter ? 0.0 : -total(st, kAccZQ) / st->pq_prev;
@@ -563,18 +564,61 @@ __global__ void __launch_bounds__(kThreads) mg_up_kernel(const __grid_constant__
     });
 }
 
-// Learned preconditioner, first half: zp = N(r) = y / s on active cells (y the network's output for the current
-// residual, s = sqrt(n / ||r||^2) its input scale), 0 elsewhere; 0 everywhere once the solve fell back to the plain
-// preconditioner. mg_smooth_kernel<true> then post-smooths it, z = zp + w D^-1 (r - A zp): the network supplies the
-// smooth part of the correction, the Jacobi step the rough part (and all of it after the fallback).
-__global__ void __launch_bounds__(kThreads) mg_net_zp_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
+// Learned preconditioner, part 1: the residual the V-cycle leaves, r_V = r - A z_V on active cells (z_V = t of level
+// 0, just smoothed), into level 0's zp (free after the smoothing), and ||r_V||^2 into st->net_rr: the network's input
+// and its scale. Nothing to do once the solve fell back to the V-cycle alone.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) mg_net_residual_kernel(const __grid_constant__ MgSolveArgs A) {
     const MgLevel& F = A.H.L[0];
-    const double rn2 = A.st->rnorm2;
-    const bool fallback = A.st->fallback != 0;  // then z is the Jacobi step alone: the plain preconditioner
-    const float inv_s = rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n))) : 0.0f;
+    MgState* st = A.st;
+    if (st->fallback) return;  // uniform over the grid
+    const float* r = A.W.r[st->parity];
+    T rr = 0;
     for_tiles(F, [&](const Cell& c) {
-        if (c.in) F.zp[c.q] = active(F.code[c.q]) && !fallback ? y[c.q] * inv_s : 0.0f;
+        if (!c.in) return;
+        uint32_t nb[6];
+        nbr_all(F, A.H.fper, c, nb);
+        const uint16_t code = F.code[c.q];
+        const float rv = r[c.q], z0 = F.t[c.q];
+        float zn[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) zn[k] = F.t[nb[k]];
+        const float rv_net = active(code) ? rv - masked_stencil(code, z0, zn) : 0.0f;
+        F.zp[c.q] = rv_net;
+        rr += static_cast<T>(rv_net) * static_cast<T>(rv_net);
     });
+    block_accumulate<T>(st, kAccNet, rr, -1, T(0));
+    if (!last_block(&st->done[5])) return;
+    st->net_rr = total(st, kAccNet);
+    zero_acc(st, kAccNet);
+}
+
+// Learned preconditioner, part 2: z = z_V + N(r_V) on active cells, N(r_V) = y / s with y the network's output and
+// s = sqrt(n / ||r_V||^2) its input scale (z = z_V after a fallback); then (z, r) and (z, q), and the last block
+// computes beta (0 on a pass's first iteration), as level 0's smoothing does for the V-cycle alone.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) mg_net_add_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
+    const MgLevel& F = A.H.L[0];
+    MgState* st = A.st;
+    const bool use_net = st->fallback == 0;
+    const double rn2 = st->net_rr;
+    const float inv_s = use_net && rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n))) : 0.0f;
+    const float* r = A.W.r[st->parity];
+    T zr = 0, zq = 0;
+    for_tiles(F, [&](const Cell& c) {
+        if (!c.in) return;
+        const uint16_t code = F.code[c.q];
+        if (!active(code)) return;  // t stays 0 there
+        const float z = use_net ? F.t[c.q] + y[c.q] * inv_s : F.t[c.q];
+        F.t[c.q] = z;
+        zr += static_cast<T>(z) * static_cast<T>(r[c.q]);
+        zq += static_cast<T>(z) * static_cast<T>(A.W.q[c.q]);
+    });
+    block_accumulate<T>(st, kAccZR, zr, kAccZQ, zq);
+    if (!last_block(&st->done[3])) return;
+    const double beta = st->first_iter ? 0.0 : -total(st, kAccZQ) / st->pq_prev;
+    if (!isfinite(beta) || !isfinite(total(st, kAccZR))) st->fail = SMOKE_B200_SOLVE_NOT_FINITE;
+    st->beta = static_cast<float>(beta);
 }
 
 // Initial guess of a learned solve: x64 = the network's estimate on active cells, 0 elsewhere.
@@ -769,6 +813,47 @@ __global__ void __launch_bounds__(kBlockLevelThreads) mg_block_kernel(const __gr
     for (uint32_t q = t; q < S.n; q += NT) H.L[g].t[q] = active(S.code[q]) ? S.t[q] : __uint_as_float(kTag);
 }
 
+// Standalone V-cycle, level 0 down: zp = w D^-1 r, and (r - A zp) / 2 restricted into level 1 (the pre-smoothing the
+// solve's update kernel performs, for an r given by the caller).
+__global__ void __launch_bounds__(kThreads) mg_presmooth_kernel(const __grid_constant__ MgHierarchy H, const float* __restrict__ r) {
+    const MgLevel& L0 = H.L[0];
+    for_tiles(L0, [&](const Cell& c) {
+        float res = 0.0f;
+        if (c.in) {
+            uint32_t nb[6];
+            nbr_all(L0, H.fper, c, nb);
+            const uint16_t code = L0.code[c.q];
+            const float rv = r[c.q];
+            float un[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) un[k] = wdiag(L0.code[nb[k]]) * r[nb[k]];
+            float zp = 0.0f;
+            if (active(code)) {
+                zp = wdiag(code) * rv;
+                res = 0.5f * (rv - masked_stencil(code, zp, un));
+            }
+            L0.zp[c.q] = zp;
+        }
+        restrict_tile(res, H.L[1], c);
+    });
+}
+
+// Standalone V-cycle, level 0 up: z = zp + w D^-1 (r - A zp) on active cells, 0 elsewhere.
+__global__ void __launch_bounds__(kThreads) mg_postsmooth_kernel(const __grid_constant__ MgHierarchy H, const float* __restrict__ r, float* __restrict__ z) {
+    const MgLevel& F = H.L[0];
+    for_tiles(F, [&](const Cell& c) {
+        if (!c.in) return;
+        uint32_t nb[6];
+        nbr_all(F, H.fper, c, nb);
+        const uint16_t code = F.code[c.q];
+        const float s0 = F.zp[c.q];
+        float sn[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sn[k] = F.zp[nb[k]];
+        z[c.q] = active(code) ? s0 + wdiag(code) * (r[c.q] - masked_stencil(code, s0, sn)) : 0.0f;
+    });
+}
+
 // Refinement: x64 = (first pass of a cold start ? 0 : x64) + e.
 __global__ void __launch_bounds__(kThreads) mg_accumulate_kernel(const __grid_constant__ MgSolveArgs A) {
     const MgState* st = A.st;
@@ -933,20 +1018,10 @@ void launch_update(const MgSolveArgs& A, int initial, cudaGraphConditionalHandle
     else mg_update_kernel<T, false><<<wave(mg_update_kernel<T, false>, A.H.L[0], A.wave), kBlock, 0, s>>>(A, initial, h, in_graph);
 }
 
-// One iteration's loop body (everything after the update that tests convergence, up to the next update).
-template <typename T>
-void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_graph, uint32_t block_bytes, cudaStream_t bs) {
+// The V-cycle below level 0: restrictions of levels 1..g-1, the block-level cycle, the up passes of levels g-1..1,
+// then the prolongation into level 0's zp (level 1's right-hand side must be in place).
+void launch_coarse_cycle(const MgSolveArgs& A, uint32_t block_bytes, cudaStream_t bs) {
     const MgHierarchy& H = A.H;
-    const MgLevel& L0 = H.L[0];
-    if (A.learned) {  // z = N(r): the network on the current residual (its parity and norm read on the device)
-        const LearnedSolve& N = *A.net;
-        if (net_forward(N.images, N.acts, A.W.r[0], A.W.r[1], &A.st->parity, &A.st->rnorm2, N.occupancy, bs, &A.st->fallback) != cudaSuccess) return;
-        mg_net_zp_kernel<<<wave(mg_net_zp_kernel, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
-        mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
-        mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
-        mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
-        return;
-    }
     const int g = H.grid_levels;
     for (int l = 1; l < g; ++l) mg_restrict_kernel<<<wave(mg_restrict_kernel, H.L[l], A.wave), kBlock, 0, bs>>>(H, l);
     mg_block_kernel<<<1, kBlockLevelThreads, block_bytes, bs>>>(H);
@@ -955,10 +1030,27 @@ void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_grap
             mg_up_kernel<<<wave(mg_up_kernel, H.L[l], A.wave), kBlock, 0, bs>>>(H, l);
         } else {
             mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[l + 1], A.wave), kBlock, 0, bs>>>(H, l);
-            mg_smooth_kernel<false, T><<<wave(mg_smooth_kernel<false, T>, H.L[l], A.wave), kBlock, 0, bs>>>(A, l);
+            mg_smooth_kernel<false, float><<<wave(mg_smooth_kernel<false, float>, H.L[l], A.wave), kBlock, 0, bs>>>(A, l);
         }
     }
     mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[1], A.wave), kBlock, 0, bs>>>(H, 0);
+}
+
+// One iteration's loop body (everything after the update that tests convergence, up to the next update).
+template <typename T>
+void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_graph, uint32_t block_bytes, cudaStream_t bs) {
+    const MgLevel& L0 = A.H.L[0];
+    launch_coarse_cycle(A, block_bytes, bs);
+    if (A.learned) {  // z = z_V + N(r - A z_V): the network corrects what the V-cycle leaves
+        const LearnedSolve& N = *A.net;
+        mg_smooth_kernel<true, T, false><<<wave(mg_smooth_kernel<true, T, false>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
+        mg_net_residual_kernel<T><<<wave(mg_net_residual_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
+        if (net_forward(N.images, N.acts, L0.zp, nullptr, nullptr, &A.st->net_rr, N.occupancy, bs, &A.st->fallback) != cudaSuccess) return;
+        mg_net_add_kernel<T><<<wave(mg_net_add_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
+        mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
+        mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
+        return;
+    }
     mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
     mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
     mg_update_kernel<T, false><<<wave(mg_update_kernel<T, false>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
@@ -1138,6 +1230,16 @@ cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uin
 
 cudaError_t launch_mg_apply(const MgHierarchy& H, const float* x, float* out, cudaStream_t s) {
     mg_apply_kernel<<<wave(mg_apply_kernel, H.L[0], kMgWaveDefault), kBlock, 0, s>>>(H, x, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mg_vcycle(const MgHierarchy& H, int wave_depth, const float* r, float* z, cudaStream_t s) {
+    MgSolveArgs A{};
+    A.H = H;
+    A.wave = wave_depth;
+    mg_presmooth_kernel<<<wave(mg_presmooth_kernel, H.L[0], wave_depth), kBlock, 0, s>>>(H, r);
+    launch_coarse_cycle(A, block_level_bytes(H), s);
+    mg_postsmooth_kernel<<<wave(mg_postsmooth_kernel, H.L[0], wave_depth), kBlock, 0, s>>>(H, r, z);
     return cudaGetLastError();
 }
 

@@ -73,6 +73,30 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
     }
 }
 
+// The same wait that also gives up as soon as the block-wide flag *abort (shared memory) is nonzero.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, long long max_cycles, const volatile int* abort) {
+    const uint32_t a = smem_addr(bar);
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (*abort) return false;
+        if (clock64() - t0 > max_cycles) return false;
+    }
+}
+
+// One plain arrival on the mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // Tensor-memory allocation of `cols` columns (a power of two >= 32) by one whole warp; the address lands in *slot.
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(slot)), "r"(cols) : "memory");

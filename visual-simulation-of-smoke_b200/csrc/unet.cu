@@ -1,11 +1,12 @@
 // Kernels of the learned preconditioner (unet.h): tcgen05 implicit-GEMM 3x3x3 convolutions on channels-last BF16
-// volumes with FP32 accumulation in tensor memory, and the glue between the U-Net's layers.
+// volumes with FP32 accumulation in tensor memory, their weight gradients, and the glue between the U-Net's layers.
 //
 // Convolution as a GEMM: D[cell][co] = sum over k = (tap, ci) of A[cell][k] * B[co][k], with A[cell][(tap, ci)] =
-// in[cell + offset(tap)][ci] (0 outside the volume). One block of 128 threads computes tiles of M = 128 consecutive
-// cells, N = 16 output channels: every thread gathers its cell's 27 neighbour channel vectors (16 or 32 bytes each)
-// straight into the core-matrix layout of the A operand in shared memory, then one thread issues the K/16 MMAs, whose
-// accumulators stay in tensor memory until the epilogue (bias, ReLU, gate) reads them back.
+// in[cell + offset(tap)][ci] (0 outside the volume). A block computes tiles of M = 128 cells and N = NC output
+// channels (one chunk of the output; gridDim.y chunks cover all of them) with its chunk of the weights resident in
+// shared memory. A producer warp streams each tile's input halo box into shared memory with TMA and issues the
+// MMAs into one of two tensor-memory accumulators; four epilogue warps read the other accumulator back (bias,
+// ReLU, gate) and store, so a tile's epilogue overlaps the next tile's loads and MMAs.
 #include <algorithm>
 #include <cstdio>
 #include <map>
@@ -20,35 +21,44 @@
 namespace smoke_b200 {
 namespace {
 
-constexpr int kConvThreads = 128;
-constexpr long long kSpinCycles = 4000000000ll;  // ~2 s: bound of every tensor-core completion wait
+constexpr int kEpiThreads = 128;                  // epilogue warps 0-3: thread t owns tensor-memory lane t
+constexpr int kConvThreads = kEpiThreads + 32;    // + warp 4: TMA producer and MMA issuer (lane 0)
+constexpr long long kSpinCycles = 4000000000ll;   // ~2 s: default bound of every completion wait
 
 // Tiles of 8 x 16 x 1 cells (M = 128 rows, row m = cell (m % 8, m / 8) of the tile). A tile's input is its halo box
 // of 10 x 18 x 3 cells, brought into shared memory by one TMA load per 8-channel plane (zeros outside the volume):
 // cell (x, y, z) of the box at byte ((z * 18 + y) * 10 + x) * 16 of its plane. The A operand of tap (dx, dy, dz) is
 // that box read from offset ((1 + dz) * 18 + 1 + dy) * 160 + (1 + dx) * 16: every 8 cells of a tile row are 8
 // consecutive 16-byte rows of the box, i.e. one core matrix, and the next tile row starts one box row (160 bytes) on
-// (SBO). So no im2col copy exists: each MMA reads its two K columns (two taps of an 8-channel input, or the two
-// planes of one tap of a 16-channel input; LBO = their distance) straight from the box.
-template <int CIN>
-struct ConvShape {
-    static constexpr int kTX = 8, kTY = 16;
-    static constexpr int kHX = kTX + 2, kHY = kTY + 2, kHZ = 3;
-    static constexpr uint32_t kRow = kHX * 16;                               // bytes of one box row (SBO)
-    static constexpr uint32_t kBox = kHX * kHY * kHZ * 16;                   // 8640 bytes per plane
-    static constexpr uint32_t kPlane = 8704;                                 // plane pitch: box + zero slack, 128-aligned
-    static constexpr int kPlanes = CIN / 8;
-    static constexpr uint32_t kStage = (kPlanes * kPlane + 1023u) & ~1023u;  // one pipeline stage
-    static constexpr int kKSteps = conv_taps(CIN) * CIN / 16;                // MMAs per tile (K = 16 each)
-    static constexpr uint32_t kBBytes = conv_pack_bytes(CIN);
-    static constexpr uint32_t kSmem = 2 * kStage + kBBytes;
-};
+// (SBO). So no im2col copy exists: each MMA reads its two K columns (two taps of an 8-channel input, or two channel
+// planes of one tap) straight from the boxes.
+constexpr int kTX = 8, kTY = 16;
+constexpr int kHX = kTX + 2, kHY = kTY + 2, kHZ = 3;
+constexpr uint32_t kRow = kHX * 16;                 // bytes of one box row (SBO)
+constexpr uint32_t kBox = kHX * kHY * kHZ * 16;     // 8640 bytes per plane
+constexpr uint32_t kPlane = 8704;                   // plane pitch: box + zero slack, 128-aligned
 __host__ __device__ constexpr uint32_t tap_offset(int tap) {
     return ((tap / 9) * 18 + (tap / 3) % 3) * 160u + (tap % 3) * 16u;  // (dz + 1, dy + 1, dx + 1) of the tap
 }
 // the padding tap's K column (tap 26's rows, 16 bytes on) stays inside the plane's zero slack
-static_assert(tap_offset(26) + 16 + 15 * ConvShape<8>::kRow + 128 <= ConvShape<8>::kPlane, "zero slack");
-static_assert(tap_offset(26) + 15 * ConvShape<8>::kRow + 128 <= ConvShape<8>::kBox, "box");
+static_assert(tap_offset(26) + 16 + 15 * kRow + 128 <= kPlane, "zero slack");
+static_assert(tap_offset(26) + 15 * kRow + 128 <= kBox, "box");
+
+// CS stored input channels, NC output channels per block. A K group is one plane (CS = 8: its 27 taps paired into
+// 14 MMAs, the 28th tap zero) or two planes (16 channels: one MMA per tap); a tile has CS / 16 groups.
+template <int CS, int NC>
+struct ConvShape {
+    static constexpr int kGP = CS == 8 ? 1 : 2;      // planes per group (one TMA stage)
+    static constexpr int kGroups = CS / (8 * kGP);
+    static constexpr int kStages = 3;
+    static constexpr uint32_t kStage = kGP * kPlane;
+    static constexpr int kMmas = CS == 8 ? 14 : 27;  // MMAs of one group (K = 16 each)
+    static constexpr uint32_t kBChunk = static_cast<uint32_t>(conv_taps(CS) * CS * NC * 2);
+    static constexpr uint32_t kSmem = kStages * kStage + kBChunk;
+    static constexpr uint32_t kTmemCols = 2 * NC < 32 ? 32u : static_cast<uint32_t>(2 * NC);  // two accumulators
+    static_assert(NC == 16 || NC == 32, "N per block");
+    static_assert(kSmem <= 200 * 1024, "shared memory");
+};
 
 struct ConvArgs {
     const __nv_bfloat16* in;
@@ -59,6 +69,8 @@ struct ConvArgs {
     float* out_f32;
     unsigned* error;
     const uint32_t* skip;  // optional: the launch does nothing when *skip is nonzero
+    long long wait_cycles; // bound of every wait
+    int drop_loads;        // test only: the producer expects its loads but never issues them
     int relu, cout_store;
     int nx, ny, nz;
     uint32_t n;
@@ -69,149 +81,198 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// Persistent over tiles with two pipeline stages: while the tensor core works on tile j (stage j % 2, accumulator
-// j % 2 in tensor memory), the TMA load of tile j + 1 fills the other stage. Thread 0 issues the loads and the MMAs;
-// all 128 threads run the epilogue (tensor memory -> bias, ReLU, gate -> BF16/FP32 stores).
-template <int CIN>
+template <int CS, int NC>
 __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_constant__ ConvArgs a, const __grid_constant__ CUtensorMap map) {
-    using S = ConvShape<CIN>;
+    using S = ConvShape<CS, NC>;
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* Bs = smem + 2 * S::kStage;
-    __shared__ uint64_t full[2], done[2];
+    uint8_t* Bs = smem + S::kStages * S::kStage;
+    __shared__ uint64_t full[S::kStages], freed[S::kStages], done[2], drained[2];
     __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag;
     if (a.skip && *a.skip) return;  // uniform: every block reads the same word
     const int t = threadIdx.x, warp = t >> 5;
-    const uint4* wsrc = reinterpret_cast<const uint4*>(a.wpack);
-    for (uint32_t i = t; i < S::kBBytes / 16u; i += kConvThreads) reinterpret_cast<uint4*>(Bs)[i] = wsrc[i];
-    for (int st = 0; st < 2; ++st)  // the slack after each box stays zero (read by the padding tap, times zero weights)
-        for (int p = 0; p < S::kPlanes; ++p)
-            for (uint32_t i = t; i < (S::kPlane - S::kBox) / 16u; i += kConvThreads) reinterpret_cast<uint4*>(smem + st * S::kStage + p * S::kPlane + S::kBox)[i] = make_uint4(0, 0, 0, 0);
+    const int chunk = blockIdx.y;
+    const uint4* wsrc = reinterpret_cast<const uint4*>(a.wpack + static_cast<size_t>(chunk) * S::kBChunk);
+    for (uint32_t i = t; i < S::kBChunk / 16u; i += kConvThreads) reinterpret_cast<uint4*>(Bs)[i] = wsrc[i];
+    for (int st = 0; st < S::kStages; ++st)  // the slack after each box stays zero (read by the padding tap, times zero weights)
+        for (int p = 0; p < S::kGP; ++p)
+            for (uint32_t i = t; i < (kPlane - kBox) / 16u; i += kConvThreads) reinterpret_cast<uint4*>(smem + st * S::kStage + p * kPlane + kBox)[i] = make_uint4(0, 0, 0, 0);
     if (t == 0) {
-        for (int st = 0; st < 2; ++st) {
+        for (int st = 0; st < S::kStages; ++st) {
             tc::mbar_init(&full[st], 1);
-            tc::mbar_init(&done[st], 1);
+            tc::mbar_init(&freed[st], 1);
         }
+        for (int b = 0; b < 2; ++b) {
+            tc::mbar_init(&done[b], 1);
+            tc::mbar_init(&drained[b], kEpiThreads);
+        }
+        abort_flag = 0;
     }
-    if (warp == 0) tc::tmem_alloc(&tmem_slot, 32);
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, S::kTmemCols);
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
-    constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 16, false, false);
-    const uint32_t b_base = tc::smem_addr(Bs);
-    const int ntx = (a.nx + S::kTX - 1) / S::kTX, nty = (a.ny + S::kTY - 1) / S::kTY;
+    const long long wait = a.wait_cycles > 0 ? a.wait_cycles : kSpinCycles;
+    volatile int* abort = &abort_flag;
+    const int ntx = (a.nx + kTX - 1) / kTX, nty = (a.ny + kTY - 1) / kTY;
     const uint32_t tiles = static_cast<uint32_t>(ntx) * nty * a.nz;
-    auto load = [&](uint32_t tile, int st) {
-        const int tx = static_cast<int>(tile % ntx), rest = static_cast<int>(tile / ntx);
-        const int ty = rest % nty, tz = rest / nty;
-        tc::mbar_arrive_expect_tx(&full[st], S::kPlanes * S::kBox);
-        for (int p = 0; p < S::kPlanes; ++p) tc::tma_load_4d(smem + st * S::kStage + p * S::kPlane, &map, 8 * p, tx * S::kTX - 1, ty * S::kTY - 1, tz - 1, &full[st]);
-    };
-    float bias[16];
-#pragma unroll
-    for (int c = 0; c < 16; ++c) bias[c] = a.bias ? __ldg(a.bias + c) : 0.0f;
-    if (t == 0 && blockIdx.x < tiles) load(blockIdx.x, 0);
-    uint32_t j = 0;
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++j) {
-        const int st = static_cast<int>(j & 1u);
-        const uint32_t parity = (j >> 1) & 1u;
-        if (t == 0) {
-            // the other stage was last read by the MMAs of tile j - 1, which completed before that tile's epilogue
-            if (tile + gridDim.x < tiles) load(tile + gridDim.x, st ^ 1);
-            if (tc::mbar_wait(&full[st], parity, kSpinCycles)) {
+    const uint32_t my_tiles = blockIdx.x < tiles ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0u;
+
+    if (warp == 4) {
+        if ((t & 31) == 0) {
+            // ---------------------------------------------------------------- producer and MMA issuer
+            const uint32_t items = my_tiles * S::kGroups;  // (tile, K group) pairs in order
+            constexpr uint32_t idesc = tc::idesc_bf16_f32(128, NC, false, false);
+            const uint32_t b_base = tc::smem_addr(Bs);
+            uint32_t loaded = 0, consumed = 0, issued = 0;  // items whose TMA was issued / whose box arrived / whose MMAs were issued
+            bool ok = true;
+            auto issue_load = [&](uint32_t k) -> bool {
+                const int st = static_cast<int>(k % S::kStages);
+                // stage st last held item k - kStages: its MMAs must have completed before the box is overwritten
+                if (k >= static_cast<uint32_t>(S::kStages) && !tc::mbar_wait_or_abort(&freed[st], ((k / S::kStages) - 1u) & 1u, wait, abort)) return false;
+                const uint32_t tile = blockIdx.x + (k / S::kGroups) * gridDim.x;
+                const int g = static_cast<int>(k % S::kGroups);
+                const int tx = static_cast<int>(tile % ntx), rest = static_cast<int>(tile / ntx);
+                const int ty = rest % nty, tz = rest / nty;
+                tc::mbar_arrive_expect_tx(&full[st], S::kGP * kBox);
+                if (!a.drop_loads) {
+                    for (int p = 0; p < S::kGP; ++p) tc::tma_load_4d(smem + st * S::kStage + p * kPlane, &map, 8 * (g * S::kGP + p), tx * kTX - 1, ty * kTY - 1, tz - 1, &full[st]);
+                    loaded = k + 1;
+                }
+                return true;
+            };
+            for (uint32_t k = 0; k < static_cast<uint32_t>(S::kStages - 1) && k < items && ok; ++k) ok = issue_load(k);
+            for (uint32_t i = 0; ok && i < items; ++i) {
+                const uint32_t jl = i / S::kGroups;
+                const int g = static_cast<int>(i % S::kGroups), b = static_cast<int>(jl & 1u), st = static_cast<int>(i % S::kStages);
+                // accumulator b last held tile jl - 2: its epilogue must have read it out
+                if (g == 0 && jl >= 2 && !tc::mbar_wait_or_abort(&drained[b], ((jl >> 1) - 1u) & 1u, wait, abort)) {
+                    ok = false;
+                    break;
+                }
+                if (!tc::mbar_wait_or_abort(&full[st], (i / S::kStages) & 1u, wait, abort)) {
+                    ok = false;
+                    break;
+                }
+                consumed = i + 1;
                 tc::fence_after_sync();
                 const uint32_t a_base = tc::smem_addr(smem + st * S::kStage);
 #pragma unroll 1
-                for (int k = 0; k < S::kKSteps; ++k) {
-                    uint32_t start, lbo;
-                    if constexpr (CIN == 8) {  // taps 2k and 2k + 1 (tap 27: zero weights, any finite A)
+                for (int k = 0; k < S::kMmas; ++k) {
+                    uint32_t start, lbo, k0;
+                    if constexpr (CS == 8) {  // taps 2k and 2k + 1 (tap 27: zero weights, any finite A)
                         start = a_base + tap_offset(2 * k);
                         lbo = 2 * k + 1 < 27 ? tap_offset(2 * k + 1) - tap_offset(2 * k) : 16u;
-                    } else {  // tap k, channel planes 0 and 1
+                        k0 = 16u * k;
+                    } else {  // tap k, channel planes 2g and 2g + 1
                         start = a_base + tap_offset(k);
-                        lbo = S::kPlane;
+                        lbo = kPlane;
+                        k0 = static_cast<uint32_t>(k * CS + 16 * g);
                     }
-                    tc::mma_bf16(tmem + st * 16, tc::smem_desc(start, lbo, S::kRow), tc::smem_desc(b_base + k * 512u, 256u, 128u), idesc, k > 0 ? 1u : 0u);
+                    const uint64_t bd = tc::smem_desc(b_base + (k0 / 8u) * (NC / 8) * 128u, (NC / 8) * 128u, 128u);
+                    tc::mma_bf16(tmem + static_cast<uint32_t>(b * NC), tc::smem_desc(start, lbo, kRow), bd, idesc, (g > 0 || k > 0) ? 1u : 0u);
                 }
-                tc::commit(&done[st]);
-            } else {
+                tc::commit(&freed[st]);
+                if (g == S::kGroups - 1) tc::commit(&done[b]);
+                issued = i + 1;
+                if (i + S::kStages - 1 < items && !issue_load(i + S::kStages - 1)) ok = false;
+            }
+            if (!ok) {
                 atomicOr(a.error, 1u);
+                *abort = 1;
             }
+            // nothing may still write this block's shared or tensor memory when it exits: every issued box must have
+            // landed and the last MMAs completed (bounded waits again)
+            for (uint32_t k = consumed; k < loaded; ++k) tc::mbar_wait(&full[k % S::kStages], (k / S::kStages) & 1u, wait);
+            if (issued > 0) tc::mbar_wait(&freed[(issued - 1) % S::kStages], ((issued - 1) / S::kStages) & 1u, wait);
         }
-        __syncwarp();
-        const bool ok = __syncthreads_and(tc::mbar_wait(&done[st], parity, kSpinCycles) ? 1 : 0) != 0;
-        if (!ok) {
-            if (t == 0) atomicOr(a.error, 1u);
-            break;
-        }
-        tc::fence_after_sync();
-        float acc[16];
-        tc::tmem_load16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + st * 16, acc);
-        const int tx = static_cast<int>(tile % ntx), rest = static_cast<int>(tile / ntx);
-        const int x = tx * S::kTX + (t & 7), y = (rest % nty) * S::kTY + (t >> 3), z = rest / nty;
-        if (x < a.nx && y < a.ny) {
-            const uint32_t q = (static_cast<uint32_t>(z) * a.ny + y) * a.nx + x;
-            float v[16];
+    } else {
+        // -------------------------------------------------------------------- epilogue (threads 0-127)
+        float bias[NC];
 #pragma unroll
-            for (int c = 0; c < 16; ++c) {
-                v[c] = acc[c] + bias[c];
-                if (a.relu) v[c] = fmaxf(v[c], 0.0f);
+        for (int c = 0; c < NC; ++c) bias[c] = a.bias ? __ldg(a.bias + chunk * NC + c) : 0.0f;
+        const int n0 = chunk * NC;
+        for (uint32_t jl = 0; jl < my_tiles; ++jl) {
+            const int b = static_cast<int>(jl & 1u);
+            // warp-uniform outcome: the accumulator loads below are warp-collective
+            const bool ready = __all_sync(0xffffffffu, tc::mbar_wait_or_abort(&done[b], (jl >> 1) & 1u, wait, abort) ? 1 : 0) != 0;
+            if (!ready) {
+                if (t == 0) atomicOr(a.error, 1u);
+                *abort = 1;
+                break;
             }
-            if (a.gate) {
-                const uint4* g = reinterpret_cast<const uint4*>(a.gate) + static_cast<size_t>(q) * (a.cout_store / 8);
+            tc::fence_after_sync();
+            float acc[NC];
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    if (h * 8 >= a.cout_store) break;
-                    const uint4 gv = __ldg(g + h);
-                    const __nv_bfloat16* gb = reinterpret_cast<const __nv_bfloat16*>(&gv);
+            for (int c = 0; c < NC; c += 16) tc::tmem_load16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(b * NC + c), acc + c);
+            tc::fence_before_sync();
+            tc::mbar_arrive(&drained[b]);
+            const uint32_t tile = blockIdx.x + jl * gridDim.x;
+            const int tx = static_cast<int>(tile % ntx), rest = static_cast<int>(tile / ntx);
+            const int x = tx * kTX + (t & 7), y = (rest % nty) * kTY + (t >> 3), z = rest / nty;
+            if (x < a.nx && y < a.ny) {
+                const uint32_t q = (static_cast<uint32_t>(z) * a.ny + y) * a.nx + x;
 #pragma unroll
-                    for (int c = 0; c < 8; ++c)
-                        if (!(__bfloat162float(gb[c]) > 0.0f)) v[h * 8 + c] = 0.0f;
+                for (int c = 0; c < NC; ++c) {
+                    acc[c] += bias[c];
+                    if (a.relu) acc[c] = fmaxf(acc[c], 0.0f);
+                }
+                if (a.gate) {
+                    const uint4* g = reinterpret_cast<const uint4*>(a.gate + static_cast<size_t>(q) * a.cout_store + n0);
+#pragma unroll
+                    for (int h = 0; h < NC / 8; ++h) {
+                        const uint4 gv = __ldg(g + h);
+                        const __nv_bfloat16* gb = reinterpret_cast<const __nv_bfloat16*>(&gv);
+#pragma unroll
+                        for (int c = 0; c < 8; ++c)
+                            if (!(__bfloat162float(gb[c]) > 0.0f)) acc[h * 8 + c] = 0.0f;
+                    }
+                }
+                if (a.out_f32 && chunk == 0) a.out_f32[q] = acc[0];
+                if (a.out) {
+                    uint4* o = reinterpret_cast<uint4*>(a.out + static_cast<size_t>(q) * a.cout_store + n0);
+#pragma unroll
+                    for (int h = 0; h < NC / 8; ++h)
+                        o[h] = make_uint4(pack_bf16x2(acc[8 * h], acc[8 * h + 1]), pack_bf16x2(acc[8 * h + 2], acc[8 * h + 3]), pack_bf16x2(acc[8 * h + 4], acc[8 * h + 5]),
+                                          pack_bf16x2(acc[8 * h + 6], acc[8 * h + 7]));
                 }
             }
-            if (a.out_f32) a.out_f32[q] = v[0];
-            if (a.out) {
-                uint4* o = reinterpret_cast<uint4*>(a.out) + static_cast<size_t>(q) * (a.cout_store / 8);
-                o[0] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
-                if (a.cout_store == 16) o[1] = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]), pack_bf16x2(v[14], v[15]));
-            }
         }
-        tc::fence_before_sync();
-        __syncthreads();  // this accumulator is read out before tile j + 2's MMAs overwrite it
-        tc::fence_after_sync();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (warp == 0) tc::tmem_free(tmem, 32);
+    if (warp == 0) tc::tmem_free(tmem, S::kTmemCols);
 }
 
-// Operand image of B (N = 16 rows = output channels, K = taps x stored input channels), K-major core matrices:
-// element (co, k) at byte ((k / 8) * 2 + co / 8) * 128 + (co % 8) * 16 + (k % 8) * 2.
-__global__ void pack_conv_kernel(const float* __restrict__ w, int cin, int cout, int transpose, uint8_t* __restrict__ pack) {
+// Operand image of B for a convolution whose input has `cs` stored channels: K = taps x cs rows (tap-major), N =
+// the output channels in chunks of nc; K-major core matrices, element (co, k) of chunk co / nc at byte
+// ((k / 8) * (nc / 8) + (co % nc) / 8) * 128 + (co % 8) * 16 + (k % 8) * 2 of that chunk's image.
+__global__ void pack_conv_kernel(const float* __restrict__ w, int cin, int cout, int transpose, int cs, uint8_t* __restrict__ pack) {
     const int in_ch = transpose ? cout : cin, out_ch = transpose ? cin : cout;
-    const int store = net_store(in_ch);
-    const int K = conv_taps(store) * store;
-    const int total = K * 16;
+    const int nc = conv_nc(cs, out_ch), cpad = net_cout_pad(out_ch);
+    const int K = conv_taps(cs) * cs;
+    const size_t chunk_bytes = static_cast<size_t>(K) * nc * 2;
+    const int total = K * cpad;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        const int k = i / 16, co = i % 16;
-        const int tap = k / store, ci = k % store;
+        const int k = i / cpad, co = i % cpad;
+        const int tap = k / cs, ci = k % cs;
         float v = 0.0f;
         if (tap < 27 && ci < in_ch && co < out_ch) {
             // forward: W[tap][ci][co]; backward-data: input channel = forward output, mirrored tap
             v = transpose ? w[(static_cast<size_t>(26 - tap) * cin + co) * cout + ci] : w[(static_cast<size_t>(tap) * cin + ci) * cout + co];
         }
-        const size_t off = static_cast<size_t>((k / 8) * 2 + co / 8) * 128 + (co % 8) * 16 + (k % 8) * 2;
+        const int cl = co % nc;
+        const size_t off = (co / nc) * chunk_bytes + static_cast<size_t>((k / 8) * (nc / 8) + cl / 8) * 128 + (cl % 8) * 16 + (k % 8) * 2;
         *reinterpret_cast<__nv_bfloat16*>(pack + off) = __float2bfloat16_rn(v);
     }
 }
 
-// Resident blocks of a kernel that uses `smem` bytes of dynamic shared memory (per SM x SMs): the shared memory of
-// an SM over what one block takes (its dynamic bytes, 1 KB of static data and the 1 KB the system reserves per
-// block), at most 6 (tensor memory: 6 x 64 columns at most of 512). These kernels' 128 threads and < 64 registers
-// never bind first. Cached per kernel and device.
-int resident_blocks(const void* kernel, size_t smem) {
+// Resident blocks of a kernel per device: by shared memory (its dynamic bytes plus about 2 KB of static data and
+// the per-block reservation), by tensor memory (512 columns per SM) and by threads; at most 8 per SM. Cached.
+int resident_blocks(const void* kernel, size_t smem, uint32_t tmem_cols, int threads) {
     static std::mutex lock;
     static std::map<std::pair<const void*, int>, int> cache;
     int dev = 0;
@@ -219,11 +280,14 @@ int resident_blocks(const void* kernel, size_t smem) {
     std::lock_guard<std::mutex> guard(lock);
     auto it = cache.find({kernel, dev});
     if (it != cache.end()) return it->second;
-    int sms = 1, smem_sm = 0;
+    int sms = 1, smem_sm = 0, threads_sm = 2048;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    const int per_sm = std::min(6, std::max(1, smem_sm / static_cast<int>(smem + 2048)));
-    const int r = std::max(1, sms * per_sm);
+    cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    int per_sm = std::max(1, smem_sm / static_cast<int>(smem + 2048));
+    if (tmem_cols > 0) per_sm = std::min(per_sm, static_cast<int>(512u / tmem_cols));
+    per_sm = std::min({per_sm, threads_sm / threads, 8});
+    const int r = std::max(1, sms * std::max(1, per_sm));
     cache.emplace(std::make_pair(kernel, dev), r);
     return r;
 }
@@ -240,107 +304,117 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// Tensor map of a channels-last BF16 volume with `cin` stored channels: dimensions (channel, x, y, z), boxes of
-// 8 channels x the halo of one tile, zeros outside.
-template <int CIN>
-cudaError_t halo_map(CUtensorMap* map, const ConvArgs& a) {
-    using S = ConvShape<CIN>;
+// Tensor map of a channels-last BF16 volume with `cs` stored channels: dimensions (channel, x, y, z), boxes of
+// 8 channels x the halo of one tile, zeros outside. Every box starts at a channel coordinate that is a multiple of
+// 8 (16 bytes).
+cudaError_t halo_map(CUtensorMap* map, int cs, const ConvArgs& a) {
     const auto encode = tensor_map_encoder();
     if (encode == nullptr) return cudaErrorNotSupported;
-    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(CIN), static_cast<cuuint64_t>(a.nx), static_cast<cuuint64_t>(a.ny), static_cast<cuuint64_t>(a.nz)};
-    const cuuint64_t strides[3] = {static_cast<cuuint64_t>(CIN) * 2, static_cast<cuuint64_t>(a.nx) * CIN * 2, static_cast<cuuint64_t>(a.nx) * a.ny * CIN * 2};
-    const cuuint32_t box[4] = {8, S::kHX, S::kHY, S::kHZ};
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(cs), static_cast<cuuint64_t>(a.nx), static_cast<cuuint64_t>(a.ny), static_cast<cuuint64_t>(a.nz)};
+    const cuuint64_t strides[3] = {static_cast<cuuint64_t>(cs) * 2, static_cast<cuuint64_t>(a.nx) * cs * 2, static_cast<cuuint64_t>(a.nx) * a.ny * cs * 2};
+    const cuuint32_t box[4] = {8, kHX, kHY, kHZ};
     const cuuint32_t step[4] = {1, 1, 1, 1};
     const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(a.in), dims, strides, box, step, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-template <int CIN>
-cudaError_t conv_typed(const VolumeDims& d, const ConvArgs& a, cudaStream_t s) {
-    using S = ConvShape<CIN>;
-    static bool configured = false;
-    if (!configured) {  // all of the unified L1 as shared memory, so that several blocks fit on an SM
-        cudaError_t e = cudaFuncSetAttribute(conv3_kernel<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::kSmem));
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(conv3_kernel<CIN>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+template <int CS, int NC>
+cudaError_t conv_typed(const VolumeDims& d, int chunks, const ConvArgs& a, cudaStream_t s) {
+    using S = ConvShape<CS, NC>;
+    static std::once_flag once;
+    static cudaError_t configured = cudaSuccess;
+    std::call_once(once, [] {  // all of the unified L1 as shared memory, so that several blocks fit on an SM
+        configured = cudaFuncSetAttribute(conv3_kernel<CS, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::kSmem));
+        if (configured == cudaSuccess) configured = cudaFuncSetAttribute(conv3_kernel<CS, NC>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    });
+    if (configured != cudaSuccess) return configured;
     if ((reinterpret_cast<uintptr_t>(a.in) & 15u) != 0) return cudaErrorMisalignedAddress;
     CUtensorMap map;
-    const cudaError_t e = halo_map<CIN>(&map, a);
+    const cudaError_t e = halo_map(&map, CS, a);
     if (e != cudaSuccess) return e;
-    const uint64_t tiles = static_cast<uint64_t>((d.nx + S::kTX - 1) / S::kTX) * ((d.ny + S::kTY - 1) / S::kTY) * d.nz;
-    const int grid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(resident_blocks(reinterpret_cast<const void*>(conv3_kernel<CIN>), S::kSmem))));
-    conv3_kernel<CIN><<<grid, kConvThreads, S::kSmem, s>>>(a, map);
+    const uint64_t tiles = static_cast<uint64_t>((d.nx + kTX - 1) / kTX) * ((d.ny + kTY - 1) / kTY) * d.nz;
+    const int resident = resident_blocks(reinterpret_cast<const void*>(conv3_kernel<CS, NC>), S::kSmem, S::kTmemCols, kConvThreads);
+    const int gx = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(tiles, static_cast<uint64_t>(std::max(1, resident / chunks)))));
+    conv3_kernel<CS, NC><<<dim3(gx, chunks), kConvThreads, S::kSmem, s>>>(a, map);
     return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------------------------------ weight gradient
-// dW[tap][ci][co] = sum over cells q of in[q + offset(tap)][ci] * g[q][co], as a GEMM with M = (tap, ci) (taps padded
-// to 32: M-tiles of 128 rows), N = 16 (co), K = cells. Both operands are MN-major in shared memory: a core matrix is
-// 8 cells (K) x 16 bytes = 8 consecutive channels, so every 16-byte channel vector lands as one core-matrix row.
-// Row (tap 27, channel 0) of A is 1 for every cell, which makes D[27 * CIN][co] the bias gradient sum_q g[q][co].
-// Every block accumulates its share of the cells in tensor memory and writes its partial D; wgrad_reduce sums them.
+// dW[tap][ci][co] = sum over cells q of in[q + offset(tap)][ci] * g[q][co], as a GEMM with M = (tap, ci) rows
+// (row tap * CS + ci; row 27 * CS is 1 for every cell, which makes its D row the bias gradient sum_q g[q][co]; M
+// padded to a multiple of 128), N = GN gradient channels, K = cells. Both operands are MN-major in shared memory: a
+// core matrix is 8 cells (K) x 16 bytes = 8 consecutive channels, so every 16-byte channel vector lands as one
+// core-matrix row. A block owns MT M-tiles (blockIdx.y picks which) and a share of the cells (blockIdx.x), keeps
+// its D in tensor memory and writes it as a partial sum; wgrad_reduce adds the partials.
 constexpr int kWgradCells = 64;  // cells (K) per gather round: 8 core-matrix groups, 4 MMA K-steps
+constexpr int kWgradMaxBlocksX = 296;
 
-template <int CIN>
+__host__ __device__ constexpr int wgrad_mpad(int cs) { return ((27 * cs + 1 + 127) / 128) * 128; }
+__host__ __device__ constexpr int wgrad_mt(int gn) { return gn >= 128 ? 2 : 4; }
+
+template <int CS, int GN>
 struct WgradShape {
-    static constexpr int kMPad = 32 * CIN;                 // 256 or 512 rows
-    static constexpr int kMTiles = kMPad / 128;            // 2 or 4
-    static constexpr int kMGroups = kMPad / 8;             // core matrices along M
+    static constexpr int kMPad = wgrad_mpad(CS);
+    static constexpr int kMT = wgrad_mt(GN);             // M-tiles per block
+    static constexpr int kMGroups = kMT * 16;            // core matrices along M per block
     static constexpr uint32_t kABytes = (kWgradCells / 8) * kMGroups * 128u;
-    static constexpr uint32_t kARegion = kABytes;
-    static constexpr uint32_t kBBytes = (kWgradCells / 8) * 2u * 128u;
-    static constexpr uint32_t kBRegion = kBBytes;
-    static constexpr uint32_t kSmem = kARegion + kBRegion;
-    static constexpr uint32_t kTmemCols = kMTiles * 16 <= 32 ? 32u : 64u;
+    static constexpr uint32_t kBBytes = (kWgradCells / 8) * (GN / 8) * 128u;
+    static constexpr uint32_t kSmem = kABytes + kBBytes;
+    static constexpr uint32_t kTmemCols = kMT * GN;      // 64..256
+    static_assert(kTmemCols >= 32 && kTmemCols <= 256 && (kTmemCols & (kTmemCols - 1)) == 0, "tensor memory columns");
+    // dynamic shared memory requested at launch: blocks of 256 tensor-memory columns ask for enough that at most two
+    // fit on an SM (2 x 256 = all 512 columns), so no block's allocation waits for another's
+    static constexpr uint32_t kSmemLaunch = kTmemCols >= 256 && kSmem < 80u * 1024u ? 80u * 1024u : kSmem;
 };
 
 struct WgradArgs {
-    const __nv_bfloat16* in;  // [n][CIN]
-    const __nv_bfloat16* g;   // [n][gc]
-    float* partial;           // [gridDim.x][kMPad][16]
+    const __nv_bfloat16* in;  // [n][CS]
+    const __nv_bfloat16* g;   // [n][GN]
+    float* partial;           // [gridDim.x][kMPad][GN]
     unsigned* error;
-    int gc;                   // stored channels of g (8 or 16)
     int nx, ny, nz;
     uint32_t n;
 };
 
-template <int CIN>
-__global__ void __launch_bounds__(kConvThreads) wgrad_kernel(const __grid_constant__ WgradArgs a) {
-    using S = WgradShape<CIN>;
+template <int CS, int GN>
+__global__ void __launch_bounds__(kEpiThreads) wgrad_kernel(const __grid_constant__ WgradArgs a) {
+    using S = WgradShape<CS, GN>;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* As = smem;
-    uint8_t* Bs = smem + S::kARegion;
+    uint8_t* Bs = smem + S::kABytes;
     __shared__ uint64_t bar;
     __shared__ uint32_t tmem_slot;
     const int t = threadIdx.x, warp = t >> 5;
-    constexpr int kCg = CIN / 8;
-    // rows of taps 27..31 are constant: zero, except channel 0 of tap 27, which is 1 (bias gradient)
-    for (int i = t; i < (kWgradCells / 8) * (S::kMGroups - 27 * kCg) * 8; i += kConvThreads) {
+    constexpr int kCg = CS / 8;
+    constexpr int kRealGroups = 27 * kCg;                        // row groups read from the input
+    const int g0 = blockIdx.y * S::kMGroups;                     // first row group of this block
+    const int m_tiles = min(S::kMT, S::kMPad / 128 - static_cast<int>(blockIdx.y) * S::kMT);
+    // constant row groups (bias row, padding): 1 in channel 0 of group 27 * kCg, zero elsewhere
+    for (int i = t; i < (kWgradCells / 8) * S::kMGroups * 8; i += kEpiThreads) {
         const int row = i % 8, rest = i / 8;
-        const int kg = rest % (kWgradCells / 8), mg = 27 * kCg + rest / (kWgradCells / 8);
-        const uint32_t one = mg == 27 * kCg ? 0x3F80u : 0u;  // BF16 1.0 in channel 0
+        const int kg = rest % (kWgradCells / 8), mg = rest / (kWgradCells / 8);
+        if (g0 + mg < kRealGroups) continue;
+        const uint32_t one = g0 + mg == kRealGroups ? 0x3F80u : 0u;  // BF16 1.0 in channel 0
         *reinterpret_cast<uint4*>(As + (kg * S::kMGroups + mg) * 128 + row * 16) = make_uint4(one, 0, 0, 0);
     }
-    for (int i = t; i < static_cast<int>(S::kBBytes / 16u); i += kConvThreads) reinterpret_cast<uint4*>(Bs)[i] = make_uint4(0, 0, 0, 0);
     if (t == 0) tc::mbar_init(&bar, 1);
     if (warp == 0) tc::tmem_alloc(&tmem_slot, S::kTmemCols);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
-    constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 16, true, true);
+    constexpr uint32_t idesc = tc::idesc_bf16_f32(128, GN, true, true);
     const uint32_t a_base = tc::smem_addr(As), b_base = tc::smem_addr(Bs);
     const uint32_t chunks = (a.n + kWgradCells - 1) / kWgradCells;
+    const int real_here = max(0, min(S::kMGroups, kRealGroups - g0));  // input row groups of this block
     uint32_t phase = 0;
     bool any = false, ok = true;
     for (uint32_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x) {
         const uint32_t q0 = chunk * kWgradCells;
-        for (int i = t; i < kWgradCells * 27 * kCg; i += kConvThreads) {
-            const int cell = i % kWgradCells, rest = i / kWgradCells;
-            const int tap = rest / kCg, cg = rest % kCg;
+        for (int i = t; i < kWgradCells * real_here; i += kEpiThreads) {
+            const int cell = i % kWgradCells, mg = i / kWgradCells;
+            const int G = g0 + mg, tap = G / kCg, cg = G % kCg;
             const uint32_t q = q0 + cell;
             bool inside = q < a.n;
             uint32_t nq = 0;
@@ -353,14 +427,13 @@ __global__ void __launch_bounds__(kConvThreads) wgrad_kernel(const __grid_consta
                 nq = inside ? (static_cast<uint32_t>(z) * a.ny + y) * a.nx + x : 0u;
             }
             const uint4 v = inside ? __ldg(reinterpret_cast<const uint4*>(a.in) + static_cast<size_t>(nq) * kCg + cg) : make_uint4(0, 0, 0, 0);
-            const int mg = tap * kCg + cg, kg = cell / 8;
-            *reinterpret_cast<uint4*>(As + (kg * S::kMGroups + mg) * 128 + (cell % 8) * 16) = v;
+            *reinterpret_cast<uint4*>(As + ((cell / 8) * S::kMGroups + mg) * 128 + (cell % 8) * 16) = v;
         }
-        for (int i = t; i < kWgradCells * (a.gc / 8); i += kConvThreads) {
+        for (int i = t; i < kWgradCells * (GN / 8); i += kEpiThreads) {
             const int cell = i % kWgradCells, ng = i / kWgradCells;
             const uint32_t q = q0 + cell;
-            const uint4 v = q < a.n ? __ldg(reinterpret_cast<const uint4*>(a.g) + static_cast<size_t>(q) * (a.gc / 8) + ng) : make_uint4(0, 0, 0, 0);
-            *reinterpret_cast<uint4*>(Bs + ((cell / 8) * 2 + ng) * 128 + (cell % 8) * 16) = v;
+            const uint4 v = q < a.n ? __ldg(reinterpret_cast<const uint4*>(a.g) + static_cast<size_t>(q) * (GN / 8) + ng) : make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4*>(Bs + ((cell / 8) * (GN / 8) + ng) * 128 + (cell % 8) * 16) = v;
         }
         tc::fence_async_smem();
         tc::fence_before_sync();
@@ -368,13 +441,13 @@ __global__ void __launch_bounds__(kConvThreads) wgrad_kernel(const __grid_consta
         tc::fence_after_sync();
         if (t == 0) {
 #pragma unroll 1
-            for (int mt = 0; mt < S::kMTiles; ++mt)
+            for (int mt = 0; mt < m_tiles; ++mt)
 #pragma unroll 1
                 for (int k = 0; k < kWgradCells / 16; ++k) {
                     // K step k: cell groups 2k, 2k + 1 (LBO: next cell group); SBO: next 8 rows of M (or N)
                     const uint64_t ad = tc::smem_desc(a_base + (2 * k * S::kMGroups + mt * 16) * 128u, S::kMGroups * 128u, 128u);
-                    const uint64_t bd = tc::smem_desc(b_base + (2 * k * 2) * 128u, 256u, 128u);
-                    tc::mma_bf16(tmem + mt * 16, ad, bd, idesc, (any || k > 0) ? 1u : 0u);
+                    const uint64_t bd = tc::smem_desc(b_base + (2 * k * (GN / 8)) * 128u, (GN / 8) * 128u, 128u);
+                    tc::mma_bf16(tmem + static_cast<uint32_t>(mt * GN), ad, bd, idesc, (any || k > 0) ? 1u : 0u);
                 }
             tc::commit(&bar);
         }
@@ -383,23 +456,29 @@ __global__ void __launch_bounds__(kConvThreads) wgrad_kernel(const __grid_consta
         phase ^= 1u;
         any = true;
         if (!ok) {
-            if (t == 0) atomicOr(a.error, 1u);
+            if (t == 0) {
+                atomicOr(a.error, 1u);
+                tc::mbar_wait(&bar, phase ^ 1u, kSpinCycles);  // once more, so no MMA is left running at exit
+            }
             break;
         }
         tc::fence_after_sync();
     }
-    float* out = a.partial + static_cast<size_t>(blockIdx.x) * S::kMPad * 16;
-    for (int mt = 0; mt < S::kMTiles; ++mt) {
-        float v[16];
-        if (any && ok) {
-            tc::tmem_load16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + mt * 16, v);
-        } else {
+    float* out = a.partial + static_cast<size_t>(blockIdx.x) * S::kMPad * GN;
+    for (int mt = 0; mt < m_tiles; ++mt) {
+        const int row = (blockIdx.y * S::kMT + mt) * 128 + t;
+        for (int c = 0; c < GN; c += 16) {
+            float v[16];
+            if (any && ok) {
+                tc::tmem_load16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(mt * GN + c), v);
+            } else {
 #pragma unroll
-            for (int c = 0; c < 16; ++c) v[c] = 0.0f;
+                for (int i = 0; i < 16; ++i) v[i] = 0.0f;
+            }
+            float4* o = reinterpret_cast<float4*>(out + static_cast<size_t>(row) * GN + c);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
         }
-        float4* o = reinterpret_cast<float4*>(out + static_cast<size_t>(mt * 128 + t) * 16);
-#pragma unroll
-        for (int c = 0; c < 4; ++c) o[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -407,22 +486,22 @@ __global__ void __launch_bounds__(kConvThreads) wgrad_kernel(const __grid_consta
     if (warp == 0) tc::tmem_free(tmem, S::kTmemCols);
 }
 
-// grad[w(tap, ci, co)] (+)= sum over blocks of partial[b][tap * cin_store + ci][co]; grad[bias co] likewise from
-// row 27 * cin_store.
-__global__ void wgrad_reduce_kernel(const float* __restrict__ partial, int blocks, int m_pad, int cin_store, int cin, int cout, int accumulate, float* __restrict__ grad) {
+// grad[w(tap, ci, co)] (+)= sum over blocks of partial[b][tap * cs + ci][co]; grad[bias co] likewise from row
+// 27 * cs.
+__global__ void wgrad_reduce_kernel(const float* __restrict__ partial, int blocks, int m_pad, int gn, int cs, int cin, int cout, int accumulate, float* __restrict__ grad) {
     const int wcount = 27 * cin * cout;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < wcount + cout; i += gridDim.x * blockDim.x) {
         int row, co;
         if (i < wcount) {
             co = i % cout;
             const int ci = (i / cout) % cin, tap = i / (cout * cin);
-            row = tap * cin_store + ci;
+            row = tap * cs + ci;
         } else {
             co = i - wcount;
-            row = 27 * cin_store;
+            row = 27 * cs;
         }
         float sum = 0.0f;
-        for (int b = 0; b < blocks; ++b) sum += partial[(static_cast<size_t>(b) * m_pad + row) * 16 + co];
+        for (int b = 0; b < blocks; ++b) sum += partial[(static_cast<size_t>(b) * m_pad + row) * gn + co];
         grad[i] = accumulate ? grad[i] + sum : sum;
     }
 }
@@ -584,7 +663,7 @@ __global__ void net_output_kernel(VolumeDims d, const float* __restrict__ y, con
 }
 
 // Loss of one sample: L = sum_fluid (y - s t)^2 / sum_fluid (s t)^2 (s the input scale); dy = dL/dy into channel 0 of
-// gy ([n][8] BF16), L added into *loss. tt = sum_fluid t^2 (from sumsq of the masked target).
+// gy ([n][16] BF16, the other channels 0), L added into *loss. tt = sum_fluid t^2 (from sumsq of the masked target).
 __global__ void net_loss_kernel(VolumeDims d, const float* __restrict__ y, const float* __restrict__ target, const uint8_t* __restrict__ occ, const double* __restrict__ norm2, const double* __restrict__ tt, __nv_bfloat16* __restrict__ gy, double* __restrict__ loss) {
     const double nn = *norm2;
     const double s = nn > 0.0 ? sqrt(static_cast<double>(d.n) / nn) : 0.0;
@@ -595,8 +674,10 @@ __global__ void net_loss_kernel(VolumeDims d, const float* __restrict__ y, const
         const bool fluid = occ[q] == 0;
         const float e = fluid ? y[q] - static_cast<float>(s) * target[q] : 0.0f;
         l += static_cast<double>(e) * e;
-        float v[8] = {scale * e, 0, 0, 0, 0, 0, 0, 0};
-        store_bf16x8(gy + static_cast<size_t>(q) * 8, v);
+        const float v[8] = {scale * e, 0, 0, 0, 0, 0, 0, 0};
+        const float z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        store_bf16x8(gy + static_cast<size_t>(q) * 16, v);
+        store_bf16x8(gy + static_cast<size_t>(q) * 16 + 8, z);
     }
     for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
     if ((threadIdx.x & 31) == 0 && denom > 0.0) atomicAdd(loss, l / denom);
@@ -620,17 +701,18 @@ __global__ void adam_kernel(int count, float* __restrict__ w, const float* __res
     }
 }
 
-// bias16[c] = bias[c] for c < cout, else 0
-__global__ void bias16_kernel(const float* __restrict__ bias, int cout, float* __restrict__ out) {
-    const int c = threadIdx.x;
-    if (c < 16) out[c] = c < cout ? bias[c] : 0.0f;
+// padded bias: out[c] = bias[c] for c < cout, else 0 (cpad entries)
+__global__ void bias_pad_kernel(const float* __restrict__ bias, int cout, int cpad, float* __restrict__ out) {
+    for (int c = threadIdx.x; c < cpad; c += blockDim.x) out[c] = c < cout ? bias[c] : 0.0f;
 }
 
 }  // namespace
 
-cudaError_t launch_conv3(const VolumeDims& d, int cin_store, const __nv_bfloat16* in, const uint8_t* wpack, const float* bias, int relu, const __nv_bfloat16* gate, __nv_bfloat16* out, int cout_store, float* out_f32, unsigned* error, cudaStream_t s, const uint32_t* skip) {
+cudaError_t launch_conv3(const VolumeDims& d, int cin_store, int cout, const __nv_bfloat16* in, const uint8_t* wpack, const float* bias, int relu, const __nv_bfloat16* gate, __nv_bfloat16* out,
+                         int cout_store, float* out_f32, unsigned* error, cudaStream_t s, const uint32_t* skip, long long wait_cycles, int drop_loads) {
     if (d.n == 0) return cudaSuccess;
-    if ((cin_store != 8 && cin_store != 16) || (cout_store != 8 && cout_store != 16) || error == nullptr) return cudaErrorInvalidValue;
+    const int nc = conv_nc(cin_store, cout), cpad = net_cout_pad(cout);
+    if (error == nullptr || cout < 1 || cout > 128 || (out != nullptr && (cout_store < cpad || cout_store % 8 != 0)) || (gate != nullptr && cout_store < cpad)) return cudaErrorInvalidValue;
     ConvArgs a{};
     a.in = in;
     a.wpack = wpack;
@@ -640,17 +722,30 @@ cudaError_t launch_conv3(const VolumeDims& d, int cin_store, const __nv_bfloat16
     a.out_f32 = out_f32;
     a.error = error;
     a.skip = skip;
+    a.wait_cycles = wait_cycles;
+    a.drop_loads = drop_loads;
     a.relu = relu;
     a.cout_store = cout_store;
     a.nx = d.nx;
     a.ny = d.ny;
     a.nz = d.nz;
     a.n = d.n;
-    return cin_store == 8 ? conv_typed<8>(d, a, s) : conv_typed<16>(d, a, s);
+    const int chunks = cpad / nc;
+    switch (cin_store * 1000 + nc) {
+        case 8016: return conv_typed<8, 16>(d, chunks, a, s);
+        case 16016: return conv_typed<16, 16>(d, chunks, a, s);
+        case 16032: return conv_typed<16, 32>(d, chunks, a, s);
+        case 32016: return conv_typed<32, 16>(d, chunks, a, s);
+        case 32032: return conv_typed<32, 32>(d, chunks, a, s);
+        case 64016: return conv_typed<64, 16>(d, chunks, a, s);
+        case 64032: return conv_typed<64, 32>(d, chunks, a, s);
+        case 128016: return conv_typed<128, 16>(d, chunks, a, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
-cudaError_t launch_pack_conv(const float* w, int cin, int cout, int transpose, uint8_t* pack, cudaStream_t s) {
-    pack_conv_kernel<<<32, 256, 0, s>>>(w, cin, cout, transpose, pack);
+cudaError_t launch_pack_conv(const float* w, int cin, int cout, int transpose, int cin_store, uint8_t* pack, cudaStream_t s) {
+    pack_conv_kernel<<<64, 256, 0, s>>>(w, cin, cout, transpose, cin_store, pack);
     return cudaGetLastError();
 }
 
@@ -661,59 +756,86 @@ namespace {
 constexpr int kGlueThreads = 256;
 unsigned glue_blocks(uint32_t n) { return std::max(1u, std::min<uint32_t>((n + kGlueThreads - 1) / kGlueThreads, 148u * 8u)); }
 
-template <int CIN>
-cudaError_t wgrad_typed(const VolumeDims& d, const WgradArgs& a, int blocks, cudaStream_t s) {
-    using S = WgradShape<CIN>;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(wgrad_kernel<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::kSmem));
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(wgrad_kernel<CIN>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
-    wgrad_kernel<CIN><<<blocks, kConvThreads, S::kSmem, s>>>(a);
-    return cudaGetLastError();
-}
-
-// Blocks of the weight-gradient kernel for a volume of n cells (at most one per SM: the partials buffer holds
-// kWgradMaxBlocks of them).
-constexpr int kWgradMaxBlocks = 160;
-int wgrad_blocks(uint32_t n) {
+// Blocks of the weight-gradient kernel along the cells for a volume of n cells and gy M-chunks.
+int wgrad_blocks_x(uint32_t n, int gy) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t chunks = (n + kWgradCells - 1) / kWgradCells;
-    return static_cast<int>(std::max<uint32_t>(1u, std::min<uint32_t>({chunks, static_cast<uint32_t>(sms), static_cast<uint32_t>(kWgradMaxBlocks)})));
+    const uint32_t want = static_cast<uint32_t>(std::max(1, 2 * sms / gy));
+    return static_cast<int>(std::max<uint32_t>(1u, std::min<uint32_t>({chunks, want, static_cast<uint32_t>(kWgradMaxBlocksX)})));
+}
+int wgrad_gy(int cs, int gn) { return (wgrad_mpad(cs) / 128 + wgrad_mt(gn) - 1) / wgrad_mt(gn); }
+
+template <int CS, int GN>
+cudaError_t wgrad_typed(const WgradArgs& a, int bx, cudaStream_t s) {
+    using S = WgradShape<CS, GN>;
+    static std::once_flag once;
+    static cudaError_t configured = cudaSuccess;
+    std::call_once(once, [] {
+        configured = cudaFuncSetAttribute(wgrad_kernel<CS, GN>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::kSmemLaunch));
+        if (configured == cudaSuccess) configured = cudaFuncSetAttribute(wgrad_kernel<CS, GN>, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    });
+    if (configured != cudaSuccess) return configured;
+    wgrad_kernel<CS, GN><<<dim3(bx, wgrad_gy(CS, GN)), kEpiThreads, S::kSmemLaunch, s>>>(a);
+    return cudaGetLastError();
 }
 
 // Layer L's weight and bias gradient from its input `in` and its output-side gradient `g` (pre-activation).
 cudaError_t layer_wgrad(int L, const VolumeDims& d, const __nv_bfloat16* in, const __nv_bfloat16* g, const NetGrads& G, float* grad, int accumulate, unsigned* error, cudaStream_t s) {
-    const int cs = net_store(kNet[L].cin), gs = net_store(kNet[L].cout);
+    const int cs = net_store(kNet[L].cin), gn = net_grad_store(kNet[L].cout);
     WgradArgs a{};
     a.in = in;
     a.g = g;
     a.partial = G.partial;
     a.error = error;
-    a.gc = gs;
     a.nx = d.nx;
     a.ny = d.ny;
     a.nz = d.nz;
     a.n = d.n;
-    const int blocks = wgrad_blocks(d.n);
-    cudaError_t e = cs == 8 ? wgrad_typed<8>(d, a, blocks, s) : wgrad_typed<16>(d, a, blocks, s);
+    const int bx = wgrad_blocks_x(d.n, wgrad_gy(cs, gn));
+    cudaError_t e;
+    switch (cs * 1000 + gn) {
+        case 8016: e = wgrad_typed<8, 16>(a, bx, s); break;
+        case 16032: e = wgrad_typed<16, 32>(a, bx, s); break;
+        case 32064: e = wgrad_typed<32, 64>(a, bx, s); break;
+        case 64128: e = wgrad_typed<64, 128>(a, bx, s); break;
+        case 128064: e = wgrad_typed<128, 64>(a, bx, s); break;
+        case 64032: e = wgrad_typed<64, 32>(a, bx, s); break;
+        case 32016: e = wgrad_typed<32, 16>(a, bx, s); break;
+        case 16016: e = wgrad_typed<16, 16>(a, bx, s); break;
+        default: return cudaErrorInvalidValue;
+    }
     if (e != cudaSuccess) return e;
-    wgrad_reduce_kernel<<<16, 256, 0, s>>>(G.partial, blocks, 32 * cs, cs, kNet[L].cin, kNet[L].cout, accumulate, grad + net_param_offset(L));
+    wgrad_reduce_kernel<<<64, 256, 0, s>>>(G.partial, bx, wgrad_mpad(cs), gn, cs, kNet[L].cin, kNet[L].cout, accumulate, grad + net_param_offset(L));
     return cudaGetLastError();
+}
+
+// Largest partial-sum buffer (floats) any layer's weight gradient needs on a level-0 volume d0: blocks along the
+// cells (at most one per 64 cells of the layer's level, at most kWgradMaxBlocksX) x padded rows x columns.
+size_t wgrad_partial_floats(const VolumeDims& d0) {
+    VolumeDims d = d0;
+    size_t most = 0;
+    for (int level = 0; level < kNetLevels; ++level) {
+        const size_t bx = std::min<size_t>((d.n + kWgradCells - 1) / kWgradCells, kWgradMaxBlocksX);
+        for (int L = 0; L < kNetLayers; ++L) {
+            if (kNet[L].level != level) continue;
+            const int cs = net_store(kNet[L].cin), gn = net_grad_store(kNet[L].cout);
+            most = std::max(most, std::max<size_t>(bx, 1) * wgrad_mpad(cs) * gn);
+        }
+        d = coarse_dims(d);
+    }
+    return most;
 }
 
 cudaError_t conv_layer(int L, const VolumeDims& d, const NetImages& I, const __nv_bfloat16* in, __nv_bfloat16* out, float* out_f32, unsigned* error, cudaStream_t s, const uint32_t* skip = nullptr) {
     const int relu = L < kNetLayers - 1;
-    return launch_conv3(d, net_store(kNet[L].cin), in, I.fwd[L], I.bias16[L], relu, nullptr, out, net_store(kNet[L].cout), out_f32, error, s, skip);
+    return launch_conv3(d, net_store(kNet[L].cin), kNet[L].cout, in, I.fwd[L], I.bias[L], relu, nullptr, out, net_store(kNet[L].cout), out_f32, error, s, skip);
 }
 // Gradient through layer L's convolution: gin = conv^T(g), gated by `gate` (the layer's input activation when it is
 // a ReLU output consumed only by this layer).
 cudaError_t conv_layer_bwd(int L, const VolumeDims& d, const NetImages& I, const __nv_bfloat16* g, const __nv_bfloat16* gate, __nv_bfloat16* gin, unsigned* error, cudaStream_t s) {
-    return launch_conv3(d, net_store(kNet[L].cout), g, I.bwd[L], nullptr, 0, gate, gin, net_store(kNet[L].cin), nullptr, error, s, nullptr);
+    return launch_conv3(d, net_grad_store(kNet[L].cout), kNet[L].cin, g, I.bwd[L], nullptr, 0, gate, gin, net_store(kNet[L].cin), nullptr, error, s, nullptr);
 }
 
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
@@ -723,9 +845,9 @@ size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 size_t net_images_bytes() {
     size_t b = 0;
     for (int L = 0; L < kNetLayers; ++L) {
-        b += align256(conv_pack_bytes(net_store(kNet[L].cin)));
-        if (L > 0) b += align256(conv_pack_bytes(net_store(kNet[L].cout)));
-        b += align256(16 * sizeof(float));
+        b += align256(conv_pack_bytes(net_store(kNet[L].cin), kNet[L].cout));
+        if (L > 0) b += align256(conv_pack_bytes(net_grad_store(kNet[L].cout), kNet[L].cin));
+        b += align256(net_cout_pad(kNet[L].cout) * sizeof(float));
     }
     return b;
 }
@@ -734,24 +856,24 @@ void net_images_bind(NetImages& I, void* base) {
     char* p = static_cast<char*>(base);
     for (int L = 0; L < kNetLayers; ++L) {
         I.fwd[L] = reinterpret_cast<uint8_t*>(p);
-        p += align256(conv_pack_bytes(net_store(kNet[L].cin)));
+        p += align256(conv_pack_bytes(net_store(kNet[L].cin), kNet[L].cout));
         I.bwd[L] = nullptr;
         if (L > 0) {
             I.bwd[L] = reinterpret_cast<uint8_t*>(p);
-            p += align256(conv_pack_bytes(net_store(kNet[L].cout)));
+            p += align256(conv_pack_bytes(net_grad_store(kNet[L].cout), kNet[L].cin));
         }
-        I.bias16[L] = reinterpret_cast<float*>(p);
-        p += align256(16 * sizeof(float));
+        I.bias[L] = reinterpret_cast<float*>(p);
+        p += align256(net_cout_pad(kNet[L].cout) * sizeof(float));
     }
 }
 
 cudaError_t net_pack(const float* w, const NetImages& I, cudaStream_t s) {
     for (int L = 0; L < kNetLayers; ++L) {
         const float* wl = w + net_param_offset(L);
-        cudaError_t e = launch_pack_conv(wl, kNet[L].cin, kNet[L].cout, 0, I.fwd[L], s);
-        if (e == cudaSuccess && L > 0) e = launch_pack_conv(wl, kNet[L].cin, kNet[L].cout, 1, I.bwd[L], s);
+        cudaError_t e = launch_pack_conv(wl, kNet[L].cin, kNet[L].cout, 0, net_store(kNet[L].cin), I.fwd[L], s);
+        if (e == cudaSuccess && L > 0) e = launch_pack_conv(wl, kNet[L].cin, kNet[L].cout, 1, net_grad_store(kNet[L].cout), I.bwd[L], s);
         if (e != cudaSuccess) return e;
-        bias16_kernel<<<1, 32, 0, s>>>(wl + net_weight_count(L), kNet[L].cout, I.bias16[L]);
+        bias_pad_kernel<<<1, 128, 0, s>>>(wl + net_weight_count(L), kNet[L].cout, net_cout_pad(kNet[L].cout), I.bias[L]);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -762,17 +884,18 @@ namespace {
 struct Slot {
     int level, channels;
 };
-constexpr Slot kActSlots[] = {{0, 8}, {0, 8}, {0, 8}, {0, 8}, {1, 8}, {1, 8}, {1, 16}, {1, 16}, {2, 16}, {2, 16}};
-constexpr Slot kGradSlots[] = {{0, 8}, {0, 8}, {0, 8}, {0, 8}, {1, 8}, {1, 8}, {1, 16}, {1, 16}, {2, 16}, {2, 16}};
-void levels_of(const VolumeDims& d0, VolumeDims d[3]) {
+constexpr Slot kActSlots[] = {{0, 8}, {0, 16}, {0, 16}, {1, 16}, {1, 16}, {1, 32}, {1, 32}, {2, 32}, {2, 32}, {2, 64}, {2, 64}, {3, 64}, {3, 64}, {3, 128}};
+constexpr Slot kGradSlots[] = {{0, 16}, {0, 16}, {0, 16}, {1, 16}, {1, 16}, {1, 32}, {1, 32}, {2, 32}, {2, 32}, {2, 64}, {2, 64}, {3, 64}, {3, 64}, {3, 128}};
+constexpr int kActCount = sizeof(kActSlots) / sizeof(kActSlots[0]);
+constexpr int kGradCount = sizeof(kGradSlots) / sizeof(kGradSlots[0]);
+void levels_of(const VolumeDims& d0, VolumeDims d[kNetLevels]) {
     d[0] = d0;
-    d[1] = coarse_dims(d[0]);
-    d[2] = coarse_dims(d[1]);
+    for (int l = 1; l < kNetLevels; ++l) d[l] = coarse_dims(d[l - 1]);
 }
 }  // namespace
 
 size_t net_acts_bytes(const VolumeDims& d0) {
-    VolumeDims d[3];
+    VolumeDims d[kNetLevels];
     levels_of(d0, d);
     size_t b = 0;
     for (const Slot& sl : kActSlots) b += align256(static_cast<size_t>(d[sl.level].n) * sl.channels * 2);
@@ -782,8 +905,8 @@ size_t net_acts_bytes(const VolumeDims& d0) {
 void net_acts_bind(NetActs& A, void* base, const VolumeDims& d0) {
     levels_of(d0, A.d);
     char* p = static_cast<char*>(base);
-    __nv_bfloat16** v[] = {&A.x0, &A.e0, &A.s0, &A.d0, &A.p1, &A.d1, &A.e1, &A.s1, &A.p2, &A.e2};
-    for (int i = 0; i < 10; ++i) {
+    __nv_bfloat16** v[kActCount] = {&A.x0, &A.e0, &A.s0, &A.p1, &A.u1, &A.e1, &A.s1, &A.p2, &A.u2, &A.e2, &A.s2, &A.p3, &A.m3, &A.e3};
+    for (int i = 0; i < kActCount; ++i) {
         *v[i] = reinterpret_cast<__nv_bfloat16*>(p);
         p += align256(static_cast<size_t>(A.d[kActSlots[i].level].n) * kActSlots[i].channels * 2);
     }
@@ -795,31 +918,31 @@ void net_acts_bind(NetActs& A, void* base, const VolumeDims& d0) {
 }
 
 size_t net_grads_bytes(const VolumeDims& d0) {
-    VolumeDims d[3];
+    VolumeDims d[kNetLevels];
     levels_of(d0, d);
     size_t b = 0;
     for (const Slot& sl : kGradSlots) b += align256(static_cast<size_t>(d[sl.level].n) * sl.channels * 2);
-    return b + align256(static_cast<size_t>(kWgradMaxBlocks) * 512 * 16 * 4) + align256(static_cast<size_t>(d0.n) * 4) + align256(16);
+    return b + align256(wgrad_partial_floats(d0) * 4) + align256(static_cast<size_t>(d0.n) * 4) + align256(16);
 }
 
 void net_grads_bind(NetGrads& G, void* base, const VolumeDims& d0) {
-    VolumeDims d[3];
+    VolumeDims d[kNetLevels];
     levels_of(d0, d);
     char* p = static_cast<char*>(base);
-    __nv_bfloat16** v[] = {&G.gy, &G.ge, &G.gs0, &G.ga, &G.gd, &G.gp1, &G.gs1, &G.gb, &G.gc, &G.gp2};
-    for (int i = 0; i < 10; ++i) {
+    __nv_bfloat16** v[kGradCount] = {&G.gy, &G.gs0, &G.ge0, &G.gu1, &G.gp1, &G.gs1, &G.ge1, &G.gu2, &G.gp2, &G.gs2, &G.ge2, &G.gm3, &G.gp3, &G.ge3};
+    for (int i = 0; i < kGradCount; ++i) {
         *v[i] = reinterpret_cast<__nv_bfloat16*>(p);
         p += align256(static_cast<size_t>(d[kGradSlots[i].level].n) * kGradSlots[i].channels * 2);
     }
     G.partial = reinterpret_cast<float*>(p);
-    p += align256(static_cast<size_t>(kWgradMaxBlocks) * 512 * 16 * 4);
+    p += align256(wgrad_partial_floats(d0) * 4);
     G.tmask = reinterpret_cast<float*>(p);
     p += align256(static_cast<size_t>(d0.n) * 4);
     G.sums = reinterpret_cast<double*>(p);
 }
 
 cudaError_t net_forward(const NetImages& I, const NetActs& A, const float* r0, const float* r1, const int* parity, const double* norm2, const uint8_t* occ, cudaStream_t s, const uint32_t* skip) {
-    const VolumeDims *d = A.d;
+    const VolumeDims* d = A.d;
     cudaError_t e;
     if (norm2 == nullptr) {
         if ((e = cudaMemsetAsync(A.norm2, 0, sizeof(double), s)) != cudaSuccess) return e;
@@ -828,16 +951,22 @@ cudaError_t net_forward(const NetImages& I, const NetActs& A, const float* r0, c
     }
     net_input_kernel<<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], r0, r1, parity, norm2, occ, A.x0, skip);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // encoder
     if ((e = conv_layer(0, d[0], I, A.x0, A.e0, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    pool_kernel<8><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[0], d[1], A.e0, A.p1, skip);
+    pool_kernel<16><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[0], d[1], A.e0, A.p1, skip);
     if ((e = conv_layer(1, d[1], I, A.p1, A.e1, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    pool_kernel<16><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[1], d[2], A.e1, A.p2, skip);
+    pool_kernel<32><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[1], d[2], A.e1, A.p2, skip);
     if ((e = conv_layer(2, d[2], I, A.p2, A.e2, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    up_add_kernel<16><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[1], d[2], A.e2, A.e1, A.s1, skip);
-    if ((e = conv_layer(3, d[1], I, A.s1, A.d1, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    up_add_kernel<8><<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], d[1], A.d1, A.e0, A.s0, skip);
-    if ((e = conv_layer(4, d[0], I, A.s0, A.d0, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    return conv_layer(5, d[0], I, A.d0, nullptr, A.y, A.error, s, skip);
+    pool_kernel<64><<<glue_blocks(d[3].n), kGlueThreads, 0, s>>>(d[2], d[3], A.e2, A.p3, skip);
+    if ((e = conv_layer(3, d[3], I, A.p3, A.e3, nullptr, A.error, s, skip)) != cudaSuccess) return e;
+    // bottom and decoder
+    if ((e = conv_layer(4, d[3], I, A.e3, A.m3, nullptr, A.error, s, skip)) != cudaSuccess) return e;
+    up_add_kernel<64><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[2], d[3], A.m3, A.e2, A.s2, skip);
+    if ((e = conv_layer(5, d[2], I, A.s2, A.u2, nullptr, A.error, s, skip)) != cudaSuccess) return e;
+    up_add_kernel<32><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[1], d[2], A.u2, A.e1, A.s1, skip);
+    if ((e = conv_layer(6, d[1], I, A.s1, A.u1, nullptr, A.error, s, skip)) != cudaSuccess) return e;
+    up_add_kernel<16><<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], d[1], A.u1, A.e0, A.s0, skip);
+    return conv_layer(7, d[0], I, A.s0, nullptr, A.y, A.error, s, skip);
 }
 
 cudaError_t net_output(const NetActs& A, const double* norm2, const uint8_t* occ, float* out, cudaStream_t s) {
@@ -854,26 +983,35 @@ cudaError_t net_backward(const NetImages& I, const NetActs& A, const NetGrads& G
     sumsq_kernel<<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(G.tmask, d[0].n, G.sums);
     net_loss_kernel<<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], A.y, target, occ, norm2, G.sums, G.gy, G.sums + 1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    // f: y = conv(d0); e: d0 = relu(conv(s0))
-    if ((e = layer_wgrad(5, d[0], A.d0, G.gy, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
-    if ((e = conv_layer_bwd(5, d[0], I, G.gy, A.d0, G.ge, A.error, s)) != cudaSuccess) return e;
-    if ((e = layer_wgrad(4, d[0], A.s0, G.ge, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
-    if ((e = conv_layer_bwd(4, d[0], I, G.ge, nullptr, G.gs0, A.error, s)) != cudaSuccess) return e;
-    // s0 = up(d1) + e0; d1 = relu(conv_d(s1))
-    up_bwd_relu_kernel<8><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[0], d[1], G.gs0, A.d1, G.gd);
-    if ((e = layer_wgrad(3, d[1], A.s1, G.gd, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
-    if ((e = conv_layer_bwd(3, d[1], I, G.gd, nullptr, G.gs1, A.error, s)) != cudaSuccess) return e;
-    // s1 = up(e2) + e1; e2 = relu(conv_c(p2))
-    up_bwd_relu_kernel<16><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[1], d[2], G.gs1, A.e2, G.gc);
-    if ((e = layer_wgrad(2, d[2], A.p2, G.gc, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
-    if ((e = conv_layer_bwd(2, d[2], I, G.gc, nullptr, G.gp2, A.error, s)) != cudaSuccess) return e;
-    // p2 = pool(e1); e1 = relu(conv_b(p1))
-    pool_bwd_add_relu_kernel<16><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[1], d[2], G.gs1, G.gp2, A.e1, G.gb);
-    if ((e = layer_wgrad(1, d[1], A.p1, G.gb, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
-    if ((e = conv_layer_bwd(1, d[1], I, G.gb, nullptr, G.gp1, A.error, s)) != cudaSuccess) return e;
-    // p1 = pool(e0); e0 = relu(conv_a(x0))
-    pool_bwd_add_relu_kernel<8><<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], d[1], G.gs0, G.gp1, A.e0, G.ga);
-    return layer_wgrad(0, d[0], A.x0, G.ga, G, grad, accumulate, A.error, s);
+    // g: y = conv_g(s0); s0 = up(u1) + e0
+    if ((e = layer_wgrad(7, d[0], A.s0, G.gy, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
+    if ((e = conv_layer_bwd(7, d[0], I, G.gy, nullptr, G.gs0, A.error, s)) != cudaSuccess) return e;
+    // f: u1 = relu(conv_f(s1)); s1 = up(u2) + e1
+    up_bwd_relu_kernel<16><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[0], d[1], G.gs0, A.u1, G.gu1);
+    if ((e = layer_wgrad(6, d[1], A.s1, G.gu1, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
+    if ((e = conv_layer_bwd(6, d[1], I, G.gu1, nullptr, G.gs1, A.error, s)) != cudaSuccess) return e;
+    // e: u2 = relu(conv_e(s2)); s2 = up(m3) + e2
+    up_bwd_relu_kernel<32><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[1], d[2], G.gs1, A.u2, G.gu2);
+    if ((e = layer_wgrad(5, d[2], A.s2, G.gu2, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
+    if ((e = conv_layer_bwd(5, d[2], I, G.gu2, nullptr, G.gs2, A.error, s)) != cudaSuccess) return e;
+    // m: m3 = relu(conv_m(e3)); e3 = relu(conv_d(p3)) feeds m only, so its ReLU gate goes into m's backward
+    up_bwd_relu_kernel<64><<<glue_blocks(d[3].n), kGlueThreads, 0, s>>>(d[2], d[3], G.gs2, A.m3, G.gm3);
+    if ((e = layer_wgrad(4, d[3], A.e3, G.gm3, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
+    if ((e = conv_layer_bwd(4, d[3], I, G.gm3, A.e3, G.ge3, A.error, s)) != cudaSuccess) return e;
+    // d: e3 = relu(conv_d(p3)); p3 = pool(e2)
+    if ((e = layer_wgrad(3, d[3], A.p3, G.ge3, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
+    if ((e = conv_layer_bwd(3, d[3], I, G.ge3, nullptr, G.gp3, A.error, s)) != cudaSuccess) return e;
+    // c: e2 = relu(conv_c(p2)) feeds p3 and s2
+    pool_bwd_add_relu_kernel<64><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[2], d[3], G.gs2, G.gp3, A.e2, G.ge2);
+    if ((e = layer_wgrad(2, d[2], A.p2, G.ge2, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
+    if ((e = conv_layer_bwd(2, d[2], I, G.ge2, nullptr, G.gp2, A.error, s)) != cudaSuccess) return e;
+    // b: e1 = relu(conv_b(p1)) feeds p2 and s1
+    pool_bwd_add_relu_kernel<32><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[1], d[2], G.gs1, G.gp2, A.e1, G.ge1);
+    if ((e = layer_wgrad(1, d[1], A.p1, G.ge1, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
+    if ((e = conv_layer_bwd(1, d[1], I, G.ge1, nullptr, G.gp1, A.error, s)) != cudaSuccess) return e;
+    // a: e0 = relu(conv_a(x0)) feeds p1 and s0
+    pool_bwd_add_relu_kernel<16><<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], d[1], G.gs0, G.gp1, A.e0, G.ge0);
+    return layer_wgrad(0, d[0], A.x0, G.ge0, G, grad, accumulate, A.error, s);
 }
 
 cudaError_t net_adam(float* w, const float* grad, float* m, float* v, float lr, int step, float gscale, const NetImages& I, cudaStream_t s) {

@@ -50,15 +50,16 @@ def source_box(n: int):
 
 class SceneDriver:
     """Per-step inputs of a plume scene with any grid and any source boxes, for one Simulation (any library). Every
-    box holds density 1 and temperature 1 and drives an inflow v_y = 1 + xi (xi drawn per cell and step, the
-    boxes' cells in box order). All work is enqueued on the simulation's stream; `inputs_for(step)` is the host-side
-    input of that step (pinned)."""
+    box holds density and temperature `strength` (1 by default) and drives an inflow v_y = strength * (1 + xi) (xi
+    drawn per cell and step, the boxes' cells in box order). All work is enqueued on the simulation's stream;
+    `inputs_for(step)` is the host-side input of that step (pinned)."""
 
-    def __init__(self, sim, boxes, seed: int = 1):
+    def __init__(self, sim, boxes, seed: int = 1, strength: float = 1.0):
         import torch
 
         self.sim = sim
         self.seed = seed
+        self.strength = float(strength)
         self.dt = float(sim.config.dt)
         nx, ny, nz = sim.config.nx, sim.config.ny, sim.config.nz
         self.shape = (nz, ny, nx)
@@ -101,9 +102,15 @@ class SceneDriver:
                 count = size[0] * size[1] * size[2]
                 xi_box = self.xi_dev[start:start + count].reshape(size)
                 start += count
-                self.force_y[zs, ys, xs] = (1.0 + xi_box - vy[zs, ys, xs]) / self.dt
-                self.density_source[zs, ys, xs] = (1.0 - rho[zs, ys, xs]) / self.dt
-                self.temperature_source[zs, ys, xs] = (1.0 - tem[zs, ys, xs]) / self.dt
+                k = self.strength
+                if k == 1.0:
+                    self.force_y[zs, ys, xs] = (1.0 + xi_box - vy[zs, ys, xs]) / self.dt
+                    self.density_source[zs, ys, xs] = (1.0 - rho[zs, ys, xs]) / self.dt
+                    self.temperature_source[zs, ys, xs] = (1.0 - tem[zs, ys, xs]) / self.dt
+                else:
+                    self.force_y[zs, ys, xs] = (k * (1.0 + xi_box) - vy[zs, ys, xs]) / self.dt
+                    self.density_source[zs, ys, xs] = (k - rho[zs, ys, xs]) / self.dt
+                    self.temperature_source[zs, ys, xs] = (k - tem[zs, ys, xs]) / self.dt
             sim.update_force(None, self.force_y, None)
             sim.update_density_source(self.density_source)
             sim.update_temperature_source(self.temperature_source)

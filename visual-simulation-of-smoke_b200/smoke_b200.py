@@ -67,6 +67,7 @@ class SmokeLibrary:
         ("smoke_b200_net_train_cuda", [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_double), C.c_void_p]),
         ("smoke_b200_set_preconditioner_net_cuda", [C.c_void_p, C.c_void_p]),
         ("smoke_b200_apply_operator_cuda", [C.c_void_p, C.c_void_p, C.c_void_p]),
+        ("smoke_b200_apply_multigrid_cuda", [C.c_void_p, C.c_void_p, C.c_void_p]),
         ("smoke_b200_conv3d_cuda", [C.c_int] * 5 + [C.c_void_p] * 3 + [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
         ("smoke_b200_test_barrier_timeout_cuda", [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(abi.SolverStatus)]),
     ]
@@ -257,6 +258,15 @@ class Simulation:
         out = torch.empty_like(x)
         with torch.cuda.stream(self.stream):
             _check(self.lib.smoke_b200_apply_operator_cuda(self.handle, _ptr(x), _ptr(out)), "apply_operator")
+        return out
+
+    def apply_multigrid(self, r):
+        """V(r), one V-cycle of the multigrid preconditioner (r: float32 CUDA tensor of nz x ny x nx values)."""
+        import torch
+
+        out = torch.empty_like(r)
+        with torch.cuda.stream(self.stream):
+            _check(self.lib.smoke_b200_apply_multigrid_cuda(self.handle, _ptr(r), _ptr(out)), "apply_multigrid")
         return out
 
     def set_preconditioner_net(self, net: "Net"):
