@@ -39,6 +39,8 @@ def test_batch_equals_individual_steps(smoke_lib, cuda_stream, solver):
     with smoke_b200.Batch([s for s, _ in batched]) as batch:
         for _ in range(3):
             batch.step()
+        times = batch.member_times()  # each member's completion time inside the last batch step
+        assert times.shape == (len(MEMBERS),) and np.all(times > 0) and np.all(np.isfinite(times))
         for (a, _), (b, _) in zip(alone, batched):
             ra, rb = a.snapshot(KINDS), b.snapshot(KINDS)
             for key in ra:

@@ -245,7 +245,10 @@ def test_full_steps_against_oracle(smoke_lib, cuda_stream, name, mode):
     sim.close()
     del keep
     report(f"full3/{name}/mode{mode}", worst)
-    assert max(worst.values()) < 2e-3, worst
+    # measured on a B200: fields <= 3e-6, pressure <= 2.6e-5 (both sides solve to 1e-7; the pressure differs by the
+    # two solves' leftover errors)
+    assert max(v for k, v in worst.items() if k != "pressure") < 1e-5, worst
+    assert worst["pressure"] < 1e-4, worst
 
 
 def test_fixed_cg_matches_reference_semantics(smoke_lib, cuda_stream):

@@ -405,12 +405,17 @@ struct SmokeB200Batch_t {
     cudaStream_t stream = nullptr;
     bool owns_stream = false;
     cudaGraphExec_t exec = nullptr;
-    std::vector<cudaEvent_t> ready;  // one per context: the context's stream reached the batch step
-    cudaEvent_t done = nullptr;      // the batch step finished
+    std::vector<cudaEvent_t> ready;     // one per context: the context's stream reached the batch step
+    cudaEvent_t done = nullptr;         // the batch step finished
+    cudaEvent_t started = nullptr;      // recorded by the graph when the batch step starts (timing event)
+    std::vector<cudaEvent_t> finished;  // recorded by each member's branch when that member's step is done
 
     ~SmokeB200Batch_t() {
         if (exec) cudaGraphExecDestroy(exec);
         for (cudaEvent_t e : ready) cudaEventDestroy(e);
+        for (cudaEvent_t e : finished)
+            if (e) cudaEventDestroy(e);
+        if (started) cudaEventDestroy(started);
         if (done) cudaEventDestroy(done);
         if (owns_stream && stream) cudaStreamDestroy(stream);
     }
@@ -424,11 +429,13 @@ struct SmokeB200Batch_t {
         cudaError_t err = cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal);
         try {
             check(err, "begin batch capture");
+            check(cudaEventRecord(started, root), "batch start time");
             check(cudaEventRecord(fork, root), "batch fork");
             for (size_t i = 0; i < contexts.size(); ++i) {
                 SmokeSimulationContext_t* c = contexts[i];
                 if (i > 0) check(cudaStreamWaitEvent(c->capture_stream, fork, 0), "batch branch");
                 c->enqueue_stages(c->capture_stream, SMOKE_B200_STAGE_SCALARS, true);
+                check(cudaEventRecord(finished[i], c->capture_stream), "batch member time");
                 if (i > 0) {
                     check(cudaEventCreateWithFlags(&joins[i], cudaEventDisableTiming), "batch join event");
                     check(cudaEventRecord(joins[i], c->capture_stream), "batch join");
@@ -798,6 +805,9 @@ SmokeSimulationResult smoke_b200_batch_create_cuda(const SmokeSimulationContext*
         }
         b->ready.assign(count, nullptr);
         for (cudaEvent_t& e : b->ready) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "batch event");
+        b->finished.assign(count, nullptr);
+        for (cudaEvent_t& e : b->finished) check(cudaEventCreate(&e), "batch member time event");
+        check(cudaEventCreate(&b->started), "batch start time event");
         check(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "batch event");
         for (SmokeSimulationContext_t* c : b->contexts) check(cudaStreamSynchronize(c->stream), "batch: contexts idle");
         b->build();
@@ -823,6 +833,15 @@ SmokeSimulationResult smoke_b200_batch_step_cuda(SmokeB200Batch batch) {
             c->views_stale = kViewsAll;
             c->stepped = true;
         }
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
+}
+
+SmokeSimulationResult smoke_b200_batch_member_times_cuda(SmokeB200Batch batch, float* ms_out) {
+    if (batch == nullptr || ms_out == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        check(cudaEventSynchronize(batch->done), "batch member times: wait");
+        for (size_t i = 0; i < batch->contexts.size(); ++i) check(cudaEventElapsedTime(ms_out + i, batch->started, batch->finished[i]), "batch member time");
         return SMOKE_SIMULATION_RESULT_OK;
     });
 }

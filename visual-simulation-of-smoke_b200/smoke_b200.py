@@ -12,6 +12,8 @@ from __future__ import annotations
 import ctypes as C
 import os
 
+import numpy as np
+
 import smoke_abi as abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -55,6 +57,7 @@ class SmokeLibrary:
         ("smoke_b200_batch_create_cuda", [C.POINTER(C.c_void_p), C.c_uint32, C.c_void_p, C.POINTER(C.c_void_p)]),
         ("smoke_b200_batch_step_cuda", [C.c_void_p]),
         ("smoke_b200_batch_destroy_cuda", [C.c_void_p]),
+        ("smoke_b200_batch_member_times_cuda", [C.c_void_p, C.c_void_p]),
         ("smoke_b200_set_launch_tune_cuda", [C.c_void_p, C.POINTER(abi.LaunchTune)]),
         ("smoke_b200_get_launch_tune_cuda", [C.c_void_p, C.POINTER(abi.LaunchTune)]),
         ("smoke_b200_autotune_cuda", [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(abi.TuneReport)]),
@@ -378,6 +381,12 @@ class Batch:
 
     def step(self):
         _check(self.lib.smoke_b200_batch_step_cuda(self.handle), "batch_step")
+
+    def member_times(self):
+        """Milliseconds from the start of the last batch step to the end of each member's step inside it."""
+        out = (C.c_float * len(self.sims))()
+        _check(self.lib.smoke_b200_batch_member_times_cuda(self.handle, out), "batch_member_times")
+        return np.array(out[:], dtype=np.float64)
 
     def close(self):
         if self.handle is not None and self.handle.value:
