@@ -68,7 +68,9 @@ def run(lib, shape, cin, cout, relu, seed):
 def test_conv3d_matches_float64(smoke_lib, cin, cout, relu):
     got, got0, ref = run(smoke_lib.lib, (21, 13, 11), cin, cout, relu, seed=cin * 100 + cout)
     scale = np.abs(ref).max()
-    assert np.abs(got0 - ref[..., 0]).max() <= 2e-6 * scale
+    # FP32 accumulation of K = 27 x cin products: the rounding grows like sqrt(K) (2e-6 at K <= 216)
+    k = 27 * store(cin)
+    assert np.abs(got0 - ref[..., 0]).max() <= 2e-6 * max(1.0, np.sqrt(k / 216.0)) * scale
     assert np.abs(got[..., :cout] - ref).max() <= 8e-3 * scale
     assert not got[..., cout:].any()  # stored channels past cout are 0
 
