@@ -764,7 +764,8 @@ def bench_reference(args, rank, world, local):
 
 def profile_workload(args):
     """Profiling workloads (for ncu; prints one status line, no benchmark JSON): the 128^3 plume after the spin-up,
-    then --profile-count repetitions of: `solve` an eager multigrid solve (every kernel a plain launch), `solve-graph`
+    then --profile-count repetitions of: `solve` an eager multigrid solve (every kernel a plain launch), `learned-solve`
+    an eager learned solve (packaged weights), `solve-graph`
     the multigrid solve graph, `step` an eager step (stage kernels launched one by one, the solve as its graph), `net`
     the learned preconditioner's network on the step's right-hand side (packaged weights)."""
     import torch
@@ -782,6 +783,10 @@ def profile_workload(args):
         a, w, g = (int(v) for v in args.shapes.split(","))
         sim.set_launch_tune(advect_tile=a, mg_wave=w, pcg_grid=g)
     run_steps(sim, driver, 0, SPINUP_STEPS, None)
+    if args.profile == "learned-solve":  # the learned form's solve from zero, every kernel a plain launch
+        net = learned_net(lib)
+        sim.set_preconditioner_net(net)
+        sim.set_solver(**dict(LEARNED_FORM, warm_start=False))
     if args.profile == "net":  # the learned preconditioner's network on the step's right-hand side
         import train_preconditioner
 
@@ -803,7 +808,7 @@ def profile_workload(args):
             driver.apply(SPINUP_STEPS + k)
             sim.step_stages(abi.STAGE_SCALARS)
         else:
-            sim.solve_pressure(eager=args.profile == "solve")
+            sim.solve_pressure(eager=args.profile in ("solve", "learned-solve"))
     stream.synchronize()
     st = sim.solver_status()
     print(json.dumps({"profile": args.profile, "count": args.profile_count, "iterations": st.iterations, "passes": st.passes, "status": st.status,
@@ -849,7 +854,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--calibrate-reference", action="store_true")
     ap.add_argument("--calibrate-counts", type=int, nargs="*", default=[200, 300, 400, 500, 600, 800, 1000])
-    ap.add_argument("--profile", choices=["solve", "solve-graph", "step", "net"], help="run a profiling workload instead of the benchmark")
+    ap.add_argument("--profile", choices=["solve", "solve-graph", "step", "net", "learned-solve"], help="run a profiling workload instead of the benchmark")
     ap.add_argument("--workload", default="plume128", choices=["plume128", "plume64", "large", "batched"],
                     help="plume128: the headline (default); plume64, large, batched: the other benchmark configurations")
     ap.add_argument("--profile-count", type=int, default=1)
