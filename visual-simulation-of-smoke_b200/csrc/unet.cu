@@ -194,6 +194,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
 #pragma unroll
         for (int c = 0; c < NC; ++c) bias[c] = a.bias ? __ldg(a.bias + chunk * NC + c) : 0.0f;
         const int n0 = chunk * NC;
+        const int stored = min(NC, a.cout_store - n0);  // output channels this chunk stores (fewer than NC for cout <= 8)
         for (uint32_t jl = 0; jl < my_tiles; ++jl) {
             const int b = static_cast<int>(jl & 1u);
             // warp-uniform outcome: the accumulator loads below are warp-collective
@@ -223,6 +224,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
                     const uint4* g = reinterpret_cast<const uint4*>(a.gate + static_cast<size_t>(q) * a.cout_store + n0);
 #pragma unroll
                     for (int h = 0; h < NC / 8; ++h) {
+                        if (8 * h >= stored) break;
                         const uint4 gv = __ldg(g + h);
                         const __nv_bfloat16* gb = reinterpret_cast<const __nv_bfloat16*>(&gv);
 #pragma unroll
@@ -235,7 +237,8 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
                     uint4* o = reinterpret_cast<uint4*>(a.out + static_cast<size_t>(q) * a.cout_store + n0);
 #pragma unroll
                     for (int h = 0; h < NC / 8; ++h)
-                        o[h] = make_uint4(pack_bf16x2(acc[8 * h], acc[8 * h + 1]), pack_bf16x2(acc[8 * h + 2], acc[8 * h + 3]), pack_bf16x2(acc[8 * h + 4], acc[8 * h + 5]),
+                        if (8 * h < stored)
+                            o[h] = make_uint4(pack_bf16x2(acc[8 * h], acc[8 * h + 1]), pack_bf16x2(acc[8 * h + 2], acc[8 * h + 3]), pack_bf16x2(acc[8 * h + 4], acc[8 * h + 5]),
                                           pack_bf16x2(acc[8 * h + 6], acc[8 * h + 7]));
                 }
             }
@@ -712,7 +715,9 @@ cudaError_t launch_conv3(const VolumeDims& d, int cin_store, int cout, const __n
                          int cout_store, float* out_f32, unsigned* error, cudaStream_t s, const uint32_t* skip, long long wait_cycles, int drop_loads) {
     if (d.n == 0) return cudaSuccess;
     const int nc = conv_nc(cin_store, cout), cpad = net_cout_pad(cout);
-    if (error == nullptr || cout < 1 || cout > 128 || (out != nullptr && (cout_store < cpad || cout_store % 8 != 0)) || (gate != nullptr && cout_store < cpad)) return cudaErrorInvalidValue;
+    // stored output channels: all padded columns, or (cout <= 8) the 8 channels of a narrow output
+    const bool stores_ok = cout_store % 8 == 0 && (cout_store >= cpad || (cout <= 8 && cout_store == 8));
+    if (error == nullptr || cout < 1 || cout > 128 || ((out != nullptr || gate != nullptr) && !stores_ok)) return cudaErrorInvalidValue;
     ConvArgs a{};
     a.in = in;
     a.wpack = wpack;
