@@ -120,7 +120,7 @@ SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_batch_create_cuda(const Sm
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_batch_step_cuda(SmokeB200Batch batch);
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_batch_destroy_cuda(SmokeB200Batch batch);
 /* Per-member latency of the last batch step: ms_out[i] = milliseconds from the start of the batch graph to the end of
- * member i's step inside it (events recorded by the graph itself). Waits for the last batch step. */
+ * member i's step inside it (the device's global timer, stamped by the graph itself). Waits for the last batch step. */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_batch_member_times_cuda(SmokeB200Batch batch, float* ms_out);
 
 /* Launch shapes of a context's step (no reference counterpart; the reference fixes its launch shapes at compile

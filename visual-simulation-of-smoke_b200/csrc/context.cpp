@@ -407,15 +407,13 @@ struct SmokeB200Batch_t {
     cudaGraphExec_t exec = nullptr;
     std::vector<cudaEvent_t> ready;     // one per context: the context's stream reached the batch step
     cudaEvent_t done = nullptr;         // the batch step finished
-    cudaEvent_t started = nullptr;      // recorded by the graph when the batch step starts (timing event)
-    std::vector<cudaEvent_t> finished;  // recorded by each member's branch when that member's step is done
+    // globaltimer stamps written by the graph: [0] when the batch step starts, [1 + i] when member i's step is done
+    unsigned long long* stamps = nullptr;
 
     ~SmokeB200Batch_t() {
         if (exec) cudaGraphExecDestroy(exec);
         for (cudaEvent_t e : ready) cudaEventDestroy(e);
-        for (cudaEvent_t e : finished)
-            if (e) cudaEventDestroy(e);
-        if (started) cudaEventDestroy(started);
+        if (stamps) cudaFree(stamps);
         if (done) cudaEventDestroy(done);
         if (owns_stream && stream) cudaStreamDestroy(stream);
     }
@@ -429,13 +427,13 @@ struct SmokeB200Batch_t {
         cudaError_t err = cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal);
         try {
             check(err, "begin batch capture");
-            check(cudaEventRecord(started, root), "batch start time");
+            check(launch_time_stamp(stamps, root), "batch start time");
             check(cudaEventRecord(fork, root), "batch fork");
             for (size_t i = 0; i < contexts.size(); ++i) {
                 SmokeSimulationContext_t* c = contexts[i];
                 if (i > 0) check(cudaStreamWaitEvent(c->capture_stream, fork, 0), "batch branch");
                 c->enqueue_stages(c->capture_stream, SMOKE_B200_STAGE_SCALARS, true);
-                check(cudaEventRecord(finished[i], c->capture_stream), "batch member time");
+                check(launch_time_stamp(stamps + 1 + i, c->capture_stream), "batch member time");
                 if (i > 0) {
                     check(cudaEventCreateWithFlags(&joins[i], cudaEventDisableTiming), "batch join event");
                     check(cudaEventRecord(joins[i], c->capture_stream), "batch join");
@@ -805,9 +803,8 @@ SmokeSimulationResult smoke_b200_batch_create_cuda(const SmokeSimulationContext*
         }
         b->ready.assign(count, nullptr);
         for (cudaEvent_t& e : b->ready) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "batch event");
-        b->finished.assign(count, nullptr);
-        for (cudaEvent_t& e : b->finished) check(cudaEventCreate(&e), "batch member time event");
-        check(cudaEventCreate(&b->started), "batch start time event");
+        check(cudaMalloc(&b->stamps, (count + 1) * sizeof(unsigned long long)), "batch time stamps");
+        check(cudaMemset(b->stamps, 0, (count + 1) * sizeof(unsigned long long)), "batch time stamps");
         check(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "batch event");
         for (SmokeSimulationContext_t* c : b->contexts) check(cudaStreamSynchronize(c->stream), "batch: contexts idle");
         b->build();
@@ -841,7 +838,9 @@ SmokeSimulationResult smoke_b200_batch_member_times_cuda(SmokeB200Batch batch, f
     if (batch == nullptr || ms_out == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return guarded([&] {
         check(cudaEventSynchronize(batch->done), "batch member times: wait");
-        for (size_t i = 0; i < batch->contexts.size(); ++i) check(cudaEventElapsedTime(ms_out + i, batch->started, batch->finished[i]), "batch member time");
+        std::vector<unsigned long long> t(batch->contexts.size() + 1);
+        check(cudaMemcpy(t.data(), batch->stamps, t.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "batch member times");
+        for (size_t i = 0; i < batch->contexts.size(); ++i) ms_out[i] = static_cast<float>(static_cast<double>(t[i + 1] - t[0]) * 1e-6);
         return SMOKE_SIMULATION_RESULT_OK;
     });
 }

@@ -215,6 +215,8 @@ struct MgSolveArgs {
 int mg_level_count(int nx, int ny, int nz);
 // Largest refinement count the multigrid solve honours (the graph unrolls refinement + 1 passes).
 int mg_max_refinement();
+// Writes the device's global nanosecond timer into *slot when the stream reaches it (batch member latencies).
+cudaError_t launch_time_stamp(unsigned long long* slot, cudaStream_t s);
 // z = V(r): one V-cycle of the multigrid preconditioner on the residual r (the solve's preconditioner, standalone).
 cudaError_t launch_mg_vcycle(const MgHierarchy& H, int wave_depth, const float* r, float* z, cudaStream_t s);
 // out = A x with the fine operator (the pressure system's matrix, matrix-free from the level-0 codes).

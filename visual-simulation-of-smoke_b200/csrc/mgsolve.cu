@@ -593,9 +593,12 @@ __global__ void __launch_bounds__(kThreads) mg_net_residual_kernel(const __grid_
     zero_acc(st, kAccNet);
 }
 
-// Learned preconditioner, part 2: z = z_V + N(r_V) on active cells, N(r_V) = y / s with y the network's output and
-// s = sqrt(n / ||r_V||^2) its input scale (z = z_V after a fallback); then (z, r) and (z, q), and the last block
-// computes beta (0 on a pass's first iteration), as level 0's smoothing does for the V-cycle alone.
+// Learned preconditioner, part 2: the network's correction N = y / s (y its output, s = sqrt(n / ||r_V||^2) its input
+// scale) added to the V-cycle's z_V and post-smoothed by one damped Jacobi step on what it leaves of r_V:
+// z = z_V + N + w D^-1 (r_V - A N) on active cells (z = z_V after a fallback). The network supplies the smooth part of
+// the correction; the Jacobi step removes the rough part of its error (BF16 output and fitting noise), which the
+// energy norm the FCG minimises would amplify. Then (z, r) and (z, q), and the last block computes beta (0 on a
+// pass's first iteration), as level 0's smoothing does for the V-cycle alone.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) mg_net_add_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
     const MgLevel& F = A.H.L[0];
@@ -609,7 +612,16 @@ __global__ void __launch_bounds__(kThreads) mg_net_add_kernel(const __grid_const
         if (!c.in) return;
         const uint16_t code = F.code[c.q];
         if (!active(code)) return;  // t stays 0 there
-        const float z = use_net ? F.t[c.q] + y[c.q] * inv_s : F.t[c.q];
+        float z = F.t[c.q];
+        if (use_net) {
+            uint32_t nb[6];
+            nbr_all(F, A.H.fper, c, nb);
+            const float n0 = y[c.q] * inv_s;
+            float nn[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) nn[k] = y[nb[k]] * inv_s;
+            z += n0 + wdiag(code) * (F.zp[c.q] - masked_stencil(code, n0, nn));
+        }
         F.t[c.q] = z;
         zr += static_cast<T>(z) * static_cast<T>(r[c.q]);
         zq += static_cast<T>(z) * static_cast<T>(A.W.q[c.q]);
@@ -1041,7 +1053,7 @@ template <typename T>
 void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_graph, uint32_t block_bytes, cudaStream_t bs) {
     const MgLevel& L0 = A.H.L[0];
     launch_coarse_cycle(A, block_bytes, bs);
-    if (A.learned) {  // z = z_V + N(r - A z_V): the network corrects what the V-cycle leaves
+    if (A.learned) {  // z = z_V + N(r - A z_V), post-smoothed: the network corrects what the V-cycle leaves
         const LearnedSolve& N = *A.net;
         mg_smooth_kernel<true, T, false><<<wave(mg_smooth_kernel<true, T, false>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
         mg_net_residual_kernel<T><<<wave(mg_net_residual_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);

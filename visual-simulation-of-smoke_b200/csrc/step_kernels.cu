@@ -692,6 +692,18 @@ K pick_advect(const StepParams& P, K k000, K k001, K k010, K k011, K k100, K k10
     return all[(P.cubic ? 4 : 0) + (P.tile[0] >= 0 ? 2 : 0) + (P.h_pow2 ? 1 : 0)];
 }
 
+// The device's global nanosecond timer into *slot (one thread).
+__global__ void time_stamp_kernel(unsigned long long* slot) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    *slot = t;
+}
+
+cudaError_t launch_time_stamp(unsigned long long* slot, cudaStream_t s) {
+    time_stamp_kernel<<<1, 1, 0, s>>>(slot);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, ConstFaces pad, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
     const unsigned bu = advect_blocks(P, P.nx + 1, P.ny, P.nz), bv = advect_blocks(P, P.nx, P.ny + 1, P.nz), bw = advect_blocks(P, P.nx, P.ny, P.nz + 1);
     const PadField u = pad_field(P, 0, in.u, pad.u), v = pad_field(P, 1, in.v, pad.v), w = pad_field(P, 2, in.w, pad.w);

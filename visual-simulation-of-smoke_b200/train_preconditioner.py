@@ -164,8 +164,8 @@ def train(net, data, steps: int, batch: int = 4, lr: float = 1e-3, seed: int = 0
 
 def load(net, path: str = DEFAULT_WEIGHTS):
     values = np.fromfile(path, dtype="<f4")
-    if values.size != net.parameter_count():
-        raise ValueError(f"{path}: {values.size} parameters, the network has {net.parameter_count()}")
+    if values.size != net.parameter_count:
+        raise ValueError(f"{path}: {values.size} parameters, the network has {net.parameter_count}")
     net.set_parameters(values)
     return net
 
