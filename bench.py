@@ -72,7 +72,7 @@ def solver_launches(n, iterations, refinement, learned=False):
     # coarse grid levels of at most 64^3 cells fuse prolongation and smoothing (mg_up_kernel)
     per_iteration = sum(2 if -(-n // (1 << l)) ** 3 <= 64 ** 3 else 3 for l in range(1, g)) + 5
     if learned:
-        per_iteration += 2 + NET_FORWARD_KERNELS
+        per_iteration += 3 + NET_FORWARD_KERNELS
     return 2 + 3 * (refinement + 1) + per_iteration * iterations
 
 

@@ -178,13 +178,14 @@ struct MgWork {
 };
 // Device-side scalars of one multigrid solve (reset at the start of every solve).
 constexpr int kMgSlots = 32;  // addresses each FP64 dot-product accumulator is spread over
-enum MgAccumulator { kAccBB = 0, kAccRR, kAccZR, kAccZQ, kAccPQ, kAccPR, kAccNet, kAccCount };
+enum MgAccumulator { kAccBB = 0, kAccRR, kAccZR, kAccZQ, kAccPQ, kAccPR, kAccNet, kAccNetA, kAccCount };
 struct MgState {
     double acc[kAccCount][kMgSlots];
     double bb, rnorm2, pq_prev, target2, pass_rr0, true_rel;
     double net_rr;         // learned solve: ||r - A z_V||^2, the squared norm of the network's input
+    double net_gamma;      // learned solve: the energy-optimal step along the network's correction
     float alpha, beta;     // step sizes, computed by the last block of the kernel that completes their sums
-    unsigned int done[6];  // last-block election counters
+    unsigned int done[7];  // last-block election counters
     int parity, first_iter, it, passes;
     uint32_t status, fail, halt, zero_solution;
     uint32_t loop;         // the loop condition the last update set (read by the host in eager mode)

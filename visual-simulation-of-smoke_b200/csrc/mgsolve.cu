@@ -593,9 +593,41 @@ __global__ void __launch_bounds__(kThreads) mg_net_residual_kernel(const __grid_
     zero_acc(st, kAccNet);
 }
 
-// Learned preconditioner, part 2: the network's correction N = y / s (y its output, s = sqrt(n / ||r_V||^2) its input
-// scale) added to the V-cycle's z_V and post-smoothed by one damped Jacobi step on what it leaves of r_V:
-// z = z_V + N + w D^-1 (r_V - A N) on active cells (z = z_V after a fallback). The network supplies the smooth part of
+// Learned preconditioner, part 2: the step along the network's correction N = y / s that minimises the energy norm of
+// what z_V + gamma N leaves of the error e - z_V (whose residual is r_V): gamma = (N, r_V) / (N, A N), 0 when that is
+// not defined. So a network that helps little is scaled down instead of being added at full weight.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) mg_net_gamma_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
+    const MgLevel& F = A.H.L[0];
+    MgState* st = A.st;
+    if (st->fallback) return;  // uniform over the grid
+    const double rn2 = st->net_rr;
+    const float inv_s = rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n))) : 0.0f;
+    T nr = 0, nan_ = 0;
+    for_tiles(F, [&](const Cell& c) {
+        if (!c.in) return;
+        const uint16_t code = F.code[c.q];
+        if (!active(code)) return;
+        uint32_t nb[6];
+        nbr_all(F, A.H.fper, c, nb);
+        const float n0 = y[c.q] * inv_s;
+        float nn[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) nn[k] = y[nb[k]] * inv_s;
+        nr += static_cast<T>(n0) * static_cast<T>(F.zp[c.q]);
+        nan_ += static_cast<T>(n0) * static_cast<T>(masked_stencil(code, n0, nn));
+    });
+    block_accumulate<T>(st, kAccNet, nr, kAccNetA, nan_);
+    if (!last_block(&st->done[6])) return;
+    const double a = total(st, kAccNet), b = total(st, kAccNetA);
+    st->net_gamma = (b > 0.0 && isfinite(a) && isfinite(b)) ? a / b : 0.0;
+    zero_acc(st, kAccNet);
+    zero_acc(st, kAccNetA);
+}
+
+// Learned preconditioner, part 3: the network's correction N = y / s (y its output, s = sqrt(n / ||r_V||^2) its input
+// scale), scaled by gamma, added to the V-cycle's z_V and post-smoothed by one damped Jacobi step on what it leaves of
+// r_V: z = z_V + gamma N + w D^-1 (r_V - gamma A N) on active cells (z = z_V after a fallback). The network supplies the smooth part of
 // the correction; the Jacobi step removes the rough part of its error (BF16 output and fitting noise), which the
 // energy norm the FCG minimises would amplify. Then (z, r) and (z, q), and the last block computes beta (0 on a
 // pass's first iteration), as level 0's smoothing does for the V-cycle alone.
@@ -605,7 +637,7 @@ __global__ void __launch_bounds__(kThreads) mg_net_add_kernel(const __grid_const
     MgState* st = A.st;
     const bool use_net = st->fallback == 0;
     const double rn2 = st->net_rr;
-    const float inv_s = use_net && rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n))) : 0.0f;
+    const float inv_s = use_net && rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n)) * st->net_gamma) : 0.0f;
     const float* r = A.W.r[st->parity];
     T zr = 0, zq = 0;
     for_tiles(F, [&](const Cell& c) {
@@ -1058,6 +1090,7 @@ void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_grap
         mg_smooth_kernel<true, T, false><<<wave(mg_smooth_kernel<true, T, false>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
         mg_net_residual_kernel<T><<<wave(mg_net_residual_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
         if (net_forward(N.images, N.acts, L0.zp, nullptr, nullptr, &A.st->net_rr, N.occupancy, bs, &A.st->fallback) != cudaSuccess) return;
+        mg_net_gamma_kernel<T><<<wave(mg_net_gamma_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
         mg_net_add_kernel<T><<<wave(mg_net_add_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
         mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
         mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
