@@ -200,14 +200,18 @@ def test_multigrid_apply_is_the_solvers_preconditioner(smoke_lib):
     assert abs(its - st_m.iterations) <= 1, (its, st_m.iterations)
 
 
-def test_stalled_network_falls_back_to_the_multigrid_preconditioner(smoke_lib):
-    """A network of huge random weights is a useless correction: the solve detects the stall, drops it (flags
-    bit 0) and still reaches the tolerance with the V-cycle alone."""
+def test_useless_network_costs_no_iterations(smoke_lib):
+    """A network of huge random weights is a useless correction: the energy-optimal step along it (or, if the solve
+    stalls anyway, dropping it: flags bit 0) leaves the multigrid V-cycle's convergence, and the solve reaches the
+    tolerance with the Jacobi-PCG answer in about the multigrid form's iterations."""
     sim, keep = held_out_system(smoke_lib)
+    st_m, _ = solve(sim, MULTIGRID)
     with smoke_b200.Net(smoke_lib, seed=0) as bad:
         bad.set_parameters(U.initial_like(7, scale=30.0))
         st, p = solve(sim, dict(LEARNED, max_iterations=600), bad)
     st_j, p_j = solve(sim, JACOBI)
-    assert st.status == abi.SOLVE_CONVERGED and (st.flags & 1)
+    report("learned/useless_network", {"iterations": st.iterations, "multigrid": st_m.iterations, "dropped": int(st.flags & 1)})
+    assert st.status == abi.SOLVE_CONVERGED
+    assert st.iterations <= st_m.iterations + 2
     assert np.abs(p - p_j).max() <= 5e-3 * np.abs(p_j).max()
     sim.close()
