@@ -214,6 +214,11 @@ SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_apply_multigrid_cuda(Smoke
  * rebuilds the step graph. */
 SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_set_preconditioner_net_cuda(SmokeSimulationContext context, SmokeB200Net net);
 
+/* Schedule of the learned solve: the network corrects the V-cycle in the first `count` iterations of every
+ * refinement pass and the V-cycle preconditions alone after them (0, the default: every iteration). Rebuilds the step
+ * graph. */
+SMOKE_SIMULATION_API SmokeSimulationResult smoke_b200_set_learned_iterations_cuda(SmokeSimulationContext context, uint32_t count);
+
 /* 3x3x3 convolution (zero padding) of a channels-last BF16 volume on the tensor cores, the layer of the learned
  * preconditioner's network. `in`: nx*ny*nz cells x S(cin) BF16 values, S(c) = 8 for c <= 8, else c rounded up to a
  * multiple of 16 (channels past cin must be 0); `weights`: FP32 [27][cin][cout] on the device, tap = (dz+1)*9 +

@@ -266,10 +266,13 @@ struct SmokeSimulationContext_t {
         A.learned = solver.mode == SMOKE_B200_SOLVER_LEARNED_FCG ? 1 : 0;
         A.net = A.learned ? &learned : nullptr;
         A.net_warm = A.learned && A.warm && solver.warm_start == 2 ? 1 : 0;
+        A.net_iterations = static_cast<int>(net_iterations);
         return A;
     }
 
     // The multigrid FCG machinery runs the multigrid and the learned solves.
+    uint32_t net_iterations = 0;  // learned solve: network iterations per refinement pass (0: all)
+
     bool uses_mg() const { return solver.mode == SMOKE_B200_SOLVER_MG_FCG || solver.mode == SMOKE_B200_SOLVER_LEARNED_FCG; }
 
     // The context's copy of a network: its packed images and an activation workspace on this grid.
@@ -860,6 +863,15 @@ SmokeSimulationResult smoke_b200_apply_operator_cuda(SmokeSimulationContext c, c
 SmokeSimulationResult smoke_b200_apply_multigrid_cuda(SmokeSimulationContext c, const float* r, float* z) {
     if (c == nullptr || r == nullptr || z == nullptr || r == z) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
     return ok_or_fail(launch_mg_vcycle(c->mg, static_cast<int>(c->tune.mg_wave), r, z, c->stream));
+}
+
+SmokeSimulationResult smoke_b200_set_learned_iterations_cuda(SmokeSimulationContext c, uint32_t count) {
+    if (c == nullptr) return SMOKE_SIMULATION_RESULT_BACKEND_FAILURE;
+    return guarded([&] {
+        c->net_iterations = count;
+        c->capture_step_graph();
+        return SMOKE_SIMULATION_RESULT_OK;
+    });
 }
 
 SmokeSimulationResult smoke_b200_set_preconditioner_net_cuda(SmokeSimulationContext c, SmokeB200Net net) {

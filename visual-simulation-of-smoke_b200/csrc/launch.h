@@ -192,6 +192,8 @@ struct MgState {
     uint32_t fallback;     // learned solve: 1 once the network is dropped (the V-cycle alone preconditions)
     int stall_it;          // learned solve: iteration of the last stagnation checkpoint
     double stall_ref;      // learned solve: ||r||^2 at that checkpoint
+    int pass_it0;          // learned solve: iteration count when the current refinement pass started
+    uint32_t net_off;      // learned solve: 1 when this iteration runs without the network (fallback or schedule)
 };
 // Learned solve: the network is dropped, leaving the V-cycle alone, when ||r|| shrank less than 10x
 // (||r||^2 less than kLearnedStallReduction2) over kLearnedStallWindow iterations; the V-cycle alone gains about
@@ -210,6 +212,7 @@ struct MgSolveArgs {
     int wave;                        // grid depth of the level kernels (kMgWaveCount codes)
     int learned;                     // 1: the V-cycle's result is corrected by the network of `net`
     int net_warm;                    // 1 (learned): the initial guess is the network's estimate N(b)
+    int net_iterations;              // learned: the network corrects the first this many iterations of a pass (0: all)
     const struct LearnedSolve* net;  // host-side: the network's images, workspace and mask (learned only)
 };
 // Level extents and the number of grid-wide levels for a fine grid.

@@ -398,6 +398,10 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
             st->stall_ref = st->rnorm2;
         }
     }
+    if (LEARNED) {  // the next loop body runs the network unless dropped or past the schedule's iterations
+        if (initial) st->pass_it0 = st->it;
+        st->net_off = (st->fallback || (A.net_iterations > 0 && st->it - st->pass_it0 >= A.net_iterations)) ? 1u : 0u;
+    }
     st->parity ^= 1;
     for (int k = kAccRR; k < kAccCount; ++k) zero_acc(st, k);
     st->loop = stop ? 0u : 1u;
@@ -571,7 +575,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) mg_net_residual_kernel(const __grid_constant__ MgSolveArgs A) {
     const MgLevel& F = A.H.L[0];
     MgState* st = A.st;
-    if (st->fallback) return;  // uniform over the grid
+    if (st->net_off) return;  // uniform over the grid
     const float* r = A.W.r[st->parity];
     T rr = 0;
     for_tiles(F, [&](const Cell& c) {
@@ -600,7 +604,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) mg_net_gamma_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
     const MgLevel& F = A.H.L[0];
     MgState* st = A.st;
-    if (st->fallback) return;  // uniform over the grid
+    if (st->net_off) return;  // uniform over the grid
     const double rn2 = st->net_rr;
     const float inv_s = rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n))) : 0.0f;
     T nr = 0, nan_ = 0;
@@ -627,7 +631,7 @@ __global__ void __launch_bounds__(kThreads) mg_net_gamma_kernel(const __grid_con
 
 // Learned preconditioner, part 3: the network's correction N = y / s (y its output, s = sqrt(n / ||r_V||^2) its input
 // scale), scaled by gamma, added to the V-cycle's z_V and post-smoothed by one damped Jacobi step on what it leaves of
-// r_V: z = z_V + gamma N + w D^-1 (r_V - gamma A N) on active cells (z = z_V after a fallback). The network supplies the smooth part of
+// r_V: z = z_V + gamma N + w D^-1 (r_V - gamma A N) on active cells (z = z_V in iterations without the network). The network supplies the smooth part of
 // the correction; the Jacobi step removes the rough part of its error (BF16 output and fitting noise), which the
 // energy norm the FCG minimises would amplify. Then (z, r) and (z, q), and the last block computes beta (0 on a
 // pass's first iteration), as level 0's smoothing does for the V-cycle alone.
@@ -635,7 +639,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) mg_net_add_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
     const MgLevel& F = A.H.L[0];
     MgState* st = A.st;
-    const bool use_net = st->fallback == 0;
+    const bool use_net = st->net_off == 0;
     const double rn2 = st->net_rr;
     const float inv_s = use_net && rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n)) * st->net_gamma) : 0.0f;
     const float* r = A.W.r[st->parity];
@@ -1089,7 +1093,7 @@ void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_grap
         const LearnedSolve& N = *A.net;
         mg_smooth_kernel<true, T, false><<<wave(mg_smooth_kernel<true, T, false>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
         mg_net_residual_kernel<T><<<wave(mg_net_residual_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
-        if (net_forward(N.images, N.acts, L0.zp, nullptr, nullptr, &A.st->net_rr, N.occupancy, bs, &A.st->fallback) != cudaSuccess) return;
+        if (net_forward(N.images, N.acts, L0.zp, nullptr, nullptr, &A.st->net_rr, N.occupancy, bs, &A.st->net_off) != cudaSuccess) return;
         mg_net_gamma_kernel<T><<<wave(mg_net_gamma_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
         mg_net_add_kernel<T><<<wave(mg_net_add_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
         mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);

@@ -69,6 +69,7 @@ class SmokeLibrary:
         ("smoke_b200_net_gradient_cuda", [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
         ("smoke_b200_net_train_cuda", [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_double), C.c_void_p]),
         ("smoke_b200_set_preconditioner_net_cuda", [C.c_void_p, C.c_void_p]),
+        ("smoke_b200_set_learned_iterations_cuda", [C.c_void_p, C.c_uint32]),
         ("smoke_b200_apply_operator_cuda", [C.c_void_p, C.c_void_p, C.c_void_p]),
         ("smoke_b200_apply_multigrid_cuda", [C.c_void_p, C.c_void_p, C.c_void_p]),
         ("smoke_b200_conv3d_cuda", [C.c_int] * 5 + [C.c_void_p] * 3 + [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -274,6 +275,10 @@ class Simulation:
 
     def set_preconditioner_net(self, net: "Net"):
         _check(self.lib.smoke_b200_set_preconditioner_net_cuda(self.handle, net.handle), "set_preconditioner_net")
+
+    def set_learned_iterations(self, count: int):
+        """The network corrects the first `count` iterations of each refinement pass (0: all)."""
+        _check(self.lib.smoke_b200_set_learned_iterations_cuda(self.handle, count), "set_learned_iterations")
 
     def solve_pressure(self, eager: bool = False):
         """Pressure solve of the current right-hand side (eager: every kernel launched directly, host-driven loop)."""
