@@ -383,6 +383,7 @@ HEADLINE = "multigrid_fp64"
 # (z = V(r) + N(r - A V(r))), FP64 dots and refinement, warm start; measured when the package's trained weights exist.
 LEARNED_NAME = "learned_fp64"
 LEARNED_FORM = dict(mode=abi.SOLVER_LEARNED_FCG, reduction=abi.REDUCTION_FP64, max_iterations=500, tolerance=1e-5, refinement=1, warm_start=True)
+LEARNED_SCHEDULES = (1, 2, 4)  # also measured: the network in the first k iterations of each pass only
 
 
 def bench_b200(args, rank, world, local):
@@ -430,7 +431,21 @@ def bench_b200(args, rank, world, local):
         barrier(world)
         flags = sim.solver_status().flags
         results[name] = (max_over_ranks(statistics.mean(t), world), statistics.mean(its), max(res), flags)
+    schedules = {}
+    if net is not None:  # the learned form with the network in the first k iterations of each pass only
+        for k in LEARNED_SCHEDULES:
+            restore_state(sim, state)
+            sim.set_solver(**LEARNED_FORM)
+            sim.set_learned_iterations(k)
+            run_steps(sim, driver, step0, args.warmup, flush)
+            barrier(world)
+            t, its, res = run_steps(sim, driver, step0 + args.warmup, args.steps, flush, status=True)
+            schedules[k] = (max_over_ranks(statistics.mean(t), world), statistics.mean(its), max(res))
+        sim.set_learned_iterations(0)
     learned = bench_learned(sim, net, n, results.get(LEARNED_NAME), results) if net is not None else {"unavailable": "no trained weights in the package"}
+    if schedules:
+        learned["schedules"] = {f"network in the first {k} iterations of a pass": {"ms_per_step": round(v[0], 4), "pcg_iterations": round(v[1], 1), "true_rel_residual_max": v[2]}
+                                for k, v in schedules.items()}
     # e2e through the ABI (headline form), same state
     restore_state(sim, state)
     sim.set_solver(**forms[headline])

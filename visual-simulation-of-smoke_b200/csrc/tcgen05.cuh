@@ -133,6 +133,14 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const void* map, int c0, 
         : "memory");
 }
 
+// Bulk (non-tensor) asynchronous copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from global to
+// shared memory, completing on the mbarrier (which must expect the bytes). No multicast.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes),
+                 "r"(smem_addr(bar))
+                 : "memory");
+}
+
 #endif  // __CUDACC__
 
 }  // namespace tc

@@ -54,6 +54,7 @@ struct ConvShape {
     static constexpr uint32_t kStage = kGP * kPlane;
     static constexpr int kMmas = CS == 8 ? 14 : 27;  // MMAs of one group (K = 16 each)
     static constexpr uint32_t kBChunk = static_cast<uint32_t>(conv_taps(CS) * CS * NC * 2);
+    static_assert(kBChunk % 16 == 0, "bulk copy size");
     static constexpr uint32_t kSmem = kStages * kStage + kBChunk;
     static constexpr uint32_t kTmemCols = 2 * NC < 32 ? 32u : static_cast<uint32_t>(2 * NC);  // two accumulators
     static_assert(NC == 16 || NC == 32, "N per block");
@@ -86,14 +87,12 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
     using S = ConvShape<CS, NC>;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* Bs = smem + S::kStages * S::kStage;
-    __shared__ uint64_t full[S::kStages], freed[S::kStages], done[2], drained[2];
+    __shared__ uint64_t full[S::kStages], freed[S::kStages], done[2], drained[2], wbar;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
     if (a.skip && *a.skip) return;  // uniform: every block reads the same word
     const int t = threadIdx.x, warp = t >> 5;
     const int chunk = blockIdx.y;
-    const uint4* wsrc = reinterpret_cast<const uint4*>(a.wpack + static_cast<size_t>(chunk) * S::kBChunk);
-    for (uint32_t i = t; i < S::kBChunk / 16u; i += kConvThreads) reinterpret_cast<uint4*>(Bs)[i] = wsrc[i];
     for (int st = 0; st < S::kStages; ++st)  // the slack after each box stays zero (read by the padding tap, times zero weights)
         for (int p = 0; p < S::kGP; ++p)
             for (uint32_t i = t; i < (kPlane - kBox) / 16u; i += kConvThreads) reinterpret_cast<uint4*>(smem + st * S::kStage + p * kPlane + kBox)[i] = make_uint4(0, 0, 0, 0);
@@ -106,6 +105,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
             tc::mbar_init(&done[b], 1);
             tc::mbar_init(&drained[b], kEpiThreads);
         }
+        tc::mbar_init(&wbar, 1);
         abort_flag = 0;
     }
     if (warp == 0) tc::tmem_alloc(&tmem_slot, S::kTmemCols);
@@ -128,6 +128,13 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
             const uint32_t b_base = tc::smem_addr(Bs);
             uint32_t loaded = 0, consumed = 0, issued = 0;  // items whose TMA was issued / whose box arrived / whose MMAs were issued
             bool ok = true;
+            // this block's chunk of the packed weights: bulk copies into shared memory, overlapping the first boxes
+            bool weights_ready = false;
+            {
+                const uint8_t* wsrc = a.wpack + static_cast<size_t>(chunk) * S::kBChunk;
+                tc::mbar_arrive_expect_tx(&wbar, S::kBChunk);
+                for (uint32_t off = 0; off < S::kBChunk; off += 16384u) tc::bulk_copy_g2s(Bs + off, wsrc + off, min(16384u, S::kBChunk - off), &wbar);
+            }
             auto issue_load = [&](uint32_t k) -> bool {
                 const int st = static_cast<int>(k % S::kStages);
                 // stage st last held item k - kStages: its MMAs must have completed before the box is overwritten
@@ -157,6 +164,13 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
                     break;
                 }
                 consumed = i + 1;
+                if (!weights_ready) {
+                    if (!tc::mbar_wait_or_abort(&wbar, 0, wait, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    weights_ready = true;
+                }
                 tc::fence_after_sync();
                 const uint32_t a_base = tc::smem_addr(smem + st * S::kStage);
 #pragma unroll 1
@@ -186,6 +200,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
             // nothing may still write this block's shared or tensor memory when it exits: every issued box must have
             // landed and the last MMAs completed (bounded waits again)
             for (uint32_t k = consumed; k < loaded; ++k) tc::mbar_wait(&full[k % S::kStages], (k / S::kStages) & 1u, wait);
+            if (!weights_ready) tc::mbar_wait(&wbar, 0, wait);
             if (issued > 0) tc::mbar_wait(&freed[(issued - 1) % S::kStages], ((issued - 1) / S::kStages) & 1u, wait);
         }
     } else {
@@ -547,14 +562,21 @@ __global__ void net_input_kernel(VolumeDims d, const float* __restrict__ r0, con
     }
 }
 
+// The glue kernels run one thread per (cell, group of 8 channels): work item i is cell i / (C / 8), channels
+// 8 * (i % (C / 8)) .. +7, so consecutive threads read consecutive 16-byte channel groups.
+
 // coarse[Q][c] = mean of the existing children fine[q][c]
 template <int C>
 __global__ void pool_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __restrict__ fine, __nv_bfloat16* __restrict__ coarse, const uint32_t* __restrict__ skip) {
     if (skip && *skip) return;
-    for (uint32_t Q = blockIdx.x * blockDim.x + threadIdx.x; Q < c.n; Q += gridDim.x * blockDim.x) {
+    constexpr int G = C / 8;
+    const uint64_t items = static_cast<uint64_t>(c.n) * G;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < items; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t Q = static_cast<uint32_t>(i / G);
+        const int h = static_cast<int>(i % G);
         int X, Y, Z;
         cell_of(c, Q, X, Y, Z);
-        float acc[C] = {};
+        float acc[8] = {};
         int count = 0;
         for (int dz = 0; dz < 2; ++dz)
             for (int dy = 0; dy < 2; ++dy)
@@ -562,23 +584,15 @@ __global__ void pool_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __r
                     const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
                     if (x >= f.nx || y >= f.ny || z >= f.nz) continue;
                     ++count;
-                    const __nv_bfloat16* p = fine + static_cast<size_t>(cell_at(f, x, y, z)) * C;
+                    float v[8];
+                    load_bf16x8(fine + static_cast<size_t>(cell_at(f, x, y, z)) * C + 8 * h, v);
 #pragma unroll
-                    for (int h = 0; h < C / 8; ++h) {
-                        float v[8];
-                        load_bf16x8(p + 8 * h, v);
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) acc[8 * h + k] += v[k];
-                    }
+                    for (int k = 0; k < 8; ++k) acc[k] += v[k];
                 }
         const float inv = 1.0f / static_cast<float>(count);
 #pragma unroll
-        for (int h = 0; h < C / 8; ++h) {
-            float v[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = acc[8 * h + k] * inv;
-            store_bf16x8(coarse + static_cast<size_t>(Q) * C + 8 * h, v);
-        }
+        for (int k = 0; k < 8; ++k) acc[k] *= inv;
+        store_bf16x8(coarse + static_cast<size_t>(Q) * C + 8 * h, acc);
     }
 }
 
@@ -586,51 +600,49 @@ __global__ void pool_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __r
 template <int C>
 __global__ void up_add_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip, __nv_bfloat16* __restrict__ out, const uint32_t* __restrict__ off) {
     if (off && *off) return;
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < f.n; q += gridDim.x * blockDim.x) {
+    constexpr int G = C / 8;
+    const uint64_t items = static_cast<uint64_t>(f.n) * G;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < items; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t q = static_cast<uint32_t>(i / G);
+        const int h = static_cast<int>(i % G);
         int x, y, z;
         cell_of(f, q, x, y, z);
         const uint32_t Q = cell_at(c, x / 2, y / 2, z / 2);
+        float a[8], b[8];
+        load_bf16x8(coarse + static_cast<size_t>(Q) * C + 8 * h, a);
+        load_bf16x8(skip + static_cast<size_t>(q) * C + 8 * h, b);
 #pragma unroll
-        for (int h = 0; h < C / 8; ++h) {
-            float a[8], b[8];
-            load_bf16x8(coarse + static_cast<size_t>(Q) * C + 8 * h, a);
-            load_bf16x8(skip + static_cast<size_t>(q) * C + 8 * h, b);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) a[k] += b[k];
-            store_bf16x8(out + static_cast<size_t>(q) * C + 8 * h, a);
-        }
+        for (int k = 0; k < 8; ++k) a[k] += b[k];
+        store_bf16x8(out + static_cast<size_t>(q) * C + 8 * h, a);
     }
 }
 
 // Backward of up (sum over the children), then the ReLU gate of the coarse activation: dc[Q] = (sum df[q]) * [act > 0]
 template <int C>
 __global__ void up_bwd_relu_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __restrict__ dfine, const __nv_bfloat16* __restrict__ act, __nv_bfloat16* __restrict__ dcoarse) {
-    for (uint32_t Q = blockIdx.x * blockDim.x + threadIdx.x; Q < c.n; Q += gridDim.x * blockDim.x) {
+    constexpr int G = C / 8;
+    const uint64_t items = static_cast<uint64_t>(c.n) * G;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < items; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t Q = static_cast<uint32_t>(i / G);
+        const int h = static_cast<int>(i % G);
         int X, Y, Z;
         cell_of(c, Q, X, Y, Z);
-        float acc[C] = {};
+        float acc[8] = {};
         for (int dz = 0; dz < 2; ++dz)
             for (int dy = 0; dy < 2; ++dy)
                 for (int dx = 0; dx < 2; ++dx) {
                     const int x = 2 * X + dx, y = 2 * Y + dy, z = 2 * Z + dz;
                     if (x >= f.nx || y >= f.ny || z >= f.nz) continue;
-                    const __nv_bfloat16* p = dfine + static_cast<size_t>(cell_at(f, x, y, z)) * C;
+                    float v[8];
+                    load_bf16x8(dfine + static_cast<size_t>(cell_at(f, x, y, z)) * C + 8 * h, v);
 #pragma unroll
-                    for (int h = 0; h < C / 8; ++h) {
-                        float v[8];
-                        load_bf16x8(p + 8 * h, v);
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) acc[8 * h + k] += v[k];
-                    }
+                    for (int k = 0; k < 8; ++k) acc[k] += v[k];
                 }
+        float g[8];
+        load_bf16x8(act + static_cast<size_t>(Q) * C + 8 * h, g);
 #pragma unroll
-        for (int h = 0; h < C / 8; ++h) {
-            float g[8], v[8];
-            load_bf16x8(act + static_cast<size_t>(Q) * C + 8 * h, g);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = g[k] > 0.0f ? acc[8 * h + k] : 0.0f;
-            store_bf16x8(dcoarse + static_cast<size_t>(Q) * C + 8 * h, v);
-        }
+        for (int k = 0; k < 8; ++k) acc[k] = g[k] > 0.0f ? acc[k] : 0.0f;
+        store_bf16x8(dcoarse + static_cast<size_t>(Q) * C + 8 * h, acc);
     }
 }
 
@@ -638,23 +650,24 @@ __global__ void up_bwd_relu_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat
 // gate of the fine activation: df[q] = (skip[q] + dc[parent] / count) * [act > 0]
 template <int C>
 __global__ void pool_bwd_add_relu_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __restrict__ skip, const __nv_bfloat16* __restrict__ dcoarse, const __nv_bfloat16* __restrict__ act, __nv_bfloat16* __restrict__ dfine) {
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < f.n; q += gridDim.x * blockDim.x) {
+    constexpr int G = C / 8;
+    const uint64_t items = static_cast<uint64_t>(f.n) * G;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < items; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t q = static_cast<uint32_t>(i / G);
+        const int h = static_cast<int>(i % G);
         int x, y, z;
         cell_of(f, q, x, y, z);
         const int X = x / 2, Y = y / 2, Z = z / 2;
         const int cx = min(2, f.nx - 2 * X), cy = min(2, f.ny - 2 * Y), cz = min(2, f.nz - 2 * Z);
         const float inv = 1.0f / static_cast<float>(cx * cy * cz);
         const uint32_t Q = cell_at(c, X, Y, Z);
+        float s[8], d[8], g[8];
+        load_bf16x8(skip + static_cast<size_t>(q) * C + 8 * h, s);
+        load_bf16x8(dcoarse + static_cast<size_t>(Q) * C + 8 * h, d);
+        load_bf16x8(act + static_cast<size_t>(q) * C + 8 * h, g);
 #pragma unroll
-        for (int h = 0; h < C / 8; ++h) {
-            float s[8], d[8], g[8];
-            load_bf16x8(skip + static_cast<size_t>(q) * C + 8 * h, s);
-            load_bf16x8(dcoarse + static_cast<size_t>(Q) * C + 8 * h, d);
-            load_bf16x8(act + static_cast<size_t>(q) * C + 8 * h, g);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) s[k] = g[k] > 0.0f ? s[k] + d[k] * inv : 0.0f;
-            store_bf16x8(dfine + static_cast<size_t>(q) * C + 8 * h, s);
-        }
+        for (int k = 0; k < 8; ++k) s[k] = g[k] > 0.0f ? s[k] + d[k] * inv : 0.0f;
+        store_bf16x8(dfine + static_cast<size_t>(q) * C + 8 * h, s);
     }
 }
 
@@ -759,7 +772,9 @@ cudaError_t launch_pack_conv(const float* w, int cin, int cout, int transpose, i
 namespace {
 
 constexpr int kGlueThreads = 256;
-unsigned glue_blocks(uint32_t n) { return std::max(1u, std::min<uint32_t>((n + kGlueThreads - 1) / kGlueThreads, 148u * 8u)); }
+unsigned glue_blocks(uint64_t n) { return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n + kGlueThreads - 1) / kGlueThreads, 148u * 8u))); }
+// Blocks of a per-(cell, 8-channel group) glue kernel over n cells of C channels.
+unsigned glue_blocks_c(uint32_t n, int c) { return glue_blocks(static_cast<uint64_t>(n) * (c / 8)); }
 
 // Blocks of the weight-gradient kernel along the cells for a volume of n cells and gy M-chunks.
 int wgrad_blocks_x(uint32_t n, int gy) {
@@ -958,19 +973,19 @@ cudaError_t net_forward(const NetImages& I, const NetActs& A, const float* r0, c
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // encoder
     if ((e = conv_layer(0, d[0], I, A.x0, A.e0, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    pool_kernel<16><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[0], d[1], A.e0, A.p1, skip);
+    pool_kernel<16><<<glue_blocks_c(d[1].n, 16), kGlueThreads, 0, s>>>(d[0], d[1], A.e0, A.p1, skip);
     if ((e = conv_layer(1, d[1], I, A.p1, A.e1, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    pool_kernel<32><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[1], d[2], A.e1, A.p2, skip);
+    pool_kernel<32><<<glue_blocks_c(d[2].n, 32), kGlueThreads, 0, s>>>(d[1], d[2], A.e1, A.p2, skip);
     if ((e = conv_layer(2, d[2], I, A.p2, A.e2, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    pool_kernel<64><<<glue_blocks(d[3].n), kGlueThreads, 0, s>>>(d[2], d[3], A.e2, A.p3, skip);
+    pool_kernel<64><<<glue_blocks_c(d[3].n, 64), kGlueThreads, 0, s>>>(d[2], d[3], A.e2, A.p3, skip);
     if ((e = conv_layer(3, d[3], I, A.p3, A.e3, nullptr, A.error, s, skip)) != cudaSuccess) return e;
     // bottom and decoder
     if ((e = conv_layer(4, d[3], I, A.e3, A.m3, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    up_add_kernel<64><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[2], d[3], A.m3, A.e2, A.s2, skip);
+    up_add_kernel<64><<<glue_blocks_c(d[2].n, 64), kGlueThreads, 0, s>>>(d[2], d[3], A.m3, A.e2, A.s2, skip);
     if ((e = conv_layer(5, d[2], I, A.s2, A.u2, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    up_add_kernel<32><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[1], d[2], A.u2, A.e1, A.s1, skip);
+    up_add_kernel<32><<<glue_blocks_c(d[1].n, 32), kGlueThreads, 0, s>>>(d[1], d[2], A.u2, A.e1, A.s1, skip);
     if ((e = conv_layer(6, d[1], I, A.s1, A.u1, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    up_add_kernel<16><<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], d[1], A.u1, A.e0, A.s0, skip);
+    up_add_kernel<16><<<glue_blocks_c(d[0].n, 16), kGlueThreads, 0, s>>>(d[0], d[1], A.u1, A.e0, A.s0, skip);
     return conv_layer(7, d[0], I, A.s0, nullptr, A.y, A.error, s, skip);
 }
 
@@ -992,30 +1007,30 @@ cudaError_t net_backward(const NetImages& I, const NetActs& A, const NetGrads& G
     if ((e = layer_wgrad(7, d[0], A.s0, G.gy, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
     if ((e = conv_layer_bwd(7, d[0], I, G.gy, nullptr, G.gs0, A.error, s)) != cudaSuccess) return e;
     // f: u1 = relu(conv_f(s1)); s1 = up(u2) + e1
-    up_bwd_relu_kernel<16><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[0], d[1], G.gs0, A.u1, G.gu1);
+    up_bwd_relu_kernel<16><<<glue_blocks_c(d[1].n, 16), kGlueThreads, 0, s>>>(d[0], d[1], G.gs0, A.u1, G.gu1);
     if ((e = layer_wgrad(6, d[1], A.s1, G.gu1, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
     if ((e = conv_layer_bwd(6, d[1], I, G.gu1, nullptr, G.gs1, A.error, s)) != cudaSuccess) return e;
     // e: u2 = relu(conv_e(s2)); s2 = up(m3) + e2
-    up_bwd_relu_kernel<32><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[1], d[2], G.gs1, A.u2, G.gu2);
+    up_bwd_relu_kernel<32><<<glue_blocks_c(d[2].n, 32), kGlueThreads, 0, s>>>(d[1], d[2], G.gs1, A.u2, G.gu2);
     if ((e = layer_wgrad(5, d[2], A.s2, G.gu2, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
     if ((e = conv_layer_bwd(5, d[2], I, G.gu2, nullptr, G.gs2, A.error, s)) != cudaSuccess) return e;
     // m: m3 = relu(conv_m(e3)); e3 = relu(conv_d(p3)) feeds m only, so its ReLU gate goes into m's backward
-    up_bwd_relu_kernel<64><<<glue_blocks(d[3].n), kGlueThreads, 0, s>>>(d[2], d[3], G.gs2, A.m3, G.gm3);
+    up_bwd_relu_kernel<64><<<glue_blocks_c(d[3].n, 64), kGlueThreads, 0, s>>>(d[2], d[3], G.gs2, A.m3, G.gm3);
     if ((e = layer_wgrad(4, d[3], A.e3, G.gm3, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
     if ((e = conv_layer_bwd(4, d[3], I, G.gm3, A.e3, G.ge3, A.error, s)) != cudaSuccess) return e;
     // d: e3 = relu(conv_d(p3)); p3 = pool(e2)
     if ((e = layer_wgrad(3, d[3], A.p3, G.ge3, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
     if ((e = conv_layer_bwd(3, d[3], I, G.ge3, nullptr, G.gp3, A.error, s)) != cudaSuccess) return e;
     // c: e2 = relu(conv_c(p2)) feeds p3 and s2
-    pool_bwd_add_relu_kernel<64><<<glue_blocks(d[2].n), kGlueThreads, 0, s>>>(d[2], d[3], G.gs2, G.gp3, A.e2, G.ge2);
+    pool_bwd_add_relu_kernel<64><<<glue_blocks_c(d[2].n, 64), kGlueThreads, 0, s>>>(d[2], d[3], G.gs2, G.gp3, A.e2, G.ge2);
     if ((e = layer_wgrad(2, d[2], A.p2, G.ge2, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
     if ((e = conv_layer_bwd(2, d[2], I, G.ge2, nullptr, G.gp2, A.error, s)) != cudaSuccess) return e;
     // b: e1 = relu(conv_b(p1)) feeds p2 and s1
-    pool_bwd_add_relu_kernel<32><<<glue_blocks(d[1].n), kGlueThreads, 0, s>>>(d[1], d[2], G.gs1, G.gp2, A.e1, G.ge1);
+    pool_bwd_add_relu_kernel<32><<<glue_blocks_c(d[1].n, 32), kGlueThreads, 0, s>>>(d[1], d[2], G.gs1, G.gp2, A.e1, G.ge1);
     if ((e = layer_wgrad(1, d[1], A.p1, G.ge1, G, grad, accumulate, A.error, s)) != cudaSuccess) return e;
     if ((e = conv_layer_bwd(1, d[1], I, G.ge1, nullptr, G.gp1, A.error, s)) != cudaSuccess) return e;
     // a: e0 = relu(conv_a(x0)) feeds p1 and s0
-    pool_bwd_add_relu_kernel<16><<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], d[1], G.gs0, G.gp1, A.e0, G.ge0);
+    pool_bwd_add_relu_kernel<16><<<glue_blocks_c(d[0].n, 16), kGlueThreads, 0, s>>>(d[0], d[1], G.gs0, G.gp1, A.e0, G.ge0);
     return layer_wgrad(0, d[0], A.x0, G.ge0, G, grad, accumulate, A.error, s);
 }
 
