@@ -63,17 +63,20 @@ def mg_grid_levels(n):
 NET_FORWARD_KERNELS = 15
 
 
-def solver_launches(n, iterations, refinement, learned=False):
+def solver_launches(n, iterations, refinement, learned=False, net_iterations=0):
     """Kernels the multigrid solve graph launches: set-up and write-back, per refinement pass the first update, the
     accumulation and the FP64 residual, and per iteration the loop body (restriction and the fused prolongation +
-    smoothing of every grid level below 0, the block-level cycle, level-0 prolongation, smoothing, p/q and update;
-    the learned form adds the residual after the V-cycle, the network and the correction)."""
+    smoothing of every grid level below 0, the block-level cycle, level-0 prolongation, smoothing, p/q and update).
+    The learned form adds per pass the gate of its second loop, and per iteration with the network (the first
+    `net_iterations`, 0: all) the residual after the V-cycle, the network and the correction."""
     _, g = mg_grid_levels(n)
     # coarse grid levels of at most 64^3 cells fuse prolongation and smoothing (mg_up_kernel)
     per_iteration = sum(2 if -(-n // (1 << l)) ** 3 <= 64 ** 3 else 3 for l in range(1, g)) + 5
+    total = 2 + 3 * (refinement + 1) + per_iteration * iterations
     if learned:
-        per_iteration += 3 + NET_FORWARD_KERNELS
-    return 2 + 3 * (refinement + 1) + per_iteration * iterations
+        with_net = iterations if net_iterations == 0 else min(net_iterations, iterations)
+        total += (refinement + 1) + (3 + NET_FORWARD_KERNELS) * with_net
+    return total
 
 
 def load_peaks():
@@ -383,7 +386,9 @@ HEADLINE = "multigrid_fp64"
 # (z = V(r) + N(r - A V(r))), FP64 dots and refinement, warm start; measured when the package's trained weights exist.
 LEARNED_NAME = "learned_fp64"
 LEARNED_FORM = dict(mode=abi.SOLVER_LEARNED_FCG, reduction=abi.REDUCTION_FP64, max_iterations=500, tolerance=1e-5, refinement=1, warm_start=True)
-LEARNED_SCHEDULES = (1, 2, 4)  # also measured: the network in the first k iterations of each pass only
+# Schedules of the learned form, measured before the forms: the network in the first k iterations of each pass only
+# (0: in every iteration); the fastest one that meets the tolerance is the learned form's schedule.
+LEARNED_SCHEDULES = (1, 2, 4, 0)
 
 
 def bench_b200(args, rank, world, local):
@@ -414,6 +419,20 @@ def bench_b200(args, rank, world, local):
     results = {}
     tunes = {}
     clocks = None
+    schedules = {}
+    schedule = 0
+    if net is not None:  # the learned form's schedule: the fastest that meets the tolerance
+        for k in LEARNED_SCHEDULES:
+            restore_state(sim, state)
+            sim.set_solver(**LEARNED_FORM)
+            sim.set_learned_iterations(k)
+            run_steps(sim, driver, step0, args.warmup, flush)
+            barrier(world)
+            t, its, res = run_steps(sim, driver, step0 + args.warmup, args.steps, flush, status=True)
+            schedules[k] = (max_over_ranks(statistics.mean(t), world), statistics.mean(its), max(res))
+        ok = [k for k, v in schedules.items() if v[2] <= LEARNED_FORM["tolerance"]] or list(schedules)
+        schedule = min(ok, key=lambda k: schedules[k][0])
+        sim.set_learned_iterations(schedule)
     for name, form in forms.items():
         restore_state(sim, state)
         sim.set_solver(**form)
@@ -431,20 +450,10 @@ def bench_b200(args, rank, world, local):
         barrier(world)
         flags = sim.solver_status().flags
         results[name] = (max_over_ranks(statistics.mean(t), world), statistics.mean(its), max(res), flags)
-    schedules = {}
-    if net is not None:  # the learned form with the network in the first k iterations of each pass only
-        for k in LEARNED_SCHEDULES:
-            restore_state(sim, state)
-            sim.set_solver(**LEARNED_FORM)
-            sim.set_learned_iterations(k)
-            run_steps(sim, driver, step0, args.warmup, flush)
-            barrier(world)
-            t, its, res = run_steps(sim, driver, step0 + args.warmup, args.steps, flush, status=True)
-            schedules[k] = (max_over_ranks(statistics.mean(t), world), statistics.mean(its), max(res))
-        sim.set_learned_iterations(0)
     learned = bench_learned(sim, net, n, results.get(LEARNED_NAME), results) if net is not None else {"unavailable": "no trained weights in the package"}
     if schedules:
-        learned["schedules"] = {f"network in the first {k} iterations of a pass": {"ms_per_step": round(v[0], 4), "pcg_iterations": round(v[1], 1), "true_rel_residual_max": v[2]}
+        learned["schedule"] = schedule_name(schedule)
+        learned["schedules"] = {schedule_name(k): {"ms_per_step": round(v[0], 4), "pcg_iterations": round(v[1], 1), "true_rel_residual_max": v[2]}
                                 for k, v in schedules.items()}
     # e2e through the ABI (headline form), same state
     restore_state(sim, state)
@@ -476,7 +485,7 @@ def bench_b200(args, rank, world, local):
                        if headline == LEARNED_NAME else "multigrid-preconditioned FCG, FP64 dots, FP64 refinement, warm start from the previous step's pressure"), "grid": [n, n, n], "dt": 0.01,
                    "source_box": "16x8x16 at x,z in [56,72), y in [0,8)" if n == 128 else "n/8 x n/16 x n/8", "spinup_steps": SPINUP_STEPS,
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                   "learned_preconditioner": "headline form" if headline == LEARNED_NAME else "not used (no trained weights)"},
+                   "learned_preconditioner": f"headline form, {schedule_name(schedule)}" if headline == LEARNED_NAME else "not used (no trained weights)"},
         "pcg_iterations": round(its, 1), "true_rel_residual_max": res,
         "cells_per_s": round(cells * world / (ms * 1e-3), 1),
         "forms": {k: {"ms_per_step": round(v[0], 4), "pcg_iterations": round(v[1], 1), "rel_residual_max": v[2]} for k, v in results.items()},
@@ -485,7 +494,7 @@ def bench_b200(args, rank, world, local):
         "roofline": roof,
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": driver.h2d_bytes, "d2h_bytes_per_step": driver.d2h_bytes,
                 "includes": "per-step box inputs H2D, velocity/density/temperature views, source/force updates, step, total-density D2H, host sync"},
-        "gpu_launches": round(args.steps * (STEP_KERNELS + 1 + solver_launches(n, its, forms[headline]["refinement"], learned=headline == LEARNED_NAME))),
+        "gpu_launches": round(args.steps * (STEP_KERNELS + 1 + solver_launches(n, its, forms[headline]["refinement"], learned=headline == LEARNED_NAME, net_iterations=schedule))),
         "clocks": clocks.summary() if clocks is not None else None,
         "launch_tune": {k: tune_summary(v) for k, v in tunes.items()} if tunes else "defaults (--no-tune)",
         "learned": learned,
@@ -499,6 +508,10 @@ def bench_b200(args, rank, world, local):
 
 # (cin, cout, level) of the network's convolutions (unet.h: 4 levels, 16/32/64/128 channels)
 NET_LAYERS = [(2, 16, 0), (16, 32, 1), (32, 64, 2), (64, 128, 3), (128, 64, 3), (64, 32, 2), (32, 16, 1), (16, 1, 0)]
+
+
+def schedule_name(k):
+    return "network in every iteration" if k == 0 else f"network in the first {k} iteration{'s' if k > 1 else ''} of a pass"
 
 
 def net_flops(nx, ny, nz, executed=False):
@@ -811,13 +824,17 @@ def profile_workload(args):
             rhs = sim.view(abi.VIEW_FLOW_PRESSURE_RHS).clone()
             occ = torch.zeros(rhs.shape, dtype=torch.uint8, device="cuda")
         stream.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()  # ncu --profile-from-start off captures from here
         for k in range(args.profile_count):
             out = net.apply(rhs, occ)
         torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
         print(json.dumps({"profile": "net", "count": args.profile_count, "out_norm": float(out.norm())}), flush=True)
         net.close()
         sim.close()
         return
+    stream.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()  # ncu --profile-from-start off captures from here
     for k in range(args.profile_count):
         if args.profile == "step":
             driver.apply(SPINUP_STEPS + k)
@@ -825,6 +842,7 @@ def profile_workload(args):
         else:
             sim.solve_pressure(eager=args.profile in ("solve", "learned-solve"))
     stream.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
     st = sim.solver_status()
     print(json.dumps({"profile": args.profile, "count": args.profile_count, "iterations": st.iterations, "passes": st.passes, "status": st.status,
                       "true_rel_residual": st.true_relative_residual}), flush=True)

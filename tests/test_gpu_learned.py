@@ -215,3 +215,25 @@ def test_useless_network_costs_no_iterations(smoke_lib):
     assert st.iterations <= st_m.iterations + 2
     assert np.abs(p - p_j).max() <= 5e-3 * np.abs(p_j).max()
     sim.close()
+
+
+@pytest.mark.parametrize("schedule", [1, 3, 0])
+def test_schedule_graph_matches_eager(smoke_lib, trained, schedule):
+    """With the network in the first `schedule` iterations of each pass (0: all), the graph solve (a loop with the
+    network, then a loop with the V-cycle alone) and the host-driven solve (which picks each iteration's body from
+    the network flag the update left) take the same iterations to the same answer; every schedule reaches the
+    tolerance."""
+    net, _ = trained
+    sim, keep = held_out_system(smoke_lib)
+    sim.set_learned_iterations(schedule)
+    st_g, p_g = solve(sim, LEARNED, net)
+    sim.solve_pressure(eager=True)
+    st_e = sim.solver_status()
+    p_e = sim.snapshot([abi.VIEW_FLOW_PRESSURE])["pressure"]
+    sim.set_learned_iterations(0)
+    sim.close()
+    report(f"learned/schedule{schedule}", {"graph": st_g.iterations, "eager": st_e.iterations})
+    for st in (st_g, st_e):
+        assert st.status == abi.SOLVE_CONVERGED and st.true_relative_residual <= 1e-5
+    assert abs(st_g.iterations - st_e.iterations) <= 1 and st_g.passes == st_e.passes
+    assert np.abs(p_g - p_e).max() <= 1e-5 * np.abs(p_g).max()

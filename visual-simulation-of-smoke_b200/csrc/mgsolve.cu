@@ -24,7 +24,11 @@
 // the body of a graph `while` node runs: coarse restrictions, the block-level cycle, coarse prolongation +
 // smoothing, level-0 prolongation, level-0 smoothing with (z, r) (z, q), p/q with (p, q) (p, r), and the level-0
 // update r -= alpha q, e += alpha p with pre-smoothing, restriction and ||r||^2. The last block of the update
-// kernel tests convergence and sets the loop condition (cudaGraphSetConditional), so the host never waits.
+// kernel tests convergence and sets the loop condition (cudaGraphSetConditional), so the host never waits. A learned
+// solve's pass has two `while` nodes: the first body runs the network, and its update ends that loop when the next
+// iteration goes without it (past the schedule's iterations, or after a fallback); the second body is the V-cycle
+// alone, entered when the first loop ended without stopping. So iterations without the network launch none of the
+// network's kernels.
 // Dot products: block sums, then FP64 atomic adds spread over kMgSlots addresses, summed in slot order.
 // Each restriction block covers whole 2x2x2 parents and writes the coarse right-hand side directly.
 #include <algorithm>
@@ -321,9 +325,10 @@ __global__ void __launch_bounds__(kThreads) mg_setup_kernel(const __grid_constan
 
 // Level-0 update: r' = r - alpha q, e += alpha p, zp = w D^-1 r', restriction of r' - A zp into level 1, ||r'||^2.
 // initial = 1: the pass's first round (alpha = 0, no iteration counted). The last block tests convergence, flips
-// the buffer parity and sets the loop condition `cond`.
+// the buffer parity and sets the loop condition `cond`: continue unless stopped, and (net_loop = 1, the loop of a
+// learned solve whose body runs the network) unless the next iteration goes without the network.
 template <typename T, bool LEARNED>
-__global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_constant__ MgSolveArgs A, int initial, cudaGraphConditionalHandle cond, int in_graph) {
+__global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_constant__ MgSolveArgs A, int initial, cudaGraphConditionalHandle cond, int in_graph, int net_loop) {
     const MgLevel& L0 = A.H.L[0];
     MgState* st = A.st;
     const bool skip = st->halt || st->fail;  // uniform over the grid
@@ -406,7 +411,13 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
     for (int k = kAccRR; k < kAccCount; ++k) zero_acc(st, k);
     st->loop = stop ? 0u : 1u;
     __threadfence();
-    if (in_graph) cudaGraphSetConditional(cond, stop ? 0u : 1u);
+    if (in_graph) cudaGraphSetConditional(cond, (stop || (LEARNED && net_loop && st->net_off)) ? 0u : 1u);
+}
+
+// The condition of a learned solve's second loop (the V-cycle alone, after the network's iterations): the loop flag
+// the last update left.
+__global__ void mg_loop_gate_kernel(const MgState* __restrict__ st, cudaGraphConditionalHandle cond) {
+    cudaGraphSetConditional(cond, st->loop);
 }
 
 // Level l >= 1: zp = w D^-1 r (pre-smoothing from zero), restriction of r - A zp into level l + 1.
@@ -1061,9 +1072,9 @@ cudaError_t add_while(cudaStream_t s, cudaStream_t body_stream, cudaGraphConditi
 
 // The level-0 update of the solve's preconditioner kind.
 template <typename T>
-void launch_update(const MgSolveArgs& A, int initial, cudaGraphConditionalHandle h, int in_graph, cudaStream_t s) {
-    if (A.learned) mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, A.H.L[0], A.wave), kBlock, 0, s>>>(A, initial, h, in_graph);
-    else mg_update_kernel<T, false><<<wave(mg_update_kernel<T, false>, A.H.L[0], A.wave), kBlock, 0, s>>>(A, initial, h, in_graph);
+void launch_update(const MgSolveArgs& A, int initial, cudaGraphConditionalHandle h, int in_graph, int net_loop, cudaStream_t s) {
+    if (A.learned) mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, A.H.L[0], A.wave), kBlock, 0, s>>>(A, initial, h, in_graph, net_loop);
+    else mg_update_kernel<T, false><<<wave(mg_update_kernel<T, false>, A.H.L[0], A.wave), kBlock, 0, s>>>(A, initial, h, in_graph, 0);
 }
 
 // The V-cycle below level 0: restrictions of levels 1..g-1, the block-level cycle, the up passes of levels g-1..1,
@@ -1084,12 +1095,14 @@ void launch_coarse_cycle(const MgSolveArgs& A, uint32_t block_bytes, cudaStream_
     mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[1], A.wave), kBlock, 0, bs>>>(H, 0);
 }
 
-// One iteration's loop body (everything after the update that tests convergence, up to the next update).
+// One iteration's loop body (everything after the update that tests convergence, up to the next update); net = 1:
+// a learned solve's iteration with the network, net = 0: the V-cycle alone (a learned solve's iterations past its
+// schedule or after it dropped the network run this body, with the learned solve's update).
 template <typename T>
-void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_graph, uint32_t block_bytes, cudaStream_t bs) {
+void launch_body(const MgSolveArgs& A, int net, cudaGraphConditionalHandle h, int in_graph, uint32_t block_bytes, cudaStream_t bs) {
     const MgLevel& L0 = A.H.L[0];
     launch_coarse_cycle(A, block_bytes, bs);
-    if (A.learned) {  // z = z_V + N(r - A z_V), post-smoothed: the network corrects what the V-cycle leaves
+    if (net) {  // z = z_V + N(r - A z_V), post-smoothed: the network corrects what the V-cycle leaves
         const LearnedSolve& N = *A.net;
         mg_smooth_kernel<true, T, false><<<wave(mg_smooth_kernel<true, T, false>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
         mg_net_residual_kernel<T><<<wave(mg_net_residual_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
@@ -1097,12 +1110,12 @@ void launch_body(const MgSolveArgs& A, cudaGraphConditionalHandle h, int in_grap
         mg_net_gamma_kernel<T><<<wave(mg_net_gamma_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
         mg_net_add_kernel<T><<<wave(mg_net_add_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
         mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
-        mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
+        mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph, 1);
         return;
     }
     mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
     mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
-    mg_update_kernel<T, false><<<wave(mg_update_kernel<T, false>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph);
+    launch_update<T>(A, 0, h, in_graph, 0, bs);
 }
 
 // Learned solve with the network's warm start: x64 = N(b) (through the q array, which the set-up clears), so the
@@ -1141,9 +1154,17 @@ cudaError_t enqueue_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream
         cudaGraphConditionalHandle h;
         e = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
         if (e != cudaSuccess) return e;
-        launch_update<T>(A, 1, h, 1, s);
-        e = add_while(s, body_stream, h, [&](cudaStream_t bs) { launch_body<T>(A, h, 1, block_bytes, bs); });
+        launch_update<T>(A, 1, h, 1, A.learned, s);
+        e = add_while(s, body_stream, h, [&](cudaStream_t bs) { launch_body<T>(A, A.learned, h, 1, block_bytes, bs); });
         if (e != cudaSuccess) return e;
+        if (A.learned) {  // then the V-cycle alone, for the iterations past the schedule or after a fallback
+            cudaGraphConditionalHandle h2;
+            e = cudaGraphConditionalHandleCreate(&h2, graph, 0, cudaGraphCondAssignDefault);
+            if (e != cudaSuccess) return e;
+            mg_loop_gate_kernel<<<1, 1, 0, s>>>(A.st, h2);
+            e = add_while(s, body_stream, h2, [&](cudaStream_t bs) { launch_body<T>(A, 0, h2, 1, block_bytes, bs); });
+            if (e != cudaSuccess) return e;
+        }
         if (A.ir) {
             mg_accumulate_kernel<<<wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s>>>(A);
             mg_residual_kernel<<<wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s>>>(A);
@@ -1162,17 +1183,18 @@ cudaError_t run_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream_t s
     if ((e = learned_guess(A, s)) != cudaSuccess) return e;
     mg_setup_kernel<T><<<wave(mg_setup_kernel<T>, L0, A.wave), kBlock, 0, s>>>(A);
     const int passes = A.ir ? A.refinement + 1 : 1;
-    auto loop_flag = [&](uint32_t& flag) {
-        const cudaError_t r = cudaMemcpyAsync(&flag, &A.st->loop, sizeof(flag), cudaMemcpyDeviceToHost, s);
+    auto loop_flags = [&](uint32_t& flag, uint32_t& net_off) {
+        cudaError_t r = cudaMemcpyAsync(&flag, &A.st->loop, sizeof(flag), cudaMemcpyDeviceToHost, s);
+        if (r == cudaSuccess) r = cudaMemcpyAsync(&net_off, &A.st->net_off, sizeof(net_off), cudaMemcpyDeviceToHost, s);
         return r == cudaSuccess ? cudaStreamSynchronize(s) : r;
     };
     for (int pass = 0; pass < passes; ++pass) {
-        launch_update<T>(A, 1, 0, 0, s);
+        launch_update<T>(A, 1, 0, 0, 0, s);
         for (;;) {  // bounded: every update counts an iteration and stops at max_iterations
-            uint32_t flag = 0;
-            if ((e = loop_flag(flag)) != cudaSuccess) return e;
+            uint32_t flag = 0, net_off = 1;
+            if ((e = loop_flags(flag, net_off)) != cudaSuccess) return e;
             if (!flag) break;
-            launch_body<T>(A, 0, 0, block_bytes, s);
+            launch_body<T>(A, A.learned && !net_off, 0, 0, block_bytes, s);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (A.ir) {
