@@ -269,9 +269,14 @@ def restore_state(sim, state):
 #    smoothing 14) plus the restricted right-hand sides -> 85 B per fine cell and iteration.
 JACOBI_BYTES_PER_CELL_ITERATION = 42.0
 MG_BYTES_PER_CELL_ITERATION = 85.0
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum over every kernel) of one multigrid FCG solve from zero
+# on the 128^3 plume after the spin-up, 12 iterations, 1 pass: the kernels of the graph launched one by one
+# (bench.py --profile solve, ncu --cache-control none so that L2 carries over between kernels as in the graph);
+# 41.8 MB read + 434.4 MB written, per grid size. Scaled by iterations when a solve takes another count.
+MG_SOLVE_DRAM_BYTES = {128: (476.2e6, 12)}
 
 
-def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5, bytes_per_iteration=JACOBI_BYTES_PER_CELL_ITERATION, kernel="pcg_kernel"):
+def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5, bytes_per_iteration=JACOBI_BYTES_PER_CELL_ITERATION, kernel="pcg_kernel", traffic_table=None):
     """Times the pressure solve alone (smoke_b200_solve_pressure_cuda on the step's right-hand side: one graph launch
     on the context stream) with CUDA events on that stream; algorithmic bytes = cells x (bytes per iteration x
     iterations + set-up 24 B + 46 B per refinement pass)."""
@@ -297,10 +302,17 @@ def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5, bytes_p
     it = statistics.median(iters)
     algo_bytes = n_cells * (bytes_per_iteration * it + 24.0 + 46.0 * passes)
     achieved = algo_bytes / (ms * 1e-3) / 1e9
+    n = round(n_cells ** (1.0 / 3.0))
+    traffic = None
+    if traffic_table and n in traffic_table:
+        measured, measured_its = traffic_table[n]
+        traffic = round(measured * it / measured_its)
     return {"bound": "hbm", "kernel": kernel, "achieved": round(achieved, 1), "peak": peak_gbs, "peak_kind": peak_kind, "unit": "GB/s",
-            "frac": round(achieved / peak_gbs, 3), "traffic": None, "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(ms, 4), "iterations": it,
+            "frac": round(achieved / peak_gbs, 3), "traffic": traffic, "traffic_over_algorithmic": round(traffic / algo_bytes, 3) if traffic else None,
+            "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(ms, 4), "iterations": it,
             "bytes_per_cell_iteration": bytes_per_iteration,
-            "note": "the solve's working set (~90 MB) is mostly L2-resident at 128^3; per-kernel times and DRAM traffic are in profiles/"}
+            "note": "traffic: DRAM bytes of one solve from an ncu capture of its kernels (cache control off, so L2 carries over as in the graph); "
+                    "the working set (~90 MB at 128^3) stays mostly in the 126 MB L2, so the solve is bound by latency, not by HBM"}
 
 
 def divergence_norms(cfg, u, v, w):
@@ -469,7 +481,7 @@ def bench_b200(args, rank, world, local):
     cpu, accuracy = cpu_baseline(sim, driver, cfg, step0 + args.warmup + args.steps) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else (None, None)
     # the solve alone, cold (a warm start would begin each repeat from the converged answer of the previous one)
     sim.set_solver(**FORMS["multigrid_fp64_cold"])
-    roof = solver_kernel_roofline(sim, n ** 3, *load_peaks(), bytes_per_iteration=MG_BYTES_PER_CELL_ITERATION, kernel="multigrid-preconditioned FCG solve from zero (one graph launch of the mg_* kernels)")
+    roof = solver_kernel_roofline(sim, n ** 3, *load_peaks(), bytes_per_iteration=MG_BYTES_PER_CELL_ITERATION, kernel="multigrid-preconditioned FCG solve from zero (one graph launch of the mg_* kernels)", traffic_table=MG_SOLVE_DRAM_BYTES)
     sim.close()
     if net is not None:
         net.close()
@@ -662,7 +674,7 @@ def bench_large(args, rank, world, local):
         t, its, res = run_steps(sim, driver, spin + args.warmup, args.steps, flush, status=True)
     cells = cfg.nx * cfg.ny * cfg.nz
     sim.set_solver(**FORMS["multigrid_fp64_cold"])  # the solve alone, from zero
-    roof = solver_kernel_roofline(sim, cells, *load_peaks(), repeats=3, bytes_per_iteration=MG_BYTES_PER_CELL_ITERATION, kernel="multigrid-preconditioned FCG solve from zero (one graph launch of the mg_* kernels)")
+    roof = solver_kernel_roofline(sim, cells, *load_peaks(), repeats=3, bytes_per_iteration=MG_BYTES_PER_CELL_ITERATION, kernel="multigrid-preconditioned FCG solve from zero (one graph launch of the mg_* kernels)", traffic_table=MG_SOLVE_DRAM_BYTES)
     sim.close()
     ms = max_over_ranks(statistics.mean(t), world)
     if rank != 0:

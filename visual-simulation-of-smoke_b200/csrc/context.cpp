@@ -161,6 +161,8 @@ struct SmokeSimulationContext_t {
         slots.push_back({reinterpret_cast<void**>(&anchor), sizeof(int32_t)});
         slots.push_back({reinterpret_cast<void**>(&control), sizeof(PcgControl)});
         slots.push_back({reinterpret_cast<void**>(&mg_state), sizeof(MgState)});
+        mg_work.part_stride = mg_partial_blocks(P.nx, P.ny, P.nz);
+        slots.push_back({reinterpret_cast<void**>(&mg_work.part), static_cast<size_t>(kAccCount) * mg_work.part_stride * sizeof(double)});
         // multigrid levels: level 0 shares the Jacobi solver's vectors; coarser levels get their own arrays
         mg.levels = mg_level_count(P.nx, P.ny, P.nz);
         for (int a = 0; a < 3; ++a) mg.fper[a] = P.fper[a];

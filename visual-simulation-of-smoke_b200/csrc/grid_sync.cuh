@@ -1,4 +1,4 @@
-// Grid-wide synchronisation for the persistent cooperative solver kernels (pcg.cu, mgpcg.cu): a bounded-wait grid
+// Grid-wide synchronisation for the persistent cooperative solver kernels (pcg.cu): a bounded-wait grid
 // barrier fused with an all-reduce of four sums, and block-level helpers. THREADS is the kernel's block size.
 #pragma once
 

@@ -130,7 +130,12 @@ struct PcgWork {
     float* p;
     float* e;      // FP32 correction iterate of a refinement pass
     double* x64;   // FP64 solution accumulator (refinement); kept between steps as the warm start
+    double* part;  // per-block partial sums of the dot products, [kAccCount][part_stride] (FP64)
+    uint32_t part_stride;  // blocks of the largest level-0 grid (mg_partial_blocks)
 };
+// Blocks of the largest grid a level-0 kernel of the multigrid solve launches on an nx x ny x nz grid (one
+// 32 x 4 x 2 tile per block): the length of each accumulator's row of per-block partial sums.
+uint32_t mg_partial_blocks(int nx, int ny, int nz);
 
 struct PcgLaunchShape {
     int blocks;
@@ -140,7 +145,7 @@ struct PcgLaunchShape {
 };
 
 // ------------------------------------------------------------------------------------------ multigrid hierarchy
-// Geometric multigrid for the pressure operator (mgpcg.cu). Level 0 is the grid itself; level l+1 halves every
+// Geometric multigrid for the pressure operator (mgsolve.cu). Level 0 is the grid itself; level l+1 halves every
 // extent (rounding up). A coarse cell is fluid when any of its children is; every level's operator is the masked
 // 7-point stencil of its fluid cells (the fine rules without the anchor).
 constexpr int kMgMaxLevels = 12;
@@ -175,12 +180,15 @@ struct MgWork {
     float* q;
     float* e;      // FP32 correction iterate of a refinement pass
     double* x64;   // FP64 solution accumulator (refinement); kept between steps as the warm start
+    double* part;  // per-block partial sums of the dot products, [kAccCount][part_stride] (FP64)
+    uint32_t part_stride;  // blocks of the largest level-0 grid (mg_partial_blocks)
 };
+// Blocks of the largest grid a level-0 kernel of the multigrid solve launches on an nx x ny x nz grid (one
+// 32 x 4 x 2 tile per block): the length of each accumulator's row of per-block partial sums.
+uint32_t mg_partial_blocks(int nx, int ny, int nz);
 // Device-side scalars of one multigrid solve (reset at the start of every solve).
-constexpr int kMgSlots = 32;  // addresses each FP64 dot-product accumulator is spread over
 enum MgAccumulator { kAccBB = 0, kAccRR, kAccZR, kAccZQ, kAccPQ, kAccPR, kAccNet, kAccNetA, kAccCount };
 struct MgState {
-    double acc[kAccCount][kMgSlots];
     double bb, rnorm2, pq_prev, target2, pass_rr0, true_rel;
     double net_rr;         // learned solve: ||r - A z_V||^2, the squared norm of the network's input
     double net_gamma;      // learned solve: the energy-optimal step along the network's correction

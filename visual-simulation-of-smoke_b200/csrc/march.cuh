@@ -1,4 +1,4 @@
-// z-marching ("2.5D") traversal shared by the persistent solver kernels (pcg.cu, mgpcg.cu).
+// z-marching ("2.5D") traversal shared by the persistent solver kernels (pcg.cu).
 //
 // The grid is cut into 32x8-cell columns; each block owns a fixed, balanced range of column-planes and walks each
 // of its column segments in z. Every thread owns one (x, y) cell of the column, so one plane step costs one

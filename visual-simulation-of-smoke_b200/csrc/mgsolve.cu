@@ -29,7 +29,8 @@
 // iteration goes without it (past the schedule's iterations, or after a fallback); the second body is the V-cycle
 // alone, entered when the first loop ended without stopping. So iterations without the network launch none of the
 // network's kernels.
-// Dot products: block sums, then FP64 atomic adds spread over kMgSlots addresses, summed in slot order.
+// Dot products: block sums in a fixed order, stored per block in FP64 and added in block order by the last block to
+// finish, so the solve is deterministic.
 // Each restriction block covers whole 2x2x2 parents and writes the coarse right-hand side directly.
 #include <algorithm>
 #include <map>
@@ -203,9 +204,19 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
-// Block sums of a and b added (FP64) into accumulators ka and kb (kb < 0: only a), in slot block % kMgSlots.
+// Programmatic dependent launch. The iteration's kernels are launched with programmatic stream serialisation
+// (pdl_launch): each lets the stream's next kernel start launching at once, and then waits in griddepcontrol.wait
+// until the previous kernel has completed and its writes are visible. So a kernel's launch and block dispatch
+// overlap its predecessor's tail instead of following it; nothing is read before the wait.
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Block sums of a and b (in a fixed order) stored as this block's partials of accumulators ka and kb (kb < 0: only
+// a). Thread 0 writes them.
 template <typename T>
-__device__ __forceinline__ void block_accumulate(MgState* st, int ka, T a, int kb, T b) {
+__device__ __forceinline__ void block_accumulate(const MgWork& W, int ka, T a, int kb, T b) {
     __shared__ T part[2][kThreads / 32];
     const int t = tid(), lane = t & 31, warp = t >> 5;
     a = warp_sum(a);
@@ -219,23 +230,58 @@ __device__ __forceinline__ void block_accumulate(MgState* st, int ka, T a, int k
         a = warp_sum(lane < kThreads / 32 ? part[0][lane] : T(0));
         b = warp_sum(lane < kThreads / 32 ? part[1][lane] : T(0));
         if (lane == 0) {
-            const uint32_t slot = block_linear() % kMgSlots;
-            atomicAdd(&st->acc[ka][slot], static_cast<double>(a));
-            if (kb >= 0) atomicAdd(&st->acc[kb][slot], static_cast<double>(b));
+            const uint32_t blk = block_linear();
+            W.part[static_cast<size_t>(ka) * W.part_stride + blk] = static_cast<double>(a);
+            if (kb >= 0) W.part[static_cast<size_t>(kb) * W.part_stride + blk] = static_cast<double>(b);
         }
     }
 }
 
-// Sum of accumulator k in slot order (read through L2).
-__device__ __forceinline__ double total(const MgState* st, int k) {
-    double s = 0.0;
-#pragma unroll 8
-    for (int i = 0; i < kMgSlots; ++i) s += __ldcg(&st->acc[k][i]);
-    return s;
+// Last-block election with the totals of accumulators ka and kb (kb < 0: only ka): true in every thread of the block
+// that finishes last, after every block's partials are visible to it. The partials are added in a fixed order
+// (thread i takes blocks i, i + kThreads, ..., then a fixed tree over lanes and warps), so a solve's scalars do not
+// depend on the order in which blocks finish, and every thread of the last block holds the same totals.
+__device__ bool last_block_totals(unsigned int* counter, const MgWork& W, int ka, int kb, double& ta, double& tb) {
+    __shared__ bool s_last;
+    __shared__ double red[2][kThreads / 32];
+    __syncthreads();
+    if (tid() == 0) {
+        __threadfence();
+        const unsigned int ticket = atomicAdd(counter, 1u);
+        s_last = ticket == grid_blocks() - 1;
+        if (s_last) {
+            *counter = 0;
+            __threadfence();
+        }
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    const uint32_t nb = grid_blocks();
+    const double* pa = W.part + static_cast<size_t>(ka) * W.part_stride;
+    const double* pb = W.part + static_cast<size_t>(kb < 0 ? ka : kb) * W.part_stride;
+    double a = 0.0, b = 0.0;
+    for (uint32_t i = tid(); i < nb; i += kThreads) {
+        a += __ldcg(pa + i);
+        if (kb >= 0) b += __ldcg(pb + i);
+    }
+    const int lane = tid() & 31, warp = tid() >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) {
+        red[0][warp] = a;
+        red[1][warp] = b;
+    }
+    __syncthreads();
+    ta = 0.0;
+    tb = 0.0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+        ta += red[0][w];
+        tb += red[1][w];
+    }
+    return true;
 }
-__device__ __forceinline__ void zero_acc(MgState* st, int k) {
-    for (int i = 0; i < kMgSlots; ++i) st->acc[k][i] = 0.0;
-}
+
 
 // The 2x2x2 child sums of a tile's cells written into the coarse level's right-hand side (whole block calls it).
 __device__ __forceinline__ void restrict_tile(float c, const MgLevel& C, const Cell& cell) {
@@ -253,22 +299,153 @@ __device__ __forceinline__ void restrict_tile(float c, const MgLevel& C, const C
     __syncthreads();
 }
 
-// Last-block election: true in thread 0 of the block that finishes last, after every block's earlier writes and
-// atomics are visible to it. The counter returns to 0.
-__device__ __forceinline__ bool last_block(unsigned int* counter) {
-    __shared__ bool s_last;
-    __syncthreads();
-    if (tid() == 0) {
-        __threadfence();
-        const unsigned int ticket = atomicAdd(counter, 1u);
-        s_last = ticket == grid_blocks() - 1;
-        if (s_last) {
-            *counter = 0;
-            __threadfence();
+// ---------------------------------------------------------------------------------------------- level-0 z-march
+// The level-0 passes of an iteration (update, smoothing, p/q) march in z. Level 0 is cut into MX x MY = 32 x 8
+// columns; each block owns a balanced range of (column, plane pair) units and walks its column segments in z, two
+// planes per unit. Thread (tx, ty) owns one cell of the column plane, and a warp holds two y rows of 16 x cells
+// (lanes 0-15 row 2k, lanes 16-31 row 2k + 1), so the 2 x 2 x 2 children of a coarse cell are a lane pair (^1), a
+// half-warp pair (^16) and two consecutive planes: the restriction is two shuffles and a register. The value whose
+// stencil a pass takes is formed once per cell and plane. The 32 x 8 plane and its 84-cell halo go through a
+// three-plane ring in shared memory (the in-plane neighbours); the column's own -z / +z values stay in registers.
+// The loads of plane z + 2 are issued before plane z is computed; one __syncthreads per plane.
+constexpr int MX = 32, MY = 8, MPX = MX + 2, MPY = MY + 2;
+constexpr int kMPlane = MPX * MPY;
+constexpr int kMHalo = kMPlane - MX * MY;
+static_assert(MX * MY == kThreads && kMHalo <= kThreads, "one column cell per thread, at most one halo slot");
+
+struct MarchUnits {
+    int ncx, ncy, nzu;  // columns along x and y, plane pairs along z
+    uint32_t total;     // ncx * ncy * nzu
+};
+__host__ __device__ inline MarchUnits march_units(const MgLevel& L) {
+    MarchUnits u;
+    u.ncx = (L.nx + MX - 1) / MX;
+    u.ncy = (L.ny + MY - 1) / MY;
+    u.nzu = (L.nz + 1) / 2;
+    u.total = static_cast<uint32_t>(u.ncx) * static_cast<uint32_t>(u.ncy) * static_cast<uint32_t>(u.nzu);
+    return u;
+}
+
+// A ring slot: the in-plane cell it holds (wrapped across periodic edges), if that cell exists.
+struct MSlot {
+    int slot;
+    uint32_t off;  // y * nx + x of the cell
+    bool load;
+};
+__device__ __forceinline__ MSlot march_slot(const MgLevel& L, const int* per, int x0, int y0, int hx, int hy) {
+    MSlot s;
+    s.slot = (hy + 1) * MPX + hx + 1;
+    int x = x0 + hx, y = y0 + hy;
+    bool ok = true;
+    if (x < 0 || x >= L.nx) {
+        if (per[0]) x = wrapi(x, L.nx);
+        else ok = false;
+    }
+    if (y < 0 || y >= L.ny) {
+        if (per[1]) y = wrapi(y, L.ny);
+        else ok = false;
+    }
+    s.load = ok;
+    s.off = ok ? static_cast<uint32_t>(y) * static_cast<uint32_t>(L.nx) + static_cast<uint32_t>(x) : 0u;
+    return s;
+}
+
+// March over this block's units of level L. Per plane z of a segment:
+//   lo(ok, q) -> Own, lh(ok, q) -> Halo       loads of the own cell / the halo slot (zeros when !ok)
+//   uo(Own), uh(Halo) -> float                 the value whose stencil is taken (into the ring)
+//   cell(out, q, Own, um1, u0, u1, plane, slot) -> float
+//       the own cell's work at plane z (out: the cell is inside the level; um1 / u1 its -z / +z values, plane the
+//       ring plane of z); called by every thread. RESTRICT: its result (0 outside the level) is the cell's residual,
+//       summed over the 2 x 2 x 2 children into C.r, in restrict_tile's order.
+template <bool RESTRICT, class Own, class Halo, class LO, class LH, class UO, class UH, class CellF>
+__device__ __forceinline__ void march0(const MgLevel& L, const int* per, const MgLevel& C, float (*ring)[kMPlane], LO&& lo, LH&& lh, UO&& uo, UH&& uh, CellF&& cell) {
+    const MarchUnits U = march_units(L);
+    const uint32_t a = static_cast<uint32_t>((static_cast<uint64_t>(blockIdx.x) * U.total) / gridDim.x);
+    const uint32_t b = static_cast<uint32_t>((static_cast<uint64_t>(blockIdx.x + 1) * U.total) / gridDim.x);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tx = (lane & 15) + 16 * (warp & 1), ty = (lane >> 4) + 2 * (warp >> 1);
+    const bool halo = threadIdx.x < kMHalo;
+    int hx = 0, hy = 0;
+    if (halo) {
+        const int h = threadIdx.x;
+        if (h < MPX) {
+            hx = h - 1;
+            hy = -1;
+        } else if (h < 2 * MPX) {
+            hx = h - MPX - 1;
+            hy = MY;
+        } else if (h < 2 * MPX + MY) {
+            hx = -1;
+            hy = h - 2 * MPX;
+        } else {
+            hx = MX;
+            hy = h - 2 * MPX - MY;
         }
     }
-    __syncthreads();
-    return s_last && tid() == 0;
+    const uint32_t slab = static_cast<uint32_t>(L.nx) * static_cast<uint32_t>(L.ny);
+    uint32_t u = a;
+    while (u < b) {
+        const uint32_t col = u / static_cast<uint32_t>(U.nzu);
+        const int zu = static_cast<int>(u - col * static_cast<uint32_t>(U.nzu));
+        const int zub = zu + static_cast<int>(min(static_cast<uint32_t>(U.nzu - zu), b - u));
+        u += static_cast<uint32_t>(zub - zu);
+        const int za = 2 * zu, zb = min(L.nz, 2 * zub);
+        const int x0 = static_cast<int>(col % static_cast<uint32_t>(U.ncx)) * MX, y0 = static_cast<int>(col / static_cast<uint32_t>(U.ncx)) * MY;
+        const MSlot so = march_slot(L, per, x0, y0, tx, ty);
+        const MSlot sh = march_slot(L, per, x0, y0, hx, hy);
+        const bool out = x0 + tx < L.nx && y0 + ty < L.ny;
+        // plane z's offset (wrapped across a periodic z edge); false outside a non-periodic level
+        auto zbase = [&](int z, uint32_t& base) {
+            if (z < 0 || z >= L.nz) {
+                if (!per[2]) return false;
+                z = wrapi(z, L.nz);
+            }
+            base = static_cast<uint32_t>(z) * slab;
+            return true;
+        };
+        auto fetch = [&](int z, Own& od, Halo& hd, bool with_halo) {
+            uint32_t base = 0;
+            const bool ok = zbase(z, base);
+            od = lo(ok && so.load, base + so.off);
+            if (with_halo && halo) hd = lh(ok && sh.load, base + sh.off);
+        };
+        Own om1, o0, o1, o2;
+        Halo hunused, h0, h1, h2;
+        fetch(za - 1, om1, hunused, false);
+        fetch(za, o0, h0, true);
+        fetch(za + 1, o1, h1, true);
+        float um1 = uo(om1), u0 = uo(o0);
+        ring[za % 3][so.slot] = u0;
+        if (halo) ring[za % 3][sh.slot] = uh(h0);
+        float pair = 0.0f;
+        for (int z = za; z < zb; ++z) {
+            if (z + 2 <= zb) fetch(z + 2, o2, h2, true);
+            const float u1 = uo(o1);
+            ring[(z + 1) % 3][so.slot] = u1;
+            if (halo) ring[(z + 1) % 3][sh.slot] = uh(h1);
+            __syncthreads();
+            const float res = cell(out, static_cast<uint32_t>(z) * slab + so.off, o0, um1, u0, u1, ring[z % 3], so.slot);
+            if (RESTRICT) {
+                // restrict_tile's association: ((a + b) + c) + d over the x pairs a, b (even plane, rows 2Y, 2Y + 1)
+                // and c, d (odd plane); the writer is the even-x lane of row 2Y
+                const float xs = res + __shfl_xor_sync(0xffffffffu, res, 1);
+                const float other = __shfl_xor_sync(0xffffffffu, xs, 16);
+                const bool last = (z & 1) != 0 || z == L.nz - 1;
+                if ((z & 1) == 0) pair = xs + other;
+                else pair = (pair + xs) + other;
+                if (last && (tx & 1) == 0 && (ty & 1) == 0) {
+                    const int X = (x0 + tx) >> 1, Y = (y0 + ty) >> 1, Z = z >> 1;
+                    if (X < C.nx && Y < C.ny) C.r[lidx(C, X, Y, Z)] = pair;
+                }
+            }
+            um1 = u0;
+            u0 = u1;
+            o0 = o1;
+            o1 = o2;
+            h1 = h2;
+        }
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------------------------- kernels
@@ -299,9 +476,9 @@ __global__ void __launch_bounds__(kThreads) mg_setup_kernel(const __grid_constan
             rr += static_cast<T>(bv) * static_cast<T>(bv);
         }
     });
-    block_accumulate<T>(st, kAccBB, bb, kAccRR, rr);
-    if (!last_block(&st->done[0])) return;
-    const double btot = total(st, kAccBB), rtot = total(st, kAccRR);
+    block_accumulate<T>(A.W, kAccBB, bb, kAccRR, rr);
+    double btot, rtot;
+    if (!last_block_totals(&st->done[0], A.W, kAccBB, kAccRR, btot, rtot) || tid() != 0) return;
     st->bb = btot;
     st->rnorm2 = rtot;
     st->pass_rr0 = rtot;
@@ -320,15 +497,18 @@ __global__ void __launch_bounds__(kThreads) mg_setup_kernel(const __grid_constan
         st->zero_solution = 1;
         st->rnorm2 = 0.0;
     }
-    zero_acc(st, kAccRR);
 }
 
 // Level-0 update: r' = r - alpha q, e += alpha p, zp = w D^-1 r', restriction of r' - A zp into level 1, ||r'||^2.
 // initial = 1: the pass's first round (alpha = 0, no iteration counted). The last block tests convergence, flips
 // the buffer parity and sets the loop condition `cond`: continue unless stopped, and (net_loop = 1, the loop of a
 // learned solve whose body runs the network) unless the next iteration goes without the network.
+// z-march: the ring holds w D^-1 (r - alpha q) of every cell (the pre-smoothed zp on active cells; the stencil's
+// mask never reaches the others).
 template <typename T, bool LEARNED>
 __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_constant__ MgSolveArgs A, int initial, cudaGraphConditionalHandle cond, int in_graph, int net_loop) {
+    pdl_begin();
+    __shared__ float ring[3][kMPlane];
     const MgLevel& L0 = A.H.L[0];
     MgState* st = A.st;
     const bool skip = st->halt || st->fail;  // uniform over the grid
@@ -339,35 +519,60 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
         const float* r = A.W.r[par];
         float* rn_out = A.W.r[par ^ 1];
         const float* pn = A.W.p[par ^ 1];
-        for_tiles(L0, [&](const Cell& c) {
-            float res = 0.0f;
-            if (c.in) {
-                uint32_t nb[6];
-                nbr_all(L0, A.H.fper, c, nb);
-                const uint16_t code = L0.code[c.q];
-                const float rq = r[c.q], qq = A.W.q[c.q];
-                const float pq = initial ? 0.0f : pn[c.q], eq = initial ? 0.0f : A.e[c.q];
-                const float rn = rq - a * qq;
-                {  // pre-smoothing and the residual restricted to level 1
-                    float un[6];
-#pragma unroll
-                    for (int k = 0; k < 6; ++k) un[k] = wdiag(L0.code[nb[k]]) * (r[nb[k]] - a * A.W.q[nb[k]]);
-                    float zp = 0.0f;
-                    if (active(code)) {
-                        zp = wdiag(code) * rn;
-                        res = 0.5f * (rn - masked_stencil(code, zp, un));
+        struct Own {
+            uint32_t code;
+            float r, q, p, e;
+        };
+        struct Halo {
+            uint32_t code;
+            float r, q;
+        };
+        march0<true, Own, Halo>(
+            L0, A.H.fper, A.H.L[1], ring,
+            [&](bool ok, uint32_t q) {
+                Own d{0u, 0.0f, 0.0f, 0.0f, 0.0f};
+                if (ok) {
+                    d.code = L0.code[q];
+                    d.r = r[q];
+                    d.q = A.W.q[q];
+                    if (!initial) {
+                        d.p = pn[q];
+                        d.e = A.e[q];
                     }
-                    L0.zp[c.q] = zp;
                 }
-                rn_out[c.q] = rn;
-                if (!initial) A.e[c.q] = eq + a * pq;
+                return d;
+            },
+            [&](bool ok, uint32_t q) {
+                Halo d{0u, 0.0f, 0.0f};
+                if (ok) {
+                    d.code = L0.code[q];
+                    d.r = r[q];
+                    d.q = A.W.q[q];
+                }
+                return d;
+            },
+            [&](const Own& d) { return wdiag(static_cast<uint16_t>(d.code)) * (d.r - a * d.q); },
+            [&](const Halo& d) { return wdiag(static_cast<uint16_t>(d.code)) * (d.r - a * d.q); },
+            [&](bool out, uint32_t q, const Own& d, float um1, float u0, float u1, const float* pl, int s) {
+                if (!out) return 0.0f;
+                const uint16_t code = static_cast<uint16_t>(d.code);
+                const float rn = d.r - a * d.q;
+                float zp = 0.0f, res = 0.0f;
+                if (active(code)) {
+                    zp = u0;
+                    const float un[6] = {pl[s - 1], pl[s + 1], pl[s - MPX], pl[s + MPX], um1, u1};
+                    res = 0.5f * (rn - masked_stencil(code, zp, un));
+                }
+                L0.zp[q] = zp;
+                rn_out[q] = rn;
+                if (!initial) A.e[q] = d.e + a * d.p;
                 rr += static_cast<T>(rn) * static_cast<T>(rn);
-            }
-            restrict_tile(res, A.H.L[1], c);
-        });
-        block_accumulate<T>(st, kAccRR, rr, -1, T(0));
+                return res;
+            });
+        block_accumulate<T>(A.W, kAccRR, rr, -1, T(0));
     }
-    if (!last_block(&st->done[1])) return;
+    double rn2_total, unused;
+    if (!last_block_totals(&st->done[1], A.W, kAccRR, -1, rn2_total, unused) || tid() != 0) return;
     if (st->halt) {
         st->loop = 0;
         if (in_graph) cudaGraphSetConditional(cond, 0);
@@ -378,7 +583,7 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
         st->status = st->fail;
         stop = 1;
     } else {
-        const double rn2 = total(st, kAccRR);
+        const double rn2 = rn2_total;
         if (!initial) st->it += 1;
         st->rnorm2 = rn2;
         if (!isfinite(rn2)) {
@@ -408,7 +613,6 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
         st->net_off = (st->fallback || (A.net_iterations > 0 && st->it - st->pass_it0 >= A.net_iterations)) ? 1u : 0u;
     }
     st->parity ^= 1;
-    for (int k = kAccRR; k < kAccCount; ++k) zero_acc(st, k);
     st->loop = stop ? 0u : 1u;
     __threadfence();
     if (in_graph) cudaGraphSetConditional(cond, (stop || (LEARNED && net_loop && st->net_off)) ? 0u : 1u);
@@ -417,11 +621,13 @@ __global__ void __launch_bounds__(kThreads) mg_update_kernel(const __grid_consta
 // The condition of a learned solve's second loop (the V-cycle alone, after the network's iterations): the loop flag
 // the last update left.
 __global__ void mg_loop_gate_kernel(const MgState* __restrict__ st, cudaGraphConditionalHandle cond) {
+    pdl_begin();
     cudaGraphSetConditional(cond, st->loop);
 }
 
 // Level l >= 1: zp = w D^-1 r (pre-smoothing from zero), restriction of r - A zp into level l + 1.
 __global__ void __launch_bounds__(kThreads) mg_restrict_kernel(const __grid_constant__ MgHierarchy H, int l) {
+    pdl_begin();
     const MgLevel& F = H.L[l];
     for_tiles(F, [&](const Cell& c) {
         float res = 0.0f;
@@ -448,6 +654,7 @@ __global__ void __launch_bounds__(kThreads) mg_restrict_kernel(const __grid_cons
 // loads the 3 x 3 x 3 coarse neighbourhood once and writes its up to 8 children, each a trilinear blend of the
 // parent and the 7 corners toward the child (see prolong_corners).
 __global__ void __launch_bounds__(kThreads) mg_prolong_kernel(const __grid_constant__ MgHierarchy H, int l) {
+    pdl_begin();
     const MgLevel& F = H.L[l];
     const MgLevel& C = H.L[l + 1];
     for_tiles(C, [&](const Cell& c) {
@@ -490,50 +697,83 @@ __global__ void __launch_bounds__(kThreads) mg_prolong_kernel(const __grid_const
     });
 }
 
-// Level l post-smoothing: t = zp + w D^-1 (r - A zp) on active cells; inactive cells get kTag (coarse levels) or 0
-// (level 0, whose t is the preconditioned residual z). Level 0 also accumulates (z, r) and (z, q), and its last
-// block computes beta (0 on a pass's first iteration).
-// DOTS = false (level 0 of a learned solve): z only; the network's correction and the dot products follow.
-template <bool LEVEL0, typename T, bool DOTS = true>
+// Level l >= 1 post-smoothing: t = zp + w D^-1 (r - A zp) on active cells, kTag on inactive cells.
 __global__ void __launch_bounds__(kThreads) mg_smooth_kernel(const __grid_constant__ MgSolveArgs A, int l) {
-    const MgLevel& F = A.H.L[LEVEL0 ? 0 : l];
-    MgState* st = A.st;
-    const float* r = LEVEL0 ? A.W.r[st->parity] : F.r;
-    const float inactive_value = LEVEL0 ? 0.0f : __uint_as_float(kTag);
-    T zr = 0, zq = 0;
+    pdl_begin();
+    const MgLevel& F = A.H.L[l];
     for_tiles(F, [&](const Cell& c) {
         if (!c.in) return;
         uint32_t nb[6];
         nbr_all(F, A.H.fper, c, nb);
         const uint16_t code = F.code[c.q];
-        const float s0 = F.zp[c.q], rv = r[c.q];
-        const float qv = LEVEL0 ? A.W.q[c.q] : 0.0f;
+        const float s0 = F.zp[c.q], rv = F.r[c.q];
         float sn[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) sn[k] = F.zp[nb[k]];
-        float z = inactive_value;
-        if (active(code)) {
-            z = s0 + wdiag(code) * (rv - masked_stencil(code, s0, sn));
-            if (LEVEL0 && DOTS) {
-                zr += static_cast<T>(z) * static_cast<T>(rv);
-                zq += static_cast<T>(z) * static_cast<T>(qv);
-            }
-        }
-        F.t[c.q] = z;
+        F.t[c.q] = active(code) ? s0 + wdiag(code) * (rv - masked_stencil(code, s0, sn)) : __uint_as_float(kTag);
     });
-    if (!LEVEL0 || !DOTS) return;
-    block_accumulate<T>(st, kAccZR, zr, kAccZQ, zq);
-    if (!last_block(&st->done[3])) return;
-    const double beta = st->first_iter ? 0.0 : -total(st, kAccZQ) / st->pq_prev;
-    if (!isfinite(beta) || !isfinite(total(st, kAccZR))) st->fail = SMOKE_B200_SOLVE_NOT_FINITE;
+}
+
+// Level-0 post-smoothing (z-march): z = zp + w D^-1 (r - A zp) on active cells, 0 elsewhere, into t; with DOTS,
+// (z, r) and (z, q), and the last block computes beta (0 on a pass's first iteration). DOTS = false (a learned
+// solve's iteration with the network): z only; the network's correction and the dot products follow.
+template <typename T, bool DOTS>
+__global__ void __launch_bounds__(kThreads) mg_smooth0_kernel(const __grid_constant__ MgSolveArgs A) {
+    pdl_begin();
+    __shared__ float ring[3][kMPlane];
+    const MgLevel& F = A.H.L[0];
+    MgState* st = A.st;
+    const float* r = A.W.r[st->parity];
+    T zr = 0, zq = 0;
+    struct Own {
+        uint32_t code;
+        float s, r, q;
+    };
+    march0<false, Own, float>(
+        F, A.H.fper, F, ring,
+        [&](bool ok, uint32_t q) {
+            Own d{0u, 0.0f, 0.0f, 0.0f};
+            if (ok) {
+                d.code = F.code[q];
+                d.s = F.zp[q];
+                d.r = r[q];
+                if (DOTS) d.q = A.W.q[q];
+            }
+            return d;
+        },
+        [&](bool ok, uint32_t q) { return ok ? F.zp[q] : 0.0f; },
+        [&](const Own& d) { return d.s; },
+        [&](float v) { return v; },
+        [&](bool out, uint32_t q, const Own& d, float um1, float u0, float u1, const float* pl, int s) {
+            if (!out) return 0.0f;
+            const uint16_t code = static_cast<uint16_t>(d.code);
+            float z = 0.0f;
+            if (active(code)) {
+                const float sn[6] = {pl[s - 1], pl[s + 1], pl[s - MPX], pl[s + MPX], um1, u1};
+                z = u0 + wdiag(code) * (d.r - masked_stencil(code, u0, sn));
+                if (DOTS) {
+                    zr += static_cast<T>(z) * static_cast<T>(d.r);
+                    zq += static_cast<T>(z) * static_cast<T>(d.q);
+                }
+            }
+            F.t[q] = z;
+            return 0.0f;
+        });
+    if (!DOTS) return;
+    block_accumulate<T>(A.W, kAccZR, zr, kAccZQ, zq);
+    double tzr, tzq;
+    if (!last_block_totals(&st->done[3], A.W, kAccZR, kAccZQ, tzr, tzq) || tid() != 0) return;
+    const double beta = st->first_iter ? 0.0 : -tzq / st->pq_prev;
+    if (!isfinite(beta) || !isfinite(tzr)) st->fail = SMOKE_B200_SOLVE_NOT_FINITE;
     st->beta = static_cast<float>(beta);
 }
 
-// Level l >= 1 up-pass in one kernel: mg_prolong_kernel(l) followed by mg_smooth_kernel<false>(l), with the same
+// Level l >= 1 up-pass in one kernel: mg_prolong_kernel(l) followed by mg_smooth_kernel(l), with the same
 // arithmetic. Per tile, zp + P(t_{l+1}) is formed for the tile and a one-cell halo in shared memory (every fine cell
 // from its own 8 coarse corners, as the prolongation kernel forms each child), then the tile is smoothed from there;
 // the prolonged zp is not written back (nothing reads it after the smoothing).
 __global__ void __launch_bounds__(kThreads) mg_up_kernel(const __grid_constant__ MgHierarchy H, int l) {
+    pdl_begin();
     constexpr int RX = TX + 2, RY = TY + 2, RZ = TZ + 2;
     __shared__ float s_zp[RZ][RY][RX];
     const MgLevel& F = H.L[l];
@@ -584,6 +824,7 @@ __global__ void __launch_bounds__(kThreads) mg_up_kernel(const __grid_constant__
 // and its scale. Nothing to do once the solve fell back to the V-cycle alone.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) mg_net_residual_kernel(const __grid_constant__ MgSolveArgs A) {
+    pdl_begin();
     const MgLevel& F = A.H.L[0];
     MgState* st = A.st;
     if (st->net_off) return;  // uniform over the grid
@@ -602,10 +843,10 @@ __global__ void __launch_bounds__(kThreads) mg_net_residual_kernel(const __grid_
         F.zp[c.q] = rv_net;
         rr += static_cast<T>(rv_net) * static_cast<T>(rv_net);
     });
-    block_accumulate<T>(st, kAccNet, rr, -1, T(0));
-    if (!last_block(&st->done[5])) return;
-    st->net_rr = total(st, kAccNet);
-    zero_acc(st, kAccNet);
+    block_accumulate<T>(A.W, kAccNet, rr, -1, T(0));
+    double tnet, unused;
+    if (!last_block_totals(&st->done[5], A.W, kAccNet, -1, tnet, unused) || tid() != 0) return;
+    st->net_rr = tnet;
 }
 
 // Learned preconditioner, part 2: the step along the network's correction N = y / s that minimises the energy norm of
@@ -613,6 +854,7 @@ __global__ void __launch_bounds__(kThreads) mg_net_residual_kernel(const __grid_
 // not defined. So a network that helps little is scaled down instead of being added at full weight.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) mg_net_gamma_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
+    pdl_begin();
     const MgLevel& F = A.H.L[0];
     MgState* st = A.st;
     if (st->net_off) return;  // uniform over the grid
@@ -632,12 +874,10 @@ __global__ void __launch_bounds__(kThreads) mg_net_gamma_kernel(const __grid_con
         nr += static_cast<T>(n0) * static_cast<T>(F.zp[c.q]);
         nan_ += static_cast<T>(n0) * static_cast<T>(masked_stencil(code, n0, nn));
     });
-    block_accumulate<T>(st, kAccNet, nr, kAccNetA, nan_);
-    if (!last_block(&st->done[6])) return;
-    const double a = total(st, kAccNet), b = total(st, kAccNetA);
+    block_accumulate<T>(A.W, kAccNet, nr, kAccNetA, nan_);
+    double a, b;
+    if (!last_block_totals(&st->done[6], A.W, kAccNet, kAccNetA, a, b) || tid() != 0) return;
     st->net_gamma = (b > 0.0 && isfinite(a) && isfinite(b)) ? a / b : 0.0;
-    zero_acc(st, kAccNet);
-    zero_acc(st, kAccNetA);
 }
 
 // Learned preconditioner, part 3: the network's correction N = y / s (y its output, s = sqrt(n / ||r_V||^2) its input
@@ -648,6 +888,7 @@ __global__ void __launch_bounds__(kThreads) mg_net_gamma_kernel(const __grid_con
 // pass's first iteration), as level 0's smoothing does for the V-cycle alone.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) mg_net_add_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
+    pdl_begin();
     const MgLevel& F = A.H.L[0];
     MgState* st = A.st;
     const bool use_net = st->net_off == 0;
@@ -673,10 +914,11 @@ __global__ void __launch_bounds__(kThreads) mg_net_add_kernel(const __grid_const
         zr += static_cast<T>(z) * static_cast<T>(r[c.q]);
         zq += static_cast<T>(z) * static_cast<T>(A.W.q[c.q]);
     });
-    block_accumulate<T>(st, kAccZR, zr, kAccZQ, zq);
-    if (!last_block(&st->done[3])) return;
-    const double beta = st->first_iter ? 0.0 : -total(st, kAccZQ) / st->pq_prev;
-    if (!isfinite(beta) || !isfinite(total(st, kAccZR))) st->fail = SMOKE_B200_SOLVE_NOT_FINITE;
+    block_accumulate<T>(A.W, kAccZR, zr, kAccZQ, zq);
+    double tzr, tzq;
+    if (!last_block_totals(&st->done[3], A.W, kAccZR, kAccZQ, tzr, tzq) || tid() != 0) return;
+    const double beta = st->first_iter ? 0.0 : -tzq / st->pq_prev;
+    if (!isfinite(beta) || !isfinite(tzr)) st->fail = SMOKE_B200_SOLVE_NOT_FINITE;
     st->beta = static_cast<float>(beta);
 }
 
@@ -688,9 +930,12 @@ __global__ void __launch_bounds__(kThreads) mg_net_guess_kernel(const __grid_con
     });
 }
 
-// p' = z + beta p, q = A p'; (p', q) and (p', r). The last block computes alpha = (p', r) / (p', q).
+// p' = z + beta p, q = A p'; (p', q) and (p', r). The last block computes alpha = (p', r) / (p', q). z-march: the
+// ring holds p' of every cell.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) mg_pq_kernel(const __grid_constant__ MgSolveArgs A) {
+    pdl_begin();
+    __shared__ float ring[3][kMPlane];
     const MgLevel& F = A.H.L[0];
     MgState* st = A.st;
     const bool skip = st->fail;  // uniform over the grid
@@ -702,26 +947,49 @@ __global__ void __launch_bounds__(kThreads) mg_pq_kernel(const __grid_constant__
         const float* po = A.W.p[par];
         float* pn = A.W.p[par ^ 1];
         const float* r = A.W.r[par];
-        for_tiles(F, [&](const Cell& c) {
-            if (!c.in) return;
-            uint32_t nb[6];
-            nbr_all(F, A.H.fper, c, nb);
-            const uint16_t code = F.code[c.q];
-            const float rv = r[c.q];  // loaded with the rest, before this tile's stores
-            const float pv = Z[c.q] + fb * po[c.q];
-            float pnb[6];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) pnb[k] = Z[nb[k]] + fb * po[nb[k]];
-            const float qv = masked_stencil(code, pv, pnb);
-            pn[c.q] = pv;
-            A.W.q[c.q] = qv;
-            pq += static_cast<T>(pv) * static_cast<T>(qv);
-            pr += static_cast<T>(pv) * static_cast<T>(rv);
-        });
-        block_accumulate<T>(st, kAccPQ, pq, kAccPR, pr);
+        struct Own {
+            uint32_t code;
+            float z, p, r;
+        };
+        struct Halo {
+            float z, p;
+        };
+        march0<false, Own, Halo>(
+            F, A.H.fper, F, ring,
+            [&](bool ok, uint32_t q) {
+                Own d{0u, 0.0f, 0.0f, 0.0f};
+                if (ok) {
+                    d.code = F.code[q];
+                    d.z = Z[q];
+                    d.p = po[q];
+                    d.r = r[q];
+                }
+                return d;
+            },
+            [&](bool ok, uint32_t q) {
+                Halo d{0.0f, 0.0f};
+                if (ok) {
+                    d.z = Z[q];
+                    d.p = po[q];
+                }
+                return d;
+            },
+            [&](const Own& d) { return d.z + fb * d.p; },
+            [&](const Halo& d) { return d.z + fb * d.p; },
+            [&](bool out, uint32_t q, const Own& d, float um1, float u0, float u1, const float* pl, int s) {
+                if (!out) return 0.0f;
+                const float pnb[6] = {pl[s - 1], pl[s + 1], pl[s - MPX], pl[s + MPX], um1, u1};
+                const float qv = masked_stencil(static_cast<uint16_t>(d.code), u0, pnb);
+                pn[q] = u0;
+                A.W.q[q] = qv;
+                pq += static_cast<T>(u0) * static_cast<T>(qv);
+                pr += static_cast<T>(u0) * static_cast<T>(d.r);
+                return 0.0f;
+            });
+        block_accumulate<T>(A.W, kAccPQ, pq, kAccPR, pr);
     }
-    if (!last_block(&st->done[4]) || skip) return;
-    const double pqt = total(st, kAccPQ), prt = total(st, kAccPR);
+    double pqt, prt;
+    if (!last_block_totals(&st->done[4], A.W, kAccPQ, kAccPR, pqt, prt) || tid() != 0 || skip) return;
     if (!(pqt > 0.0) || !isfinite(prt)) {
         st->fail = isfinite(pqt) ? SMOKE_B200_SOLVE_BREAKDOWN : SMOKE_B200_SOLVE_NOT_FINITE;
         return;
@@ -730,7 +998,7 @@ __global__ void __launch_bounds__(kThreads) mg_pq_kernel(const __grid_constant__
     st->pq_prev = pqt;
 }
 
-// Block-level part of the V-cycle (one block): see block_cycle.
+// Block-level part of the V-cycle: the levels of at most kMgBlockLevelCells cells, in one block's shared memory.
 template <int THREADS>
 __device__ MgLevel smem_level(const MgHierarchy& H, float* area, int l) {
     uint32_t off = 0;
@@ -744,132 +1012,188 @@ __device__ MgLevel smem_level(const MgHierarchy& H, float* area, int l) {
     return S;
 }
 
-template <typename R, class V>
-__device__ __forceinline__ R stencil_q(const MgLevel& L, uint32_t q, uint16_t code, R v0, V&& v) {
-    if (!(code & 63u)) return static_cast<R>(diagf(code)) * v0;
-    int x, y, z;
-    lxyz(L, q, x, y, z);
-    return stencil_xyz<R>(L, q, x, y, z, code, v0, v);
+// Cell q of a block level: its coordinates and the indices of its 6 stencil neighbours (nbr_all's rule).
+__device__ __forceinline__ Cell block_cell(const MgLevel& L, const int* per, uint32_t q, uint32_t nb[6]) {
+    Cell c;
+    lxyz(L, q, c.x, c.y, c.z);
+    c.bx = c.by = c.bz = 0;
+    c.q = q;
+    c.in = true;
+    nbr_all(L, per, c, nb);
+    return c;
 }
 
-// Trilinear prolongation of C.t (shared memory) at fine cell (x, y, z), C's codes marking its active cells.
+// Trilinear prolongation of C.t (shared memory) at fine cell (x, y, z), C's codes marking its active cells: a corner
+// beyond an OUTFLOW face takes minus the parent, a corner outside the level or on an inactive coarse cell the parent.
+// Every corner's value and code are loaded before any is used; the sum runs over the corners in order.
 __device__ __forceinline__ float prolong_codes(const MgLevel& C, const int* fper, const int* fout, int x, int y, int z) {
     const int X = x >> 1, Y = y >> 1, Z = z >> 1;
     const int sx = (x & 1) ? 1 : -1, sy = (y & 1) ? 1 : -1, sz = (z & 1) ? 1 : -1;
-    const float parent = C.t[lidx(C, X, Y, Z)];
+    const uint32_t pq = lidx(C, X, Y, Z);
+    uint32_t idx[8];
+    bool outflow[8], inside[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        int cx = X + ((m & 1) ? sx : 0), cy = Y + ((m & 2) ? sy : 0), cz = Z + ((m & 4) ? sz : 0);
+        const bool ox = (m & 1) && (cx < 0 || cx >= C.nx) && fout[sx > 0 ? 1 : 0];
+        const bool oy = (m & 2) && (cy < 0 || cy >= C.ny) && fout[sy > 0 ? 3 : 2];
+        const bool oz = (m & 4) && (cz < 0 || cz >= C.nz) && fout[sz > 0 ? 5 : 4];
+        outflow[m] = ox || oy || oz;
+        inside[m] = !outflow[m] && wrap_c(cx, C.nx, fper[0]) && wrap_c(cy, C.ny, fper[1]) && wrap_c(cz, C.nz, fper[2]);
+        idx[m] = inside[m] ? lidx(C, cx, cy, cz) : pq;
+    }
+    float tv[8];
+    uint16_t code[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        tv[m] = C.t[idx[m]];
+        code[m] = C.code[idx[m]];
+    }
+    const float parent = tv[0];
     float acc = 0.0f;
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
         const float w = ((m & 1) ? 0.25f : 0.75f) * ((m & 2) ? 0.25f : 0.75f) * ((m & 4) ? 0.25f : 0.75f);
         float v = parent;
         if (m) {
-            int cx = X + ((m & 1) ? sx : 0), cy = Y + ((m & 2) ? sy : 0), cz = Z + ((m & 4) ? sz : 0);
-            // a corner beyond an OUTFLOW face takes minus the parent (prolong_corners); fout is 0 on periodic axes
-            const bool ox = (m & 1) && (cx < 0 || cx >= C.nx) && fout[sx > 0 ? 1 : 0];
-            const bool oy = (m & 2) && (cy < 0 || cy >= C.ny) && fout[sy > 0 ? 3 : 2];
-            const bool oz = (m & 4) && (cz < 0 || cz >= C.nz) && fout[sz > 0 ? 5 : 4];
-            if (ox || oy || oz) {
-                v = -parent;
-            } else if (wrap_c(cx, C.nx, fper[0]) && wrap_c(cy, C.ny, fper[1]) && wrap_c(cz, C.nz, fper[2])) {
-                const uint32_t cq = lidx(C, cx, cy, cz);
-                if (active(C.code[cq])) v = C.t[cq];
-            }
+            if (outflow[m]) v = -parent;
+            else if (inside[m] && active(code[m])) v = tv[m];
         }
         acc += w * v;
     }
     return acc;
 }
 
-// The coarse part of the V-cycle below the grid levels, in one block: reads r of level g (global), runs the
-// pre-smoothing and restriction, the coarsest Jacobi sweeps and the up passes in shared memory, and writes t of
-// level g (kTag on inactive cells).
+// The coarse part of the V-cycle below the grid levels, in one block, one cell per thread on every level (a block
+// level has at most kMgBlockLevelCells = kBlockLevelThreads cells): reads r of level g (global), pre-smooths and
+// restricts level by level, runs the coarsest Jacobi sweeps, then the up passes, and writes t of level g (kTag on
+// inactive cells). The level codes do not change during a solve, so they are copied before the wait for the
+// previous kernel. The restriction gathers each coarse cell's children in a fixed order (deterministic sums); every
+// stencil issues its 6 neighbour loads before using any.
 __global__ void __launch_bounds__(kBlockLevelThreads) mg_block_kernel(const __grid_constant__ MgHierarchy H) {
     extern __shared__ __align__(16) float area[];
     constexpr int NT = kBlockLevelThreads;
+    static_assert(NT >= kMgBlockLevelCells, "one thread per cell of a block level");
     const int g = H.grid_levels, lc = H.levels - 1;
-    const int t = threadIdx.x;
+    const uint32_t t = threadIdx.x;
     for (int l = g; l <= lc; ++l) {  // codes as aligned pairs (the arrays carry two spare entries)
         const MgLevel S = smem_level<NT>(H, area, l);
         const uint32_t* src = reinterpret_cast<const uint32_t*>(H.L[l].code);
         uint32_t* dst = reinterpret_cast<uint32_t*>(S.code);
         for (uint32_t i = t; i < (S.n + 1) / 2; i += NT) dst[i] = src[i];
     }
+    pdl_begin();
     {
         const MgLevel S = smem_level<NT>(H, area, g);
-        for (uint32_t q = t; q < S.n; q += NT) S.r[q] = H.L[g].r[q];
+        if (t < S.n) S.r[t] = H.L[g].r[t];
     }
     __syncthreads();
-    for (int l = g; l < lc; ++l) {
+    for (int l = g; l < lc; ++l) {  // down: zp = w D^-1 r, then r of l + 1 = 1/2 sum of the children's r - A zp
         const MgLevel F = smem_level<NT>(H, area, l);
         const MgLevel C = smem_level<NT>(H, area, l + 1);
-        for (uint32_t q = t; q < C.n; q += NT) C.r[q] = 0.0f;
-        for (uint32_t q = t; q < F.n; q += NT) {
-            const uint16_t code = F.code[q];
-            F.zp[q] = active(code) ? wdiag(code) * F.r[q] : 0.0f;
+        uint16_t code = 0;
+        float rv = 0.0f, zp = 0.0f;
+        if (t < F.n) {
+            code = F.code[t];
+            rv = F.r[t];
+            zp = active(code) ? wdiag(code) * rv : 0.0f;
+            F.zp[t] = zp;
         }
         __syncthreads();
-        for (uint32_t q = t; q < F.n; q += NT) {
-            const uint16_t code = F.code[q];
-            if (!active(code)) continue;
-            const float res = F.r[q] - stencil_q<float>(F, q, code, F.zp[q], [&](uint32_t nb) { return F.zp[nb]; });
-            int x, y, z;
-            lxyz(F, q, x, y, z);
-            atomicAdd(C.r + lidx(C, x >> 1, y >> 1, z >> 1), 0.5f * res);
+        if (t < F.n) {
+            uint32_t nb[6];
+            block_cell(F, H.fper, t, nb);
+            float vn[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) vn[k] = F.zp[nb[k]];
+            F.t[t] = active(code) ? 0.5f * (rv - masked_stencil(code, zp, vn)) : 0.0f;  // t is free until the up pass
+        }
+        __syncthreads();
+        if (t < C.n) {
+            int X, Y, Z;
+            lxyz(C, t, X, Y, Z);
+            float v[8];
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                const int x = 2 * X + (m & 1), y = 2 * Y + ((m >> 1) & 1), z = 2 * Z + (m >> 2);
+                v[m] = (x < F.nx && y < F.ny && z < F.nz) ? F.t[lidx(F, x, y, z)] : 0.0f;
+            }
+            float sum = 0.0f;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) sum += v[m];
+            C.r[t] = sum;
         }
         __syncthreads();
     }
-    {  // coarsest level: Jacobi sweeps from zero, ping-pong between t and zp, result in t
+    {  // coarsest level: Jacobi sweeps from zero, result in t
         const MgLevel L = smem_level<NT>(H, area, lc);
-        // a coarsest level of at most kWarpCoarsestCells cells sweeps in warp 0 alone, __syncwarp between sweeps
-        const bool by_warp = L.n <= kWarpCoarsestCells;
-        const int lanes = by_warp ? 32 : NT;
-        if (t < lanes) {
-            for (uint32_t q = t; q < L.n; q += lanes) {
-                const uint16_t code = L.code[q];
-                L.t[q] = active(code) ? wdiag(code) * L.r[q] : 0.0f;
+        if (L.n == 1) {  // one cell (its stencil neighbours, across periodic edges, are itself): in registers
+            if (t == 0) {
+                const uint16_t code = L.code[0];
+                const float rv = L.r[0];
+                float v = active(code) ? wdiag(code) * rv : 0.0f;
+                for (int sweep = 0; sweep < kCoarsestSweeps; ++sweep) {
+                    const float vn[6] = {v, v, v, v, v, v};
+                    v = active(code) ? v + wdiag(code) * (rv - masked_stencil(code, v, vn)) : 0.0f;
+                }
+                L.t[0] = v;
             }
-            for (int sweep = 0; sweep < kCoarsestSweeps; ++sweep) {
-                if (by_warp) __syncwarp();
-                else __syncthreads();
-                float* src = (sweep & 1) ? L.zp : L.t;
-                float* dst = (sweep & 1) ? L.t : L.zp;
+        } else {  // ping-pong between t and zp; a level of at most kWarpCoarsestCells cells sweeps in warp 0
+            const bool by_warp = L.n <= kWarpCoarsestCells;
+            const uint32_t lanes = by_warp ? 32u : static_cast<uint32_t>(NT);
+            if (t < lanes) {
                 for (uint32_t q = t; q < L.n; q += lanes) {
                     const uint16_t code = L.code[q];
-                    float v = 0.0f;
-                    if (active(code)) {
-                        const float s0 = src[q];
-                        v = s0 + wdiag(code) * (L.r[q] - stencil_q<float>(L, q, code, s0, [&](uint32_t nb) { return src[nb]; }));
+                    L.t[q] = active(code) ? wdiag(code) * L.r[q] : 0.0f;
+                }
+                for (int sweep = 0; sweep < kCoarsestSweeps; ++sweep) {
+                    if (by_warp) __syncwarp();
+                    else __syncthreads();
+                    float* src = (sweep & 1) ? L.zp : L.t;
+                    float* dst = (sweep & 1) ? L.t : L.zp;
+                    for (uint32_t q = t; q < L.n; q += lanes) {
+                        const uint16_t code = L.code[q];
+                        uint32_t nb[6];
+                        block_cell(L, H.fper, q, nb);
+                        const float s0 = src[q], rv = L.r[q];
+                        float vn[6];
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) vn[k] = src[nb[k]];
+                        dst[q] = active(code) ? s0 + wdiag(code) * (rv - masked_stencil(code, s0, vn)) : 0.0f;
                     }
-                    dst[q] = v;
                 }
             }
         }
         __syncthreads();
     }
     static_assert(kCoarsestSweeps % 2 == 0, "the coarsest sweeps end in t");
-    for (int l = lc - 1; l >= g; --l) {
+    for (int l = lc - 1; l >= g; --l) {  // up: zp += P(t of l + 1), then t = zp + w D^-1 (r - A zp)
         const MgLevel F = smem_level<NT>(H, area, l);
         const MgLevel C = smem_level<NT>(H, area, l + 1);
-        for (uint32_t q = t; q < F.n; q += NT) {
-            if (!active(F.code[q])) continue;
-            int x, y, z;
-            lxyz(F, q, x, y, z);
-            F.zp[q] += prolong_codes(C, H.fper, H.fout, x, y, z);
+        uint16_t code = 0;
+        float rv = 0.0f, zp = 0.0f;
+        uint32_t nb[6];
+        if (t < F.n) {
+            code = F.code[t];
+            rv = F.r[t];
+            zp = F.zp[t];
+            const Cell c = block_cell(F, H.fper, t, nb);
+            if (active(code)) {
+                zp += prolong_codes(C, H.fper, H.fout, c.x, c.y, c.z);
+                F.zp[t] = zp;
+            }
         }
         __syncthreads();
-        for (uint32_t q = t; q < F.n; q += NT) {
-            const uint16_t code = F.code[q];
-            float v = 0.0f;
-            if (active(code)) {
-                const float s0 = F.zp[q];
-                v = s0 + wdiag(code) * (F.r[q] - stencil_q<float>(F, q, code, s0, [&](uint32_t nb) { return F.zp[nb]; }));
-            }
-            F.t[q] = v;
+        if (t < F.n) {
+            float vn[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) vn[k] = F.zp[nb[k]];
+            F.t[t] = active(code) ? zp + wdiag(code) * (rv - masked_stencil(code, zp, vn)) : 0.0f;
         }
         __syncthreads();
     }
     const MgLevel S = smem_level<NT>(H, area, g);
-    for (uint32_t q = t; q < S.n; q += NT) H.L[g].t[q] = active(S.code[q]) ? S.t[q] : __uint_as_float(kTag);
+    if (t < S.n) H.L[g].t[t] = active(S.code[t]) ? S.t[t] : __uint_as_float(kTag);
 }
 
 // Standalone V-cycle, level 0 down: zp = w D^-1 r, and (r - A zp) / 2 restricted into level 1 (the pre-smoothing the
@@ -915,6 +1239,7 @@ __global__ void __launch_bounds__(kThreads) mg_postsmooth_kernel(const __grid_co
 
 // Refinement: x64 = (first pass of a cold start ? 0 : x64) + e.
 __global__ void __launch_bounds__(kThreads) mg_accumulate_kernel(const __grid_constant__ MgSolveArgs A) {
+    pdl_begin();
     const MgState* st = A.st;
     if (st->halt) return;
     const bool fresh = st->passes == 1 && !A.warm;
@@ -927,6 +1252,7 @@ __global__ void __launch_bounds__(kThreads) mg_accumulate_kernel(const __grid_co
 // Refinement: r = b - A x64 (FP64) into the current residual buffer, e = q = 0, ||r||^2. The last block decides
 // between another pass and the end of the solve.
 __global__ void __launch_bounds__(kThreads) mg_residual_kernel(const __grid_constant__ MgSolveArgs A) {
+    pdl_begin();
     const MgLevel& L0 = A.H.L[0];
     MgState* st = A.st;
     if (st->halt) return;  // uniform: no block reaches the election
@@ -942,9 +1268,9 @@ __global__ void __launch_bounds__(kThreads) mg_residual_kernel(const __grid_cons
         A.W.q[c.q] = 0.0f;
         rr += rv * rv;
     });
-    block_accumulate<double>(st, kAccRR, rr, -1, 0.0);
-    if (!last_block(&st->done[2])) return;
-    const double rtot = total(st, kAccRR);
+    block_accumulate<double>(A.W, kAccRR, rr, -1, 0.0);
+    double rtot, unused;
+    if (!last_block_totals(&st->done[2], A.W, kAccRR, -1, rtot, unused) || tid() != 0) return;
     const double true_rel = sqrt(rtot / st->bb);
     st->true_rel = true_rel;
     if (true_rel <= static_cast<double>(A.tol)) {
@@ -962,11 +1288,11 @@ __global__ void __launch_bounds__(kThreads) mg_residual_kernel(const __grid_cons
         st->first_iter = 1;
         st->status = SMOKE_B200_SOLVE_ITERATION_CAP;
     }
-    zero_acc(st, kAccRR);
 }
 
 // Solution write-back and status record.
 __global__ void __launch_bounds__(kThreads) mg_finalize_kernel(const __grid_constant__ MgSolveArgs A, PcgStatusDevice* out) {
+    pdl_begin();
     const MgState* st = A.st;
     const MgLevel& L0 = A.H.L[0];
     if (st->zero_solution || A.ir) {
@@ -1009,28 +1335,50 @@ __global__ void __launch_bounds__(kThreads) mg_apply_kernel(const __grid_constan
 // ---------------------------------------------------------------------------------------------- host side
 const dim3 kBlock(TX, TY, TZ);
 
+// Launch with programmatic stream serialisation: the kernel may begin launching while the stream's previous kernel
+// still runs; its pdl_begin waits for that kernel's completion before anything is read. Captured into a graph, the
+// dependency becomes a programmatic edge.
+template <class... P, class... A>
+void pdl_launch(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 // Grid for `kernel` on level L: the level's tile columns (x, y), and as many z shares as `depth` waves of resident
 // blocks (per SM x SMs, cached per kernel and device) allow: depth code 0..3 = 1/2, 1, 2, 4 waves, 4 = one z tile
 // per block.
+// Blocks of `kernel` (kThreads each) resident on the device at once (SMs x blocks per SM), cached per kernel and
+// device.
 template <class K>
-dim3 wave(K kernel, const MgLevel& L, int depth) {
+int resident_blocks(K kernel) {
     static std::mutex lock;
     static std::map<std::pair<const void*, int>, int> cache;
     int dev = 0;
     cudaGetDevice(&dev);
-    int resident = 0;
-    {
-        std::lock_guard<std::mutex> guard(lock);
-        const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
-        auto it = cache.find(key);
-        if (it == cache.end()) {
-            int sms = 0, per_sm = 0;
-            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
-            it = cache.emplace(key, sms * per_sm).first;
-        }
-        resident = it->second;
+    std::lock_guard<std::mutex> guard(lock);
+    const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+        int sms = 0, per_sm = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+        it = cache.emplace(key, sms * per_sm).first;
     }
+    return it->second;
+}
+
+template <class K>
+dim3 wave(K kernel, const MgLevel& L, int depth) {
+    const int resident = resident_blocks(kernel);
     const int tx = (L.nx + TX - 1) / TX, ty = (L.ny + TY - 1) / TY, tz = (L.nz + TZ - 1) / TZ;
     if (depth >= kMgWaveCount - 1) return dim3(tx, ty, tz);
     const long long blocks = depth <= 0 ? resident / 2 : static_cast<long long>(resident) << (depth - 1);
@@ -1039,6 +1387,19 @@ dim3 wave(K kernel, const MgLevel& L, int depth) {
     if (gz > tz) gz = tz;
     gz = (tz + ((tz + gz - 1) / gz) - 1) / ((tz + gz - 1) / gz);  // no empty z shares
     return dim3(tx, ty, gz);
+}
+
+// Grid of a level-0 z-march kernel: the same depth codes over its (column, plane pair) units (4 = one unit per
+// block).
+template <class K>
+unsigned march_grid(K kernel, const MgLevel& L, int depth) {
+    const long long units = march_units(L).total;
+    long long blocks = units;
+    if (depth < kMgWaveCount - 1) {
+        const int resident = resident_blocks(kernel);
+        blocks = depth <= 0 ? resident / 2 : static_cast<long long>(resident) << (depth - 1);
+    }
+    return static_cast<unsigned>(std::max<long long>(1, std::min(blocks, units)));
 }
 
 // Adds a `while` node after the capture's current dependencies and captures `body` into it on `body_stream`.
@@ -1073,8 +1434,8 @@ cudaError_t add_while(cudaStream_t s, cudaStream_t body_stream, cudaGraphConditi
 // The level-0 update of the solve's preconditioner kind.
 template <typename T>
 void launch_update(const MgSolveArgs& A, int initial, cudaGraphConditionalHandle h, int in_graph, int net_loop, cudaStream_t s) {
-    if (A.learned) mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, A.H.L[0], A.wave), kBlock, 0, s>>>(A, initial, h, in_graph, net_loop);
-    else mg_update_kernel<T, false><<<wave(mg_update_kernel<T, false>, A.H.L[0], A.wave), kBlock, 0, s>>>(A, initial, h, in_graph, 0);
+    if (A.learned) pdl_launch(mg_update_kernel<T, true>, march_grid(mg_update_kernel<T, true>, A.H.L[0], A.wave), kThreads, 0, s, A, initial, h, in_graph, net_loop);
+    else pdl_launch(mg_update_kernel<T, false>, march_grid(mg_update_kernel<T, false>, A.H.L[0], A.wave), kThreads, 0, s, A, initial, h, in_graph, 0);
 }
 
 // The V-cycle below level 0: restrictions of levels 1..g-1, the block-level cycle, the up passes of levels g-1..1,
@@ -1082,17 +1443,17 @@ void launch_update(const MgSolveArgs& A, int initial, cudaGraphConditionalHandle
 void launch_coarse_cycle(const MgSolveArgs& A, uint32_t block_bytes, cudaStream_t bs) {
     const MgHierarchy& H = A.H;
     const int g = H.grid_levels;
-    for (int l = 1; l < g; ++l) mg_restrict_kernel<<<wave(mg_restrict_kernel, H.L[l], A.wave), kBlock, 0, bs>>>(H, l);
-    mg_block_kernel<<<1, kBlockLevelThreads, block_bytes, bs>>>(H);
+    for (int l = 1; l < g; ++l) pdl_launch(mg_restrict_kernel, wave(mg_restrict_kernel, H.L[l], A.wave), kBlock, 0, bs, H, l);
+    pdl_launch(mg_block_kernel, 1, kBlockLevelThreads, block_bytes, bs, H);
     for (int l = g - 1; l >= 1; --l) {
         if (H.L[l].n <= kFusedUpCells) {
-            mg_up_kernel<<<wave(mg_up_kernel, H.L[l], A.wave), kBlock, 0, bs>>>(H, l);
+            pdl_launch(mg_up_kernel, wave(mg_up_kernel, H.L[l], A.wave), kBlock, 0, bs, H, l);
         } else {
-            mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[l + 1], A.wave), kBlock, 0, bs>>>(H, l);
-            mg_smooth_kernel<false, float><<<wave(mg_smooth_kernel<false, float>, H.L[l], A.wave), kBlock, 0, bs>>>(A, l);
+            pdl_launch(mg_prolong_kernel, wave(mg_prolong_kernel, H.L[l + 1], A.wave), kBlock, 0, bs, H, l);
+            pdl_launch(mg_smooth_kernel, wave(mg_smooth_kernel, H.L[l], A.wave), kBlock, 0, bs, A, l);
         }
     }
-    mg_prolong_kernel<<<wave(mg_prolong_kernel, H.L[1], A.wave), kBlock, 0, bs>>>(H, 0);
+    pdl_launch(mg_prolong_kernel, wave(mg_prolong_kernel, H.L[1], A.wave), kBlock, 0, bs, H, 0);
 }
 
 // One iteration's loop body (everything after the update that tests convergence, up to the next update); net = 1:
@@ -1104,17 +1465,17 @@ void launch_body(const MgSolveArgs& A, int net, cudaGraphConditionalHandle h, in
     launch_coarse_cycle(A, block_bytes, bs);
     if (net) {  // z = z_V + N(r - A z_V), post-smoothed: the network corrects what the V-cycle leaves
         const LearnedSolve& N = *A.net;
-        mg_smooth_kernel<true, T, false><<<wave(mg_smooth_kernel<true, T, false>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
-        mg_net_residual_kernel<T><<<wave(mg_net_residual_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
+        pdl_launch(mg_smooth0_kernel<T, false>, march_grid(mg_smooth0_kernel<T, false>, L0, A.wave), kThreads, 0, bs, A);
+        pdl_launch(mg_net_residual_kernel<T>, wave(mg_net_residual_kernel<T>, L0, A.wave), kBlock, 0, bs, A);
         if (net_forward(N.images, N.acts, L0.zp, nullptr, nullptr, &A.st->net_rr, N.occupancy, bs, &A.st->net_off) != cudaSuccess) return;
-        mg_net_gamma_kernel<T><<<wave(mg_net_gamma_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
-        mg_net_add_kernel<T><<<wave(mg_net_add_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A, N.acts.y);
-        mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
-        mg_update_kernel<T, true><<<wave(mg_update_kernel<T, true>, L0, A.wave), kBlock, 0, bs>>>(A, 0, h, in_graph, 1);
+        pdl_launch(mg_net_gamma_kernel<T>, wave(mg_net_gamma_kernel<T>, L0, A.wave), kBlock, 0, bs, A, N.acts.y);
+        pdl_launch(mg_net_add_kernel<T>, wave(mg_net_add_kernel<T>, L0, A.wave), kBlock, 0, bs, A, N.acts.y);
+        pdl_launch(mg_pq_kernel<T>, march_grid(mg_pq_kernel<T>, L0, A.wave), kThreads, 0, bs, A);
+        pdl_launch(mg_update_kernel<T, true>, march_grid(mg_update_kernel<T, true>, L0, A.wave), kThreads, 0, bs, A, 0, h, in_graph, 1);
         return;
     }
-    mg_smooth_kernel<true, T><<<wave(mg_smooth_kernel<true, T>, L0, A.wave), kBlock, 0, bs>>>(A, 0);
-    mg_pq_kernel<T><<<wave(mg_pq_kernel<T>, L0, A.wave), kBlock, 0, bs>>>(A);
+    pdl_launch(mg_smooth0_kernel<T, true>, march_grid(mg_smooth0_kernel<T, true>, L0, A.wave), kThreads, 0, bs, A);
+    pdl_launch(mg_pq_kernel<T>, march_grid(mg_pq_kernel<T>, L0, A.wave), kThreads, 0, bs, A);
     launch_update<T>(A, 0, h, in_graph, 0, bs);
 }
 
@@ -1161,16 +1522,16 @@ cudaError_t enqueue_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream
             cudaGraphConditionalHandle h2;
             e = cudaGraphConditionalHandleCreate(&h2, graph, 0, cudaGraphCondAssignDefault);
             if (e != cudaSuccess) return e;
-            mg_loop_gate_kernel<<<1, 1, 0, s>>>(A.st, h2);
+            pdl_launch(mg_loop_gate_kernel, 1, 1, 0, s, A.st, h2);
             e = add_while(s, body_stream, h2, [&](cudaStream_t bs) { launch_body<T>(A, 0, h2, 1, block_bytes, bs); });
             if (e != cudaSuccess) return e;
         }
         if (A.ir) {
-            mg_accumulate_kernel<<<wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s>>>(A);
-            mg_residual_kernel<<<wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s>>>(A);
+            pdl_launch(mg_accumulate_kernel, wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s, A);
+            pdl_launch(mg_residual_kernel, wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s, A);
         }
     }
-    mg_finalize_kernel<<<wave(mg_finalize_kernel, L0, A.wave), kBlock, 0, s>>>(A, out);
+    pdl_launch(mg_finalize_kernel, wave(mg_finalize_kernel, L0, A.wave), kBlock, 0, s, A, out);
     return cudaGetLastError();
 }
 
@@ -1198,11 +1559,11 @@ cudaError_t run_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream_t s
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (A.ir) {
-            mg_accumulate_kernel<<<wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s>>>(A);
-            mg_residual_kernel<<<wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s>>>(A);
+            pdl_launch(mg_accumulate_kernel, wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s, A);
+            pdl_launch(mg_residual_kernel, wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s, A);
         }
     }
-    mg_finalize_kernel<<<wave(mg_finalize_kernel, L0, A.wave), kBlock, 0, s>>>(A, out);
+    pdl_launch(mg_finalize_kernel, wave(mg_finalize_kernel, L0, A.wave), kBlock, 0, s, A, out);
     return cudaGetLastError();
 }
 
@@ -1275,6 +1636,10 @@ __global__ void mg_code_tail_kernel(uint16_t* code, uint32_t n) {
 }
 
 }  // namespace
+
+uint32_t mg_partial_blocks(int nx, int ny, int nz) {
+    return static_cast<uint32_t>((nx + TX - 1) / TX) * static_cast<uint32_t>((ny + TY - 1) / TY) * static_cast<uint32_t>((nz + TZ - 1) / TZ);
+}
 
 int mg_level_count(int nx, int ny, int nz) {
     int levels = 1;
