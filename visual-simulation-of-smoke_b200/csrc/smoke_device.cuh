@@ -143,21 +143,88 @@ __device__ inline float scalar_tap_slow(const float* __restrict__ f, int x, int 
 
 // ---------------------------------------------------------------------------------------------- samplers
 // Hermite cubic with central slopes, slopes zeroed where they disagree in sign with the secant or the secant
-// is below 1e-6 (backend-cuda.cu:378-392).
-__device__ __forceinline__ float mono_cubic(float p0, float p1, float p2, float p3, float t) {
-    const float delta = p2 - p1;
-    float m1 = 0.5f * (p2 - p0);
-    float m2 = 0.5f * (p3 - p1);
-    if (fabsf(delta) < 1.0e-6f) {
-        m1 = 0.0f;
-        m2 = 0.0f;
-    } else {
-        if (m1 * delta <= 0.0f) m1 = 0.0f;
-        if (m2 * delta <= 0.0f) m2 = 0.0f;
-    }
-    const float t2 = t * t;
-    const float t3 = t2 * t;
-    return (2.0f * t3 - 3.0f * t2 + 1.0f) * p1 + (t3 - 2.0f * t2 + t) * m1 + (-2.0f * t3 + 3.0f * t2) * p2 + (t3 - t2) * m2;
+// is below 1e-6 (backend-cuda.cu:378-392). Every operation is spelled out (IEEE single, round to nearest), so that
+// the two-lane form below, which the padded samplers use, gives the same bits as this scalar form.
+struct HermiteW {
+    float h00, h10, h01, h11;  // weights of p1, m1, p2, m2
+};
+__device__ __forceinline__ HermiteW hermite_weights(float t) {
+    const float t2 = __fmul_rn(t, t);
+    const float t3 = __fmul_rn(t2, t);
+    HermiteW w;
+    w.h00 = __fmaf_rn(2.0f, t3, __fmaf_rn(-3.0f, t2, 1.0f));  // 2t^3 - 3t^2 + 1
+    w.h10 = __fadd_rn(t3, __fmaf_rn(-2.0f, t2, t));            // t^3 - 2t^2 + t
+    w.h01 = __fmaf_rn(-2.0f, t3, __fmul_rn(3.0f, t2));         // -2t^3 + 3t^2
+    w.h11 = __fsub_rn(t3, t2);                                  // t^3 - t^2
+    return w;
+}
+__device__ __forceinline__ float mono_cubic(float p0, float p1, float p2, float p3, const HermiteW& w) {
+    const float delta = __fsub_rn(p2, p1);
+    float m1 = __fmul_rn(0.5f, __fsub_rn(p2, p0));
+    float m2 = __fmul_rn(0.5f, __fsub_rn(p3, p1));
+    const bool flat = fabsf(delta) < 1.0e-6f;
+    if (flat || __fmul_rn(m1, delta) <= 0.0f) m1 = 0.0f;
+    if (flat || __fmul_rn(m2, delta) <= 0.0f) m2 = 0.0f;
+    float r = __fmul_rn(w.h00, p1);
+    r = __fmaf_rn(w.h10, m1, r);
+    r = __fmaf_rn(w.h01, p2, r);
+    return __fmaf_rn(w.h11, m2, r);
+}
+__device__ __forceinline__ float mono_cubic(float p0, float p1, float p2, float p3, float t) { return mono_cubic(p0, p1, p2, p3, hermite_weights(t)); }
+
+// Two lanes of FP32 in one 64-bit register, for sm_100's paired FP32 instructions (add/sub/mul/fma .rn.f32x2): two
+// IEEE single operations per instruction, each lane rounded exactly as the scalar instruction rounds it.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float a, float b) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(f32x2 v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+struct HermiteW2 {
+    f32x2 h00, h10, h01, h11;
+};
+__device__ __forceinline__ HermiteW2 hermite_pair(const HermiteW& a, const HermiteW& b) {
+    return HermiteW2{f2_pack(a.h00, b.h00), f2_pack(a.h10, b.h10), f2_pack(a.h01, b.h01), f2_pack(a.h11, b.h11)};
+}
+// Two monotone cubics at once (lane by lane the scalar mono_cubic, same operations in the same order): the slope and
+// polynomial arithmetic in paired instructions, the limiter's tests per lane.
+__device__ __forceinline__ f32x2 mono_cubic2(f32x2 p0, f32x2 p1, f32x2 p2, f32x2 p3, const HermiteW2& w) {
+    const f32x2 half = f2_pack(0.5f, 0.5f);
+    const f32x2 delta = f2_sub(p2, p1);
+    const f32x2 m1 = f2_mul(half, f2_sub(p2, p0));
+    const f32x2 m2 = f2_mul(half, f2_sub(p3, p1));
+    const f32x2 s1 = f2_mul(m1, delta), s2 = f2_mul(m2, delta);
+    float d0, d1, a0, a1, b0, b1, m10, m11, m20, m21;
+    f2_unpack(delta, d0, d1);
+    f2_unpack(s1, a0, a1);
+    f2_unpack(s2, b0, b1);
+    f2_unpack(m1, m10, m11);
+    f2_unpack(m2, m20, m21);
+    const bool flat0 = fabsf(d0) < 1.0e-6f, flat1 = fabsf(d1) < 1.0e-6f;
+    if (flat0 || a0 <= 0.0f) m10 = 0.0f;
+    if (flat1 || a1 <= 0.0f) m11 = 0.0f;
+    if (flat0 || b0 <= 0.0f) m20 = 0.0f;
+    if (flat1 || b1 <= 0.0f) m21 = 0.0f;
+    f32x2 r = f2_mul(w.h00, p1);
+    r = f2_fma(w.h10, f2_pack(m10, m11), r);
+    r = f2_fma(w.h01, p2, r);
+    return f2_fma(w.h11, f2_pack(m20, m21), r);
 }
 
 __device__ __forceinline__ float wrap_pos(float p, int n, float h) {
@@ -237,6 +304,50 @@ struct PadField {
     uint32_t px, pxy;  // padded row and slab pitch
 };
 
+// Tensor monotone cubic of the 4 x 4 x 4 taps at f (x fastest; row pitch sy, slab pitch sz): 16 cubics along x, 4 along
+// y, 1 along z, the scalar mono_cubic's arithmetic. The x cubics run two rows per paired instruction, the y cubics two
+// slabs per instruction.
+__device__ __forceinline__ float cubic_taps(const float* __restrict__ f, uint32_t sy, uint32_t sz, float tx, float ty, float tz) {
+    const HermiteW wx = hermite_weights(tx), wy = hermite_weights(ty);
+    const HermiteW2 wx2 = hermite_pair(wx, wx), wy2 = hermite_pair(wy, wy);
+    float ys[4][4];
+#pragma unroll
+    for (int dz = 0; dz < 4; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 4; dy += 2) {
+            const float* r0 = f + dz * sz + dy * sy;
+            const float* r1 = r0 + sy;
+            const f32x2 c = mono_cubic2(f2_pack(__ldg(r0), __ldg(r1)), f2_pack(__ldg(r0 + 1), __ldg(r1 + 1)), f2_pack(__ldg(r0 + 2), __ldg(r1 + 2)), f2_pack(__ldg(r0 + 3), __ldg(r1 + 3)), wx2);
+            f2_unpack(c, ys[dz][dy], ys[dz][dy + 1]);
+        }
+    float zs[4];
+#pragma unroll
+    for (int dz = 0; dz < 4; dz += 2) {
+        const f32x2 c = mono_cubic2(f2_pack(ys[dz][0], ys[dz + 1][0]), f2_pack(ys[dz][1], ys[dz + 1][1]), f2_pack(ys[dz][2], ys[dz + 1][2]), f2_pack(ys[dz][3], ys[dz + 1][3]), wy2);
+        f2_unpack(c, zs[dz], zs[dz + 1]);
+    }
+    return mono_cubic(zs[0], zs[1], zs[2], zs[3], tz);
+}
+
+// The same tensor cubic for two fields with the same tap box (lane 0: f, lane 1: g), every cubic one paired
+// instruction stream for both.
+__device__ __forceinline__ void cubic_taps_pair(const float* __restrict__ f, const float* __restrict__ g, uint32_t sy, uint32_t sz, float tx, float ty, float tz, float& out_f, float& out_g) {
+    const HermiteW wx = hermite_weights(tx), wy = hermite_weights(ty), wz = hermite_weights(tz);
+    const HermiteW2 wx2 = hermite_pair(wx, wx), wy2 = hermite_pair(wy, wy), wz2 = hermite_pair(wz, wz);
+    f32x2 zs[4];
+#pragma unroll
+    for (int dz = 0; dz < 4; ++dz) {
+        f32x2 ys[4];
+#pragma unroll
+        for (int dy = 0; dy < 4; ++dy) {
+            const uint32_t o = dz * sz + dy * sy;
+            ys[dy] = mono_cubic2(f2_pack(__ldg(f + o), __ldg(g + o)), f2_pack(__ldg(f + o + 1), __ldg(g + o + 1)), f2_pack(__ldg(f + o + 2), __ldg(g + o + 2)), f2_pack(__ldg(f + o + 3), __ldg(g + o + 3)), wx2);
+        }
+        zs[dz] = mono_cubic2(ys[0], ys[1], ys[2], ys[3], wy2);
+    }
+    f2_unpack(mono_cubic2(zs[0], zs[1], zs[2], zs[3], wz2), out_f, out_g);
+}
+
 // Samples field KIND at world position (x,y,z): periodic wrap of the position, conversion to grid coordinates
 // (cell-centred axes offset by -0.5, backend-cuda.cu:413-415, 505-507), then trilinear (8 taps) or tensor monotone
 // cubic (64 taps) from the padded copy; a tap box reaching beyond the padding goes through sample_edge.
@@ -276,20 +387,31 @@ __device__ __forceinline__ float sample_pad(const PadField& F, float x, float y,
         // taps x0-1 .. x0+2 within [-kPad, ex+kPad]
         if (!(x0 >= 1 - kPad && x0 <= ex + kPad - 2 && y0 >= 1 - kPad && y0 <= ey + kPad - 2 && z0 >= 1 - kPad && z0 <= ez + kPad - 2)) return sample_edge(F.raw, KIND, 1, x0, y0, z0, tx, ty, tz, P);
         const uint32_t base = static_cast<uint32_t>(z0 - 1 + kPad) * sz + static_cast<uint32_t>(y0 - 1 + kPad) * sy + static_cast<uint32_t>(x0 - 1 + kPad);
-        const float* f = F.p;
-        float zs[4];
-#pragma unroll
-        for (int dz = 0; dz < 4; ++dz) {
-            float ys[4];
-#pragma unroll
-            for (int dy = 0; dy < 4; ++dy) {
-                const uint32_t b = base + dz * sz + dy * sy;
-                ys[dy] = mono_cubic(__ldg(f + b), __ldg(f + b + 1), __ldg(f + b + 2), __ldg(f + b + 3), tx);
-            }
-            zs[dz] = mono_cubic(ys[0], ys[1], ys[2], ys[3], ty);
-        }
-        return mono_cubic(zs[0], zs[1], zs[2], zs[3], tz);
+        return cubic_taps(F.p + base, sy, sz, tx, ty, tz);
     }
+}
+
+// Temperature (KIND 4) and density (KIND 3) at the same world position, as sample_pad<4> and sample_pad<3> give them.
+// Both are cell-centred with padded copies of the same shape, so when their periodic axes agree and the cubic tap box
+// lies within the padding, one tap box serves both and the cubic runs with the fields in the two lanes.
+template <bool CUBIC, bool POW2>
+__device__ __forceinline__ void sample_pad_scalars(const PadField& T, const PadField& D, float x, float y, float z, const StepParams& P, float& out_t, float& out_d) {
+    if (CUBIC && (P.tper[0] != 0) == (P.dper[0] != 0) && (P.tper[1] != 0) == (P.dper[1] != 0) && (P.tper[2] != 0) == (P.dper[2] != 0) && T.px == D.px && T.pxy == D.pxy) {
+        float px = x, py = y, pz = z;
+        if (P.dper[0]) px = wrap_pos(px, P.nx, P.h);
+        if (P.dper[1]) py = wrap_pos(py, P.ny, P.h);
+        if (P.dper[2]) pz = wrap_pos(pz, P.nz, P.h);
+        const float gx = over_h<POW2>(px, P) - 0.5f, gy = over_h<POW2>(py, P) - 0.5f, gz = over_h<POW2>(pz, P) - 0.5f;
+        const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
+        const int ex = P.nx - 1, ey = P.ny - 1, ez = P.nz - 1;
+        if (x0 >= 1 - kPad && x0 <= ex + kPad - 2 && y0 >= 1 - kPad && y0 <= ey + kPad - 2 && z0 >= 1 - kPad && z0 <= ez + kPad - 2) {
+            const uint32_t base = static_cast<uint32_t>(z0 - 1 + kPad) * D.pxy + static_cast<uint32_t>(y0 - 1 + kPad) * D.px + static_cast<uint32_t>(x0 - 1 + kPad);
+            cubic_taps_pair(T.p + base, D.p + base, D.px, D.pxy, gx - static_cast<float>(x0), gy - static_cast<float>(y0), gz - static_cast<float>(z0), out_t, out_d);
+            return;
+        }
+    }
+    out_t = sample_pad<4, CUBIC, POW2>(T, x, y, z, P);
+    out_d = sample_pad<3, CUBIC, POW2>(D, x, y, z, P);
 }
 
 // Trilinear sample of field KIND at the start of a back-trace: the centre of face (i, j, k) of axis START (0-2) or of

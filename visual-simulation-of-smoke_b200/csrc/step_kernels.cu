@@ -440,8 +440,10 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_c
     }
     const float h = P.h;
     const float3 p = trace_rk2<POW2, 3>((static_cast<float>(x) + 0.5f) * h, (static_cast<float>(y) + 0.5f) * h, (static_cast<float>(z) + 0.5f) * h, x, y, z, u, v, w, occ, P);
-    t[q] = sample_pad<4, CUBIC, POW2>(t_tmp, p.x, p.y, p.z, P);
-    d[q] = sample_pad<3, CUBIC, POW2>(d_tmp, p.x, p.y, p.z, P);
+    float tv, dv;
+    sample_pad_scalars<CUBIC, POW2>(t_tmp, d_tmp, p.x, p.y, p.z, P, tv, dv);
+    t[q] = tv;
+    d[q] = dv;
 }
 
 __global__ void density_fill_kernel(const FillEntry* __restrict__ list, const uint32_t* __restrict__ count, float* __restrict__ d) {
