@@ -264,8 +264,10 @@ __device__ __forceinline__ void advect_face_one(const StepParams& P, unsigned bl
 // Samples and traces read the padded copies of the velocity (ghost cells hold the boundary taps). Blocks
 // [0, bu) advect u faces, [bu, bu + bv) v faces, the rest w faces, each in the shape P.tile selects. POW2: the cell
 // size is a power of two, so grid coordinates are products instead of divisions (over_h, the same floats).
+// Six blocks per SM (at most 42 registers): the gathers wait on L1/L2 latency, and the extra resident warps hide more
+// of it than the few spilled registers cost (240 -> 224 us at 128^3 against the compiler's 64 registers, 4 blocks).
 template <bool CUBIC, bool TILED, bool POW2>
-__global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ StepParams P, const PadField u, const PadField v, const PadField w, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou, float* __restrict__ ov,
+__global__ void __launch_bounds__(kThreads, 6) advect_velocity_kernel(const __grid_constant__ StepParams P, const PadField u, const PadField v, const PadField w, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou, float* __restrict__ ov,
                                                                     float* __restrict__ ow, unsigned bu, unsigned bv) {
     const unsigned b = blockIdx.x;
     if (b < bu) advect_face_one<0, CUBIC, TILED, POW2>(P, b, u, v, w, occ, su, ou);
