@@ -272,8 +272,8 @@ MG_BYTES_PER_CELL_ITERATION = 85.0
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum over every kernel) of one multigrid FCG solve from zero
 # on the 128^3 plume after the spin-up, 12 iterations, 1 pass: the kernels of the graph launched one by one
 # (bench.py --profile solve, ncu --cache-control none so that L2 carries over between kernels as in the graph);
-# 41.8 MB read + 434.4 MB written, per grid size. Scaled by iterations when a solve takes another count.
-MG_SOLVE_DRAM_BYTES = {128: (476.2e6, 12)}
+# 63.8 MB read + 447.9 MB written, per grid size. Scaled by iterations when a solve takes another count.
+MG_SOLVE_DRAM_BYTES = {128: (511.7e6, 12)}
 
 
 def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5, bytes_per_iteration=JACOBI_BYTES_PER_CELL_ITERATION, kernel="pcg_kernel", traffic_table=None):
@@ -311,8 +311,9 @@ def solver_kernel_roofline(sim, n_cells, peak_gbs, peak_kind, repeats=5, bytes_p
             "frac": round(achieved / peak_gbs, 3), "traffic": traffic, "traffic_over_algorithmic": round(traffic / algo_bytes, 3) if traffic else None,
             "algorithmic_bytes_per_launch": algo_bytes, "launch_ms": round(ms, 4), "iterations": it,
             "bytes_per_cell_iteration": bytes_per_iteration,
-            "note": "traffic: DRAM bytes of one solve from an ncu capture of its kernels (cache control off, so L2 carries over as in the graph); "
-                    "the working set (~90 MB at 128^3) stays mostly in the 126 MB L2, so the solve is bound by latency, not by HBM"}
+            "note": ("traffic: DRAM bytes of one solve from an ncu capture of its kernels (cache control off, so L2 carries over as in the graph); "
+                     "the working set (~90 MB at 128^3) stays mostly in the 126 MB L2, so the solve is bound by latency, not by HBM") if n_cells * 43 < 126e6 else
+                    "the solve's arrays (about 43 B per cell) are far larger than L2, so the level-0 passes stream from HBM; no ncu traffic capture at this size"}
 
 
 def divergence_norms(cfg, u, v, w):
