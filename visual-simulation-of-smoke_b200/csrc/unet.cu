@@ -265,6 +265,179 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
     if (warp == 0) tc::tmem_free(tmem, S::kTmemCols);
 }
 
+// ------------------------------------------------------------------------------------------ single-output layer
+// The network's last convolution has one output channel (16 -> 1). Padding it to N = 16 output channels runs 16x the
+// MMAs it needs, each reading a 4 KB A operand. Here the N = 16 accumulator columns are 16 output z-planes instead: a
+// tile is 8 x 16 cells x kBandZ planes (z0 .. z0 + 15), its inputs are the 18 planes z0 - 1 .. z0 + 16 (six 3-deep halo
+// boxes), and input plane j (z' = z0 - 1 + j) contributes through each in-plane tap (dx, dy) with the banded matrix
+// B[j][tap][n][ci] = w[dz][dy][dx][ci] for dz = j - 1 - n in {-1, 0, 1}, else 0. So a tile costs 18 x 9 MMAs
+// instead of 16 x 27, and every A operand (the box at the tap's offset) is read once per input plane.
+// The 18 banded matrices of a tap are windows of one tall matrix: rows i = 0 .. 32 (16 bytes = 8 channels each, in
+// two K column blocks of kBandRows rows) hold dz = 16 - i (zero but for i = 15, 16, 17), and the matrix of input plane
+// j is rows 17 - j .. 32 - j (a descriptor starting 16 (17 - j) bytes in, SBO 128 bytes, LBO one column block). 9.5 KB
+// of weights instead of 83 KB, so three blocks fit on an SM.
+constexpr int kBandZ = 16;                                                // output planes per tile (N)
+constexpr int kBandJ = kBandZ + 2;                                        // input planes per tile
+constexpr int kBandRows = kBandZ + kBandJ - 1;                            // rows of a tap's tall matrix
+constexpr uint32_t kBandBlock = static_cast<uint32_t>(kBandRows) * 16u;   // one K column block (LBO)
+constexpr uint32_t kBandTap = 2u * kBandBlock;                            // a tap's two column blocks (16 channels)
+constexpr uint32_t kBandBytes = 9u * kBandTap;                            // 9504
+static_assert(kBandBytes % 16 == 0, "bulk copy size");
+constexpr int kBandStages = 3;
+constexpr uint32_t kBandStage = 2 * kPlane;                               // one 3-deep box of both 8-channel planes
+constexpr uint32_t kBandSmem = kBandStages * kBandStage + kBandBytes;
+constexpr int kBandItems = kBandJ / 3;                                    // boxes per tile
+static_assert(kBandJ % 3 == 0, "whole boxes");
+
+__global__ void __launch_bounds__(kConvThreads) conv3_band_kernel(const __grid_constant__ ConvArgs a, const __grid_constant__ CUtensorMap map) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* Bs = smem + kBandStages * kBandStage;
+    __shared__ uint64_t full[kBandStages], freed[kBandStages], done[2], drained[2], wbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag;
+    constexpr uint32_t kCols = 32;  // two 16-column accumulators
+    if (a.skip && *a.skip) return;  // uniform: every block reads the same word
+    const int t = threadIdx.x, warp = t >> 5;
+    if (t == 0) {
+        for (int st = 0; st < kBandStages; ++st) {
+            tc::mbar_init(&full[st], 1);
+            tc::mbar_init(&freed[st], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            tc::mbar_init(&done[b], 1);
+            tc::mbar_init(&drained[b], kEpiThreads);
+        }
+        tc::mbar_init(&wbar, 1);
+        abort_flag = 0;
+    }
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, kCols);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+    const long long wait = a.wait_cycles > 0 ? a.wait_cycles : kSpinCycles;
+    volatile int* abort = &abort_flag;
+    const int ntx = (a.nx + kTX - 1) / kTX, nty = (a.ny + kTY - 1) / kTY, ntz = (a.nz + kBandZ - 1) / kBandZ;
+    const uint32_t tiles = static_cast<uint32_t>(ntx) * nty * ntz;
+    const uint32_t my_tiles = blockIdx.x < tiles ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0u;
+
+    if (warp == 4) {
+        if ((t & 31) == 0) {
+            // ---------------------------------------------------------------- producer and MMA issuer
+            const uint32_t items = my_tiles * kBandItems;  // (tile, box) pairs in order
+            constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 16, false, false);
+            const uint32_t b_base = tc::smem_addr(Bs);
+            uint32_t loaded = 0, consumed = 0, issued = 0;
+            bool ok = true;
+            bool weights_ready = false;
+            tc::mbar_arrive_expect_tx(&wbar, kBandBytes);
+            for (uint32_t off = 0; off < kBandBytes; off += 16384u) tc::bulk_copy_g2s(Bs + off, a.wpack + off, min(16384u, kBandBytes - off), &wbar);
+            auto issue_load = [&](uint32_t k) -> bool {
+                const int st = static_cast<int>(k % kBandStages);
+                if (k >= static_cast<uint32_t>(kBandStages) && !tc::mbar_wait_or_abort(&freed[st], ((k / kBandStages) - 1u) & 1u, wait, abort)) return false;
+                const uint32_t tile = blockIdx.x + (k / kBandItems) * gridDim.x;
+                const int box = static_cast<int>(k % kBandItems);
+                const int tx = static_cast<int>(tile % ntx), rest = static_cast<int>(tile / ntx);
+                const int ty = rest % nty, tz = rest / nty;
+                tc::mbar_arrive_expect_tx(&full[st], 2 * kBox);
+                if (!a.drop_loads) {
+                    for (int p = 0; p < 2; ++p) tc::tma_load_4d(smem + st * kBandStage + p * kPlane, &map, 8 * p, tx * kTX - 1, ty * kTY - 1, tz * kBandZ - 1 + 3 * box, &full[st]);
+                    loaded = k + 1;
+                }
+                return true;
+            };
+            for (uint32_t k = 0; k < static_cast<uint32_t>(kBandStages - 1) && k < items && ok; ++k) ok = issue_load(k);
+            for (uint32_t i = 0; ok && i < items; ++i) {
+                const uint32_t jl = i / kBandItems;
+                const int box = static_cast<int>(i % kBandItems), b = static_cast<int>(jl & 1u), st = static_cast<int>(i % kBandStages);
+                if (box == 0 && jl >= 2 && !tc::mbar_wait_or_abort(&drained[b], ((jl >> 1) - 1u) & 1u, wait, abort)) {
+                    ok = false;
+                    break;
+                }
+                if (!tc::mbar_wait_or_abort(&full[st], (i / kBandStages) & 1u, wait, abort)) {
+                    ok = false;
+                    break;
+                }
+                consumed = i + 1;
+                if (!weights_ready) {
+                    if (!tc::mbar_wait_or_abort(&wbar, 0, wait, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    weights_ready = true;
+                }
+                tc::fence_after_sync();
+                const uint32_t a_base = tc::smem_addr(smem + st * kBandStage);
+#pragma unroll 1
+                for (int k = 0; k < 27; ++k) {  // box plane zz = k / 9 (input plane j = 3 box + zz), in-plane tap k % 9
+                    const int j = 3 * box + k / 9, tap = k % 9;
+                    const uint64_t bd = tc::smem_desc(b_base + static_cast<uint32_t>(tap) * kBandTap + static_cast<uint32_t>(kBandJ - 1 - j) * 16u, kBandBlock, 128u);
+                    tc::mma_bf16(tmem + static_cast<uint32_t>(b * 16), tc::smem_desc(a_base + tap_offset(k), kPlane, kRow), bd, idesc, (box > 0 || k > 0) ? 1u : 0u);
+                }
+                tc::commit(&freed[st]);
+                if (box == kBandItems - 1) tc::commit(&done[b]);
+                issued = i + 1;
+                if (i + kBandStages - 1 < items && !issue_load(i + kBandStages - 1)) ok = false;
+            }
+            if (!ok) {
+                atomicOr(a.error, 1u);
+                *abort = 1;
+            }
+            // nothing may still write this block's shared or tensor memory when it exits (bounded waits again)
+            for (uint32_t k = consumed; k < loaded; ++k) tc::mbar_wait(&full[k % kBandStages], (k / kBandStages) & 1u, wait);
+            if (!weights_ready) tc::mbar_wait(&wbar, 0, wait);
+            if (issued > 0) tc::mbar_wait(&freed[(issued - 1) % kBandStages], ((issued - 1) / kBandStages) & 1u, wait);
+        }
+    } else {
+        // -------------------------------------------------------------------- epilogue (threads 0-127)
+        const float bias = a.bias ? __ldg(a.bias) : 0.0f;
+        const uint32_t slab = static_cast<uint32_t>(a.nx) * a.ny;
+        for (uint32_t jl = 0; jl < my_tiles; ++jl) {
+            const int b = static_cast<int>(jl & 1u);
+            const bool ready = __all_sync(0xffffffffu, tc::mbar_wait_or_abort(&done[b], (jl >> 1) & 1u, wait, abort) ? 1 : 0) != 0;
+            if (!ready) {
+                if (t == 0) atomicOr(a.error, 1u);
+                *abort = 1;
+                break;
+            }
+            tc::fence_after_sync();
+            float acc[16];
+            tc::tmem_load16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(b * 16), acc);
+            tc::fence_before_sync();
+            tc::mbar_arrive(&drained[b]);
+            const uint32_t tile = blockIdx.x + jl * gridDim.x;
+            const int tx = static_cast<int>(tile % ntx), rest = static_cast<int>(tile / ntx);
+            const int x = tx * kTX + (t & 7), y = (rest % nty) * kTY + (t >> 3), z0 = (rest / nty) * kBandZ;
+            if (x < a.nx && y < a.ny) {
+                const uint32_t q0 = static_cast<uint32_t>(y) * a.nx + x;
+#pragma unroll
+                for (int n = 0; n < kBandZ; ++n)
+                    if (z0 + n < a.nz) a.out_f32[static_cast<uint32_t>(z0 + n) * slab + q0] = acc[n] + bias;
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (warp == 0) tc::tmem_free(tmem, kCols);
+}
+
+// Banded operand image of the single-output layer (w: W[tap][ci][0], tap = (dz + 1) * 9 + (dy + 1) * 3 + dx + 1, 16
+// input channels): for in-plane tap t and column block c, row i holds channels 8c .. 8c + 7 of the weight of
+// dz = 16 - i (0 outside [-1, 1]), at byte t * kBandTap + c * kBandBlock + i * 16 + (k % 8) * 2.
+__global__ void pack_band_kernel(const float* __restrict__ w, int cin, uint8_t* __restrict__ band) {
+    const int total = 9 * 2 * kBandRows * 8;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const int kk = e % 8, i = (e / 8) % kBandRows, c = (e / (8 * kBandRows)) % 2, tap = e / (16 * kBandRows);
+        const int k = 8 * c + kk, dz = kBandJ - 2 - i;
+        float v = 0.0f;
+        if (dz >= -1 && dz <= 1 && k < cin) v = w[static_cast<size_t>((dz + 1) * 9 + tap) * cin + k];
+        const size_t off = static_cast<size_t>(tap) * kBandTap + static_cast<size_t>(c) * kBandBlock + static_cast<size_t>(i) * 16 + kk * 2;
+        *reinterpret_cast<__nv_bfloat16*>(band + off) = __float2bfloat16_rn(v);
+    }
+}
+
 // Operand image of B for a convolution whose input has `cs` stored channels: K = taps x cs rows (tap-major), N =
 // the output channels in chunks of nc; K-major core matrices, element (co, k) of chunk co / nc at byte
 // ((k / 8) * (nc / 8) + (co % nc) / 8) * 128 + (co % 8) * 16 + (k % 8) * 2 of that chunk's image.
@@ -355,6 +528,26 @@ cudaError_t conv_typed(const VolumeDims& d, int chunks, const ConvArgs& a, cudaS
     const int resident = resident_blocks(reinterpret_cast<const void*>(conv3_kernel<CS, NC>), S::kSmem, S::kTmemCols, kConvThreads);
     const int gx = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(tiles, static_cast<uint64_t>(std::max(1, resident / chunks)))));
     conv3_kernel<CS, NC><<<dim3(gx, chunks), kConvThreads, S::kSmem, s>>>(a, map);
+    return cudaGetLastError();
+}
+
+// The single-output layer's forward (conv3_band_kernel): FP32 output only, 16 stored input channels.
+cudaError_t conv_band(const VolumeDims& d, const ConvArgs& a, cudaStream_t s) {
+    static std::once_flag once;
+    static cudaError_t configured = cudaSuccess;
+    std::call_once(once, [] {
+        configured = cudaFuncSetAttribute(conv3_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kBandSmem));
+        if (configured == cudaSuccess) configured = cudaFuncSetAttribute(conv3_band_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    });
+    if (configured != cudaSuccess) return configured;
+    if ((reinterpret_cast<uintptr_t>(a.in) & 15u) != 0 || a.out_f32 == nullptr || a.error == nullptr) return cudaErrorInvalidValue;
+    CUtensorMap map;
+    const cudaError_t e = halo_map(&map, 16, a);
+    if (e != cudaSuccess) return e;
+    const uint64_t tiles = static_cast<uint64_t>((d.nx + kTX - 1) / kTX) * ((d.ny + kTY - 1) / kTY) * ((d.nz + kBandZ - 1) / kBandZ);
+    const int resident = resident_blocks(reinterpret_cast<const void*>(conv3_band_kernel), kBandSmem, 32, kConvThreads);
+    const int gx = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(tiles, static_cast<uint64_t>(resident))));
+    conv3_band_kernel<<<gx, kConvThreads, kBandSmem, s>>>(a, map);
     return cudaGetLastError();
 }
 
@@ -850,6 +1043,20 @@ size_t wgrad_partial_floats(const VolumeDims& d0) {
 
 cudaError_t conv_layer(int L, const VolumeDims& d, const NetImages& I, const __nv_bfloat16* in, __nv_bfloat16* out, float* out_f32, unsigned* error, cudaStream_t s, const uint32_t* skip = nullptr) {
     const int relu = L < kNetLayers - 1;
+    if (L == kNetLayers - 1 && out == nullptr && out_f32 != nullptr && d.n > 0) {  // the single-output layer: banded
+        ConvArgs a{};
+        a.in = in;
+        a.wpack = I.band;
+        a.bias = I.bias[L];
+        a.out_f32 = out_f32;
+        a.error = error;
+        a.skip = skip;
+        a.nx = d.nx;
+        a.ny = d.ny;
+        a.nz = d.nz;
+        a.n = d.n;
+        return conv_band(d, a, s);
+    }
     return launch_conv3(d, net_store(kNet[L].cin), kNet[L].cout, in, I.fwd[L], I.bias[L], relu, nullptr, out, net_store(kNet[L].cout), out_f32, error, s, skip);
 }
 // Gradient through layer L's convolution: gin = conv^T(g), gated by `gate` (the layer's input activation when it is
@@ -869,7 +1076,7 @@ size_t net_images_bytes() {
         if (L > 0) b += align256(conv_pack_bytes(net_grad_store(kNet[L].cout), kNet[L].cin));
         b += align256(net_cout_pad(kNet[L].cout) * sizeof(float));
     }
-    return b;
+    return b + align256(kBandBytes);
 }
 
 void net_images_bind(NetImages& I, void* base) {
@@ -885,6 +1092,7 @@ void net_images_bind(NetImages& I, void* base) {
         I.bias[L] = reinterpret_cast<float*>(p);
         p += align256(net_cout_pad(kNet[L].cout) * sizeof(float));
     }
+    I.band = reinterpret_cast<uint8_t*>(p);
 }
 
 cudaError_t net_pack(const float* w, const NetImages& I, cudaStream_t s) {
@@ -896,7 +1104,9 @@ cudaError_t net_pack(const float* w, const NetImages& I, cudaStream_t s) {
         bias_pad_kernel<<<1, 128, 0, s>>>(wl + net_weight_count(L), kNet[L].cout, net_cout_pad(kNet[L].cout), I.bias[L]);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    return cudaSuccess;
+    static_assert(kNet[kNetLayers - 1].cout == 1 && kNet[kNetLayers - 1].cin == 16 && kNet[kNetLayers - 1].level == 0, "the banded layer is 16 -> 1 on level 0");
+    pack_band_kernel<<<64, 256, 0, s>>>(w + net_param_offset(kNetLayers - 1), kNet[kNetLayers - 1].cin, I.band);
+    return cudaGetLastError();
 }
 
 namespace {

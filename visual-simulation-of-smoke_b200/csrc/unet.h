@@ -78,6 +78,7 @@ struct NetImages {
     uint8_t* fwd[kNetLayers];
     uint8_t* bwd[kNetLayers];  // bwd[0] unused
     float* bias[kNetLayers];
+    uint8_t* band;             // the last (single-output) layer's banded image for its forward (unet.cu)
 };
 // Bytes of NetImages storage and the binding of its pointers inside one buffer.
 size_t net_images_bytes();
