@@ -324,19 +324,23 @@ struct SmokeSimulationContext_t {
         return S;
     }
 
+    // The ghost cells of the velocity's padded copies (the producing kernel wrote their interiors).
     cudaError_t pad_velocity(ConstFaces v, cudaStream_t s) {
         const int kinds[3] = {0, 1, 2};
         const float* fields[3] = {v.u, v.v, v.w};
         float* pads[3] = {pad.u, pad.v, pad.w};
-        return launch_pads(P, 3, kinds, fields, pads, s);
+        return launch_pads(P, 3, kinds, fields, pads, s, 1);
     }
 
     // Stages of one step, in the reference's order (backend-cuda.cu:2000-2057, views excluded).
     void enqueue_stages(cudaStream_t s, uint32_t last_stage, bool capturing) {
         const ConstFaces solid{solid_vx, solid_vy, solid_vz};
         check(launch_vorticity(P, as_const(A), occupancy, wx, wy, wz, wmag, s), "vorticity");
-        check(launch_cell_force(P, wx, wy, wz, wmag, density, temperature, force_x, force_y, force_z, occupancy, fx, fy, fz, s), "cell force");
-        check(launch_face_force(P, as_const(A), fx, fy, fz, occupancy, solid, B, s), "face force");
+        // the force kernel also forms the scalar stage's sourced temperature and density (neither changes before that
+        // stage) with their padded copies' interiors; the face kernels write the velocity's padded copies' interiors
+        const ScalarSources sources{temperature_source, density_source, solid_temperature, temperature_tmp, density_tmp, pad_t, pad_d};
+        check(launch_cell_force(P, wx, wy, wz, wmag, density, temperature, force_x, force_y, force_z, occupancy, fx, fy, fz, s, sources), "cell force");
+        check(launch_face_force(P, as_const(A), fx, fy, fz, occupancy, solid, B, s, pad), "face force");
         if (last_stage < SMOKE_B200_STAGE_ADVECT_VELOCITY) return;
         check(pad_velocity(as_const(B), s), "pad velocity");
         check(launch_advect_velocity(P, as_const(B), as_const(pad), occupancy, solid, C, s), "advect velocity");
@@ -346,15 +350,14 @@ struct SmokeSimulationContext_t {
         if (last_stage < SMOKE_B200_STAGE_PROJECT) return;
         const PcgSettings S = pcg_settings();
         const double* p64 = (!S.fixed && S.refinement > 0) ? pcg.x64 : nullptr;
-        check(launch_project(P, as_const(C), pressure, p64, occupancy, solid, A, s), "project");
+        check(launch_project(P, as_const(C), pressure, p64, occupancy, solid, A, s, pad), "project");
         if (last_stage < SMOKE_B200_STAGE_SCALARS) return;
-        check(launch_scalar_prep(P, temperature, temperature_source, density, density_source, occupancy, solid_temperature, temperature_tmp, density_tmp, s), "scalar sources");
         check(pad_velocity(as_const(A), s), "pad velocity");
         {
             const int kinds[2] = {4, 3};
             const float* fields[2] = {temperature_tmp, density_tmp};
             float* pads[2] = {pad_t, pad_d};
-            check(launch_pads(P, 2, kinds, fields, pads, s), "pad scalars");
+            check(launch_pads(P, 2, kinds, fields, pads, s, 1), "pad scalars");
         }
         check(launch_advect_scalars(P, as_const(A), as_const(pad), occupancy, temperature_tmp, pad_t, density_tmp, pad_d, solid_temperature, temperature, density, s), "advect scalars");
         check(launch_density_fill(fill_list, fill_count, density, fill_blocks, s), "density fill");

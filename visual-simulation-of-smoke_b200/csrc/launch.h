@@ -21,6 +21,18 @@ struct ConstFaces {
     const float* v;
     const float* w;
 };
+// The scalar stage's sourced fields, which the force kernel forms too when t_tmp is set: t_tmp = (solid ? solid
+// temperature : temperature) + dt * temperature source, d_tmp = density + dt * density source, and (t_pad set) the
+// interiors of their padded copies.
+struct ScalarSources {
+    const float* ts;
+    const float* ds;
+    const float* solid_t;
+    float* t_tmp;
+    float* d_tmp;
+    float* t_pad;
+    float* d_pad;
+};
 inline ConstFaces as_const(const Faces& f) { return {f.u, f.v, f.w}; }
 
 // One entry of the density fill list: a solid cell and the fluid cell it copies (-1: none, value 0).
@@ -48,22 +60,20 @@ constexpr int kPcgRegsCount = 2;
 // Forces: vorticity of the cell-centred velocity (writes the four vorticity buffers).
 cudaError_t launch_vorticity(const StepParams& P, ConstFaces vel, const uint8_t* occ, float* wx, float* wy, float* wz, float* wmag, cudaStream_t s);
 // Forces: f = user force + buoyancy + vorticity confinement per cell.
-cudaError_t launch_cell_force(const StepParams& P, const float* wx, const float* wy, const float* wz, const float* wmag, const float* density, const float* temperature, const float* ufx, const float* ufy, const float* ufz, const uint8_t* occ, float* fx, float* fy, float* fz, cudaStream_t s);
+cudaError_t launch_cell_force(const StepParams& P, const float* wx, const float* wy, const float* wz, const float* wmag, const float* density, const float* temperature, const float* ufx, const float* ufy, const float* ufz, const uint8_t* occ, float* fx, float* fy, float* fz, cudaStream_t s, const ScalarSources& S = ScalarSources{});
 // Forces: out = settled(in + dt * face-average of f) (domain, solid and periodic face rules applied).
-cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* fx, const float* fy, const float* fz, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
+cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* fx, const float* fy, const float* fz, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s, Faces pad = Faces{});
 // Padded copies (PadField): element count of the copy of field kind (0-2 face components, 3 density, 4
 // temperature).
 size_t pad_count(const StepParams& P, int kind);
 // Fills the padded copies of `count` (1..3) fields of the given kinds in one launch.
-cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const float* const* fields, float* const* pads, cudaStream_t s);
+cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const float* const* fields, float* const* pads, cudaStream_t s, int ghost_only = 0);
 // Velocity self-advection: out = settled(semi-Lagrangian sample of in along in); pad holds the padded copies of in.
 cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, ConstFaces pad, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
 // Pressure right-hand side from the advected velocity.
 cudaError_t launch_rhs(const StepParams& P, ConstFaces vel, const uint8_t* occ, const int32_t* anchor, float* rhs, cudaStream_t s);
 // Projection: out = settled(in - dt * grad p / h); pressure64 (optional) is the FP64 solution of a refined solve.
-cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const double* pressure64, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s);
-// Scalars: source terms (and solid temperature) into the temporaries.
-cudaError_t launch_scalar_prep(const StepParams& P, const float* temperature, const float* temperature_source, const float* density, const float* density_source, const uint8_t* occ, const float* solid_temperature, float* t_tmp, float* d_tmp, cudaStream_t s);
+cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const double* pressure64, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s, Faces pad = Faces{});
 // Scalars: one shared back-trace per cell, sample both scalars, solid rules (vel_pad, t_pad, d_pad: padded copies).
 cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, ConstFaces vel_pad, const uint8_t* occ, const float* t_tmp, const float* t_pad, const float* d_tmp, const float* d_pad, const float* solid_temperature, float* temperature, float* density, cudaStream_t s);
 // Scalars: solid cells copy their nearest fluid cell's density.

@@ -97,6 +97,13 @@ __device__ __forceinline__ float* pick(float* a, float* b, float* c) {
     return A == 0 ? a : (A == 1 ? b : c);
 }
 
+// Index of element (i, j, k) of a field of kind KIND (0-2 faces, 3-4 cells) in its padded copy (see PadField).
+template <int KIND>
+__device__ __forceinline__ uint32_t pad_index(const StepParams& P, int i, int j, int k) {
+    const uint32_t px = P.nx + (KIND == 0) + 2 * kPad, py = P.ny + (KIND == 1) + 2 * kPad;
+    return (static_cast<uint32_t>(k + kPad) * py + static_cast<uint32_t>(j + kPad)) * px + static_cast<uint32_t>(i + kPad);
+}
+
 // ------------------------------------------------------------------------------------------ forces
 __global__ void __launch_bounds__(kThreads) vorticity_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, float* __restrict__ wx, float* __restrict__ wy, float* __restrict__ wz, float* __restrict__ wm) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -121,9 +128,25 @@ __device__ __forceinline__ float flow_cell(const float* __restrict__ f, int x, i
 
 // f = user force; fluid cells add buoyancy (:910-918) and confinement eps*h*(N x w) (:920-948).
 __global__ void __launch_bounds__(kThreads) cell_force_kernel(const __grid_constant__ StepParams P, const float* __restrict__ wx, const float* __restrict__ wy, const float* __restrict__ wz, const float* __restrict__ wm, const float* __restrict__ density, const float* __restrict__ temperature, const float* __restrict__ ufx,
-                                                               const float* __restrict__ ufy, const float* __restrict__ ufz, const uint8_t* __restrict__ occ, float* __restrict__ fx, float* __restrict__ fy, float* __restrict__ fz) {
+                                                               const float* __restrict__ ufy, const float* __restrict__ ufz, const uint8_t* __restrict__ occ, float* __restrict__ fx, float* __restrict__ fy, float* __restrict__ fz,
+                                                               const __grid_constant__ ScalarSources S) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.n) return;
+    // The scalar stage's sourced fields and their padded copies: t_tmp = T' + dt * src_T, T' being T with solid cells at
+    // the solid temperature (the step-start apply_solid_temperature of :2001 folded in); d_tmp = rho + dt * src_rho
+    // (add_source, :852-857). T and rho do not change between this stage and the scalar advection.
+    if (S.t_tmp) {
+        const float tv = occ[q] != 0 ? S.solid_t[q] : temperature[q];
+        const float tt = tv + P.dt * S.ts[q], dd = density[q] + P.dt * S.ds[q];
+        S.t_tmp[q] = tt;
+        S.d_tmp[q] = dd;
+        if (S.t_pad) {
+            int x, y, z;
+            cell_xyz(P, q, x, y, z);
+            S.t_pad[pad_index<4>(P, x, y, z)] = tt;
+            S.d_pad[pad_index<3>(P, x, y, z)] = dd;
+        }
+    }
     float ax = ufx[q], ay = ufy[q], az = ufz[q];
     if (occ[q] == 0) {
         int x, y, z;
@@ -157,9 +180,14 @@ __global__ void __launch_bounds__(kThreads) cell_force_kernel(const __grid_const
 }
 
 template <int A>
-__device__ __forceinline__ void face_force_one(const StepParams& P, uint32_t q, const float* __restrict__ in, const float* __restrict__ f, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
+__device__ __forceinline__ void face_force_one(const StepParams& P, uint32_t q, const float* __restrict__ in, const float* __restrict__ f, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out, float* __restrict__ pad) {
     int i, j, k;
     face_ijk<A>(P, q, i, j, k);
+    // the settled value, also into the interior of the padded copy that the velocity advection reads
+    auto put = [&](float v) {
+        out[q] = v;
+        if (pad) pad[pad_index<A>(P, i, j, k)] = v;
+    };
     const int n = axis_n(P, A);
     const int s = A == 0 ? i : (A == 1 ? j : k);
     if (s > 0 && s < n) {
@@ -177,13 +205,13 @@ __device__ __forceinline__ void face_force_one(const StepParams& P, uint32_t q, 
                 value += solid[ri];
                 weight += 1.0f;
             }
-            out[q] = value / weight;
+            put(value / weight);
         } else {
-            out[q] = base + P.dt * (0.5f * (0.0f + fl + fr));
+            put(base + P.dt * (0.5f * (0.0f + fl + fr)));
         }
         return;
     }
-    out[q] = settle<A, false>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
+    put(settle<A, false>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
         const int s = A == 0 ? a : (A == 1 ? b : c);
         float sum = 0.0f, weight = 0.0f;
         int lc[3] = {a, b, c};
@@ -199,22 +227,22 @@ __device__ __forceinline__ void face_force_one(const StepParams& P, uint32_t q, 
         }
         const float base = in[fidx<A>(P, a, b, c)];
         return weight > 0.0f ? base + P.dt * (weight > 1.0f ? 0.5f * sum : sum) : base;  // exact halving
-    });
+    }));
 }
 
 // Block ranges: [0, bu) -> x faces, [bu, bu+bv) -> y faces, rest -> z faces.
 __global__ void __launch_bounds__(kThreads) face_force_kernel(const __grid_constant__ StepParams P, const float* __restrict__ iu, const float* __restrict__ iv, const float* __restrict__ iw, const float* __restrict__ fx, const float* __restrict__ fy, const float* __restrict__ fz, const uint8_t* __restrict__ occ, const float* __restrict__ su,
-                                                               const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou, float* __restrict__ ov, float* __restrict__ ow, unsigned bu, unsigned bv) {
+                                                               const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou, float* __restrict__ ov, float* __restrict__ ow, float* __restrict__ pu, float* __restrict__ pv, float* __restrict__ pw, unsigned bu, unsigned bv) {
     const unsigned b = blockIdx.x;
     if (b < bu) {
         const uint32_t q = b * kThreads + threadIdx.x;
-        if (q < P.nu) face_force_one<0>(P, q, iu, fx, occ, su, ou);
+        if (q < P.nu) face_force_one<0>(P, q, iu, fx, occ, su, ou, pu);
     } else if (b < bu + bv) {
         const uint32_t q = (b - bu) * kThreads + threadIdx.x;
-        if (q < P.nv) face_force_one<1>(P, q, iv, fy, occ, sv, ov);
+        if (q < P.nv) face_force_one<1>(P, q, iv, fy, occ, sv, ov, pv);
     } else {
         const uint32_t q = (b - bu - bv) * kThreads + threadIdx.x;
-        if (q < P.nw) face_force_one<2>(P, q, iw, fz, occ, sw, ow);
+        if (q < P.nw) face_force_one<2>(P, q, iw, fz, occ, sw, ow, pw);
     }
 }
 
@@ -320,6 +348,49 @@ __global__ void __launch_bounds__(256) pad_kernel(const __grid_constant__ StepPa
         if (kp0 + u < pz) out[(static_cast<uint32_t>(kp0 + u) * py + jp) * px + ip] = v[u];
 }
 
+// Ghost cells only, for padded copies whose interior the producing kernel wrote: thread g of field c (blockIdx.y)
+// takes ghost cell g of the shell, enumerated as the 2 kPad whole z-planes, then in each interior plane the 2 kPad
+// y-rows, then in each interior row the 2 kPad x-cells; its value is the boundary tap, as in pad_kernel.
+__global__ void __launch_bounds__(256) pad_ghost_kernel(const __grid_constant__ StepParams P, const __grid_constant__ PadJob J) {
+    const int c = blockIdx.y;
+    if (c >= J.count) return;
+    const int kind = c == 0 ? J.kind[0] : (c == 1 ? J.kind[1] : J.kind[2]);
+    const uint32_t fx = P.nx + (kind == 0), fy = P.ny + (kind == 1), fz = P.nz + (kind == 2);
+    const uint32_t px = fx + 2 * kPad, py = fy + 2 * kPad;
+    const uint32_t na = 2u * kPad * px * py, nb = fz * 2u * kPad * px, nc = fz * fy * 2u * kPad;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= na + nb + nc) return;
+    uint32_t ip, jp, kp;
+    if (g < na) {  // whole ghost z-planes
+        const uint32_t plane = g / (px * py), r = g - plane * px * py;
+        kp = plane < static_cast<uint32_t>(kPad) ? plane : fz + plane;
+        jp = r / px;
+        ip = r - jp * px;
+    } else if (g < na + nb) {  // ghost y-rows of the interior planes
+        const uint32_t h = g - na, per = 2u * kPad * px, plane = h / per, r = h - plane * per, row = r / px;
+        kp = kPad + plane;
+        jp = row < static_cast<uint32_t>(kPad) ? row : fy + row;
+        ip = r - row * px;
+    } else {  // ghost x-cells of the interior rows
+        const uint32_t h = g - na - nb, per = fy * 2u * kPad, plane = h / per, r = h - plane * per, row = r / (2u * kPad), xi = r - row * (2u * kPad);
+        kp = kPad + plane;
+        jp = kPad + row;
+        ip = xi < static_cast<uint32_t>(kPad) ? xi : fx + xi;
+    }
+    const int i = static_cast<int>(ip) - kPad, j = static_cast<int>(jp) - kPad, k = static_cast<int>(kp) - kPad;
+    const float* f = c == 0 ? J.f[0] : (c == 1 ? J.f[1] : J.f[2]);
+    float* out = c == 0 ? J.out[0] : (c == 1 ? J.out[1] : J.out[2]);
+    float v;
+    switch (kind) {
+    case 0: v = pad_value<0>(P, f, i, j, k); break;
+    case 1: v = pad_value<1>(P, f, i, j, k); break;
+    case 2: v = pad_value<2>(P, f, i, j, k); break;
+    case 3: v = pad_value<3>(P, f, i, j, k); break;
+    default: v = pad_value<4>(P, f, i, j, k); break;
+    }
+    out[(kp * py + jp) * px + ip] = v;
+}
+
 // ------------------------------------------------------------------------------------------ pressure rhs
 // b = -(h^2/dt) div u* + sum of OUTFLOW face pressures; 0 at solid cells and at the anchor (:1304-1328).
 __global__ void __launch_bounds__(kThreads) rhs_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const int32_t* __restrict__ anchor, float* __restrict__ rhs) {
@@ -347,9 +418,14 @@ __global__ void __launch_bounds__(kThreads) rhs_kernel(const __grid_constant__ S
 
 // ------------------------------------------------------------------------------------------ projection
 template <int A>
-__device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, const float* __restrict__ in, const float* __restrict__ p, const double* __restrict__ p64, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out) {
+__device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, const float* __restrict__ in, const float* __restrict__ p, const double* __restrict__ p64, const uint8_t* __restrict__ occ, const float* __restrict__ solid, float* __restrict__ out, float* __restrict__ pad) {
     int i, j, k;
     face_ijk<A>(P, q, i, j, k);
+    // the projected value, also into the interior of the padded copy that the scalar advection reads
+    auto put = [&](float v) {
+        out[q] = v;
+        if (pad) pad[pad_index<A>(P, i, j, k)] = v;
+    };
     const int s = A == 0 ? i : (A == 1 ? j : k);
     if (s > 0 && s < axis_n(P, A)) {
         // interior face: both cells exist unwrapped, so every load is issued before any rule is decided; the
@@ -370,13 +446,13 @@ __device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, con
                 value += solid[ri];
                 weight += 1.0f;
             }
-            out[q] = value / weight;
+            put(value / weight);
         } else {
-            out[q] = base - g;
+            put(base - g);
         }
         return;
     }
-    out[q] = settle<A, true>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
+    put(settle<A, true>(P, i, j, k, occ, solid, [&](int a, int b, int c) {
         int l[3] = {a, b, c};
         int r[3] = {a, b, c};
         l[A] -= 1;
@@ -391,36 +467,25 @@ __device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, con
         const float pr = p[cidx(P, r[0], r[1], r[2])];
         const float pl = p[cidx(P, l[0], l[1], l[2])];
         return base - P.dt * (pr - pl) / P.h;
-    });
+    }));
 }
 
 __global__ void __launch_bounds__(kThreads) project_kernel(const __grid_constant__ StepParams P, const float* __restrict__ iu, const float* __restrict__ iv, const float* __restrict__ iw, const float* __restrict__ p, const double* __restrict__ p64, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou,
-                                                            float* __restrict__ ov, float* __restrict__ ow, unsigned bu, unsigned bv) {
+                                                            float* __restrict__ ov, float* __restrict__ ow, float* __restrict__ pu, float* __restrict__ pv, float* __restrict__ pw, unsigned bu, unsigned bv) {
     const unsigned b = blockIdx.x;
     if (b < bu) {
         const uint32_t q = b * kThreads + threadIdx.x;
-        if (q < P.nu) project_one<0>(P, q, iu, p, p64, occ, su, ou);
+        if (q < P.nu) project_one<0>(P, q, iu, p, p64, occ, su, ou, pu);
     } else if (b < bu + bv) {
         const uint32_t q = (b - bu) * kThreads + threadIdx.x;
-        if (q < P.nv) project_one<1>(P, q, iv, p, p64, occ, sv, ov);
+        if (q < P.nv) project_one<1>(P, q, iv, p, p64, occ, sv, ov, pv);
     } else {
         const uint32_t q = (b - bu - bv) * kThreads + threadIdx.x;
-        if (q < P.nw) project_one<2>(P, q, iw, p, p64, occ, sw, ow);
+        if (q < P.nw) project_one<2>(P, q, iw, p, p64, occ, sw, ow, pw);
     }
 }
 
 // ------------------------------------------------------------------------------------------ scalars
-// t_tmp = T' + dt*src_T where T' is T with solid cells set to the solid temperature (the step-start
-// apply_solid_temperature of :2001 folded in); d_tmp = rho + dt*src_rho (add_source, :852-857).
-__global__ void __launch_bounds__(kThreads) scalar_prep_kernel(const __grid_constant__ StepParams P, const float* __restrict__ t, const float* __restrict__ ts, const float* __restrict__ d, const float* __restrict__ ds, const uint8_t* __restrict__ occ, const float* __restrict__ solid_t, float* __restrict__ t_tmp,
-                                                                float* __restrict__ d_tmp) {
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= P.n) return;
-    const float tv = occ[q] != 0 ? solid_t[q] : t[q];
-    t_tmp[q] = tv + P.dt * ts[q];
-    d_tmp[q] = d[q] + P.dt * ds[q];
-}
-
 // Fluid cells: one back-trace, then both scalars sampled with their own boundary rules (:1221-1233).
 // Solid cells: temperature = solid temperature (:1235-1241), density = 0 until the fill pass.
 template <bool CUBIC, bool TILED, bool POW2>
@@ -648,14 +713,14 @@ cudaError_t launch_vorticity(const StepParams& P, ConstFaces vel, const uint8_t*
     return cudaGetLastError();
 }
 
-cudaError_t launch_cell_force(const StepParams& P, const float* wx, const float* wy, const float* wz, const float* wmag, const float* density, const float* temperature, const float* ufx, const float* ufy, const float* ufz, const uint8_t* occ, float* fx, float* fy, float* fz, cudaStream_t s) {
-    cell_force_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, wx, wy, wz, wmag, density, temperature, ufx, ufy, ufz, occ, fx, fy, fz);
+cudaError_t launch_cell_force(const StepParams& P, const float* wx, const float* wy, const float* wz, const float* wmag, const float* density, const float* temperature, const float* ufx, const float* ufy, const float* ufz, const uint8_t* occ, float* fx, float* fy, float* fz, cudaStream_t s, const ScalarSources& S) {
+    cell_force_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, wx, wy, wz, wmag, density, temperature, ufx, ufy, ufz, occ, fx, fy, fz, S);
     return cudaGetLastError();
 }
 
-cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* fx, const float* fy, const float* fz, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
+cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* fx, const float* fy, const float* fz, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s, Faces pad) {
     const unsigned bu = blocks_for(P.nu), bv = blocks_for(P.nv), bw = blocks_for(P.nw);
-    face_force_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, fx, fy, fz, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
+    face_force_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, fx, fy, fz, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, pad.u, pad.v, pad.w, bu, bv);
     return cudaGetLastError();
 }
 
@@ -674,7 +739,7 @@ size_t pad_count(const StepParams& P, int kind) {
     return static_cast<size_t>(P.nx + (kind == 0) + 2 * kPad) * (P.ny + (kind == 1) + 2 * kPad) * (P.nz + (kind == 2) + 2 * kPad);
 }
 
-cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const float* const* fields, float* const* pads, cudaStream_t s) {
+cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const float* const* fields, float* const* pads, cudaStream_t s, int ghost_only) {
     if (count < 1 || count > 3) return cudaErrorInvalidValue;
     PadJob J{};
     J.count = count;
@@ -683,6 +748,12 @@ cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const 
         J.f[c] = fields[c];
         J.out[c] = pads[c];
         J.kind[c] = kinds[c];
+    }
+    if (ghost_only) {  // the largest shell of the fields (faces of the x, y or z axis have one more layer)
+        const uint32_t px = P.nx + 1 + 2 * kPad, py = P.ny + 1 + 2 * kPad, pz = P.nz + 1 + 2 * kPad;
+        const uint64_t most = static_cast<uint64_t>(px) * py * pz - static_cast<uint64_t>(P.nx) * P.ny * P.nz;
+        pad_ghost_kernel<<<dim3(static_cast<unsigned>((most + 255) / 256), count), 256, 0, s>>>(P, J);
+        return cudaGetLastError();
     }
     const dim3 grid((P.nx + 1 + 2 * kPad + 31) / 32, (P.ny + 1 + 2 * kPad + 7) / 8, J.pz_blocks * count);
     pad_kernel<<<grid, dim3(32, 8), 0, s>>>(P, J);
@@ -722,14 +793,9 @@ cudaError_t launch_rhs(const StepParams& P, ConstFaces vel, const uint8_t* occ, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const double* pressure64, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s) {
+cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const double* pressure64, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s, Faces pad) {
     const unsigned bu = blocks_for(P.nu), bv = blocks_for(P.nv), bw = blocks_for(P.nw);
-    project_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, pressure, pressure64, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_scalar_prep(const StepParams& P, const float* temperature, const float* temperature_source, const float* density, const float* density_source, const uint8_t* occ, const float* solid_temperature, float* t_tmp, float* d_tmp, cudaStream_t s) {
-    scalar_prep_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, temperature, temperature_source, density, density_source, occ, solid_temperature, t_tmp, d_tmp);
+    project_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, pressure, pressure64, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, pad.u, pad.v, pad.w, bu, bv);
     return cudaGetLastError();
 }
 
