@@ -177,11 +177,11 @@ def main():
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
-    ap.add_argument("--scenes64", type=int, default=96, help="64^3 scenes")
-    ap.add_argument("--scenes128", type=int, default=16, help="128^3 scenes")
+    ap.add_argument("--scenes64", type=int, default=256, help="64^3 scenes")
+    ap.add_argument("--scenes128", type=int, default=32, help="128^3 scenes")
     ap.add_argument("--per-scene", type=int, default=6, help="pressure systems per scene")
     ap.add_argument("--synthetic", type=int, default=12, help="random errors per scene")
-    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--steps", type=int, default=12000)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
