@@ -10,6 +10,8 @@ FP32 forms run on the same states and are reported beside it. `--impl reference`
 library (compiled from its sources into oracle/_ref) on the same scene through the same ABI, with the fixed CG
 iteration count that reaches its FP32 residual floor on this scene. Several GPUs run independent replicas (the
 step does not shard); timing is the max over ranks. `--profile` runs a profiling workload instead (no JSON line).
+The line's "other_configs" holds short runs of the other configurations (64^3 plain method, 256x384x256 scene, 48-
+scene batch) taken after the headline; `--no-other-configs` skips them.
 """
 from __future__ import annotations
 
@@ -790,6 +792,28 @@ def bench_batched(args, rank, world, local):
                  learned=learned if learned is not None else {"unavailable": "no trained weights in the package"})
 
 
+def other_configs(args, rank, world, local):
+    """Short runs of the other benchmark configurations after the headline (5 timed steps after 3 warm-up steps
+    each; the full runs are `--workload plume64 | large | batched`): the 64^3 plain method (C1), the 256x384x256 scene
+    with a sphere (C3) and the 48-scene batch (C5), each line as its own workload prints it. Every rank runs them."""
+    import copy
+
+    import torch
+
+    sub = copy.copy(args)
+    sub.steps, sub.warmup = min(args.steps, 5), 3
+    out = {}
+    for name, fn in (("C1_plume64_plain", bench_plume64), ("C3_large_256x384x256", bench_large), ("C5_batched_48", bench_batched)):
+        t0 = time.perf_counter()
+        res = fn(sub, rank, world, local)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        if res is not None:
+            res["wall_s"] = round(time.perf_counter() - t0, 1)
+            out[name] = res
+    return out
+
+
 def bench_reference(args, rank, world, local):
     import torch
 
@@ -929,6 +953,8 @@ def main():
                     help="plume128: the headline (default); plume64, large, batched: the other benchmark configurations")
     ap.add_argument("--profile-count", type=int, default=1)
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="keep the default launch shapes (skip the autotuner)")
+    ap.add_argument("--no-other-configs", dest="other_configs", action="store_false",
+                    help="plume128 only: skip the short runs of the other configurations (64^3 plain, 256x384x256, 48-scene batch) that the line carries")
     ap.add_argument("--shapes", default="", help="--profile only: launch shapes 'advect_tile,mg_wave,pcg_grid' (default: the defaults)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -943,6 +969,10 @@ def main():
         line = bench_reference(args, rank, world, local)
     else:
         line = {"plume128": bench_b200, "plume64": bench_plume64, "large": bench_large, "batched": bench_batched}[args.workload](args, rank, world, local)
+        if args.workload == "plume128" and args.other_configs:
+            others = other_configs(args, rank, world, local)
+            if line is not None:
+                line["other_configs"] = others
     barrier(world) if args.impl == "b200" else None
     if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
