@@ -70,14 +70,15 @@ def solver_launches(n, iterations, refinement, learned=False, net_iterations=0):
     accumulation and the FP64 residual, and per iteration the loop body (restriction and the fused prolongation +
     smoothing of every grid level below 0, the block-level cycle, level-0 prolongation, smoothing, p/q and update).
     The learned form adds per pass the gate of its second loop, and per iteration with the network (the first
-    `net_iterations`, 0: all) the residual after the V-cycle, the network and the correction."""
+    `net_iterations`, 0: all) the residual after the V-cycle and its restriction, the network on level 1, the
+    prolongation of its output and the correction."""
     _, g = mg_grid_levels(n)
     # coarse grid levels of at most 64^3 cells fuse prolongation and smoothing (mg_up_kernel)
     per_iteration = sum(2 if -(-n // (1 << l)) ** 3 <= 64 ** 3 else 3 for l in range(1, g)) + 5
     total = 2 + 3 * (refinement + 1) + per_iteration * iterations
     if learned:
         with_net = iterations if net_iterations == 0 else min(net_iterations, iterations)
-        total += (refinement + 1) + (3 + NET_FORWARD_KERNELS) * with_net
+        total += (refinement + 1) + (4 + NET_FORWARD_KERNELS) * with_net
     return total
 
 
@@ -558,35 +559,46 @@ def learned_net(lib):
 
 def bench_learned(sim, net, n, learned, results):
     """The learned form's figures beside the plain FP32 form (the metric's comparison), and the network evaluation
-    alone on the step's right-hand side: ms per apply and its tensor FLOP rate against the measured BF16 peak."""
+    alone: ms per apply on the multigrid level 1 of the step's right-hand side (the volume the solve runs it on), and
+    on the full n^3 grid with its tensor FLOP rate against the measured BF16 peak."""
     import torch
+
+    import train_preconditioner
 
     with torch.cuda.stream(sim.stream):
         rhs = sim.view(abi.VIEW_FLOW_PRESSURE_RHS).clone()
         occ = torch.zeros(rhs.shape, dtype=torch.uint8, device="cuda")
+        rhs1 = train_preconditioner._children(rhs).sum(-1).contiguous()  # the solve's restriction onto level 1
+        occ1 = torch.zeros(rhs1.shape, dtype=torch.uint8, device="cuda")
     sim.stream.synchronize()
-    net.apply(rhs, occ)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = 20
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(reps):
-        net.apply(rhs, occ)
-    e1.record()
-    torch.cuda.synchronize()
-    apply_ms = e0.elapsed_time(e1) / reps
+
+    def time_apply(x, o, reps=20):
+        net.apply(x, o)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            net.apply(x, o)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    apply1_ms, apply_ms = time_apply(rhs1, occ1), time_apply(rhs, occ)
+    n1 = (n + 1) // 2
     flops, executed = net_flops(n, n, n), net_flops(n, n, n, executed=True)
     tflops, tflops_exec = flops / (apply_ms * 1e-3) / 1e12, executed / (apply_ms * 1e-3) / 1e12
     bf16_peak = peak_tflops()
     ms, its, res, flags = learned
     plain = results["plain_fp32"][0]
-    return {"form": "FCG, z = V(r) + N(r - A V(r)): multigrid V(1,1) cycle corrected by the tcgen05 BF16 U-Net (4 levels, 16/32/64/128 channels, 582257 parameters), FP32 stencils, FP64 dots + refinement, warm start, to 1e-5",
+    return {"form": "FCG, z = V(r) + P N(R(r - A V(r))): multigrid V(1,1) cycle corrected by the tcgen05 BF16 U-Net (4 levels, 16/32/64/128 channels, 582257 parameters) run on the multigrid level 1 "
+                    f"({n1}^3; R: child sums, P: the V-cycle's trilinear prolongation), FP32 stencils, FP64 dots + refinement, warm start, to 1e-5",
             "ms_per_step": round(ms, 4), "pcg_iterations": round(its, 1), "true_rel_residual_max": res, "network_dropped": bool(flags & 1),
             "speedup_vs_plain_fp32": round(plain / ms, 2), "target": "learned+mixed >= 3x faster per step than plain FP32 PCG", "target_met": bool(plain / ms >= 3.0),
             "vs_multigrid_alone": round(results["multigrid_fp64"][0] / ms, 3),
-            "net_apply_ms": round(apply_ms, 4), "net_dense_gflop_per_apply": round(flops / 1e9, 2), "net_executed_gflop_per_apply": round(executed / 1e9, 2),
+            "net_apply_ms": round(apply1_ms, 4), "net_apply_grid": [n1, n1, n1], "net_dense_gflop_per_apply": round(net_flops(n1, n1, n1) / 1e9, 2),
+            "net_apply_full_grid_ms": round(apply_ms, 4), "net_full_grid_dense_gflop": round(flops / 1e9, 2), "net_full_grid_executed_gflop": round(executed / 1e9, 2),
             "tensor_roofline": {"bound": "tensor", "achieved": round(tflops, 2), "achieved_executed": round(tflops_exec, 2), "peak": bf16_peak, "unit": "TFLOP/s", "frac": round(tflops / bf16_peak, 5),
-                                "note": "one network evaluation (input packing, 8 convolutions, 3 pools, 3 up-adds) on the 128^3 right-hand side; dense FLOPs of the real channels, and the FLOPs the tensor cores execute with the padded channels"}}
+                                "note": f"one network evaluation (input packing, 8 convolutions, 3 pools, 3 up-adds) on the full {n}^3 right-hand side; dense FLOPs of the real channels, and the FLOPs the tensor cores execute with the padded channels"}}
 
 
 def tune_summary(rep):

@@ -224,6 +224,7 @@ struct SmokeSimulationContext_t {
         check(launch_stencil_codes(P, occupancy, anchor, codes, stream), "operator codes");
         check(launch_fill_build(P, occupancy, anchor, fill_list, fill_count, stream), "density fill list");
         check(launch_mg_setup(P, mg, occupancy, stream), "multigrid levels");
+        if (has_net) check(launch_mg_net_mask(mg, learned.occupancy, stream), "preconditioner network mask");
     }
 
     // The pressure solve of the selected mode on the context's right-hand side. The multigrid solve is a graph:
@@ -277,11 +278,13 @@ struct SmokeSimulationContext_t {
 
     bool uses_mg() const { return solver.mode == SMOKE_B200_SOLVER_MG_FCG || solver.mode == SMOKE_B200_SOLVER_LEARNED_FCG; }
 
-    // The context's copy of a network: its packed images and an activation workspace on this grid.
+    // The context's copy of a network: its packed images, an activation workspace on the multigrid level 1 (where the
+    // network runs), that level's solid mask and a level-0 array for the prolonged correction.
     void set_net(const SmokeB200Net_t* net) {
-        const VolumeDims d = volume_dims(P.nx, P.ny, P.nz);
-        const size_t ib = (net_images_bytes() + 255) & ~size_t(255);
-        const size_t need = ib + net_acts_bytes(d);
+        const VolumeDims d = volume_dims(mg.L[1].nx, mg.L[1].ny, mg.L[1].nz);
+        auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
+        const size_t ib = align(net_images_bytes()), ab = align(net_acts_bytes(d)), fb = align(static_cast<size_t>(P.n) * sizeof(float));
+        const size_t need = ib + ab + fb + align(d.n);
         check(cudaStreamSynchronize(stream), "preconditioner network: idle");
         if (need > learned_bytes) {
             if (learned_mem) check(cudaFree(learned_mem), "preconditioner network");
@@ -292,9 +295,12 @@ struct SmokeSimulationContext_t {
         }
         check(cudaMemcpy(learned_mem, smoke_b200_net_images_block(net), net_images_bytes(), cudaMemcpyDeviceToDevice), "preconditioner network");
         net_images_bind(learned.images, learned_mem);
-        net_acts_bind(learned.acts, static_cast<char*>(learned_mem) + ib, d);
-        learned.occupancy = occupancy;
+        char* base = static_cast<char*>(learned_mem);
+        net_acts_bind(learned.acts, base + ib, d);
+        learned.fine = reinterpret_cast<float*>(base + ib + ab);
+        learned.occupancy = reinterpret_cast<uint8_t*>(base + ib + ab + fb);
         check(cudaMemset(learned.acts.error, 0, sizeof(unsigned)), "preconditioner network");
+        check(launch_mg_net_mask(mg, learned.occupancy, stream), "preconditioner network mask");
         has_net = true;
     }
 

@@ -245,6 +245,8 @@ cudaError_t launch_mg_vcycle(const MgHierarchy& H, int wave_depth, const float* 
 cudaError_t launch_mg_apply(const MgHierarchy& H, const float* x, float* out, cudaStream_t s);
 // Builds level fluid masks and codes from the occupancy (after the fine codes and anchor exist).
 cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uint8_t* occ, cudaStream_t s);
+// The learned preconditioner network's solid mask on level 1 (1 where a cell has no fluid child), after the setup.
+cudaError_t launch_mg_net_mask(const MgHierarchy& H, uint8_t* solid, cudaStream_t s);
 // Records the multigrid-preconditioned FCG solve of A x = b into the graph being captured on `s` (kernels, and
 // one `while` node per pass whose body is captured on `body_stream`); the outcome lands in *status_out.
 cudaError_t enqueue_mg_solve(const MgSolveArgs& args, bool fp64, PcgStatusDevice* status_out, cudaStream_t s, cudaStream_t body_stream);

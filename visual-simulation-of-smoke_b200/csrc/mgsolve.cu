@@ -28,7 +28,8 @@
 // solve's pass has two `while` nodes: the first body runs the network, and its update ends that loop when the next
 // iteration goes without it (past the schedule's iterations, or after a fallback); the second body is the V-cycle
 // alone, entered when the first loop ended without stopping. So iterations without the network launch none of the
-// network's kernels.
+// network's kernels. The network runs on level 1: its input is the restriction of what the V-cycle leaves, and its
+// output comes back through the V-cycle's prolongation.
 // Dot products: block sums in a fixed order, stored per block in FP64 and added in block order by the last block to
 // finish, so the solve is deterministic.
 // Each restriction block covers whole 2x2x2 parents and writes the coarse right-hand side directly.
@@ -284,19 +285,25 @@ __device__ bool last_block_totals(unsigned int* counter, const MgWork& W, int ka
 
 
 // The 2x2x2 child sums of a tile's cells written into the coarse level's right-hand side (whole block calls it).
-__device__ __forceinline__ void restrict_tile(float c, const MgLevel& C, const Cell& cell) {
+// Returns the sum in the thread that wrote it, 0 in the others.
+__device__ __forceinline__ float restrict_tile(float c, const MgLevel& C, const Cell& cell) {
     __shared__ float sm[TZ][TY][TX];
     sm[threadIdx.z][threadIdx.y][threadIdx.x] = c;
     __syncthreads();
+    float written = 0.0f;
     const int t = tid();
     if (t < (TX / 2) * (TY / 2)) {
         const int cx = t % (TX / 2), cy = t / (TX / 2);
         const float s = (sm[0][2 * cy][2 * cx] + sm[0][2 * cy][2 * cx + 1]) + (sm[0][2 * cy + 1][2 * cx] + sm[0][2 * cy + 1][2 * cx + 1]) +
                         (sm[1][2 * cy][2 * cx] + sm[1][2 * cy][2 * cx + 1]) + (sm[1][2 * cy + 1][2 * cx] + sm[1][2 * cy + 1][2 * cx + 1]);
         const int X = cell.bx * (TX / 2) + cx, Y = cell.by * (TY / 2) + cy, Z = cell.bz;
-        if (X < C.nx && Y < C.ny && Z < C.nz) C.r[lidx(C, X, Y, Z)] = s;
+        if (X < C.nx && Y < C.ny && Z < C.nz) {
+            C.r[lidx(C, X, Y, Z)] = s;
+            written = s;
+        }
     }
     __syncthreads();
+    return written;
 }
 
 // ---------------------------------------------------------------------------------------------- level-0 z-march
@@ -650,51 +657,84 @@ __global__ void __launch_bounds__(kThreads) mg_restrict_kernel(const __grid_cons
     });
 }
 
-// Level l: zp += P(t_{l+1}) on active cells (in place). One thread per coarse cell (X, Y, Z) of level l + 1: it
-// loads the 3 x 3 x 3 coarse neighbourhood once and writes its up to 8 children, each a trilinear blend of the
-// parent and the 7 corners toward the child (see prolong_corners).
+// The trilinear prolongation from level C into level F = C - 1 at coarse cell c (in range): it loads the 3 x 3 x 3
+// coarse neighbourhood once (load(index): the level-C value, kTag on an inactive cell) and hands each of its up to 8
+// children to store(fine index, blend of the parent and the 7 corners toward the child; see prolong_corners).
+template <class Load, class Store>
+__device__ __forceinline__ void prolong_children(const MgLevel& F, const MgLevel& C, const int* fper, const int* fout, const Cell& c, Load&& load, Store&& store) {
+    // per axis: index of the neighbour on each side (wrapped on a periodic axis, the cell itself at a wall)
+    auto side = [](int v, int n, int per, int d) {
+        int s = v + d;
+        if (s < 0) s = per ? s + n : v;
+        else if (s >= n) s = per ? s - n : v;
+        return s;
+    };
+    const int xs[3] = {side(c.x, C.nx, fper[0], -1), c.x, side(c.x, C.nx, fper[0], 1)};
+    const int ys[3] = {side(c.y, C.ny, fper[1], -1), c.y, side(c.y, C.ny, fper[1], 1)};
+    const int zs[3] = {side(c.z, C.nz, fper[2], -1), c.z, side(c.z, C.nz, fper[2], 1)};
+    float t[3][3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const uint32_t row = (static_cast<uint32_t>(zs[k]) * C.ny + ys[j]) * C.nx;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) t[k][j][i] = load(row + xs[i]);
+        }
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) {
+                const int x = 2 * c.x + dx, y = 2 * c.y + dy, z = 2 * c.z + dz;
+                if (x >= F.nx || y >= F.ny || z >= F.nz) continue;
+                const int ix = dx ? 2 : 0, iy = dy ? 2 : 0, iz = dz ? 2 : 0;  // the corner side of each axis
+                const bool wx = xs[ix] == c.x, wy = ys[iy] == c.y, wz = zs[iz] == c.z;
+                const float p = prolong_corners(wx, wy, wz, wx && fout[dx], wy && fout[2 + dy], wz && fout[4 + dz], [&](int m) {
+                    return t[(m & 4) ? iz : 1][(m & 2) ? iy : 1][(m & 1) ? ix : 1];
+                });
+                store(lidx(F, x, y, z), p);
+            }
+}
+
+// Level l: zp += P(t_{l+1}) on active cells (in place). One thread per coarse cell (X, Y, Z) of level l + 1, which
+// writes its up to 8 children (prolong_children).
 __global__ void __launch_bounds__(kThreads) mg_prolong_kernel(const __grid_constant__ MgHierarchy H, int l) {
     pdl_begin();
     const MgLevel& F = H.L[l];
     const MgLevel& C = H.L[l + 1];
     for_tiles(C, [&](const Cell& c) {
         if (!c.in) return;
-        // per axis: index of the neighbour on each side (wrapped on a periodic axis, the cell itself at a wall)
-        auto side = [](int v, int n, int per, int d) {
-            int s = v + d;
-            if (s < 0) s = per ? s + n : v;
-            else if (s >= n) s = per ? s - n : v;
-            return s;
-        };
-        const int xs[3] = {side(c.x, C.nx, H.fper[0], -1), c.x, side(c.x, C.nx, H.fper[0], 1)};
-        const int ys[3] = {side(c.y, C.ny, H.fper[1], -1), c.y, side(c.y, C.ny, H.fper[1], 1)};
-        const int zs[3] = {side(c.z, C.nz, H.fper[2], -1), c.z, side(c.z, C.nz, H.fper[2], 1)};
-        float t[3][3][3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const uint32_t row = (static_cast<uint32_t>(zs[k]) * C.ny + ys[j]) * C.nx;
-#pragma unroll
-                for (int i = 0; i < 3; ++i) t[k][j][i] = C.t[row + xs[i]];
-            }
-#pragma unroll
-        for (int dz = 0; dz < 2; ++dz)
-#pragma unroll
-            for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-                for (int dx = 0; dx < 2; ++dx) {
-                    const int x = 2 * c.x + dx, y = 2 * c.y + dy, z = 2 * c.z + dz;
-                    if (x >= F.nx || y >= F.ny || z >= F.nz) continue;
-                    const int ix = dx ? 2 : 0, iy = dy ? 2 : 0, iz = dz ? 2 : 0;  // the corner side of each axis
-                    const bool wx = xs[ix] == c.x, wy = ys[iy] == c.y, wz = zs[iz] == c.z;
-                    const float p = prolong_corners(wx, wy, wz, wx && H.fout[dx], wy && H.fout[2 + dy], wz && H.fout[4 + dz], [&](int m) {
-                        return t[(m & 4) ? iz : 1][(m & 2) ? iy : 1][(m & 1) ? ix : 1];
-                    });
-                    const uint32_t fq = lidx(F, x, y, z);
-                    if (active(F.code[fq])) F.zp[fq] += p;
-                }
+        prolong_children(F, C, H.fper, H.fout, c, [&](uint32_t i) { return C.t[i]; }, [&](uint32_t fq, float p) {
+            if (active(F.code[fq])) F.zp[fq] += p;
+        });
     });
+}
+
+// The learned preconditioner's correction on level 0: out = P(y / s) on active cells, 0 elsewhere, for the network's
+// output y on level 1 (s = sqrt(n_1 / norm2), the input scale of net_input_kernel; inactive level-1 cells take the
+// parent's value, as in the V-cycle's prolongation). Nothing to do once the solve dropped the network (st->net_off).
+__global__ void __launch_bounds__(kThreads) mg_net_prolong_kernel(const __grid_constant__ MgHierarchy H, const MgState* __restrict__ st, const float* __restrict__ y, const double* __restrict__ norm2, float* __restrict__ out) {
+    pdl_begin();
+    if (st != nullptr && st->net_off) return;  // uniform over the grid
+    const MgLevel& F = H.L[0];
+    const MgLevel& C = H.L[1];
+    const double nn = *norm2;
+    const float inv_s = nn > 0.0 ? static_cast<float>(sqrt(nn / static_cast<double>(C.n))) : 0.0f;
+    for_tiles(C, [&](const Cell& c) {
+        if (!c.in) return;
+        prolong_children(F, C, H.fper, H.fout, c, [&](uint32_t i) { return active(C.code[i]) ? y[i] * inv_s : __uint_as_float(kTag); },
+                         [&](uint32_t fq, float p) { out[fq] = active(F.code[fq]) ? p : 0.0f; });
+    });
+}
+
+// The network's input for an initial guess: the 2 x 2 x 2 child sums of b on level 1's zp.
+__global__ void __launch_bounds__(kThreads) mg_net_restrict_kernel(const __grid_constant__ MgHierarchy H, const float* __restrict__ b) {
+    const MgLevel& F = H.L[0];
+    MgLevel C = H.L[1];
+    C.r = C.zp;
+    for_tiles(F, [&](const Cell& c) { restrict_tile(c.in ? b[c.q] : 0.0f, C, c); });
 }
 
 // Level l >= 1 post-smoothing: t = zp + w D^-1 (r - A zp) on active cells, kTag on inactive cells.
@@ -820,28 +860,34 @@ __global__ void __launch_bounds__(kThreads) mg_up_kernel(const __grid_constant__
 }
 
 // Learned preconditioner, part 1: the residual the V-cycle leaves, r_V = r - A z_V on active cells (z_V = t of level
-// 0, just smoothed), into level 0's zp (free after the smoothing), and ||r_V||^2 into st->net_rr: the network's input
-// and its scale. Nothing to do once the solve fell back to the V-cycle alone.
+// 0, just smoothed), into level 0's zp (free after the smoothing), and its 2 x 2 x 2 child sums R r_V on level 1's zp
+// (free between V-cycles) with ||R r_V||^2 into st->net_rr: the network runs on level 1, and these are its input and
+// its scale. Nothing to do once the solve fell back to the V-cycle alone.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) mg_net_residual_kernel(const __grid_constant__ MgSolveArgs A) {
     pdl_begin();
     const MgLevel& F = A.H.L[0];
+    MgLevel C = A.H.L[1];
+    C.r = C.zp;
     MgState* st = A.st;
     if (st->net_off) return;  // uniform over the grid
     const float* r = A.W.r[st->parity];
     T rr = 0;
     for_tiles(F, [&](const Cell& c) {
-        if (!c.in) return;
-        uint32_t nb[6];
-        nbr_all(F, A.H.fper, c, nb);
-        const uint16_t code = F.code[c.q];
-        const float rv = r[c.q], z0 = F.t[c.q];
-        float zn[6];
+        float rv_net = 0.0f;
+        if (c.in) {
+            uint32_t nb[6];
+            nbr_all(F, A.H.fper, c, nb);
+            const uint16_t code = F.code[c.q];
+            const float rv = r[c.q], z0 = F.t[c.q];
+            float zn[6];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) zn[k] = F.t[nb[k]];
-        const float rv_net = active(code) ? rv - masked_stencil(code, z0, zn) : 0.0f;
-        F.zp[c.q] = rv_net;
-        rr += static_cast<T>(rv_net) * static_cast<T>(rv_net);
+            for (int k = 0; k < 6; ++k) zn[k] = F.t[nb[k]];
+            rv_net = active(code) ? rv - masked_stencil(code, z0, zn) : 0.0f;
+            F.zp[c.q] = rv_net;
+        }
+        const float sum = restrict_tile(rv_net, C, c);
+        rr += static_cast<T>(sum) * static_cast<T>(sum);
     });
     block_accumulate<T>(A.W, kAccNet, rr, -1, T(0));
     double tnet, unused;
@@ -849,17 +895,16 @@ __global__ void __launch_bounds__(kThreads) mg_net_residual_kernel(const __grid_
     st->net_rr = tnet;
 }
 
-// Learned preconditioner, part 2: the step along the network's correction N = y / s that minimises the energy norm of
-// what z_V + gamma N leaves of the error e - z_V (whose residual is r_V): gamma = (N, r_V) / (N, A N), 0 when that is
-// not defined. So a network that helps little is scaled down instead of being added at full weight.
+// Learned preconditioner, part 2: the step along the network's correction N = P(y / s) (on level 0, from
+// mg_net_prolong_kernel) that minimises the energy norm of what z_V + gamma N leaves of the error e - z_V (whose
+// residual is r_V): gamma = (N, r_V) / (N, A N), 0 when that is not defined. So a network that helps little is scaled
+// down instead of being added at full weight.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) mg_net_gamma_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
+__global__ void __launch_bounds__(kThreads) mg_net_gamma_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ N) {
     pdl_begin();
     const MgLevel& F = A.H.L[0];
     MgState* st = A.st;
     if (st->net_off) return;  // uniform over the grid
-    const double rn2 = st->net_rr;
-    const float inv_s = rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n))) : 0.0f;
     T nr = 0, nan_ = 0;
     for_tiles(F, [&](const Cell& c) {
         if (!c.in) return;
@@ -867,10 +912,10 @@ __global__ void __launch_bounds__(kThreads) mg_net_gamma_kernel(const __grid_con
         if (!active(code)) return;
         uint32_t nb[6];
         nbr_all(F, A.H.fper, c, nb);
-        const float n0 = y[c.q] * inv_s;
+        const float n0 = N[c.q];
         float nn[6];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) nn[k] = y[nb[k]] * inv_s;
+        for (int k = 0; k < 6; ++k) nn[k] = N[nb[k]];
         nr += static_cast<T>(n0) * static_cast<T>(F.zp[c.q]);
         nan_ += static_cast<T>(n0) * static_cast<T>(masked_stencil(code, n0, nn));
     });
@@ -880,20 +925,19 @@ __global__ void __launch_bounds__(kThreads) mg_net_gamma_kernel(const __grid_con
     st->net_gamma = (b > 0.0 && isfinite(a) && isfinite(b)) ? a / b : 0.0;
 }
 
-// Learned preconditioner, part 3: the network's correction N = y / s (y its output, s = sqrt(n / ||r_V||^2) its input
-// scale), scaled by gamma, added to the V-cycle's z_V and post-smoothed by one damped Jacobi step on what it leaves of
-// r_V: z = z_V + gamma N + w D^-1 (r_V - gamma A N) on active cells (z = z_V in iterations without the network). The network supplies the smooth part of
-// the correction; the Jacobi step removes the rough part of its error (BF16 output and fitting noise), which the
-// energy norm the FCG minimises would amplify. Then (z, r) and (z, q), and the last block computes beta (0 on a
-// pass's first iteration), as level 0's smoothing does for the V-cycle alone.
+// Learned preconditioner, part 3: the network's correction N (level 0), scaled by gamma, added to the V-cycle's z_V
+// and post-smoothed by one damped Jacobi step on what it leaves of r_V: z = z_V + gamma N + w D^-1 (r_V - gamma A N)
+// on active cells (z = z_V in iterations without the network). The network supplies the smooth part of the
+// correction; the Jacobi step removes the rough part of its error (BF16 output, fitting noise and the prolongation),
+// which the energy norm the FCG minimises would amplify. Then (z, r) and (z, q), and the last block computes beta (0
+// on a pass's first iteration), as level 0's smoothing does for the V-cycle alone.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) mg_net_add_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ y) {
+__global__ void __launch_bounds__(kThreads) mg_net_add_kernel(const __grid_constant__ MgSolveArgs A, const float* __restrict__ N) {
     pdl_begin();
     const MgLevel& F = A.H.L[0];
     MgState* st = A.st;
     const bool use_net = st->net_off == 0;
-    const double rn2 = st->net_rr;
-    const float inv_s = use_net && rn2 > 0.0 ? static_cast<float>(sqrt(rn2 / static_cast<double>(F.n)) * st->net_gamma) : 0.0f;
+    const float g = use_net ? static_cast<float>(st->net_gamma) : 0.0f;
     const float* r = A.W.r[st->parity];
     T zr = 0, zq = 0;
     for_tiles(F, [&](const Cell& c) {
@@ -904,10 +948,10 @@ __global__ void __launch_bounds__(kThreads) mg_net_add_kernel(const __grid_const
         if (use_net) {
             uint32_t nb[6];
             nbr_all(F, A.H.fper, c, nb);
-            const float n0 = y[c.q] * inv_s;
+            const float n0 = N[c.q] * g;
             float nn[6];
 #pragma unroll
-            for (int k = 0; k < 6; ++k) nn[k] = y[nb[k]] * inv_s;
+            for (int k = 0; k < 6; ++k) nn[k] = N[nb[k]] * g;
             z += n0 + wdiag(code) * (F.zp[c.q] - masked_stencil(code, n0, nn));
         }
         F.t[c.q] = z;
@@ -1467,9 +1511,10 @@ void launch_body(const MgSolveArgs& A, int net, cudaGraphConditionalHandle h, in
         const LearnedSolve& N = *A.net;
         pdl_launch(mg_smooth0_kernel<T, false>, march_grid(mg_smooth0_kernel<T, false>, L0, A.wave), kThreads, 0, bs, A);
         pdl_launch(mg_net_residual_kernel<T>, wave(mg_net_residual_kernel<T>, L0, A.wave), kBlock, 0, bs, A);
-        if (net_forward(N.images, N.acts, L0.zp, nullptr, nullptr, &A.st->net_rr, N.occupancy, bs, &A.st->net_off) != cudaSuccess) return;
-        pdl_launch(mg_net_gamma_kernel<T>, wave(mg_net_gamma_kernel<T>, L0, A.wave), kBlock, 0, bs, A, N.acts.y);
-        pdl_launch(mg_net_add_kernel<T>, wave(mg_net_add_kernel<T>, L0, A.wave), kBlock, 0, bs, A, N.acts.y);
+        if (net_forward(N.images, N.acts, A.H.L[1].zp, nullptr, nullptr, &A.st->net_rr, N.occupancy, bs, &A.st->net_off) != cudaSuccess) return;
+        pdl_launch(mg_net_prolong_kernel, wave(mg_net_prolong_kernel, A.H.L[1], A.wave), kBlock, 0, bs, A.H, A.st, N.acts.y, &A.st->net_rr, N.fine);
+        pdl_launch(mg_net_gamma_kernel<T>, wave(mg_net_gamma_kernel<T>, L0, A.wave), kBlock, 0, bs, A, N.fine);
+        pdl_launch(mg_net_add_kernel<T>, wave(mg_net_add_kernel<T>, L0, A.wave), kBlock, 0, bs, A, N.fine);
         pdl_launch(mg_pq_kernel<T>, march_grid(mg_pq_kernel<T>, L0, A.wave), kThreads, 0, bs, A);
         pdl_launch(mg_update_kernel<T, true>, march_grid(mg_update_kernel<T, true>, L0, A.wave), kThreads, 0, bs, A, 0, h, in_graph, 1);
         return;
@@ -1479,15 +1524,16 @@ void launch_body(const MgSolveArgs& A, int net, cudaGraphConditionalHandle h, in
     launch_update<T>(A, 0, h, in_graph, 0, bs);
 }
 
-// Learned solve with the network's warm start: x64 = N(b) (through the q array, which the set-up clears), so the
-// set-up's warm path starts from r = b - A x64.
+// Learned solve with the network's warm start: x64 = P(N(R b)) (the network on level 1, its output prolonged to level
+// 0), so the set-up's warm path starts from r = b - A x64.
 cudaError_t learned_guess(const MgSolveArgs& A, cudaStream_t s) {
     if (!A.learned || !A.net_warm) return cudaSuccess;
     const LearnedSolve& N = *A.net;
-    cudaError_t e = net_forward(N.images, N.acts, A.b, nullptr, nullptr, nullptr, N.occupancy, s);
-    if (e == cudaSuccess) e = net_output(N.acts, nullptr, N.occupancy, A.W.q, s);
+    mg_net_restrict_kernel<<<wave(mg_net_restrict_kernel, A.H.L[0], A.wave), kBlock, 0, s>>>(A.H, A.b);
+    cudaError_t e = net_forward(N.images, N.acts, A.H.L[1].zp, nullptr, nullptr, nullptr, N.occupancy, s);
     if (e != cudaSuccess) return e;
-    mg_net_guess_kernel<<<wave(mg_net_guess_kernel, A.H.L[0], A.wave), kBlock, 0, s>>>(A, A.W.q);
+    mg_net_prolong_kernel<<<wave(mg_net_prolong_kernel, A.H.L[1], A.wave), kBlock, 0, s>>>(A.H, nullptr, N.acts.y, N.acts.norm2, N.fine);
+    mg_net_guess_kernel<<<wave(mg_net_guess_kernel, A.H.L[0], A.wave), kBlock, 0, s>>>(A, N.fine);
     return cudaGetLastError();
 }
 
@@ -1653,6 +1699,17 @@ int mg_level_count(int nx, int ny, int nz) {
 }
 
 int mg_max_refinement() { return kMaxPasses - 1; }
+
+// solid[q] = 1 where level-1 cell q has no fluid child (the learned preconditioner network's mask on that level).
+__global__ void mg_net_mask_kernel(uint32_t n, const uint8_t* __restrict__ fluid, uint8_t* __restrict__ solid) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) solid[q] = fluid[q] ? 0 : 1;
+}
+
+cudaError_t launch_mg_net_mask(const MgHierarchy& H, uint8_t* solid, cudaStream_t s) {
+    mg_net_mask_kernel<<<(H.L[1].n + 255) / 256, 256, 0, s>>>(H.L[1].n, H.L[1].fluid, solid);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uint8_t* occ, cudaStream_t s) {
     mg_fluid0_kernel<<<(H.L[0].n + 255) / 256, 256, 0, s>>>(H.L[0].n, occ, H.L[0].fluid);

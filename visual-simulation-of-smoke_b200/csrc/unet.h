@@ -132,12 +132,14 @@ cudaError_t net_backward(const NetImages& I, const NetActs& A, const NetGrads& G
 // One Adam step on w with moments m, v (step >= 1), gradient scaled by gscale; then the images are repacked.
 cudaError_t net_adam(float* w, const float* grad, float* m, float* v, float lr, int step, float gscale, const NetImages& I, cudaStream_t s);
 
-// What a solve with the learned preconditioner needs: the network's images, an activation workspace on the solve's
-// volume and the occupancy (the fluid-mask input channel).
+// What a solve with the learned preconditioner needs. The network runs on the multigrid hierarchy's level 1 (every
+// extent of the grid halved, rounding up): its images, an activation workspace on that volume, the level's solid mask
+// (1 = no fluid child; the fluid-mask input channel), and a level-0 array for the prolonged correction.
 struct LearnedSolve {
     NetImages images;
     NetActs acts;
-    const uint8_t* occupancy;
+    uint8_t* occupancy;
+    float* fine;
 };
 
 }  // namespace smoke_b200

@@ -3,9 +3,12 @@ solver, training on the GPU through the network's tensor-core forward and backwa
 the parameters saved as raw little-endian FP32 (smoke_b200_net_parameter_count() values).
 
 The network corrects what one multigrid V-cycle leaves of an error (SMOKE_B200_SOLVER_LEARNED_FCG preconditions
-with z = V(r) + N(r - A V(r))). For an error e with residual r = A e, the V-cycle gives z = V(r)
-(smoke_b200_apply_multigrid_cuda) and leaves the error e - z, whose residual is r - A z; so a training pair is
-(input r - A z, target e - z), with A applied by smoke_b200_apply_operator_cuda. The errors come from two sources:
+with z = V(r) + P N(R (r - A V(r)))). For an error e with residual r = A e, the V-cycle gives z = V(r)
+(smoke_b200_apply_multigrid_cuda) and leaves the error e - z, whose residual is r - A z, with A applied by
+smoke_b200_apply_operator_cuda. The network runs on the multigrid hierarchy's level 1 (every extent halved): its
+input is R(r - A z), the sums of the 2 x 2 x 2 children (as the solve restricts it), its mask marks the level-1
+cells without a fluid child, and its target is the mean of e - z over each cell's fluid children; the solve prolongs
+its output back with the V-cycle's trilinear prolongation. The errors come from two sources:
 
  - the solver's own iterates: plume scenes (seeded source position and strength U[0.5, 1.5], 0-3 solid spheres)
    are stepped with the multigrid FCG; at a step, the pressure system (b = the FLOW_PRESSURE_RHS view) is solved
@@ -85,10 +88,35 @@ def vcycle_pair(sim, e, r):
     return r - sim.apply_operator(z), e - z
 
 
+def _children(x):
+    """[nz, ny, nx] -> [nz', ny', nx', 8]: the 2 x 2 x 2 children of every level-1 cell (extents rounded up, missing
+    children 0)."""
+    import torch.nn.functional as F
+
+    nz, ny, nx = x.shape
+    x = F.pad(x, (0, nx % 2, 0, ny % 2, 0, nz % 2))
+    z, y, w = x.shape
+    return x.reshape(z // 2, 2, y // 2, 2, w // 2, 2).permute(0, 2, 4, 1, 3, 5).reshape(z // 2, y // 2, w // 2, 8)
+
+
+def coarse_mask(occ):
+    """The network's mask on level 1 (uint8, 1 = no fluid child) of a level-0 occupancy (1 = solid)."""
+    return (_children((occ == 0).float()).sum(-1) == 0).to(occ.dtype)
+
+
+def coarse_pair(r_in, t, occ):
+    """A level-0 pair (input r - A z, target e - z) on level 1: the child sums of the input (the solve's restriction)
+    and the mean of the target over the fluid children (0 where there is none)."""
+    fluid = _children((occ == 0).float())
+    count = fluid.sum(-1)
+    target = (_children(t) * fluid).sum(-1) / count.clamp(min=1.0)
+    return _children(r_in).sum(-1).contiguous(), target.contiguous()
+
+
 def generate(lib, shape, scenes: int, per_scene: int, seed: int = 0, spin: int = 8, every: int = 3, synthetic: int = 0, iterates=ITERATES):
-    """Samples (input, occupancy, target) as CUDA tensors [count, nz, ny, nx] from `scenes` plume scenes:
-    `per_scene` pressure systems each (one every `every` steps after `spin` steps), one sample per iterate count in
-    `iterates` of each, plus `synthetic` multi-scale random errors per scene."""
+    """Samples (input, mask, target) on level 1 as CUDA tensors [count, nz', ny', nx'] (extents halved, rounding up)
+    from `scenes` plume scenes on `shape`: `per_scene` pressure systems each (one every `every` steps after `spin`
+    steps), one sample per iterate count in `iterates` of each, plus `synthetic` multi-scale random errors per scene."""
     import torch
 
     import smoke_b200
@@ -101,6 +129,7 @@ def generate(lib, shape, scenes: int, per_scene: int, seed: int = 0, spin: int =
         with torch.cuda.stream(stream):
             o = torch.from_numpy(occ).cuda()
             sim.update_occupancy(o)
+            mask = coarse_mask(o)
         sim.set_solver(**STEP_SOLVER)
         driver = plume_scene.SceneDriver(sim, boxes, seed=seed * 1000 + k + 1, strength=strength)
         step = 0
@@ -122,20 +151,20 @@ def generate(lib, shape, scenes: int, per_scene: int, seed: int = 0, spin: int =
                         else:
                             sim.solve_pressure()
                             e = exact - sim.view(abi.VIEW_FLOW_PRESSURE)
-                        r_in, t = vcycle_pair(sim, e, sim.apply_operator(e))
+                        r_in, t = coarse_pair(*vcycle_pair(sim, e, sim.apply_operator(e)), o)
                         inputs.append(r_in)
                         targets.append(t)
-                        occs.append(o.clone())
+                        occs.append(mask)
                 sim.set_solver(**STEP_SOLVER)
         if synthetic:
             gen = torch.Generator().manual_seed(seed * 1000 + k)
             with torch.cuda.stream(stream):
                 fluid = (o == 0).float()
                 for e in synthetic_errors(o.shape, fluid, synthetic, gen):
-                    r_in, t = vcycle_pair(sim, e, sim.apply_operator(e))
+                    r_in, t = coarse_pair(*vcycle_pair(sim, e, sim.apply_operator(e)), o)
                     inputs.append(r_in)
                     targets.append(t)
-                    occs.append(o.clone())
+                    occs.append(mask)
         stream.synchronize()
         sim.close()
     return torch.stack(inputs), torch.stack(occs), torch.stack(targets)
