@@ -77,6 +77,13 @@ struct ConvArgs {
     uint32_t n;
 };
 
+// Programmatic dependent launch. The network's kernels are launched with programmatic stream serialisation
+// (launch_pdl): each lets the stream's next kernel start launching at once (pdl_trigger), and waits in pdl_wait until
+// its predecessor has completed and its writes are visible. Nothing a predecessor writes is read, and no global
+// memory is written, before the wait; a launch without the attribute passes the wait at once.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<const uint32_t*>(&v);
@@ -90,7 +97,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
     __shared__ uint64_t full[S::kStages], freed[S::kStages], done[2], drained[2], wbar;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
-    if (a.skip && *a.skip) return;  // uniform: every block reads the same word
+    pdl_trigger();
     const int t = threadIdx.x, warp = t >> 5;
     const int chunk = blockIdx.y;
     for (int st = 0; st < S::kStages; ++st)  // the slack after each box stays zero (read by the padding tap, times zero weights)
@@ -114,6 +121,11 @@ __global__ void __launch_bounds__(kConvThreads) conv3_kernel(const __grid_consta
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
+    pdl_wait();  // the set-up above overlaps the previous kernel's tail
+    if (a.skip && *a.skip) {  // uniform: every block reads the same word
+        if (warp == 0) tc::tmem_free(tmem, S::kTmemCols);
+        return;
+    }
     const long long wait = a.wait_cycles > 0 ? a.wait_cycles : kSpinCycles;
     volatile int* abort = &abort_flag;
     const int ntx = (a.nx + kTX - 1) / kTX, nty = (a.ny + kTY - 1) / kTY;
@@ -296,7 +308,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_band_kernel(const __grid_c
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
     constexpr uint32_t kCols = 32;  // two 16-column accumulators
-    if (a.skip && *a.skip) return;  // uniform: every block reads the same word
+    pdl_trigger();
     const int t = threadIdx.x, warp = t >> 5;
     if (t == 0) {
         for (int st = 0; st < kBandStages; ++st) {
@@ -316,6 +328,11 @@ __global__ void __launch_bounds__(kConvThreads) conv3_band_kernel(const __grid_c
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tmem_slot;
+    pdl_wait();  // the set-up above overlaps the previous kernel's tail
+    if (a.skip && *a.skip) {  // uniform: every block reads the same word
+        if (warp == 0) tc::tmem_free(tmem, kCols);
+        return;
+    }
     const long long wait = a.wait_cycles > 0 ? a.wait_cycles : kSpinCycles;
     volatile int* abort = &abort_flag;
     const int ntx = (a.nx + kTX - 1) / kTX, nty = (a.ny + kTY - 1) / kTY, ntz = (a.nz + kBandZ - 1) / kBandZ;
@@ -510,6 +527,23 @@ cudaError_t halo_map(CUtensorMap* map, int cs, const ConvArgs& a) {
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+// Launch with programmatic stream serialisation (see pdl_wait): the kernel may start while the stream's previous
+// kernel finishes.
+template <typename... P, typename... A>
+void launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 template <int CS, int NC>
 cudaError_t conv_typed(const VolumeDims& d, int chunks, const ConvArgs& a, cudaStream_t s) {
     using S = ConvShape<CS, NC>;
@@ -527,7 +561,7 @@ cudaError_t conv_typed(const VolumeDims& d, int chunks, const ConvArgs& a, cudaS
     const uint64_t tiles = static_cast<uint64_t>((d.nx + kTX - 1) / kTX) * ((d.ny + kTY - 1) / kTY) * d.nz;
     const int resident = resident_blocks(reinterpret_cast<const void*>(conv3_kernel<CS, NC>), S::kSmem, S::kTmemCols, kConvThreads);
     const int gx = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(tiles, static_cast<uint64_t>(std::max(1, resident / chunks)))));
-    conv3_kernel<CS, NC><<<dim3(gx, chunks), kConvThreads, S::kSmem, s>>>(a, map);
+    launch_pdl(conv3_kernel<CS, NC>, dim3(gx, chunks), dim3(kConvThreads), S::kSmem, s, a, map);
     return cudaGetLastError();
 }
 
@@ -547,7 +581,7 @@ cudaError_t conv_band(const VolumeDims& d, const ConvArgs& a, cudaStream_t s) {
     const uint64_t tiles = static_cast<uint64_t>((d.nx + kTX - 1) / kTX) * ((d.ny + kTY - 1) / kTY) * ((d.nz + kBandZ - 1) / kBandZ);
     const int resident = resident_blocks(reinterpret_cast<const void*>(conv3_band_kernel), kBandSmem, 32, kConvThreads);
     const int gx = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(tiles, static_cast<uint64_t>(resident))));
-    conv3_band_kernel<<<gx, kConvThreads, kBandSmem, s>>>(a, map);
+    launch_pdl(conv3_band_kernel, dim3(gx), dim3(kConvThreads), kBandSmem, s, a, map);
     return cudaGetLastError();
 }
 
@@ -745,6 +779,8 @@ __global__ void sumsq_kernel(const float* __restrict__ v, uint32_t n, double* __
 
 // X0[q] = (r[q] * s, fluid, 0, ...), s = sqrt(n / ||r||^2) (0 when r = 0); r = r_sel[*parity] when parity is given.
 __global__ void net_input_kernel(VolumeDims d, const float* __restrict__ r0, const float* __restrict__ r1, const int* __restrict__ parity, const double* __restrict__ norm2, const uint8_t* __restrict__ occ, __nv_bfloat16* __restrict__ x0, const uint32_t* __restrict__ skip) {
+    pdl_trigger();
+    pdl_wait();
     if (skip && *skip) return;
     const float* r = (parity && *parity) ? r1 : r0;
     const double nn = *norm2;
@@ -761,6 +797,8 @@ __global__ void net_input_kernel(VolumeDims d, const float* __restrict__ r0, con
 // coarse[Q][c] = mean of the existing children fine[q][c]
 template <int C>
 __global__ void pool_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __restrict__ fine, __nv_bfloat16* __restrict__ coarse, const uint32_t* __restrict__ skip) {
+    pdl_trigger();
+    pdl_wait();
     if (skip && *skip) return;
     constexpr int G = C / 8;
     const uint64_t items = static_cast<uint64_t>(c.n) * G;
@@ -792,6 +830,8 @@ __global__ void pool_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __r
 // out[q][c] = coarse[parent(q)][c] + skip[q][c]
 template <int C>
 __global__ void up_add_kernel(VolumeDims f, VolumeDims c, const __nv_bfloat16* __restrict__ coarse, const __nv_bfloat16* __restrict__ skip, __nv_bfloat16* __restrict__ out, const uint32_t* __restrict__ off) {
+    pdl_trigger();
+    pdl_wait();
     if (off && *off) return;
     constexpr int G = C / 8;
     const uint64_t items = static_cast<uint64_t>(f.n) * G;
@@ -1179,23 +1219,23 @@ cudaError_t net_forward(const NetImages& I, const NetActs& A, const float* r0, c
         sumsq_kernel<<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(r0, d[0].n, A.norm2);
         norm2 = A.norm2;
     }
-    net_input_kernel<<<glue_blocks(d[0].n), kGlueThreads, 0, s>>>(d[0], r0, r1, parity, norm2, occ, A.x0, skip);
+    launch_pdl(net_input_kernel, dim3(glue_blocks(d[0].n)), dim3(kGlueThreads), 0, s, d[0], r0, r1, parity, norm2, occ, A.x0, skip);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // encoder
     if ((e = conv_layer(0, d[0], I, A.x0, A.e0, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    pool_kernel<16><<<glue_blocks_c(d[1].n, 16), kGlueThreads, 0, s>>>(d[0], d[1], A.e0, A.p1, skip);
+    launch_pdl(pool_kernel<16>, dim3(glue_blocks_c(d[1].n, 16)), dim3(kGlueThreads), 0, s, d[0], d[1], A.e0, A.p1, skip);
     if ((e = conv_layer(1, d[1], I, A.p1, A.e1, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    pool_kernel<32><<<glue_blocks_c(d[2].n, 32), kGlueThreads, 0, s>>>(d[1], d[2], A.e1, A.p2, skip);
+    launch_pdl(pool_kernel<32>, dim3(glue_blocks_c(d[2].n, 32)), dim3(kGlueThreads), 0, s, d[1], d[2], A.e1, A.p2, skip);
     if ((e = conv_layer(2, d[2], I, A.p2, A.e2, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    pool_kernel<64><<<glue_blocks_c(d[3].n, 64), kGlueThreads, 0, s>>>(d[2], d[3], A.e2, A.p3, skip);
+    launch_pdl(pool_kernel<64>, dim3(glue_blocks_c(d[3].n, 64)), dim3(kGlueThreads), 0, s, d[2], d[3], A.e2, A.p3, skip);
     if ((e = conv_layer(3, d[3], I, A.p3, A.e3, nullptr, A.error, s, skip)) != cudaSuccess) return e;
     // bottom and decoder
     if ((e = conv_layer(4, d[3], I, A.e3, A.m3, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    up_add_kernel<64><<<glue_blocks_c(d[2].n, 64), kGlueThreads, 0, s>>>(d[2], d[3], A.m3, A.e2, A.s2, skip);
+    launch_pdl(up_add_kernel<64>, dim3(glue_blocks_c(d[2].n, 64)), dim3(kGlueThreads), 0, s, d[2], d[3], A.m3, A.e2, A.s2, skip);
     if ((e = conv_layer(5, d[2], I, A.s2, A.u2, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    up_add_kernel<32><<<glue_blocks_c(d[1].n, 32), kGlueThreads, 0, s>>>(d[1], d[2], A.u2, A.e1, A.s1, skip);
+    launch_pdl(up_add_kernel<32>, dim3(glue_blocks_c(d[1].n, 32)), dim3(kGlueThreads), 0, s, d[1], d[2], A.u2, A.e1, A.s1, skip);
     if ((e = conv_layer(6, d[1], I, A.s1, A.u1, nullptr, A.error, s, skip)) != cudaSuccess) return e;
-    up_add_kernel<16><<<glue_blocks_c(d[0].n, 16), kGlueThreads, 0, s>>>(d[0], d[1], A.u1, A.e0, A.s0, skip);
+    launch_pdl(up_add_kernel<16>, dim3(glue_blocks_c(d[0].n, 16)), dim3(kGlueThreads), 0, s, d[0], d[1], A.u1, A.e0, A.s0, skip);
     return conv_layer(7, d[0], I, A.s0, nullptr, A.y, A.error, s, skip);
 }
 
