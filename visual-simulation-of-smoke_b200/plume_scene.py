@@ -78,11 +78,16 @@ class SceneDriver:
             self.xi_dev = torch.zeros(self.box_cells.size, dtype=torch.float32, device=dev)
             self.total_dev = torch.zeros(1, dtype=torch.float32, device=dev)
         self.xi_host = torch.zeros(self.box_cells.size, dtype=torch.float32).pin_memory()
+        self.xi_read = None  # event: the last asynchronous copy out of xi_host has run
         self.total_host = torch.zeros(1, dtype=torch.float32).pin_memory()
         self.h2d_bytes = self.xi_host.numel() * 4
         self.d2h_bytes = 4
 
     def inputs_for(self, step: int):
+        # the pinned buffer is read by an asynchronous copy: a step enqueued ahead of the GPU must not see the next
+        # step's values, so wait for the previous copy before overwriting it
+        if self.xi_read is not None:
+            self.xi_read.synchronize()
         self.xi_host.copy_(__import__("torch").from_numpy(uniform(self.seed, step, self.box_cells, -0.1, 0.1)))
         return self.xi_host
 
@@ -94,6 +99,9 @@ class SceneDriver:
         xi = host_inputs if host_inputs is not None else self.inputs_for(step)
         with torch.cuda.stream(sim.stream):
             self.xi_dev.copy_(xi, non_blocking=True)
+            if xi is self.xi_host:
+                self.xi_read = torch.cuda.Event()
+                self.xi_read.record(sim.stream)
             _, vy, _ = sim.view(abi.VIEW_FLOW_VELOCITY)
             rho = sim.view(abi.VIEW_DENSITY)
             tem = sim.view(abi.VIEW_TEMPERATURE)
