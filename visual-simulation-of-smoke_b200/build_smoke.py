@@ -19,7 +19,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CU_SOURCES = ["step_kernels.cu", "pcg.cu", "mgsolve.cu", "noalloc.cu", "unet.cu"]
 CPP_SOURCES = ["context.cpp", "learned.cpp"]
 CLI = os.path.join(os.path.dirname(os.path.abspath(__file__)), "smoke_b200_benchmark")
-HEADERS = ["smoke_device.cuh", "launch.h", "config_check.h", "grid_sync.cuh", "march.cuh", "unet.h", "tcgen05.cuh"]
+HEADERS = ["smoke_device.cuh", "launch.h", "config_check.h", "grid_sync.cuh", "march.cuh", "unet.h", "tcgen05.cuh", "pdl.cuh"]
 INCLUDES = [os.path.join(ROOT, "include"), CSRC]
 
 NVCC_FLAGS = [

@@ -39,6 +39,7 @@
 #include <utility>
 
 #include "launch.h"
+#include "pdl.cuh"
 #include "unet.h"
 #include "smoke_b200_ext.h"
 
@@ -205,14 +206,8 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
-// Programmatic dependent launch. The iteration's kernels are launched with programmatic stream serialisation
-// (pdl_launch): each lets the stream's next kernel start launching at once, and then waits in griddepcontrol.wait
-// until the previous kernel has completed and its writes are visible. So a kernel's launch and block dispatch
-// overlap its predecessor's tail instead of following it; nothing is read before the wait.
-__device__ __forceinline__ void pdl_begin() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-}
+// Programmatic dependent launch (pdl.cuh): the iteration's kernels are launched with launch_pdl and begin with
+// pdl_begin, so a kernel's launch and block dispatch overlap its predecessor's tail; nothing is read before the wait.
 
 // Block sums of a and b (in a fixed order) stored as this block's partials of accumulators ka and kb (kb < 0: only
 // a). Thread 0 writes them.
@@ -1399,24 +1394,6 @@ __global__ void __launch_bounds__(kThreads) mg_apply_kernel(const __grid_constan
 // ---------------------------------------------------------------------------------------------- host side
 const dim3 kBlock(TX, TY, TZ);
 
-// Launch with programmatic stream serialisation: the kernel may begin launching while the stream's previous kernel
-// still runs; its pdl_begin waits for that kernel's completion before anything is read. Captured into a graph, the
-// dependency becomes a programmatic edge.
-template <class... P, class... A>
-void pdl_launch(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
-}
-
 // Grid for `kernel` on level L: the level's tile columns (x, y), and as many z shares as `depth` waves of resident
 // blocks (per SM x SMs, cached per kernel and device) allow: depth code 0..3 = 1/2, 1, 2, 4 waves, 4 = one z tile
 // per block.
@@ -1498,8 +1475,8 @@ cudaError_t add_while(cudaStream_t s, cudaStream_t body_stream, cudaGraphConditi
 // The level-0 update of the solve's preconditioner kind.
 template <typename T>
 void launch_update(const MgSolveArgs& A, int initial, cudaGraphConditionalHandle h, int in_graph, int net_loop, cudaStream_t s) {
-    if (A.learned) pdl_launch(mg_update_kernel<T, true>, march_grid(mg_update_kernel<T, true>, A.H.L[0], A.wave), kThreads, 0, s, A, initial, h, in_graph, net_loop);
-    else pdl_launch(mg_update_kernel<T, false>, march_grid(mg_update_kernel<T, false>, A.H.L[0], A.wave), kThreads, 0, s, A, initial, h, in_graph, 0);
+    if (A.learned) launch_pdl(mg_update_kernel<T, true>, march_grid(mg_update_kernel<T, true>, A.H.L[0], A.wave), kThreads, 0, s, A, initial, h, in_graph, net_loop);
+    else launch_pdl(mg_update_kernel<T, false>, march_grid(mg_update_kernel<T, false>, A.H.L[0], A.wave), kThreads, 0, s, A, initial, h, in_graph, 0);
 }
 
 // The V-cycle below level 0: restrictions of levels 1..g-1, the block-level cycle, the up passes of levels g-1..1,
@@ -1507,17 +1484,17 @@ void launch_update(const MgSolveArgs& A, int initial, cudaGraphConditionalHandle
 void launch_coarse_cycle(const MgSolveArgs& A, uint32_t block_bytes, cudaStream_t bs) {
     const MgHierarchy& H = A.H;
     const int g = H.grid_levels;
-    for (int l = 1; l < g; ++l) pdl_launch(mg_restrict_kernel, wave(mg_restrict_kernel, H.L[l], A.wave), kBlock, 0, bs, H, l);
-    pdl_launch(mg_block_kernel, 1, kBlockLevelThreads, block_bytes, bs, H);
+    for (int l = 1; l < g; ++l) launch_pdl(mg_restrict_kernel, wave(mg_restrict_kernel, H.L[l], A.wave), kBlock, 0, bs, H, l);
+    launch_pdl(mg_block_kernel, 1, kBlockLevelThreads, block_bytes, bs, H);
     for (int l = g - 1; l >= 1; --l) {
         if (H.L[l].n <= kFusedUpCells) {
-            pdl_launch(mg_up_kernel, wave(mg_up_kernel, H.L[l], A.wave), kBlock, 0, bs, H, l);
+            launch_pdl(mg_up_kernel, wave(mg_up_kernel, H.L[l], A.wave), kBlock, 0, bs, H, l);
         } else {
-            pdl_launch(mg_prolong_kernel, wave(mg_prolong_kernel, H.L[l + 1], A.wave), kBlock, 0, bs, H, l);
-            pdl_launch(mg_smooth_kernel, wave(mg_smooth_kernel, H.L[l], A.wave), kBlock, 0, bs, A, l);
+            launch_pdl(mg_prolong_kernel, wave(mg_prolong_kernel, H.L[l + 1], A.wave), kBlock, 0, bs, H, l);
+            launch_pdl(mg_smooth_kernel, wave(mg_smooth_kernel, H.L[l], A.wave), kBlock, 0, bs, A, l);
         }
     }
-    pdl_launch(mg_prolong_kernel, wave(mg_prolong_kernel, H.L[1], A.wave), kBlock, 0, bs, H, 0);
+    launch_pdl(mg_prolong_kernel, wave(mg_prolong_kernel, H.L[1], A.wave), kBlock, 0, bs, H, 0);
 }
 
 // One iteration's loop body (everything after the update that tests convergence, up to the next update); net = 1:
@@ -1529,18 +1506,18 @@ void launch_body(const MgSolveArgs& A, int net, cudaGraphConditionalHandle h, in
     launch_coarse_cycle(A, block_bytes, bs);
     if (net) {  // z = z_V + N(r - A z_V), post-smoothed: the network corrects what the V-cycle leaves
         const LearnedSolve& N = *A.net;
-        pdl_launch(mg_smooth0_kernel<T, false>, march_grid(mg_smooth0_kernel<T, false>, L0, A.wave), kThreads, 0, bs, A);
-        pdl_launch(mg_net_residual_kernel<T>, wave(mg_net_residual_kernel<T>, L0, A.wave), kBlock, 0, bs, A);
+        launch_pdl(mg_smooth0_kernel<T, false>, march_grid(mg_smooth0_kernel<T, false>, L0, A.wave), kThreads, 0, bs, A);
+        launch_pdl(mg_net_residual_kernel<T>, wave(mg_net_residual_kernel<T>, L0, A.wave), kBlock, 0, bs, A);
         if (net_forward(N.images, N.acts, A.H.L[1].zp, nullptr, nullptr, &A.st->net_rr, N.occupancy, bs, &A.st->net_off) != cudaSuccess) return;
-        pdl_launch(mg_net_prolong_kernel, wave(mg_net_prolong_kernel, A.H.L[1], A.wave), kBlock, 0, bs, A.H, A.st, N.acts.y, &A.st->net_rr, N.fine);
-        pdl_launch(mg_net_gamma_kernel<T>, wave(mg_net_gamma_kernel<T>, L0, A.wave), kBlock, 0, bs, A, N.fine);
-        pdl_launch(mg_net_add_kernel<T>, march_grid(mg_net_add_kernel<T>, L0, A.wave), kThreads, 0, bs, A, N.fine);
-        pdl_launch(mg_pq_kernel<T>, march_grid(mg_pq_kernel<T>, L0, A.wave), kThreads, 0, bs, A);
-        pdl_launch(mg_update_kernel<T, true>, march_grid(mg_update_kernel<T, true>, L0, A.wave), kThreads, 0, bs, A, 0, h, in_graph, 1);
+        launch_pdl(mg_net_prolong_kernel, wave(mg_net_prolong_kernel, A.H.L[1], A.wave), kBlock, 0, bs, A.H, A.st, N.acts.y, &A.st->net_rr, N.fine);
+        launch_pdl(mg_net_gamma_kernel<T>, wave(mg_net_gamma_kernel<T>, L0, A.wave), kBlock, 0, bs, A, N.fine);
+        launch_pdl(mg_net_add_kernel<T>, march_grid(mg_net_add_kernel<T>, L0, A.wave), kThreads, 0, bs, A, N.fine);
+        launch_pdl(mg_pq_kernel<T>, march_grid(mg_pq_kernel<T>, L0, A.wave), kThreads, 0, bs, A);
+        launch_pdl(mg_update_kernel<T, true>, march_grid(mg_update_kernel<T, true>, L0, A.wave), kThreads, 0, bs, A, 0, h, in_graph, 1);
         return;
     }
-    pdl_launch(mg_smooth0_kernel<T, true>, march_grid(mg_smooth0_kernel<T, true>, L0, A.wave), kThreads, 0, bs, A);
-    pdl_launch(mg_pq_kernel<T>, march_grid(mg_pq_kernel<T>, L0, A.wave), kThreads, 0, bs, A);
+    launch_pdl(mg_smooth0_kernel<T, true>, march_grid(mg_smooth0_kernel<T, true>, L0, A.wave), kThreads, 0, bs, A);
+    launch_pdl(mg_pq_kernel<T>, march_grid(mg_pq_kernel<T>, L0, A.wave), kThreads, 0, bs, A);
     launch_update<T>(A, 0, h, in_graph, 0, bs);
 }
 
@@ -1588,16 +1565,16 @@ cudaError_t enqueue_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream
             cudaGraphConditionalHandle h2;
             e = cudaGraphConditionalHandleCreate(&h2, graph, 0, cudaGraphCondAssignDefault);
             if (e != cudaSuccess) return e;
-            pdl_launch(mg_loop_gate_kernel, 1, 1, 0, s, A.st, h2);
+            launch_pdl(mg_loop_gate_kernel, 1, 1, 0, s, A.st, h2);
             e = add_while(s, body_stream, h2, [&](cudaStream_t bs) { launch_body<T>(A, 0, h2, 1, block_bytes, bs); });
             if (e != cudaSuccess) return e;
         }
         if (A.ir) {
-            pdl_launch(mg_accumulate_kernel, wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s, A);
-            pdl_launch(mg_residual_kernel, wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s, A);
+            launch_pdl(mg_accumulate_kernel, wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s, A);
+            launch_pdl(mg_residual_kernel, wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s, A);
         }
     }
-    pdl_launch(mg_finalize_kernel, wave(mg_finalize_kernel, L0, A.wave), kBlock, 0, s, A, out);
+    launch_pdl(mg_finalize_kernel, wave(mg_finalize_kernel, L0, A.wave), kBlock, 0, s, A, out);
     return cudaGetLastError();
 }
 
@@ -1625,11 +1602,11 @@ cudaError_t run_typed(const MgSolveArgs& A, PcgStatusDevice* out, cudaStream_t s
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (A.ir) {
-            pdl_launch(mg_accumulate_kernel, wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s, A);
-            pdl_launch(mg_residual_kernel, wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s, A);
+            launch_pdl(mg_accumulate_kernel, wave(mg_accumulate_kernel, L0, A.wave), kBlock, 0, s, A);
+            launch_pdl(mg_residual_kernel, wave(mg_residual_kernel, L0, A.wave), kBlock, 0, s, A);
         }
     }
-    pdl_launch(mg_finalize_kernel, wave(mg_finalize_kernel, L0, A.wave), kBlock, 0, s, A, out);
+    launch_pdl(mg_finalize_kernel, wave(mg_finalize_kernel, L0, A.wave), kBlock, 0, s, A, out);
     return cudaGetLastError();
 }
 

@@ -13,6 +13,7 @@
 #include <cmath>
 
 #include "launch.h"
+#include "pdl.cuh"
 
 namespace smoke_b200 {
 
@@ -106,6 +107,7 @@ __device__ __forceinline__ uint32_t pad_index(const StepParams& P, int i, int j,
 
 // ------------------------------------------------------------------------------------------ forces
 __global__ void __launch_bounds__(kThreads) vorticity_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, float* __restrict__ wx, float* __restrict__ wy, float* __restrict__ wz, float* __restrict__ wm) {
+    pdl_begin();
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.n) return;
     int x, y, z;
@@ -130,6 +132,7 @@ __device__ __forceinline__ float flow_cell(const float* __restrict__ f, int x, i
 __global__ void __launch_bounds__(kThreads) cell_force_kernel(const __grid_constant__ StepParams P, const float* __restrict__ wx, const float* __restrict__ wy, const float* __restrict__ wz, const float* __restrict__ wm, const float* __restrict__ density, const float* __restrict__ temperature, const float* __restrict__ ufx,
                                                                const float* __restrict__ ufy, const float* __restrict__ ufz, const uint8_t* __restrict__ occ, float* __restrict__ fx, float* __restrict__ fy, float* __restrict__ fz,
                                                                const __grid_constant__ ScalarSources S) {
+    pdl_begin();
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.n) return;
     // The scalar stage's sourced fields and their padded copies: t_tmp = T' + dt * src_T, T' being T with solid cells at
@@ -233,6 +236,7 @@ __device__ __forceinline__ void face_force_one(const StepParams& P, uint32_t q, 
 // Block ranges: [0, bu) -> x faces, [bu, bu+bv) -> y faces, rest -> z faces.
 __global__ void __launch_bounds__(kThreads) face_force_kernel(const __grid_constant__ StepParams P, const float* __restrict__ iu, const float* __restrict__ iv, const float* __restrict__ iw, const float* __restrict__ fx, const float* __restrict__ fy, const float* __restrict__ fz, const uint8_t* __restrict__ occ, const float* __restrict__ su,
                                                                const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou, float* __restrict__ ov, float* __restrict__ ow, float* __restrict__ pu, float* __restrict__ pv, float* __restrict__ pw, unsigned bu, unsigned bv) {
+    pdl_begin();
     const unsigned b = blockIdx.x;
     if (b < bu) {
         const uint32_t q = b * kThreads + threadIdx.x;
@@ -297,6 +301,7 @@ __device__ __forceinline__ void advect_face_one(const StepParams& P, unsigned bl
 template <bool CUBIC, bool TILED, bool POW2>
 __global__ void __launch_bounds__(kThreads, 6) advect_velocity_kernel(const __grid_constant__ StepParams P, const PadField u, const PadField v, const PadField w, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou, float* __restrict__ ov,
                                                                     float* __restrict__ ow, unsigned bu, unsigned bv) {
+    pdl_begin();
     const unsigned b = blockIdx.x;
     if (b < bu) advect_face_one<0, CUBIC, TILED, POW2>(P, b, u, v, w, occ, su, ou);
     else if (b < bu + bv) advect_face_one<1, CUBIC, TILED, POW2>(P, b - bu, u, v, w, occ, sv, ov);
@@ -352,6 +357,7 @@ __global__ void __launch_bounds__(256) pad_kernel(const __grid_constant__ StepPa
 // takes ghost cell g of the shell, enumerated as the 2 kPad whole z-planes, then in each interior plane the 2 kPad
 // y-rows, then in each interior row the 2 kPad x-cells; its value is the boundary tap, as in pad_kernel.
 __global__ void __launch_bounds__(256) pad_ghost_kernel(const __grid_constant__ StepParams P, const __grid_constant__ PadJob J) {
+    pdl_begin();
     const int c = blockIdx.y;
     if (c >= J.count) return;
     const int kind = c == 0 ? J.kind[0] : (c == 1 ? J.kind[1] : J.kind[2]);
@@ -394,6 +400,7 @@ __global__ void __launch_bounds__(256) pad_ghost_kernel(const __grid_constant__ 
 // ------------------------------------------------------------------------------------------ pressure rhs
 // b = -(h^2/dt) div u* + sum of OUTFLOW face pressures; 0 at solid cells and at the anchor (:1304-1328).
 __global__ void __launch_bounds__(kThreads) rhs_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, const int32_t* __restrict__ anchor, float* __restrict__ rhs) {
+    pdl_begin();
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.n) return;
     // every load is issued before the anchor/solid test (the six faces of a cell always exist)
@@ -472,6 +479,7 @@ __device__ __forceinline__ void project_one(const StepParams& P, uint32_t q, con
 
 __global__ void __launch_bounds__(kThreads) project_kernel(const __grid_constant__ StepParams P, const float* __restrict__ iu, const float* __restrict__ iv, const float* __restrict__ iw, const float* __restrict__ p, const double* __restrict__ p64, const uint8_t* __restrict__ occ, const float* __restrict__ su, const float* __restrict__ sv, const float* __restrict__ sw, float* __restrict__ ou,
                                                             float* __restrict__ ov, float* __restrict__ ow, float* __restrict__ pu, float* __restrict__ pv, float* __restrict__ pw, unsigned bu, unsigned bv) {
+    pdl_begin();
     const unsigned b = blockIdx.x;
     if (b < bu) {
         const uint32_t q = b * kThreads + threadIdx.x;
@@ -490,6 +498,7 @@ __global__ void __launch_bounds__(kThreads) project_kernel(const __grid_constant
 // Solid cells: temperature = solid temperature (:1235-1241), density = 0 until the fill pass.
 template <bool CUBIC, bool TILED, bool POW2>
 __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ StepParams P, const PadField u, const PadField v, const PadField w, const uint8_t* __restrict__ occ, const PadField t_tmp, const PadField d_tmp, const float* __restrict__ solid_t, float* __restrict__ t, float* __restrict__ d) {
+    pdl_begin();
     int x, y, z;
     uint32_t q;
     if (TILED) {
@@ -514,6 +523,7 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_c
 }
 
 __global__ void density_fill_kernel(const FillEntry* __restrict__ list, const uint32_t* __restrict__ count, float* __restrict__ d) {
+    pdl_begin();
     const uint32_t n = *count;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const FillEntry e = list[t];
@@ -524,6 +534,7 @@ __global__ void density_fill_kernel(const FillEntry* __restrict__ list, const ui
 // ------------------------------------------------------------------------------------------ views
 __global__ void __launch_bounds__(kThreads) views_kernel(const __grid_constant__ StepParams P, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, const uint8_t* __restrict__ occ, float* __restrict__ cx, float* __restrict__ cy, float* __restrict__ cz, float* __restrict__ vm, float* __restrict__ wx, float* __restrict__ wy,
                                                           float* __restrict__ wz, float* __restrict__ wm, float* __restrict__ div, uint32_t groups) {
+    pdl_begin();
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.n) return;
     int x, y, z;
@@ -714,13 +725,13 @@ cudaError_t launch_vorticity(const StepParams& P, ConstFaces vel, const uint8_t*
 }
 
 cudaError_t launch_cell_force(const StepParams& P, const float* wx, const float* wy, const float* wz, const float* wmag, const float* density, const float* temperature, const float* ufx, const float* ufy, const float* ufz, const uint8_t* occ, float* fx, float* fy, float* fz, cudaStream_t s, const ScalarSources& S) {
-    cell_force_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, wx, wy, wz, wmag, density, temperature, ufx, ufy, ufz, occ, fx, fy, fz, S);
+    launch_pdl(cell_force_kernel, dim3(blocks_for(P.n)), dim3(kThreads), 0, s, P, wx, wy, wz, wmag, density, temperature, ufx, ufy, ufz, occ, fx, fy, fz, S);
     return cudaGetLastError();
 }
 
 cudaError_t launch_face_force(const StepParams& P, ConstFaces in, const float* fx, const float* fy, const float* fz, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s, Faces pad) {
     const unsigned bu = blocks_for(P.nu), bv = blocks_for(P.nv), bw = blocks_for(P.nw);
-    face_force_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, fx, fy, fz, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, pad.u, pad.v, pad.w, bu, bv);
+    launch_pdl(face_force_kernel, dim3(bu + bv + bw), dim3(kThreads), 0, s, P, in.u, in.v, in.w, fx, fy, fz, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, pad.u, pad.v, pad.w, bu, bv);
     return cudaGetLastError();
 }
 
@@ -752,7 +763,7 @@ cudaError_t launch_pads(const StepParams& P, int count, const int* kinds, const 
     if (ghost_only) {  // the largest shell of the fields (faces of the x, y or z axis have one more layer)
         const uint32_t px = P.nx + 1 + 2 * kPad, py = P.ny + 1 + 2 * kPad, pz = P.nz + 1 + 2 * kPad;
         const uint64_t most = static_cast<uint64_t>(px) * py * pz - static_cast<uint64_t>(P.nx) * P.ny * P.nz;
-        pad_ghost_kernel<<<dim3(static_cast<unsigned>((most + 255) / 256), count), 256, 0, s>>>(P, J);
+        launch_pdl(pad_ghost_kernel, dim3(static_cast<unsigned>((most + 255) / 256), count), dim3(256), 0, s, P, J);
         return cudaGetLastError();
     }
     const dim3 grid((P.nx + 1 + 2 * kPad + 31) / 32, (P.ny + 1 + 2 * kPad + 7) / 8, J.pz_blocks * count);
@@ -784,18 +795,18 @@ cudaError_t launch_advect_velocity(const StepParams& P, ConstFaces in, ConstFace
     const PadField u = pad_field(P, 0, in.u, pad.u), v = pad_field(P, 1, in.v, pad.v), w = pad_field(P, 2, in.w, pad.w);
     auto kernel = pick_advect(P, advect_velocity_kernel<false, false, false>, advect_velocity_kernel<false, false, true>, advect_velocity_kernel<false, true, false>, advect_velocity_kernel<false, true, true>, advect_velocity_kernel<true, false, false>,
                               advect_velocity_kernel<true, false, true>, advect_velocity_kernel<true, true, false>, advect_velocity_kernel<true, true, true>);
-    kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, u, v, w, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
+    launch_pdl(kernel, dim3(bu + bv + bw), dim3(kThreads), 0, s, P, u, v, w, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, bu, bv);
     return cudaGetLastError();
 }
 
 cudaError_t launch_rhs(const StepParams& P, ConstFaces vel, const uint8_t* occ, const int32_t* anchor, float* rhs, cudaStream_t s) {
-    rhs_kernel<<<blocks_for(P.n), kThreads, 0, s>>>(P, vel.u, vel.v, vel.w, occ, anchor, rhs);
+    launch_pdl(rhs_kernel, dim3(blocks_for(P.n)), dim3(kThreads), 0, s, P, vel.u, vel.v, vel.w, occ, anchor, rhs);
     return cudaGetLastError();
 }
 
 cudaError_t launch_project(const StepParams& P, ConstFaces in, const float* pressure, const double* pressure64, const uint8_t* occ, ConstFaces solid, Faces out, cudaStream_t s, Faces pad) {
     const unsigned bu = blocks_for(P.nu), bv = blocks_for(P.nv), bw = blocks_for(P.nw);
-    project_kernel<<<bu + bv + bw, kThreads, 0, s>>>(P, in.u, in.v, in.w, pressure, pressure64, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, pad.u, pad.v, pad.w, bu, bv);
+    launch_pdl(project_kernel, dim3(bu + bv + bw), dim3(kThreads), 0, s, P, in.u, in.v, in.w, pressure, pressure64, occ, solid.u, solid.v, solid.w, out.u, out.v, out.w, pad.u, pad.v, pad.w, bu, bv);
     return cudaGetLastError();
 }
 
@@ -804,12 +815,12 @@ cudaError_t launch_advect_scalars(const StepParams& P, ConstFaces vel, ConstFace
     const PadField t = pad_field(P, 4, t_tmp, t_pad), d = pad_field(P, 3, d_tmp, d_pad);
     auto kernel = pick_advect(P, advect_scalars_kernel<false, false, false>, advect_scalars_kernel<false, false, true>, advect_scalars_kernel<false, true, false>, advect_scalars_kernel<false, true, true>, advect_scalars_kernel<true, false, false>,
                               advect_scalars_kernel<true, false, true>, advect_scalars_kernel<true, true, false>, advect_scalars_kernel<true, true, true>);
-    kernel<<<advect_blocks(P, P.nx, P.ny, P.nz), kThreads, 0, s>>>(P, u, v, w, occ, t, d, solid_temperature, temperature, density);
+    launch_pdl(kernel, dim3(advect_blocks(P, P.nx, P.ny, P.nz)), dim3(kThreads), 0, s, P, u, v, w, occ, t, d, solid_temperature, temperature, density);
     return cudaGetLastError();
 }
 
 cudaError_t launch_density_fill(const FillEntry* list, const uint32_t* count, float* density, int max_blocks, cudaStream_t s) {
-    density_fill_kernel<<<max_blocks, kThreads, 0, s>>>(list, count, density);
+    launch_pdl(density_fill_kernel, dim3(max_blocks), dim3(kThreads), 0, s, list, count, density);
     return cudaGetLastError();
 }
 

@@ -16,6 +16,7 @@
 #include <cudaTypedefs.h>
 
 #include "tcgen05.cuh"
+#include "pdl.cuh"
 #include "unet.h"
 
 namespace smoke_b200 {
@@ -77,12 +78,6 @@ struct ConvArgs {
     uint32_t n;
 };
 
-// Programmatic dependent launch. The network's kernels are launched with programmatic stream serialisation
-// (launch_pdl): each lets the stream's next kernel start launching at once (pdl_trigger), and waits in pdl_wait until
-// its predecessor has completed and its writes are visible. Nothing a predecessor writes is read, and no global
-// memory is written, before the wait; a launch without the attribute passes the wait at once.
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
@@ -527,22 +522,6 @@ cudaError_t halo_map(CUtensorMap* map, int cs, const ConvArgs& a) {
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-// Launch with programmatic stream serialisation (see pdl_wait): the kernel may start while the stream's previous
-// kernel finishes.
-template <typename... P, typename... A>
-void launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
-}
 
 template <int CS, int NC>
 cudaError_t conv_typed(const VolumeDims& d, int chunks, const ConvArgs& a, cudaStream_t s) {
