@@ -65,3 +65,32 @@ def test_network_is_positively_homogeneous():
     b = U.apply(p, 3.5 * r, occ)
     assert np.allclose(b, 3.5 * a, rtol=1e-5, atol=1e-6 * np.abs(a).max())  # the input scale s is FP32, as on the GPU
     assert not np.any(a[occ != 0])
+
+
+def test_level1_training_pairs():
+    """The network's training pairs on the multigrid level 1 (train_preconditioner.coarse_pair / coarse_mask): the
+    input is the sum of a cell's 2 x 2 x 2 children (the solve's restriction of r - A V(r)), the target the mean of
+    e - V(r) over its fluid children, the mask 1 where a cell has no fluid child; odd extents round up."""
+    import torch
+
+    import train_preconditioner as T
+
+    rng = np.random.default_rng(3)
+    nz, ny, nx = 5, 6, 7
+    r = rng.standard_normal((nz, ny, nx)).astype(np.float32)
+    t = rng.standard_normal((nz, ny, nx)).astype(np.float32)
+    occ = (rng.random((nz, ny, nx)) < 0.4).astype(np.uint8)
+    occ[0:2, 0:2, 0:2] = 1  # one level-1 cell without a fluid child
+    got_r, got_t = T.coarse_pair(torch.from_numpy(r), torch.from_numpy(t), torch.from_numpy(occ))
+    got_m = T.coarse_mask(torch.from_numpy(occ))
+    assert got_r.shape == (3, 3, 4) and got_m.shape == (3, 3, 4)
+    for Z in range(3):
+        for Y in range(3):
+            for X in range(4):
+                sl = (slice(2 * Z, 2 * Z + 2), slice(2 * Y, 2 * Y + 2), slice(2 * X, 2 * X + 2))
+                fluid = occ[sl] == 0
+                assert np.isclose(got_r[Z, Y, X].item(), r[sl].sum(), atol=1e-5)
+                assert got_m[Z, Y, X].item() == (0 if fluid.any() else 1)
+                want = t[sl][fluid].mean() if fluid.any() else 0.0
+                assert np.isclose(got_t[Z, Y, X].item(), want, atol=1e-5)
+    assert got_m[0, 0, 0].item() == 1
