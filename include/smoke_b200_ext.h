@@ -32,11 +32,13 @@ typedef enum SmokeB200SolverMode {
     SMOKE_B200_SOLVER_JACOBI_PCG = 1,
     /* Flexible CG preconditioned by one geometric multigrid V(1,1) cycle; same stopping rule as JACOBI_PCG. */
     SMOKE_B200_SOLVER_MG_FCG = 2,
-    /* Flexible CG preconditioned by the learned network set with smoke_b200_set_preconditioner_net_cuda: z = N(r)
-     * followed by one weighted-Jacobi step on r - A N(r); same stopping rule, so the network changes the iteration
-     * count, not the answer. When ||r|| shrinks less than 1.2x over 100 iterations the solve drops the network and
-     * goes on with the plain Jacobi preconditioner. With warm_start = 2 the network's estimate N(b) is also the
-     * initial guess (needs refinement >= 1). */
+    /* Flexible CG preconditioned by the MG_FCG V-cycle V, corrected by the learned network U set with
+     * smoke_b200_set_preconditioner_net_cuda: with r_V = r - A V(r) and N = P U(R r_V) (U on the multigrid level 1,
+     * every extent halved; R the 2x2x2 child sums, P the V-cycle's prolongation), z = V(r) + g N + w D^-1 (r_V - g A N),
+     * g = (N, r_V) / (N, A N). Same stopping rule, so the network changes the iteration count, not the answer. When
+     * ||r||^2 shrinks by less than 1e-2 over 6 iterations the solve drops the network and goes on with the V-cycle
+     * alone (flags bit 0). With warm_start = 2 the network's estimate P U(R b) is also the initial guess (needs
+     * refinement >= 1). */
     SMOKE_B200_SOLVER_LEARNED_FCG = 3,
 } SmokeB200SolverMode;
 
@@ -68,7 +70,7 @@ typedef struct SmokeB200SolverStatus {
     int32_t iterations;             /* inner iterations of the last solve, all refinement passes */
     int32_t passes;                 /* refinement passes run (1 = no refinement needed) */
     uint32_t status;                /* SmokeB200SolveStatus */
-    uint32_t flags;                 /* bit 0: a LEARNED_FCG solve dropped the network for the plain preconditioner */
+    uint32_t flags;                 /* bit 0: a LEARNED_FCG solve dropped the network for the V-cycle alone */
     double rhs_norm;                /* ||b||_2 */
     double relative_residual;       /* recurrence residual ||r||/||b|| at exit */
     double true_relative_residual;  /* ||b - A x||/||b|| recomputed in FP64 at exit, -1 if not computed */
