@@ -55,7 +55,7 @@ def mg_grid_levels(n):
     grid, words = len(dims) - 1, 0
     for l in range(len(dims) - 1, 0, -1):
         words += 3 * cells[l] + (cells[l] + 2) // 2
-        if cells[l] > 4096 or words * 4 > 80 * 1024:
+        if cells[l] > 512 or words * 4 > 16 * 1024:
             break
         grid = l
     return len(dims), grid

@@ -54,10 +54,10 @@ def test_solver_launch_count_formula():
     sys.path.insert(0, ROOT)
     import bench
 
-    assert bench.mg_grid_levels(128) == (8, 3)   # 128 64 32 on the grid, 16 8 4 2 1 in one block
+    assert bench.mg_grid_levels(128) == (8, 4)   # 128 64 32 16 on the grid, 8 4 2 1 in one block
     assert bench.mg_grid_levels(12) == (5, 1)    # 12 on the grid, 6 3 2 1 in one block
-    # per iteration: 2 coarse grid levels x (restrict, prolong + smooth) + block + prolong0 + smooth0 + p/q + update
-    assert bench.solver_launches(128, 15, 3) == 2 + 3 * 4 + 9 * 15
-    # 256^3: level 1 (128^3) keeps prolongation and smoothing apart, levels 2-3 fuse them
-    assert bench.mg_grid_levels(256) == (9, 4)
-    assert bench.solver_launches(256, 12, 1) == 2 + 3 * 2 + (3 + 2 + 2 + 5) * 12
+    # per iteration: 3 coarse grid levels x (restrict, prolong + smooth) + block + prolong0 + smooth0 + p/q + update
+    assert bench.solver_launches(128, 15, 3) == 2 + 3 * 4 + 11 * 15
+    # 256^3: level 1 (128^3) keeps prolongation and smoothing apart, levels 2-4 fuse them
+    assert bench.mg_grid_levels(256) == (9, 5)
+    assert bench.solver_launches(256, 12, 1) == 2 + 3 * 2 + (3 + 2 + 2 + 2 + 5) * 12

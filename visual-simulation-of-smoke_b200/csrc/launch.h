@@ -159,8 +159,8 @@ struct PcgLaunchShape {
 // extent (rounding up). A coarse cell is fluid when any of its children is; every level's operator is the masked
 // 7-point stencil of its fluid cells (the fine rules without the anchor).
 constexpr int kMgMaxLevels = 12;
-constexpr uint32_t kMgBlockLevelCells = 4096;  // levels this small may run inside one block, in shared memory
-constexpr uint32_t kMgBlockBytes = 80 * 1024;  // shared memory for those levels (3 floats + 1 code per cell)
+constexpr uint32_t kMgBlockLevelCells = 512;   // levels this small may run inside one block, in shared memory
+constexpr uint32_t kMgBlockBytes = 16 * 1024;  // shared memory for those levels (3 floats + 1 code per cell)
 // Shared-memory words of one block-level level of n cells: r, zp, t and the 16-bit codes (padded pairs).
 __host__ __device__ constexpr uint32_t mg_block_words(uint32_t n) { return 3u * n + (n + 2u) / 2u; }
 // Bit of the operator code that marks a cell whose unknown is solved for (fluid; at level 0 also not the anchor).

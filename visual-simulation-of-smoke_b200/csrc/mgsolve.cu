@@ -49,7 +49,7 @@ namespace {
 
 constexpr int TX = 32, TY = 4, TZ = 2;  // cells of one block; even extents, so blocks hold whole parents
 constexpr int kThreads = TX * TY * TZ;
-constexpr int kBlockLevelThreads = 1024;
+constexpr int kBlockLevelThreads = 512;
 constexpr float kOmega = 6.0f / 7.0f;  // damped Jacobi weight: the optimal smoothing factor of the 7-point Laplacian in 3D
 constexpr int kCoarsestSweeps = 16;
 constexpr uint32_t kWarpCoarsestCells = 128;  // coarsest levels this small sweep in one warp
@@ -1123,16 +1123,16 @@ __device__ __forceinline__ float prolong_codes(const MgLevel& C, const int* fper
     return acc;
 }
 
-// The coarse part of the V-cycle below the grid levels, in one block of kBlockLevelThreads threads (a block level has
-// at most kMgBlockLevelCells cells, up to four per thread): reads r of level g (global), pre-smooths and restricts
-// level by level, runs the coarsest Jacobi sweeps, then the up passes, and writes t of level g (kTag on inactive
-// cells). The level codes do not change during a solve, so they are copied before the wait for the previous kernel.
-// The restriction gathers each coarse cell's children in a fixed order (deterministic sums); every stencil issues its
-// 6 neighbour loads before using any.
+// The coarse part of the V-cycle below the grid levels, in one block, one cell per thread on every level (a block
+// level has at most kMgBlockLevelCells = kBlockLevelThreads cells): reads r of level g (global), pre-smooths and
+// restricts level by level, runs the coarsest Jacobi sweeps, then the up passes, and writes t of level g (kTag on
+// inactive cells). The level codes do not change during a solve, so they are copied before the wait for the
+// previous kernel. The restriction gathers each coarse cell's children in a fixed order (deterministic sums); every
+// stencil issues its 6 neighbour loads before using any.
 __global__ void __launch_bounds__(kBlockLevelThreads) mg_block_kernel(const __grid_constant__ MgHierarchy H) {
     extern __shared__ __align__(16) float area[];
     constexpr int NT = kBlockLevelThreads;
-    static_assert(4 * NT >= kMgBlockLevelCells, "at most four cells per thread on a block level");
+    static_assert(NT >= kMgBlockLevelCells, "one thread per cell of a block level");
     const int g = H.grid_levels, lc = H.levels - 1;
     const uint32_t t = threadIdx.x;
     for (int l = g; l <= lc; ++l) {  // codes as aligned pairs (the arrays carry two spare entries)
@@ -1144,31 +1144,33 @@ __global__ void __launch_bounds__(kBlockLevelThreads) mg_block_kernel(const __gr
     pdl_begin();
     {
         const MgLevel S = smem_level<NT>(H, area, g);
-        for (uint32_t q = t; q < S.n; q += NT) S.r[q] = H.L[g].r[q];
+        if (t < S.n) S.r[t] = H.L[g].r[t];
     }
     __syncthreads();
     for (int l = g; l < lc; ++l) {  // down: zp = w D^-1 r, then r of l + 1 = 1/2 sum of the children's r - A zp
         const MgLevel F = smem_level<NT>(H, area, l);
         const MgLevel C = smem_level<NT>(H, area, l + 1);
-        for (uint32_t q = t; q < F.n; q += NT) {
-            const uint16_t code = F.code[q];
-            F.zp[q] = active(code) ? wdiag(code) * F.r[q] : 0.0f;
+        uint16_t code = 0;
+        float rv = 0.0f, zp = 0.0f;
+        if (t < F.n) {
+            code = F.code[t];
+            rv = F.r[t];
+            zp = active(code) ? wdiag(code) * rv : 0.0f;
+            F.zp[t] = zp;
         }
         __syncthreads();
-        for (uint32_t q = t; q < F.n; q += NT) {
+        if (t < F.n) {
             uint32_t nb[6];
-            block_cell(F, H.fper, q, nb);
-            const uint16_t code = F.code[q];
-            const float rv = F.r[q], zp = F.zp[q];
+            block_cell(F, H.fper, t, nb);
             float vn[6];
 #pragma unroll
             for (int k = 0; k < 6; ++k) vn[k] = F.zp[nb[k]];
-            F.t[q] = active(code) ? 0.5f * (rv - masked_stencil(code, zp, vn)) : 0.0f;  // t is free until the up pass
+            F.t[t] = active(code) ? 0.5f * (rv - masked_stencil(code, zp, vn)) : 0.0f;  // t is free until the up pass
         }
         __syncthreads();
-        for (uint32_t Q = t; Q < C.n; Q += NT) {
+        if (t < C.n) {
             int X, Y, Z;
-            lxyz(C, Q, X, Y, Z);
+            lxyz(C, t, X, Y, Z);
             float v[8];
 #pragma unroll
             for (int m = 0; m < 8; ++m) {
@@ -1178,7 +1180,7 @@ __global__ void __launch_bounds__(kBlockLevelThreads) mg_block_kernel(const __gr
             float sum = 0.0f;
 #pragma unroll
             for (int m = 0; m < 8; ++m) sum += v[m];
-            C.r[Q] = sum;
+            C.r[t] = sum;
         }
         __syncthreads();
     }
@@ -1227,29 +1229,30 @@ __global__ void __launch_bounds__(kBlockLevelThreads) mg_block_kernel(const __gr
     for (int l = lc - 1; l >= g; --l) {  // up: zp += P(t of l + 1), then t = zp + w D^-1 (r - A zp)
         const MgLevel F = smem_level<NT>(H, area, l);
         const MgLevel C = smem_level<NT>(H, area, l + 1);
-        for (uint32_t q = t; q < F.n; q += NT) {
-            const uint16_t code = F.code[q];
+        uint16_t code = 0;
+        float rv = 0.0f, zp = 0.0f;
+        uint32_t nb[6];
+        if (t < F.n) {
+            code = F.code[t];
+            rv = F.r[t];
+            zp = F.zp[t];
+            const Cell c = block_cell(F, H.fper, t, nb);
             if (active(code)) {
-                uint32_t nb[6];
-                const Cell c = block_cell(F, H.fper, q, nb);
-                F.zp[q] += prolong_codes(C, H.fper, H.fout, c.x, c.y, c.z);
+                zp += prolong_codes(C, H.fper, H.fout, c.x, c.y, c.z);
+                F.zp[t] = zp;
             }
         }
         __syncthreads();
-        for (uint32_t q = t; q < F.n; q += NT) {
-            uint32_t nb[6];
-            block_cell(F, H.fper, q, nb);
-            const uint16_t code = F.code[q];
-            const float rv = F.r[q], zp = F.zp[q];
+        if (t < F.n) {
             float vn[6];
 #pragma unroll
             for (int k = 0; k < 6; ++k) vn[k] = F.zp[nb[k]];
-            F.t[q] = active(code) ? zp + wdiag(code) * (rv - masked_stencil(code, zp, vn)) : 0.0f;
+            F.t[t] = active(code) ? zp + wdiag(code) * (rv - masked_stencil(code, zp, vn)) : 0.0f;
         }
         __syncthreads();
     }
     const MgLevel S = smem_level<NT>(H, area, g);
-    for (uint32_t q = t; q < S.n; q += NT) H.L[g].t[q] = active(S.code[q]) ? S.t[q] : __uint_as_float(kTag);
+    if (t < S.n) H.L[g].t[t] = active(S.code[t]) ? S.t[t] : __uint_as_float(kTag);
 }
 
 // Standalone V-cycle, level 0 down: zp = w D^-1 r, and (r - A zp) / 2 restricted into level 1 (the pre-smoothing the
@@ -1706,10 +1709,6 @@ cudaError_t launch_mg_net_mask(const MgHierarchy& H, uint8_t* solid, cudaStream_
 }
 
 cudaError_t launch_mg_setup(const StepParams& P, const MgHierarchy& H, const uint8_t* occ, cudaStream_t s) {
-    // the block-level cycle takes up to kMgBlockBytes of dynamic shared memory (above the 48 KB default); set here,
-    // outside any graph capture, for the current device
-    cudaError_t e = cudaFuncSetAttribute(mg_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMgBlockBytes));
-    if (e != cudaSuccess) return e;
     mg_fluid0_kernel<<<(H.L[0].n + 255) / 256, 256, 0, s>>>(H.L[0].n, occ, H.L[0].fluid);
     mg_code_tail_kernel<<<1, 32, 0, s>>>(H.L[0].code, H.L[0].n);
     for (int l = 1; l < H.levels; ++l) {
